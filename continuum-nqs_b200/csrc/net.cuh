@@ -1,0 +1,86 @@
+// net.cuh — host-side interface of the wavefunction network passes (forward, forward-Laplacian,
+// spin-flip JVPs, reverse-mode per-sample Jacobian).
+#pragma once
+
+#include "nqs_common.cuh"
+
+namespace nqs {
+
+// Per-block weight pointers in the working precision T (row-major Dense kernels [in][out]).
+template <typename T>
+struct BlockW {
+  const T *ln0_s, *ln0_b, *ln1_s, *ln1_b;
+  const T *wq, *bq, *wk, *bk, *wv, *bv, *wo, *bo;
+  const T *w0, *b0, *w1, *b1;
+};
+
+template <typename T>
+struct NetW {
+  const T *emb_w, *emb_b;
+  BlockW<T> blk[NQS_MAX_DEPTH];
+  const T *lnf_s, *lnf_b;
+  const T *bf_w_re, *bf_w_im, *bf_b_re, *bf_b_im;  // backflow Dense (complex leaf split)
+  const double* theta;                              // float64 theta (head parameters)
+};
+
+// Head parameters always read from float64 theta.
+struct HeadParams {
+  const double* det_logw;  // [2K] re block then im block (nullable when K == 1)
+  const double* jas_same;  // [n_knots]
+  const double* jas_opp;   // [n_knots]
+  const double* jas_loga;  // [1]
+  const double* dW;        // [2 * N * nG * 2] complex leaf (re block, im block), nullable
+};
+
+struct HostModel {
+  NqsModelDesc desc;  // host copy (host pointers inside are not kept)
+  ModelConst mc;      // device pointers
+  double* d_Gs;
+  double* d_W;
+  double* d_knots;
+};
+
+// Scratch carved out of the caller's workspace.
+struct Arena {
+  char* base;
+  size_t cap, used;
+  template <typename X>
+  X* take(size_t n) {
+    size_t off = (used + 255) & ~(size_t)255;
+    used = off + n * sizeof(X);
+    return (used <= cap && base) ? reinterpret_cast<X*>(base + off) : nullptr;
+  }
+};
+
+// Outputs of a network pass for each job of a batch, float64:
+//   L[j] complex, dL[j][n_tan] complex, lap[j] complex (each nullable).
+struct HeadOut {
+  cplx* L;
+  cplx* dL;
+  cplx* lap;
+};
+
+// Rows per job (tokens * channels) for a batch shape.
+inline size_t job_rows(int N, int C) { return (size_t)N * C; }
+
+// Bytes of activation scratch for `rows` rows in precision T.
+template <typename T>
+size_t net_scratch_bytes(const ModelConst& mc, size_t rows);
+
+// Run the network over jb.n_jobs jobs, chunked to at most max_rows rows per chunk.
+template <typename T>
+int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, JobBatch jb,
+                HeadOut out, Arena& ws, size_t max_rows, cudaStream_t st);
+
+// Build the per-layer pointers into theta (float64 or a float32 copy) from the descriptor.
+template <typename T>
+NetW<T> make_netw(const NqsModelDesc& d, const T* theta_T, const double* theta64);
+HeadParams make_head_params(const NqsModelDesc& d, const double* theta64);
+
+// theta float64 -> float32 copy
+int theta_to_f32(const double* theta, float* out, int64_t n, cudaStream_t st);
+
+// Default row budget of one network chunk.
+constexpr size_t kMaxRows = (size_t)1 << 19;
+
+}  // namespace nqs

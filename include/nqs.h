@@ -1,0 +1,170 @@
+/*
+ * nqs.h — C ABI of libnqs.so, the B200 (sm_100a) kernels of one VMC iteration over persistent
+ * walkers for the continuum spinor Psiformer of wenqin-chen/continuum-nqs.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an int status
+ * (NQS_OK == 0). All array arguments are CALLER-OWNED DEVICE memory unless a name ends in _host.
+ * The library allocates nothing per call: scratch memory is a caller-provided workspace whose size
+ * the matching *_workspace_size function reports. Work is enqueued on the given cudaStream_t
+ * (passed as void*) and is asynchronous; no entry point synchronises the device except
+ * nqs_model_create / nqs_ewald_create (one-time uploads of constants).
+ *
+ * Layouts
+ *   theta   : float64[P]   the real ravel of the flax parameter tree (complex leaf -> re block,
+ *                          im block), leaf order = sorted dict keys (reference src/nqs/minsr.py:30-53)
+ *   R       : float64[W][N][2]  Cartesian positions;   S : int32[W][N] spins in {0,1}
+ *   complex : interleaved (re, im) float64 pairs
+ *
+ * Reference interfaces replaced (paths inside wenqin-chen/continuum-nqs):
+ *   nqs_logpsi          <- ContinuumSpinorPsiformer.__call__ / make_logpsi   src/nqs/psiformer.py:118-196
+ *   nqs_local_energy    <- make_local_energy(...)(R,S) under jax.vmap        src/nqs/local_energy.py:40-117
+ *   nqs_ewald_*         <- make_ewald_lattice / make_ewald                   src/nqs/ewald.py:26-73
+ *   nqs_mcmc_sweeps     <- make_mcmc sweep scanned over sweeps, vmapped      src/nqs/sampler.py:25-91,
+ *                                                                            src/nqs/minsr.py:107-118
+ *   nqs_per_sample_O    <- per_sample_O                                      src/nqs/minsr.py:56-65
+ *   nqs_minsr_direction <- _otil_etil + minsr_direction                      src/nqs/minsr.py:68-81
+ *   nqs_clip_energies   <- the median-MAD clip inside train_minsr            src/nqs/minsr.py:142-150
+ */
+#ifndef NQS_H_
+#define NQS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------- */
+#define NQS_OK                0
+#define NQS_ERR_INVALID_ARG   1   /* null pointer, negative size, inconsistent descriptor       */
+#define NQS_ERR_UNSUPPORTED   2   /* shape outside the compiled limits (N, d, heads, K, ...)    */
+#define NQS_ERR_WORKSPACE     3   /* workspace smaller than *_workspace_size reported           */
+#define NQS_ERR_CUDA          4   /* a CUDA runtime call or kernel launch failed                */
+#define NQS_ERR_NONFINITE     5   /* non-finite value where the algorithm cannot recover        */
+#define NQS_ERR_TIMEOUT       6   /* a bounded device wait ran out                              */
+#define NQS_ERR_NOT_SPD       7   /* Cholesky met a non-positive pivot                          */
+
+/* ---- precision of the wavefunction network ------------------------------------------------ */
+#define NQS_PREC_FP64   0   /* every stage in float64                                         */
+#define NQS_PREC_MIXED  1   /* network in float32 (tensor-core BF16 GEMMs where available);
+                               determinants, LU pivots, log-space sums, energies in float64   */
+
+/* ---- compiled limits ---------------------------------------------------------------------- */
+#define NQS_MAX_DEPTH     16
+#define NQS_MAX_ELEC      64
+#define NQS_MAX_EMBED     128
+#define NQS_MAX_DETS      16
+#define NQS_MAX_FREQ      16
+#define NQS_MAX_KNOTS     64
+
+/* index of each per-block tensor inside NqsModelDesc.off_block[b][.] (flax names) */
+enum NqsBlockParam {
+  NQS_B_DENSE0_BIAS = 0, NQS_B_DENSE0_KERNEL, NQS_B_DENSE1_BIAS, NQS_B_DENSE1_KERNEL,
+  NQS_B_LN0_BIAS, NQS_B_LN0_SCALE, NQS_B_LN1_BIAS, NQS_B_LN1_SCALE,
+  NQS_B_K_BIAS, NQS_B_K_KERNEL, NQS_B_O_BIAS, NQS_B_O_KERNEL,
+  NQS_B_Q_BIAS, NQS_B_Q_KERNEL, NQS_B_V_BIAS, NQS_B_V_KERNEL,
+  NQS_B_NPARAM
+};
+
+/* Wavefunction description: the fields of ContinuumSpinorPsiformer (src/nqs/psiformer.py:100-116)
+ * plus the offset of every parameter tensor inside theta (-1 = absent). */
+typedef struct NqsModelDesc {
+  int32_t n_elec, embed_dim, depth, n_heads, ff_mult, n_freq, n_dets, n_g;
+  int32_t learnable_env, use_jastrow, jastrow_kind /* 0 = rbf, 1 = cusp */, n_knots;
+  double cusp;
+  double A[4];                 /* cell matrix, row-major, columns are lattice vectors          */
+  const double* Gs_host;       /* [n_g][2] envelope plane waves                                */
+  const double* W_host;        /* [n_elec][n_g][2 spins] complex (interleaved re, im)          */
+  const double* knots_host;    /* [n_knots] rbf centres (numpy linspace(0, r_c, n_knots))      */
+  int64_t n_params;            /* P                                                            */
+  int64_t off_final_ln_bias, off_final_ln_scale;
+  int64_t off_embed_bias, off_embed_kernel;
+  int64_t off_backflow_bias, off_backflow_kernel;          /* complex leaves                   */
+  int64_t off_dW, off_det_logw, off_jas_c_opp, off_jas_c_same, off_jastrow_loga;
+  int64_t off_block[NQS_MAX_DEPTH][NQS_B_NPARAM];
+} NqsModelDesc;
+
+typedef struct NqsModel NqsModel;
+typedef struct NqsEwald NqsEwald;
+
+/* Library / device information. */
+int nqs_version(void);
+const char* nqs_status_string(int status);
+/* Last error detail (thread-local, human readable). */
+const char* nqs_last_error(void);
+
+/* Model handle: validates the descriptor and uploads the immutable constants (Gs, W, knots).
+ * Replaces the flax module construction in src/nqs/psiformer.py:100-116. */
+int nqs_model_create(const NqsModelDesc* desc, NqsModel** out);
+int nqs_model_destroy(NqsModel* model);
+int64_t nqs_model_n_params(const NqsModel* model);
+
+/* Workspace bytes for an operation on n_walkers walkers.  op: */
+#define NQS_OP_LOGPSI      0
+#define NQS_OP_LOCAL_E     1
+#define NQS_OP_MCMC        2
+#define NQS_OP_PER_SAMPLE_O 3
+int nqs_workspace_size(const NqsModel* model, int op, int n_walkers, int precision,
+                       size_t* bytes);
+
+/* log psi for W configurations.  out_logpsi: complex[W].
+ * Replaces model.apply(params, R, S) vmapped over walkers (src/nqs/psiformer.py:118-196). */
+int nqs_logpsi(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+               int n_walkers, double* out_logpsi, int precision,
+               void* workspace, size_t workspace_bytes, void* stream);
+
+/* Local energy E_loc = kinetic + Zeeman + Rashba SOC (+ Coulomb if ewald != NULL) per walker,
+ * with the kinetic Laplacian from the forward Laplacian. out_eloc: complex[W];
+ * out_logpsi (nullable): complex[W]. Replaces make_local_energy (src/nqs/local_energy.py:40-117)
+ * and the `e + coulomb(R)` of src/nqs/minsr.py:124-126. */
+int nqs_local_energy(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                     int n_walkers, double m_star, double lambda_r, double h_z,
+                     const NqsEwald* ewald, double* out_eloc, double* out_logpsi,
+                     int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Gradient and Laplacian of log psi (forward Laplacian): out_grad complex[W][2N],
+ * out_lap complex[W], out_logpsi complex[W] (each nullable). */
+int nqs_grad_laplacian(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                       int n_walkers, double* out_logpsi, double* out_grad, double* out_lap,
+                       int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Metropolis sweeps (src/nqs/sampler.py:36-57): per sweep one joint Gaussian move of all
+ * electrons (PBC wrapped) and n_spin_flips single-spin flips, each accepted iff
+ * u < exp(min(0, 2 Re dlogpsi)). R_io, S_io, logpsi_io (complex[W], the cached current value)
+ * are updated in place. Randomness: counter-based Philox4x32-10 keyed by (seed, counter) and
+ * (walker, sweep, draw), unless the inj_* buffers are given, in which case they are used
+ * verbatim: inj_normals f64[n_sweeps][W][N][2], inj_u_pos f64[n_sweeps][W],
+ * inj_flip_idx i32[n_sweeps][n_spin_flips][W], inj_u_flip f64[n_sweeps][n_spin_flips][W].
+ * out_acc_pos / out_acc_spin: f64[W] accepted fraction over the sweeps (nullable).
+ * out_d (nullable): f64[n_sweeps][1 + n_spin_flips][W] every log-ratio d that was tested. */
+int nqs_mcmc_sweeps(NqsModel* model, const double* theta, double* R_io, int32_t* S_io,
+                    double* logpsi_io, int n_walkers, int n_sweeps, int n_spin_flips,
+                    double step, uint64_t seed, uint64_t counter,
+                    const double* inj_normals, const double* inj_u_pos,
+                    const int32_t* inj_flip_idx, const double* inj_u_flip,
+                    double* out_acc_pos, double* out_acc_spin, double* out_d,
+                    int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Per-sample Jacobian O[w][k] = d log psi(R_w,S_w) / d theta_k written as two real rows:
+ * out_O is [2W][P] with rows 0..W-1 = Re O and rows W..2W-1 = Im O, dtype f64 (out_dtype 0)
+ * or f32 (out_dtype 1). Hand-written reverse mode (src/nqs/minsr.py:56-65). */
+int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                     int n_walkers, void* out_O, int out_dtype, int precision,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Ewald (src/nqs/ewald.py:26-73): eta = ewald_alpha, or sqrt(pi/area) when ewald_alpha <= 0. */
+int nqs_ewald_create(const double A[4], double alpha, double ewald_alpha, int n_real,
+                     int n_recip, NqsEwald** out);
+int nqs_ewald_destroy(NqsEwald* ewald);
+int nqs_ewald_zeta(const NqsEwald* ewald, double* zeta_M);
+/* ewald_pair(r) for M displacement vectors r f64[M][2] -> out f64[M]. */
+int nqs_ewald_pair(const NqsEwald* ewald, const double* r, int M, double* out, void* stream);
+/* coulomb_energy(R) for W walkers of N electrons -> out f64[W]. */
+int nqs_ewald_energy(const NqsEwald* ewald, const double* R, int n_walkers, int n_elec,
+                     double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NQS_H_ */

@@ -1,0 +1,148 @@
+"""The FP64 oracle pinned against the reference: the reference's rashba_reference outputs
+(golden fixture) and the reference's analytic known-answer tests (zero variance, Zeeman limit,
+antisymmetry, Ewald eta-independence / periodicity / alpha scaling / 1/r, MinSR == param-SR).
+CPU only; small sizes."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import TWIST, build, configs, perturb
+from nqs import rashba
+from oracle import nqs_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "rashba_gs.npz")
+
+
+def test_rashba_restatement_matches_reference_golden():
+    z = np.load(GOLD)
+    c = 0
+    while f"c{c}_params" in z:
+        N, L, lr, hz, t0, t1 = z[f"c{c}_params"]
+        N = int(N)
+        g = rashba.noninteracting_gs(N, L, 1.0, lr, hz, 10, (t0, t1))
+        K, Chi = rashba.occupied_orbital_matrix(g)
+        assert g["E_gs"] == float(z[f"c{c}_E_gs"]) and g["gap"] == float(z[f"c{c}_gap"])
+        assert np.array_equal(K, z[f"c{c}_K"]) and np.array_equal(Chi, z[f"c{c}_Chi"])
+        env = rashba.cell_rashba_envelope(L, N, 1.0, lr, hz, 10, (t0, t1))
+        assert np.array_equal(env["Gs"], z[f"c{c}_env_Gs"])
+        assert np.array_equal(env["W"], z[f"c{c}_env_W"])
+        c += 1
+    assert c >= 6
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/src/nqs"), reason="reference not mounted")
+def test_rashba_restatement_matches_reference_live():
+    import sys
+    sys.path.insert(0, "/root/reference")
+    from src.nqs.rashba_reference import noninteracting_gs
+    for N, L in ((3, 5.0), (11, 10.0)):
+        a = rashba.noninteracting_gs(N, L, 1.0, 0.7, 0.2, 8, TWIST)
+        b = noninteracting_gs(N, L, 1.0, 0.7, 0.2, 8, TWIST)
+        assert a["E_gs"] == b["E_gs"]
+
+
+def test_oracle_zero_variance_and_slater():
+    """tests/test_nqs_local_energy.py:38-46 and tests/test_nqs_psiformer.py:36-47 on the oracle."""
+    g, model = build()
+    p = model.init(0)
+    R, S = configs(5, 7.0, 3, 0)
+    f = lambda r, s: O.logpsi(model, p, r, s)  # noqa: E731
+    for w in range(3):
+        d = complex(f(R[w], S[w]) - O.slater_logpsi(model.Gs, model.W, R[w], S[w]))
+        assert abs(d.real) < 1e-12 and abs((d.imag + np.pi) % (2 * np.pi) - np.pi) < 1e-12
+        e = complex(O.local_energy(f, R[w], S[w], 1.0, 1.0, 0.5))
+        assert abs(e.real - g["E_gs"]) < 1e-10 and abs(e.imag) < 1e-10
+
+
+def test_oracle_zeeman_limit():
+    N, L, hz = 5, 9.0, 4.0
+    g, model = build(N=N, L=L, lr=0.0, hz=hz)
+    K, _ = rashba.occupied_orbital_matrix(g)
+    f = lambda r, s: O.slater_logpsi(model.Gs, model.W, r, s)  # noqa: E731
+    R, _ = configs(N, L, 1, 1)
+    E = complex(O.local_energy(f, R[0], torch.zeros(N, dtype=torch.int64), 1.0, 0.0, hz))
+    assert abs(E.real - (float(np.sum(K ** 2) / 2.0) - 0.5 * hz * N)) < 1e-10
+
+
+def test_oracle_antisymmetry():
+    g, model = build(n_dets=2, use_jastrow=True)
+    p = perturb(model.init(0), 0.05, 4)
+    R, S = configs(5, 7.0, 1, 5)
+    perm = torch.tensor([1, 0, 2, 3, 4])
+    L0 = O.logpsi(model, p, R[0], S[0])
+    L1 = O.logpsi(model, p, R[0][perm], S[0][perm])
+    assert abs(complex(torch.exp(L1 - L0)) + 1.0) < 1e-10
+
+
+def test_oracle_ewald_analytic():
+    """tests/test_nqs_ewald.py:21-77 on the oracle."""
+    L = 7.0
+    r = np.array([1.3, -2.1])
+    vals, zs = [], []
+    for c in (0.8, 1.0, 1.25):
+        e = O.Ewald(L, 1.0, c * np.sqrt(np.pi) / L, 8, 14)
+        vals.append(e.pair(r))
+        zs.append(e.zeta_M)
+    assert np.ptp(vals) < 1e-7 and np.ptp(zs) < 1e-7
+    e = O.Ewald(L, 1.0, None, 8, 12)
+    assert abs(e.pair(r) - e.pair(r + [L, 0])) < 1e-8 and abs(e.pair(r) - e.pair(-r)) < 1e-10
+    for d in (1e-3, 1e-4):
+        assert abs(e.pair(np.array([d, 0.0])) * d - 1.0) < 1.5e-2
+    e2 = O.Ewald(L, 2.5, None, 8, 12)
+    assert abs(2.5 * e.pair(r) - e2.pair(r)) < 1e-9 and abs(2.5 * e.zeta_M - e2.zeta_M) < 1e-9
+
+
+def test_oracle_minsr_equals_paramsr():
+    """tests/test_nqs_minsr.py:46-61 on the oracle (tightened to 1e-9)."""
+    g, model = build(embed=12, heads=3)
+    p = model.init(0)
+    theta, unravel = O.real_ravel(p["params"])
+    R, S = configs(5, 7.0, 10, 4)
+    O_ = O.per_sample_O(model, theta, unravel, R, S)
+    rng = np.random.default_rng(4)
+    eps = torch.as_tensor(rng.normal(size=10) + 1j * rng.normal(size=10))
+    for lam in (1e-2, 1e-4):
+        d1 = O.minsr_direction(O_, eps, lam)
+        d2 = O.paramsr_direction(O_, eps, lam)
+        assert float((d1 - d2).abs().max() / d2.abs().max()) < 1e-9
+
+
+def test_oracle_per_sample_O_central_fd():
+    """O = d log psi / d theta against central finite differences (h = 1e-5)."""
+    g, model = build(embed=8, heads=2, depth=1, n_dets=2, use_jastrow=True, n_knots=3)
+    p = perturb(model.init(0), 0.05, 8)
+    theta, unravel = O.real_ravel(p["params"])
+    R, S = configs(5, 7.0, 1, 6)
+    Ov = O.per_sample_O(model, theta, unravel, R, S)[0]
+    rng = np.random.default_rng(1)
+    for _ in range(4):
+        v = torch.as_tensor(rng.standard_normal(theta.shape[0]))
+        v /= v.norm()
+        h = 1e-5
+        fp = O.logpsi(model, unravel(theta + h * v), R[0], S[0])
+        fm = O.logpsi(model, unravel(theta - h * v), R[0], S[0])
+        fd = (fp - fm) / (2 * h)
+        assert abs(complex(fd) - complex((Ov * v).sum())) < 1e-7
+
+
+def test_oracle_real_ravel_layout():
+    """theta layout: sorted keys, complex leaf -> re block then im block (minsr.py:30-53)."""
+    g, model = build(n_dets=2)
+    p = perturb(model.init(0), 0.1, 2)
+    theta, unravel = O.real_ravel(p["params"])
+    assert theta.shape[0] == model.n_params()
+    back = unravel(theta)
+    bf = p["params"]["backflow"]["kernel"]
+    assert torch.equal(back["backflow"]["kernel"], bf)
+    for path, shape, is_c, off in model.leaves():
+        leaf = p["params"]
+        for k in path:
+            leaf = leaf[k]
+        n = leaf.numel()
+        if is_c:
+            assert torch.equal(theta[off:off + n], leaf.real.reshape(-1))
+            assert torch.equal(theta[off + n:off + 2 * n], leaf.imag.reshape(-1))
+        else:
+            assert torch.equal(theta[off:off + n], leaf.reshape(-1).to(torch.float64))
