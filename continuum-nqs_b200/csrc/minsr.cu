@@ -1,0 +1,664 @@
+// minsr.cu — MinSR natural-gradient direction in the sample space (src/nqs/minsr.py:68-88) and
+// the median-MAD energy clip of the training loop (src/nqs/minsr.py:142-153).
+//
+//   Otil = [Re(O - mean O); Im(O - mean O)]  (2W x P),  etil = [Re(e - mean e); Im(...)]
+//   T = Otil Otil^T (lower triangle),  (T + lam I) = L L^T (float64 Cholesky),
+//   y = L^-T L^-1 etil,  dtheta = Otil^T y  (optionally theta -= lr dtheta, fused)
+//
+// The Gram runs either in float64 (SIMT, 128x128 tiles, register-blocked 8x8 per thread) or in
+// BF16 on the tcgen05 tensor cores with float32 accumulation (gram_tc.cu). Everything after the
+// Gram is float64.
+#include <cstdio>
+#include <algorithm>
+#include <cmath>
+
+#include "minsr.cuh"
+
+namespace nqs {
+
+// ============================================================================================
+// centering
+// ============================================================================================
+// column means of each half of O [2W][P] (TO = double or float) -> mu [2][P] (float64)
+template <typename TO>
+__global__ void k_colmean(const TO* __restrict__ O, int W, int64_t P, double* __restrict__ mu) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int half = blockIdx.y;
+  if (p >= P) return;
+  const TO* base = O + (size_t)half * W * P + p;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int w = 0;
+  for (; w + 3 < W; w += 4) {
+    s0 += (double)base[(size_t)w * P];
+    s1 += (double)base[(size_t)(w + 1) * P];
+    s2 += (double)base[(size_t)(w + 2) * P];
+    s3 += (double)base[(size_t)(w + 3) * P];
+  }
+  for (; w < W; ++w) s0 += (double)base[(size_t)w * P];
+  mu[(size_t)half * P + p] = ((s0 + s1) + (s2 + s3)) / (double)W;
+}
+
+// Otil = O - mu (per half), written in place (float64) or converted to the Gram operand type
+template <typename TO, typename TD>
+__global__ void k_center(const TO* __restrict__ O, int W, int64_t P, const double* __restrict__ mu,
+                         TD* __restrict__ D, int64_t ldd) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;  // row of the 2W rows
+  if (p >= P) return;
+  const int half = r >= W;
+  D[(size_t)r * ldd + p] = (TD)((double)O[(size_t)r * P + p] - mu[(size_t)half * P + p]);
+}
+
+__global__ void k_center_eps(const cplx* __restrict__ e, int W, double* __restrict__ et) {
+  // single block: mean then centre
+  __shared__ double red[2][32];
+  double sr = 0, si = 0;
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    sr += e[w].re;
+    si += e[w].im;
+  }
+  sr = warp_sum(sr);
+  si = warp_sum(si);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = sr;
+    red[1][threadIdx.x >> 5] = si;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      a += red[0][i];
+      b += red[1][i];
+    }
+    red[0][0] = a / W;
+    red[1][0] = b / W;
+  }
+  __syncthreads();
+  const double mr = red[0][0], mi = red[1][0];
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    et[w] = e[w].re - mr;
+    et[W + w] = e[w].im - mi;
+  }
+}
+
+// ============================================================================================
+// float64 GEMM on lower-triangular tiles: C[i][j] = alpha sum_k A[i][k] B[j][k] + beta C[i][j]
+// for the 128x128 tiles with tile_j <= tile_i (both operands K-contiguous). Split-K over
+// blockIdx.z writes partial sums to Cpart[z] (beta ignored) when nsplit > 1.
+// ============================================================================================
+struct DTile {
+  const double* A;
+  int64_t lda;
+  const double* B;
+  int64_t ldb;
+  double* C;
+  int64_t ldc;
+  int M;       // rows = cols of the lower-triangular block region
+  int64_t K;
+  double alpha, beta;
+  int nsplit;
+  int64_t kchunk;
+  double* Cpart;  // [nsplit][M][M] when nsplit > 1
+};
+
+__device__ __forceinline__ void tile_of(int t, int* ti, int* tj) {
+  // lower-triangular enumeration: t -> (i, j), j <= i
+  int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((i + 1) * (i + 2) / 2 <= t) ++i;
+  while (i * (i + 1) / 2 > t) --i;
+  *ti = i;
+  *tj = t - i * (i + 1) / 2;
+}
+
+__global__ void __launch_bounds__(256) k_dsyrk_lower(DTile a) {
+  constexpr int BM = 128, BK = 8;
+  __shared__ __align__(16) double As[2][BK][BM];
+  __shared__ __align__(16) double Bs[2][BK][BM];
+  int ti, tj;
+  tile_of(blockIdx.x, &ti, &tj);
+  const int i0 = ti * BM, j0 = tj * BM;
+  const int64_t kb = (int64_t)blockIdx.z * a.kchunk;
+  const int64_t ke = min(a.K, kb + a.kchunk);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  // loader: row = tid / 2, k-quad = (tid & 1) * 4
+  const int lr = tid >> 1, lk = (tid & 1) * 4;
+  double ra[4], rb[4];
+  auto gload = [&](int64_t k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t k = k0 + lk + q;
+      const int gi = i0 + lr, gj = j0 + lr;
+      ra[q] = (gi < a.M && k < ke) ? a.A[(size_t)gi * a.lda + k] : 0.0;
+      rb[q] = (gj < a.M && k < ke) ? a.B[(size_t)gj * a.ldb + k] : 0.0;
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      As[buf][lk + q][lr] = ra[q];
+      Bs[buf][lk + q][lr] = rb[q];
+    }
+  };
+  gload(kb);
+  sstore(0);
+  __syncthreads();
+  int buf = 0;
+  for (int64_t k0 = kb; k0 < ke; k0 += BK) {
+    const bool more = k0 + BK < ke;
+    if (more) gload(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double av[8], bv[8];
+      const double2* pa = reinterpret_cast<const double2*>(&As[buf][kk][0]);
+      const double2* pb = reinterpret_cast<const double2*>(&Bs[buf][kk][0]);
+      double2 t0 = pa[ty * 2], t1 = pa[ty * 2 + 1], t2 = pa[32 + ty * 2], t3 = pa[32 + ty * 2 + 1];
+      av[0] = t0.x; av[1] = t0.y; av[2] = t1.x; av[3] = t1.y;
+      av[4] = t2.x; av[5] = t2.y; av[6] = t3.x; av[7] = t3.y;
+      t0 = pb[tx * 2]; t1 = pb[tx * 2 + 1]; t2 = pb[32 + tx * 2]; t3 = pb[32 + tx * 2 + 1];
+      bv[0] = t0.x; bv[1] = t0.y; bv[2] = t1.x; bv[3] = t1.y;
+      bv[4] = t2.x; bv[5] = t2.y; bv[6] = t3.x; bv[7] = t3.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+    if (more) {
+      sstore(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gi = i0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (gi >= a.M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int gj = j0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      if (gj >= a.M || gj > gi) continue;
+      if (a.nsplit > 1) {
+        a.Cpart[((size_t)blockIdx.z * a.M + gi) * a.M + gj] = acc[i][j];
+      } else {
+        double* c = a.C + (size_t)gi * a.ldc + gj;
+        *c = a.alpha * acc[i][j] + (a.beta == 0.0 ? 0.0 : a.beta * (*c));
+      }
+    }
+  }
+}
+
+__global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int M,
+                                double* __restrict__ C, int64_t ldc, double alpha, double beta) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)M * M) return;
+  const int i = (int)(idx / M), j = (int)(idx - (int64_t)i * M);
+  if (j > i) return;
+  double s = 0;
+  for (int z = 0; z < nsplit; ++z) s += part[(size_t)z * M * M + idx];
+  double* c = C + (size_t)i * ldc + j;
+  *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
+}
+
+int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, double beta,
+                double* C, int64_t ldc, double* part, size_t part_elems, int nsm,
+                cudaStream_t st) {
+  if (M <= 0) return NQS_OK;
+  const int nt = (M + 127) / 128;
+  const int tiles = nt * (nt + 1) / 2;
+  int nsplit = 1;
+  if (part && tiles < 2 * nsm && K >= 4096) {
+    nsplit = std::min<int>(16, (2 * nsm + tiles - 1) / tiles);
+    while (nsplit > 1 && (size_t)nsplit * M * M > part_elems) --nsplit;
+  }
+  DTile a{A, lda, A, lda, C, ldc, M, K, alpha, beta, nsplit, 0, part};
+  a.kchunk = ((K + nsplit - 1) / nsplit + 7) / 8 * 8;
+  k_dsyrk_lower<<<dim3(tiles, 1, nsplit), 256, 0, st>>>(a);
+  NQS_CHECK_LAUNCH("k_dsyrk_lower");
+  if (nsplit > 1) {
+    const int64_t n = (int64_t)M * M;
+    k_splitk_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, nsplit, M, C, ldc, alpha,
+                                                                  beta);
+    NQS_CHECK_LAUNCH("k_splitk_reduce");
+  }
+  return NQS_OK;
+}
+
+// general C[i][j] -= sum_k A[i][k] B[j][k] for a rectangular block (used by the Cholesky panel
+// update when the trailing matrix is lower triangular we use dsyrk_lower on the panel itself)
+
+// ============================================================================================
+// Cholesky (right-looking, block 64) and triangular solves, float64
+// ============================================================================================
+constexpr int CB = 64;
+
+// factor the diagonal block in place (lower), one CTA of 256 threads; adds lam to the diagonal
+// first if add_lam; sets *bad when a pivot is not positive
+__global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int64_t lda, int k0,
+                                                    int n, double lam, int* __restrict__ bad) {
+  __shared__ double L[CB][CB + 1];
+  const int b = min(CB, n - k0);
+  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, j = idx - i * b;
+    L[i][j] = (j <= i) ? A[(size_t)(k0 + i) * lda + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < b; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = L[j][j];
+      if (!(d > 0.0)) {
+        *bad = 1;
+        L[j][j] = NAN;
+      } else {
+        L[j][j] = sqrt(d);
+      }
+    }
+    __syncthreads();
+    const double piv = L[j][j];
+    for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) L[i][j] /= piv;
+    __syncthreads();
+    // trailing update of the block
+    for (int idx = threadIdx.x; idx < (b - j - 1) * (b - j - 1); idx += blockDim.x) {
+      const int ii = j + 1 + idx / (b - j - 1), jj = j + 1 + idx % (b - j - 1);
+      if (jj <= ii) L[ii][jj] -= L[ii][j] * L[jj][j];
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, j = idx - i * b;
+    if (j <= i) A[(size_t)(k0 + i) * lda + k0 + j] = L[i][j];
+  }
+  (void)lam;
+}
+
+// panel: rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L_kk^-T  (one warp per row)
+__global__ void __launch_bounds__(256) k_trsm_panel(double* __restrict__ A, int64_t lda, int k0,
+                                                    int n) {
+  __shared__ double L[CB][CB + 1];
+  const int b = min(CB, n - k0);
+  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, j = idx - i * b;
+    L[i][j] = (j <= i) ? A[(size_t)(k0 + i) * lda + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int r = k0 + b + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= n) return;
+  double* row = A + (size_t)r * lda + k0;
+  // x L^T = a  -> forward substitution over columns: x_j = (a_j - sum_{m<j} x_m L[j][m]) / L[j][j]
+  double x0 = lane < b ? row[lane] : 0.0, x1 = lane + 32 < b ? row[lane + 32] : 0.0;
+  for (int j = 0; j < b; ++j) {
+    const double xj_raw = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31);
+    const double xj = xj_raw / L[j][j];
+    if (lane == (j & 31)) {
+      if (j < 32)
+        x0 = xj;
+      else
+        x1 = xj;
+    }
+    // eliminate from later columns
+    if (lane > j && lane < b) x0 -= xj * L[lane][j];
+    if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[lane + 32][j];
+  }
+  if (lane < b) row[lane] = x0;
+  if (lane + 32 < b) row[lane + 32] = x1;
+}
+
+__global__ void k_add_diag(double* A, int64_t lda, int n, double lam) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[(size_t)i * lda + i] += lam;
+}
+
+int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
+                   int nsm, cudaStream_t st) {
+  for (int k0 = 0; k0 < n; k0 += CB) {
+    const int b = std::min(CB, n - k0);
+    k_potrf_diag<<<1, 256, 0, st>>>(A, lda, k0, n, 0.0, bad);
+    NQS_CHECK_LAUNCH("k_potrf_diag");
+    const int rest = n - k0 - b;
+    if (rest <= 0) break;
+    k_trsm_panel<<<(rest + 7) / 8, 256, 0, st>>>(A, lda, k0, n);
+    NQS_CHECK_LAUNCH("k_trsm_panel");
+    // trailing: A[k0+b:, k0+b:] -= P P^T, P = A[k0+b:, k0:k0+b]
+    double* P = A + (size_t)(k0 + b) * lda + k0;
+    double* C = A + (size_t)(k0 + b) * lda + k0 + b;
+    NQS_TRY(dsyrk_lower(P, lda, rest, b, -1.0, 1.0, C, lda, nullptr, 0, nsm, st));
+    (void)part;
+    (void)part_elems;
+  }
+  return NQS_OK;
+}
+
+// forward solve L z = v (in place), one CTA (1024 threads), blocked by 64: x_blk via a warp,
+// then the remaining rows are updated in parallel.
+__global__ void __launch_bounds__(1024) k_trsv_lower(const double* __restrict__ L, int64_t ldl,
+                                                     int n, double* __restrict__ v) {
+  __shared__ double xb[CB];
+  for (int k0 = 0; k0 < n; k0 += CB) {
+    const int b = min(CB, n - k0);
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
+      for (int j = 0; j < b; ++j) {
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
+                          L[(size_t)(k0 + j) * ldl + k0 + j];
+        if (lane == (j & 31)) {
+          if (j < 32) x0 = xj; else x1 = xj;
+        }
+        if (lane > j && lane < b) x0 -= xj * L[(size_t)(k0 + lane) * ldl + k0 + j];
+        if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[(size_t)(k0 + lane + 32) * ldl + k0 + j];
+      }
+      if (lane < b) xb[lane] = x0;
+      if (lane + 32 < b) xb[lane + 32] = x1;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < b; i += blockDim.x) v[k0 + i] = xb[i];
+    // update rows below: v[r] -= sum_j L[r][k0+j] xb[j]  (one warp per row)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = k0 + b + wid; r < n; r += nw) {
+      double s = 0;
+      for (int j = lane; j < b; j += 32) s += L[(size_t)r * ldl + k0 + j] * xb[j];
+      s = warp_sum(s);
+      if (lane == 0) v[r] -= s;
+    }
+    __syncthreads();
+  }
+}
+
+// backward solve L^T y = z (in place)
+__global__ void __launch_bounds__(1024) k_trsv_lower_t(const double* __restrict__ L, int64_t ldl,
+                                                       int n, double* __restrict__ v) {
+  __shared__ double xb[CB];
+  const int nblk = (n + CB - 1) / CB;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int k0 = bi * CB, b = min(CB, n - k0);
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
+      for (int j = b - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
+                          L[(size_t)(k0 + j) * ldl + k0 + j];
+        if (lane == (j & 31)) {
+          if (j < 32) x0 = xj; else x1 = xj;
+        }
+        // L^T[m][j] = L[j][m]: rows m < j get x_m -= L[j][m] x_j
+        if (lane < j) x0 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane];
+        if (lane + 32 < j) x1 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane + 32];
+      }
+      if (lane < b) xb[lane] = x0;
+      if (lane + 32 < b) xb[lane + 32] = x1;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < b; i += blockDim.x) v[k0 + i] = xb[i];
+    // rows above: v[m] -= sum_j L[k0+j][m] xb[j], m < k0  (threads over m: coalesced along m)
+    for (int m = threadIdx.x; m < k0; m += blockDim.x) {
+      double s = 0;
+      for (int j = 0; j < b; ++j) s += L[(size_t)(k0 + j) * ldl + m] * xb[j];
+      v[m] -= s;
+    }
+    __syncthreads();
+  }
+}
+
+// dtheta[p] = sum_r Otil[r][p] y[r] with Otil = O - mu (centred on the fly);
+// theta[p] -= lr dtheta[p] when theta != nullptr
+template <typename TO>
+__global__ void k_pushthrough(const TO* __restrict__ O, int W, int64_t P,
+                              const double* __restrict__ mu, const double* __restrict__ y,
+                              double* __restrict__ dtheta, double* __restrict__ theta, double lr) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  double s0 = 0, s1 = 0;
+  const double m0 = mu[p], m1 = mu[P + p];
+  double ys0 = 0, ys1 = 0;
+  for (int w = 0; w < W; ++w) {
+    const double yr = y[w], yi = y[W + w];
+    s0 = fma((double)O[(size_t)w * P + p], yr, s0);
+    s1 = fma((double)O[((size_t)W + w) * P + p], yi, s1);
+    ys0 += yr;
+    ys1 += yi;
+  }
+  const double d = (s0 - m0 * ys0) + (s1 - m1 * ys1);
+  if (dtheta) dtheta[p] = d;
+  if (theta) theta[p] -= lr * d;
+}
+
+// ============================================================================================
+// energy statistics and median-MAD clip (single CTA, bitonic sort in shared memory)
+// ============================================================================================
+__device__ void bitonic_sort(double* a, int n2) {
+  for (int k = 2; k <= n2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const double x = a[i], y = a[l];
+          if ((x > y) == up) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+__device__ double median_sorted(const double* a, int n) {
+  return (n & 1) ? a[n / 2] : 0.5 * (a[n / 2 - 1] + a[n / 2]);
+}
+
+// stats: [0] mean Re e, [1] std(Re e)/sqrt(W) (ddof 0), [2] var(Re e), [3] median, [4] MAD
+__global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W, double clip_k,
+                                               cplx* __restrict__ out, double* __restrict__ stats) {
+  extern __shared__ double sa[];
+  int n2 = 1;
+  while (n2 < W) n2 <<= 1;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) sa[i] = i < W ? e[i].re : INFINITY;
+  __syncthreads();
+  bitonic_sort(sa, n2);
+  const double med = median_sorted(sa, W);
+  __syncthreads();
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) sa[i] = i < W ? fabs(e[i].re - med) : INFINITY;
+  __syncthreads();
+  bitonic_sort(sa, n2);
+  const double mad = median_sorted(sa, W) + 1e-12;
+  __syncthreads();
+  const double lo = med - clip_k * mad, hi = med + clip_k * mad;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    const double r = e[i].re;
+    out[i] = mk(fmin(fmax(r, lo), hi), e[i].im);
+  }
+  // mean and variance (two-pass)
+  __shared__ double red[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) s += e[i].re;
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    red[0] = t / W;
+  }
+  __syncthreads();
+  const double mean = red[0];
+  __syncthreads();
+  double v = 0;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    const double dd = e[i].re - mean;
+    v += dd * dd;
+  }
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0 && stats) {
+    double t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    const double var = t / W;
+    stats[0] = mean;
+    stats[1] = sqrt(var) / sqrt((double)W);
+    stats[2] = var;
+    stats[3] = med;
+    stats[4] = mad;
+  }
+}
+
+// ============================================================================================
+// host driver
+// ============================================================================================
+size_t minsr_part_elems(int W) {
+  const size_t n = 2 * (size_t)W;
+  return std::min<size_t>(16 * n * n, (size_t)8 << 20);
+}
+
+size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
+  const size_t n = 2 * (size_t)W;
+  size_t b = 0;
+  auto add = [&](size_t x) { b += ((x + 255) / 256) * 256 + 256; };
+  add(sizeof(double) * 2 * P);          // column means
+  add(sizeof(double) * n);              // etil -> y
+  add(sizeof(double) * n * n);          // T -> L
+  add(sizeof(int) * 4);                 // status
+  add(sizeof(double) * minsr_part_elems(W));  // split-K partials
+  if (gram == 0 && odtype == 1) add(sizeof(double) * n * P);  // float64 Otil from float32 O
+  if (gram != 0) add(gram_tc_workspace(W, P, gram));
+  return b;
+}
+
+}  // namespace nqs
+
+using namespace nqs;
+
+extern "C" {
+
+int nqs_minsr_workspace_size(int W, int64_t P, int o_dtype, int gram_prec, size_t* bytes) {
+  if (!bytes || W < 1 || P < 1) return NQS_ERR_INVALID_ARG;
+  *bytes = minsr_workspace(W, P, o_dtype, gram_prec);
+  return NQS_OK;
+}
+
+int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t P, double lam,
+                        int gram_prec, double* out_dtheta, double* theta_io, double lr,
+                        int* status_dev, void* wsp, size_t wsb, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!O || !eps || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || gram_prec < 0 ||
+      gram_prec > 2 || (!out_dtheta && !theta_io)) {
+    set_error("nqs_minsr_direction: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  const size_t need = minsr_workspace(W, P, o_dtype, gram_prec);
+  if (wsb < need) {
+    set_error("nqs_minsr_direction: workspace %zu < %zu", wsb, need);
+    return NQS_ERR_WORKSPACE;
+  }
+  Arena ws{(char*)wsp, wsb, 0};
+  const int n = 2 * W;
+  double* mu = ws.take<double>(2 * P);
+  double* y = ws.take<double>(n);
+  double* T = ws.take<double>((size_t)n * n);
+  int* bad = ws.take<int>(4);
+  const size_t part_elems = minsr_part_elems(W);
+  double* part = ws.take<double>(part_elems);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaMemsetAsync(bad, 0, sizeof(int) * 4, st);
+  const dim3 cg((unsigned)((P + 255) / 256), 2);
+  if (o_dtype == 0)
+    k_colmean<double><<<cg, 256, 0, st>>>((const double*)O, W, P, mu);
+  else
+    k_colmean<float><<<cg, 256, 0, st>>>((const float*)O, W, P, mu);
+  NQS_CHECK_LAUNCH("k_colmean");
+  k_center_eps<<<1, 1024, 0, st>>>((const cplx*)eps, W, y);
+  NQS_CHECK_LAUNCH("k_center_eps");
+  const dim3 ce((unsigned)((P + 255) / 256), (unsigned)n);
+  if (gram_prec == 0) {
+    double* Ot;
+    if (o_dtype == 0) {  // centre in place
+      k_center<double, double><<<ce, 256, 0, st>>>((const double*)O, W, P, mu, (double*)O, P);
+      Ot = (double*)O;
+    } else {
+      Ot = ws.take<double>((size_t)n * P);
+      k_center<float, double><<<ce, 256, 0, st>>>((const float*)O, W, P, mu, Ot, P);
+    }
+    NQS_CHECK_LAUNCH("k_center");
+    NQS_TRY(dsyrk_lower(Ot, P, n, P, 1.0, 0.0, T, n, part, part_elems, nsm, st));
+    // mu is now zero for the push-through of an in-place centred float64 O
+    if (o_dtype == 0) cudaMemsetAsync(mu, 0, sizeof(double) * 2 * P, st);
+  } else {
+    NQS_TRY(gram_tc(O, o_dtype, mu, W, P, gram_prec, T, ws, nsm, st));
+  }
+  k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
+  NQS_CHECK_LAUNCH("k_add_diag");
+  NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st));
+  k_trsv_lower<<<1, 1024, 0, st>>>(T, n, n, y);
+  NQS_CHECK_LAUNCH("k_trsv_lower");
+  k_trsv_lower_t<<<1, 1024, 0, st>>>(T, n, n, y);
+  NQS_CHECK_LAUNCH("k_trsv_lower_t");
+  const unsigned gp = (unsigned)((P + 255) / 256);
+  if (o_dtype == 0)
+    k_pushthrough<double><<<gp, 256, 0, st>>>((const double*)O, W, P, mu, y, out_dtheta, theta_io,
+                                              lr);
+  else
+    k_pushthrough<float><<<gp, 256, 0, st>>>((const float*)O, W, P, mu, y, out_dtheta, theta_io,
+                                             lr);
+  NQS_CHECK_LAUNCH("k_pushthrough");
+  if (status_dev) cudaMemcpyAsync(status_dev, bad, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  return NQS_OK;
+}
+
+int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
+  if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
+  const size_t m = (size_t)M;
+  *bytes = sizeof(double) * (m * m + m + std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 4096;
+  return NQS_OK;
+}
+
+int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* rhs, double* x,
+                   void* wsp, size_t wsb, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  size_t need = 0;
+  NQS_TRY(nqs_gram_solve_workspace_size(M, K, &need));
+  if (!A || !rhs || !x) return NQS_ERR_INVALID_ARG;
+  if (wsb < need) return NQS_ERR_WORKSPACE;
+  Arena ws{(char*)wsp, wsb, 0};
+  double* T = ws.take<double>((size_t)M * M);
+  const size_t pe = std::min<size_t>(16 * (size_t)M * M, (size_t)8 << 20);
+  double* part = ws.take<double>(pe);
+  int* bad = ws.take<int>(4);
+  if (!bad) return NQS_ERR_WORKSPACE;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaMemsetAsync(bad, 0, sizeof(int) * 4, st);
+  NQS_TRY(dsyrk_lower(A, K, M, K, 1.0, 0.0, T, M, part, pe, nsm, st));
+  k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
+  NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
+  cudaMemcpyAsync(x, rhs, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
+  k_trsv_lower<<<1, 1024, 0, st>>>(T, M, M, x);
+  k_trsv_lower_t<<<1, 1024, 0, st>>>(T, M, M, x);
+  NQS_CHECK_LAUNCH("nqs_gram_solve");
+  return NQS_OK;
+}
+
+int nqs_clip_energies(const double* e, int W, double clip_k, double* out_eclip, double* stats,
+                      void* stream) {
+  if (!e || !out_eclip || W < 1) return NQS_ERR_INVALID_ARG;
+  if (W > 16384) {
+    set_error("nqs_clip_energies: W=%d > 16384", W);
+    return NQS_ERR_UNSUPPORTED;
+  }
+  int n2 = 1;
+  while (n2 < W) n2 <<= 1;
+  const size_t sm = sizeof(double) * n2;
+  cudaFuncSetAttribute(k_clip, cudaFuncAttributeMaxDynamicSharedMemorySize, 132 * 1024);
+  k_clip<<<1, 1024, sm, (cudaStream_t)stream>>>((const cplx*)e, W, clip_k, (cplx*)out_eclip, stats);
+  NQS_CHECK_LAUNCH("k_clip");
+  return NQS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,18 @@
+// minsr.cuh — internal interface between the MinSR driver and the tensor-core Gram.
+#pragma once
+#include "net.cuh"
+
+namespace nqs {
+
+// float64 lower-triangular C = alpha A A^T + beta C (A: M x K, K-contiguous rows)
+int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, double beta,
+                double* C, int64_t ldc, double* part, size_t part_elems, int nsm,
+                cudaStream_t st);
+
+// Tensor-core Gram of the centred O: T (lower, float64, 2W x 2W) = Otil Otil^T with Otil =
+// O - mu converted to the operand type of `prec` (1 = BF16, 2 = TF32), float32 accumulation.
+size_t gram_tc_workspace(int W, int64_t P, int prec);
+int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int prec, double* T,
+            Arena& ws, int nsm, cudaStream_t st);
+
+}  // namespace nqs

@@ -80,6 +80,14 @@ HeadParams make_head_params(const NqsModelDesc& d, const double* theta64);
 // theta float64 -> float32 copy
 int theta_to_f32(const double* theta, float* out, int64_t n, cudaStream_t st);
 
+// Reverse mode: per-sample Jacobian rows (Re in [0,W), Im in [W,2W)) of a [2W][P] matrix.
+template <typename T>
+size_t per_sample_O_scratch(const ModelConst& mc, int W);
+template <typename T, typename TO>
+int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                     const double* R, const int32_t* S, int W, TO* O, Arena& ws,
+                     cudaStream_t st);
+
 // Default row budget of one network chunk.
 constexpr size_t kMaxRows = (size_t)1 << 19;
 

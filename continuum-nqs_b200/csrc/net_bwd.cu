@@ -1,0 +1,746 @@
+// net_bwd.cu — hand-written reverse mode of the wavefunction: per-sample Jacobian
+//   O[w][k] = d log psi(R_w, S_w) / d theta_k   (src/nqs/minsr.py:56-65)
+// written as two real rows per walker (Re O in row w, Im O in row W + w of a [2W][P] matrix).
+//
+// log psi is complex and holomorphic in the complex parameters, the backbone is real, so every
+// real activation carries a complex adjoint stored as two channels (re, im) and pushed through the
+// real layers independently. For a complex leaf c = a + i b, dL/da = dL/dc and dL/db = i dL/dc.
+// The forward pass is recomputed per chunk of walkers with every block's activations kept
+// (attention probabilities are recomputed from q, k inside the attention backward).
+#include <cstdio>
+#include <algorithm>
+
+#include "net_kernels.cuh"
+
+namespace nqs {
+
+// --------------------------------------------------------------------------------------------
+// O row writer
+// --------------------------------------------------------------------------------------------
+template <typename TO>
+struct ORows {
+  TO* O;
+  int64_t P;
+  int W;  // total walkers (Im rows start at W)
+  __device__ __forceinline__ void put(int w, int64_t col, double re, double im) const {
+    O[(size_t)w * P + col] = (TO)re;
+    O[((size_t)W + w) * P + col] = (TO)im;
+  }
+  // complex leaf at theta offset `off` with `n` elements: element e gets dL/dc = g
+  __device__ __forceinline__ void put_c(int w, int64_t off, int64_t n, int64_t e, double gre,
+                                        double gim) const {
+    put(w, off + e, gre, gim);        // d/d Re c = g
+    put(w, off + n + e, -gim, gre);   // d/d Im c = i g
+  }
+};
+
+// --------------------------------------------------------------------------------------------
+// per-walker weight gradient of a Dense layer: G[i][o] = sum_tok X[tok][i] Ybar[tok][ch][o]
+// grid (walker, ceil(d_out / 128)); X rows ld ldx (+ col offset folded in the pointer);
+// Ybar rows [tok][2][ldy]
+// --------------------------------------------------------------------------------------------
+template <typename T, typename TO>
+__global__ void __launch_bounds__(256) k_wgrad(int N, int d_in, int d_out, const T* __restrict__ X,
+                                               int ldx, const T* __restrict__ Yb, int ldy,
+                                               ORows<TO> o, int w0, int64_t off_k, int64_t off_b,
+                                               int is_complex) {
+  constexpr int OT = 128;
+  const int wl = blockIdx.x, o0 = blockIdx.y * OT;
+  const int w = w0 + wl;
+  const int ot = min(OT, d_out - o0);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* xs = reinterpret_cast<T*>(smraw);  // [N][d_in]
+  T* ys = xs + (size_t)N * d_in;        // [N][2][ot]
+  const T* Xw = X + (size_t)wl * N * ldx;
+  const T* Yw = Yb + (size_t)wl * N * 2 * ldy;
+  for (int idx = threadIdx.x; idx < N * d_in; idx += blockDim.x) {
+    const int t = idx / d_in, i = idx - t * d_in;
+    xs[idx] = Xw[(size_t)t * ldx + i];
+  }
+  for (int idx = threadIdx.x; idx < N * 2 * ot; idx += blockDim.x) {
+    const int t = idx / (2 * ot), r = idx - t * 2 * ot, ch = r / ot, oo = r - ch * ot;
+    ys[idx] = Yw[((size_t)t * 2 + ch) * ldy + o0 + oo];
+  }
+  __syncthreads();
+  const int64_t nK = (int64_t)d_in * d_out;
+  for (int idx = threadIdx.x; idx < d_in * ot; idx += blockDim.x) {
+    const int i = idx / ot, oo = idx - i * ot;
+    double gr = 0, gi = 0;
+    for (int t = 0; t < N; ++t) {
+      const double xv = (double)xs[t * d_in + i];
+      gr = fma(xv, (double)ys[(t * 2) * ot + oo], gr);
+      gi = fma(xv, (double)ys[(t * 2 + 1) * ot + oo], gi);
+    }
+    const int64_t e = (int64_t)i * d_out + o0 + oo;
+    if (is_complex)
+      o.put_c(w, off_k, nK, e, gr, gi);
+    else
+      o.put(w, off_k + e, gr, gi);
+  }
+  if (off_b >= 0) {
+    for (int oo = threadIdx.x; oo < ot; oo += blockDim.x) {
+      double gr = 0, gi = 0;
+      for (int t = 0; t < N; ++t) {
+        gr += (double)ys[(t * 2) * ot + oo];
+        gi += (double)ys[(t * 2 + 1) * ot + oo];
+      }
+      if (is_complex)
+        o.put_c(w, off_b, d_out, o0 + oo, gr, gi);
+      else
+        o.put(w, off_b + o0 + oo, gr, gi);
+    }
+  }
+}
+
+template <typename T, typename TO>
+static int launch_wgrad(int nw, int N, int d_in, int d_out, const T* X, int ldx, const T* Yb,
+                        int ldy, ORows<TO> o, int w0, int64_t off_k, int64_t off_b, int is_c,
+                        cudaStream_t st) {
+  const int ot = std::min(128, d_out);
+  const size_t sm = sizeof(T) * ((size_t)N * d_in + (size_t)N * 2 * ot);
+  if (sm > 48 * 1024)
+    cudaFuncSetAttribute(k_wgrad<T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+  k_wgrad<T, TO><<<dim3(nw, (d_out + 127) / 128), 256, sm, st>>>(N, d_in, d_out, X, ldx, Yb, ldy,
+                                                                  o, w0, off_k, off_b, is_c);
+  NQS_CHECK_LAUNCH("k_wgrad");
+  return NQS_OK;
+}
+
+// --------------------------------------------------------------------------------------------
+// LayerNorm backward (one CTA per walker): x rows [tok][d], Ybar [tok][2][d]
+//   z = (x - mu) rho, zbar = ybar g, xbar = rho (zbar - mean(zbar) - z mean(zbar z))
+//   dL/dscale = sum_tok ybar z, dL/dbias = sum_tok ybar
+// --------------------------------------------------------------------------------------------
+template <typename T, typename TO>
+__global__ void __launch_bounds__(256) k_ln_bwd(int N, int d, const T* __restrict__ X,
+                                                const T* __restrict__ Yb, const T* __restrict__ g,
+                                                T* __restrict__ Xb, int accumulate, ORows<TO> o,
+                                                int w0, int64_t off_scale, int64_t off_bias) {
+  constexpr int Q = NQS_MAX_EMBED / 32;
+  const int wl = blockIdx.x, w = w0 + wl;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* zs = reinterpret_cast<T*>(smraw);  // [N][d]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const T inv_d = T(1) / T(d);
+  for (int t = wid; t < N; t += nwarp) {
+    const size_t tok = (size_t)wl * N + t;
+    const T* x = X + tok * d;
+    T u[Q], gm[Q], s = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      u[q] = f < d ? x[f] : T(0);
+      gm[q] = f < d ? g[f] : T(0);
+      s += u[q];
+    }
+    const T mu = warp_sum(s) * inv_d;
+    s = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      if (f < d) {
+        u[q] -= mu;
+        s += u[q] * u[q];
+      }
+    }
+    const T rho = T(1) / sqrt(warp_sum(s) * inv_d + T(kLnEps));
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      u[q] *= rho;  // z
+      if (f < d) zs[t * d + f] = u[q];
+    }
+    for (int ch = 0; ch < 2; ++ch) {
+      const T* yb = Yb + (tok * 2 + ch) * d;
+      T zb[Q], s1 = 0, s2 = 0;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        zb[q] = f < d ? yb[f] * gm[q] : T(0);
+        s1 += zb[q];
+        s2 += zb[q] * u[q];
+      }
+      const T m1 = warp_sum(s1) * inv_d, m2 = warp_sum(s2) * inv_d;
+      T* xb = Xb + (tok * 2 + ch) * d;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        if (f < d) {
+          const T v = rho * (zb[q] - m1 - u[q] * m2);
+          xb[f] = accumulate ? xb[f] + v : v;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < d; f += blockDim.x) {
+    double sr = 0, si = 0, br = 0, bi = 0;
+    for (int t = 0; t < N; ++t) {
+      const size_t tok = (size_t)wl * N + t;
+      const double y0 = (double)Yb[(tok * 2) * d + f], y1 = (double)Yb[(tok * 2 + 1) * d + f];
+      const double z = (double)zs[t * d + f];
+      sr = fma(y0, z, sr);
+      si = fma(y1, z, si);
+      br += y0;
+      bi += y1;
+    }
+    o.put(w, off_scale + f, sr, si);
+    o.put(w, off_bias + f, br, bi);
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// GELU backward: abar[r][ch][f] = gbar[r][ch][f] * gelu'(a[r][f])
+// --------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_gelu_bwd(size_t n_tok, int D, const T* __restrict__ A, T* __restrict__ Gb) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_tok * D) return;
+  const size_t tok = idx / D;
+  const int f = (int)(idx - tok * D);
+  const T x = A[idx];
+  const T c = T(0.7978845608028654), b3 = T(0.044715);
+  const T th = tanh(c * (x + b3 * (x * x * x)));
+  const T g1 = T(0.5) * (T(1) + th) + T(0.5) * x * (T(1) - th * th) * c * (T(1) + T(3) * b3 * x * x);
+  Gb[(tok * 2) * D + f] *= g1;
+  Gb[(tok * 2 + 1) * D + f] *= g1;
+}
+
+// --------------------------------------------------------------------------------------------
+// attention backward, one CTA per (walker, head). QKV rows [tok][3d] (value), Ob [tok][2][d],
+// QKVb out [tok][2][3d].
+// --------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) k_attn_bwd(int N, int d, int H, const T* __restrict__ QKV,
+                                                  const T* __restrict__ Ob, T* __restrict__ QKVb) {
+  const int wl = blockIdx.x / H, h = blockIdx.x - wl * H;
+  const int hd = d / H;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* q = reinterpret_cast<T*>(smraw);
+  T* k = q + N * hd;
+  T* v = k + N * hd;
+  T* a = v + N * hd;   // N*N
+  T* ob = a + N * N;   // N*hd
+  T* ab = ob + N * hd; // N*N
+  T* rs = ab + N * N;  // N
+  const T sc = T(1) / sqrt(T(hd));
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int idx = tid; idx < N * hd; idx += nth) {
+    const int i = idx / hd, e = idx - i * hd;
+    const T* p = QKV + ((size_t)wl * N + i) * 3 * d + h * hd + e;
+    q[idx] = p[0];
+    k[idx] = p[d];
+    v[idx] = p[2 * d];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * N; idx += nth) {
+    const int i = idx / N, j = idx - i * N;
+    T s = 0;
+    for (int e = 0; e < hd; ++e) s = fma(q[i * hd + e], k[j * hd + e], s);
+    a[idx] = s * sc;
+  }
+  __syncthreads();
+  for (int i = tid; i < N; i += nth) {
+    T mx = a[i * N];
+    for (int j = 1; j < N; ++j) mx = max(mx, a[i * N + j]);
+    T ssum = 0;
+    for (int j = 0; j < N; ++j) {
+      const T e = exp(a[i * N + j] - mx);
+      a[i * N + j] = e;
+      ssum += e;
+    }
+    for (int j = 0; j < N; ++j) a[i * N + j] = a[i * N + j] / ssum;
+  }
+  for (int ch = 0; ch < 2; ++ch) {
+    __syncthreads();
+    for (int idx = tid; idx < N * hd; idx += nth) {
+      const int i = idx / hd, e = idx - i * hd;
+      ob[idx] = Ob[(((size_t)wl * N + i) * 2 + ch) * d + h * hd + e];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < N * hd; idx += nth) {  // vbar
+      const int j = idx / hd, e = idx - j * hd;
+      T s = 0;
+      for (int i = 0; i < N; ++i) s = fma(a[i * N + j], ob[i * hd + e], s);
+      QKVb[(((size_t)wl * N + j) * 2 + ch) * 3 * d + 2 * d + h * hd + e] = s;
+    }
+    for (int idx = tid; idx < N * N; idx += nth) {  // abar
+      const int i = idx / N, j = idx - i * N;
+      T s = 0;
+      for (int e = 0; e < hd; ++e) s = fma(ob[i * hd + e], v[j * hd + e], s);
+      ab[idx] = s;
+    }
+    __syncthreads();
+    for (int i = tid; i < N; i += nth) {
+      T s = 0;
+      for (int j = 0; j < N; ++j) s = fma(a[i * N + j], ab[i * N + j], s);
+      rs[i] = s;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < N * N; idx += nth) {  // sbar (scaled)
+      const int i = idx / N;
+      ab[idx] = a[idx] * (ab[idx] - rs[i]) * sc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < N * hd; idx += nth) {
+      const int i = idx / hd, e = idx - i * hd;
+      T sq = 0, sk = 0;
+      for (int j = 0; j < N; ++j) {
+        sq = fma(ab[i * N + j], k[j * hd + e], sq);
+        sk = fma(ab[j * N + i], q[j * hd + e], sk);
+      }
+      T* p = QKVb + (((size_t)wl * N + i) * 2 + ch) * 3 * d + h * hd + e;
+      p[0] = sq;
+      p[d] = sk;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// features of the embedding input ([pos features | one-hot spin], value only) per token
+// --------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_features(JobBatch jb, ModelConst mc, T* __restrict__ Fo) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int F = 4 * mc.nf, Fp = F + 2;
+  if (idx >= jb.n_jobs * jb.N * Fp) return;
+  const int tokg = idx / Fp, k = idx - tokg * Fp;
+  const int j = tokg / jb.N, tok = tokg - j * jb.N;
+  const JobInfo ji = job_info(jb, j);
+  if (k >= F) {
+    Fo[idx] = (T)((k - F) == job_spin(jb, ji, tok) ? 1.0 : 0.0);
+    return;
+  }
+  const double* r = jb.R + ((size_t)ji.walker * jb.N + tok) * 2;
+  const int nf = mc.nf;
+  const int al = k / (2 * nf), rem = k - al * 2 * nf, tau = rem / nf, m = rem - tau * nf + 1;
+  const double sa = r[0] * mc.Ainv[al * 2 + 0] + r[1] * mc.Ainv[al * 2 + 1];
+  const double ang = ((2.0 * kPi) * sa) * (double)m;
+  double sn, cs;
+  sincos(ang, &sn, &cs);
+  Fo[idx] = (T)(tau == 0 ? sn : cs);
+}
+
+// --------------------------------------------------------------------------------------------
+// head backward (one CTA per walker): dL/dbf, and O of det_logw, Jastrow, dW
+// X1[tok][ch][KN] = (Re, Im) dL/dbf; X2[tok][ch][KN] = (-Im, Re) dL/dbf
+// --------------------------------------------------------------------------------------------
+struct HeadOffsets {
+  int64_t logw, jas_same, jas_opp, loga, dW;
+};
+
+inline size_t head_bwd_smem(int N, int nG, int K, bool env_grad) {
+  const size_t n2 = (size_t)N * N;
+  const size_t nc = (3 + (env_grad ? 1 : 0)) * n2 + (size_t)nG * N + N + 40 + 2 * (size_t)K;
+  return nc * 16 + 2 * N * sizeof(double) + (N + 2) * sizeof(int);
+}
+
+template <typename TIN, typename T, typename TO>
+__global__ void __launch_bounds__(256) k_head_bwd(JobBatch jb, ModelConst mc,
+                                                  const TIN* __restrict__ BF, int ldbf,
+                                                  HeadParams hp, T* __restrict__ X1,
+                                                  T* __restrict__ X2, ORows<TO> o,
+                                                  HeadOffsets off) {
+  const int wl = blockIdx.x;
+  const int N = jb.N, nG = mc.nG, K = mc.K, KN = K * N;
+  const JobInfo ji = job_info(jb, wl);
+  const int w = ji.walker;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* env = reinterpret_cast<cplx*>(smraw);
+  cplx* Wk = env + N * N;
+  cplx* inv = Wk + N * N;
+  cplx* denv = inv + N * N;  // only when learnable_env
+  cplx* ph = (mc.learnable_env ? denv + N * N : denv);
+  cplx* fcol = ph + nG * N;
+  cplx* red = fcol + N;
+  cplx* pk = red + 40;     // K
+  cplx* ldk = pk + K;      // K
+  double* rx = reinterpret_cast<double*>(ldk + K);
+  double* ry = rx + N;
+  int* sp = reinterpret_cast<int*>(ry + N);
+  int* piv_s = sp + N;
+  int* sing_s = piv_s + 1;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int i = tid; i < N; i += nth) {
+    const double* r = jb.R + ((size_t)w * N + i) * 2;
+    rx[i] = r[0];
+    ry[i] = r[1];
+    sp[i] = job_spin(jb, ji, i);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nG * N; idx += nth) {
+    const int g = idx / N, i = idx - g * N;
+    double s, c;
+    sincos(mc.Gs[2 * g] * rx[i] + mc.Gs[2 * g + 1] * ry[i], &s, &c);
+    ph[idx] = mk(c, s);
+  }
+  __syncthreads();
+  const size_t nW = (size_t)N * nG * 2;
+  for (int idx = tid; idx < N * N; idx += nth) {
+    const int a = idx / N, i = idx - a * N;
+    cplx e = mk(0, 0);
+    for (int g = 0; g < nG; ++g) {
+      const size_t oo = ((size_t)a * nG + g) * 2 + sp[i];
+      cplx wv = mk(mc.W[2 * oo], mc.W[2 * oo + 1]);
+      if (mc.learnable_env) wv = cadd(wv, mk(hp.dW[oo], hp.dW[nW + oo]));
+      cfma(e, ph[g * N + i], wv);
+    }
+    env[idx] = e;
+    if (mc.learnable_env) denv[idx] = mk(0, 0);
+  }
+  __syncthreads();
+  auto bf0 = [&](int k, int a, int i) -> cplx {
+    const TIN* p = BF + ((size_t)wl * N + i) * ldbf;
+    return mk((double)p[k * N + a], (double)p[KN + k * N + a]);
+  };
+  // pass 1: log dets
+  for (int k = 0; k < K; ++k) {
+    for (int idx = tid; idx < N * N; idx += nth) {
+      const int a = idx / N, i = idx - a * N;
+      const cplx b = bf0(k, a, i);
+      Wk[idx] = cmul(env[idx], mk(1.0 + b.re, b.im));
+    }
+    __syncthreads();
+    det_factor(Wk, nullptr, N, piv_s, fcol, red + 33, sing_s);
+    if (tid == 0) ldk[k] = *sing_s ? mk(-INFINITY, 0.0) : red[33];
+    __syncthreads();
+  }
+  // p_k = d L / d logdet_k
+  if (tid == 0) {
+    if (K == 1) {
+      pk[0] = isfinite(ldk[0].re) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+    } else {
+      double m = -INFINITY;
+      for (int k = 0; k < K; ++k) {
+        const double zr = ldk[k].re + hp.det_logw[k];
+        if (zr > m) m = zr;
+      }
+      cplx s = mk(0, 0);
+      for (int k = 0; k < K; ++k) {
+        if (!isfinite(ldk[k].re)) continue;
+        s = cadd(s, cexp_(mk(ldk[k].re + hp.det_logw[k] - m, ldk[k].im + hp.det_logw[K + k])));
+      }
+      const cplx L = mk(m + log(hypot(s.re, s.im)), atan2(s.im, s.re));
+      for (int k = 0; k < K; ++k) {
+        pk[k] = isfinite(ldk[k].re)
+                    ? cexp_(csub(mk(ldk[k].re + hp.det_logw[k], ldk[k].im + hp.det_logw[K + k]), L))
+                    : mk(0.0, 0.0);
+      }
+    }
+  }
+  __syncthreads();
+  // pass 2: inverses -> dL/dbf
+  for (int k = 0; k < K; ++k) {
+    for (int idx = tid; idx < N * N; idx += nth) {
+      const int a = idx / N, i = idx - a * N;
+      const cplx b = bf0(k, a, i);
+      Wk[idx] = cmul(env[idx], mk(1.0 + b.re, b.im));
+    }
+    __syncthreads();
+    det_factor(Wk, inv, N, piv_s, fcol, red + 33, sing_s);
+    const cplx p = pk[k];
+    for (int idx = tid; idx < N * N; idx += nth) {
+      const int i = idx / N, a = idx - i * N;  // a fastest: coalesced writes along KN
+      const cplx gM = cmul(p, inv[i * N + a]);  // dL/dM[a][i]
+      const cplx gb = (p.re == 0.0 && p.im == 0.0) ? mk(0, 0) : cmul(gM, env[a * N + i]);
+      const size_t row = ((size_t)wl * N + i) * 2;
+      const int col = k * N + a;
+      X1[row * KN + col] = (T)gb.re;
+      X1[(row + 1) * KN + col] = (T)gb.im;
+      X2[row * KN + col] = (T)(-gb.im);
+      X2[(row + 1) * KN + col] = (T)gb.re;
+      if (mc.learnable_env && !(p.re == 0.0 && p.im == 0.0)) {
+        const cplx b = bf0(k, a, i);
+        denv[a * N + i] = cadd(denv[a * N + i], cmul(gM, mk(1.0 + b.re, b.im)));
+      }
+    }
+    __syncthreads();
+  }
+  // det_logw
+  if (K > 1)
+    for (int k = tid; k < K; k += nth) o.put_c(w, off.logw, K, k, pk[k].re, pk[k].im);
+  // dW: dL/dW[a][g][s] = sum_{i: s_i = s} denv[a][i] ph[g][i]
+  if (mc.learnable_env) {
+    for (int idx = tid; idx < (int)nW; idx += nth) {
+      const int a = idx / (nG * 2), r = idx - a * nG * 2, g = r / 2, s = r - g * 2;
+      cplx acc = mk(0, 0);
+      for (int i = 0; i < N; ++i)
+        if (sp[i] == s) cfma(acc, denv[a * N + i], ph[g * N + i]);
+      o.put_c(w, off.dW, (int64_t)nW, idx, acc.re, acc.im);
+    }
+  }
+  // Jastrow
+  if (mc.use_jastrow) {
+    if (mc.jastrow_kind == 0) {
+      for (int q = tid; q < 2 * mc.n_knots; q += nth) {
+        const bool same = q < mc.n_knots;
+        const int kk = same ? q : q - mc.n_knots;
+        double acc = 0.0;
+        for (int i = 0; i < N; ++i)
+          for (int j = i + 1; j < N; ++j) {
+            if ((sp[i] == sp[j]) != same) continue;
+            double dx, dy;
+            min_image(mc, rx[i] - rx[j], ry[i] - ry[j], &dx, &dy);
+            const double r = sqrt(dx * dx + dy * dy + 1e-12);
+            const double z = (r - mc.knots[kk]) / mc.wdt;
+            acc += exp(-(z * z));
+          }
+        o.put(w, (same ? off.jas_same : off.jas_opp) + kk, acc, 0.0);
+      }
+    } else if (tid == 0) {
+      const double la = hp.jas_loga[0];
+      const double a = (la > 0 ? la + log1p(exp(-la)) : log1p(exp(la))) + 0.05;
+      const double sig = 1.0 / (1.0 + exp(-la));
+      double acc = 0.0;
+      for (int i = 0; i < N; ++i)
+        for (int j = i + 1; j < N; ++j) {
+          double dx, dy;
+          min_image(mc, rx[i] - rx[j], ry[i] - ry[j], &dx, &dy);
+          const double r = sqrt(dx * dx + dy * dy + 1e-12);
+          const double al = sp[i] == sp[j] ? mc.cusp / 3.0 : mc.cusp;
+          const double e = exp(-r / a);
+          acc += al * ((1.0 - e) - (r / a) * e);
+        }
+      o.put(w, off.loga, acc * sig, 0.0);
+    }
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// orchestration
+// --------------------------------------------------------------------------------------------
+template <typename T>
+struct SaveBufs {
+  T *xin[NQS_MAX_DEPTH], *h0[NQS_MAX_DEPTH], *qkv[NQS_MAX_DEPTH], *ao[NQS_MAX_DEPTH];
+  T *xmid[NQS_MAX_DEPTH], *h1[NQS_MAX_DEPTH], *a0[NQS_MAX_DEPTH], *g0[NQS_MAX_DEPTH];
+  T *xL, *hf, *bf, *feat;
+  T *xb, *hb, *big, *X1, *X2;
+};
+
+template <typename T>
+size_t bwd_row_elems(const ModelConst& mc) {
+  const size_t d = mc.d, D = (size_t)mc.ff * d, KN = (size_t)mc.K * mc.N;
+  const size_t per_block = 6 * d + 3 * d + 2 * D - d;  // xin h0 qkv(3d) ao xmid h1 a0 g0
+  const size_t big = std::max({6 * d, 2 * D, 2 * KN});
+  return (size_t)mc.depth * per_block + 2 * d + 2 * KN + (4 * mc.nf + 2) + 2 * d + 2 * d + big +
+         4 * KN;
+}
+
+size_t bwd_chunk_walkers(const ModelConst& mc, int W) {
+  const size_t rows = (size_t)1 << 17;
+  return std::max<size_t>(1, std::min<size_t>((size_t)W, rows / mc.N));
+}
+
+template <typename T>
+size_t per_sample_O_scratch(const ModelConst& mc, int W) {
+  const size_t nw = bwd_chunk_walkers(mc, W);
+  return nw * mc.N * bwd_row_elems<T>(mc) * sizeof(T) + 64 * 256;
+}
+
+template <typename T, typename TO>
+int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                     const double* R, const int32_t* S, int W, TO* O, Arena& ws,
+                     cudaStream_t st) {
+  const ModelConst& mc = hm.mc;
+  const NqsModelDesc& dsc = hm.desc;
+  const int N = mc.N, d = mc.d, D = mc.ff * d, KN = mc.K * N, H = mc.H;
+  const int Fp = 4 * mc.nf + 2;
+  const int nwc = (int)bwd_chunk_walkers(mc, W);
+  const size_t rows = (size_t)nwc * N;
+  const size_t save = ws.used;
+  SaveBufs<T> b{};
+  for (int l = 0; l < mc.depth; ++l) {
+    b.xin[l] = ws.take<T>(rows * d);
+    b.h0[l] = ws.take<T>(rows * d);
+    b.qkv[l] = ws.take<T>(rows * 3 * d);
+    b.ao[l] = ws.take<T>(rows * d);
+    b.xmid[l] = ws.take<T>(rows * d);
+    b.h1[l] = ws.take<T>(rows * d);
+    b.a0[l] = ws.take<T>(rows * D);
+    b.g0[l] = ws.take<T>(rows * D);
+  }
+  b.xL = ws.take<T>(rows * d);
+  b.hf = ws.take<T>(rows * d);
+  b.bf = ws.take<T>(rows * 2 * KN);
+  b.feat = ws.take<T>(rows * Fp);
+  b.xb = ws.take<T>(rows * 2 * d);
+  b.hb = ws.take<T>(rows * 2 * d);
+  b.big = ws.take<T>(rows * std::max({6 * d, 2 * D, 2 * KN}));
+  b.X1 = ws.take<T>(rows * 2 * KN);
+  b.X2 = ws.take<T>(rows * 2 * KN);
+  if (!b.X2) {
+    set_error("workspace too small for the per-sample Jacobian");
+    return NQS_ERR_WORKSPACE;
+  }
+  ORows<TO> orows{O, dsc.n_params, W};
+  const size_t hsm = head_bwd_smem(N, mc.nG, mc.K, mc.learnable_env);
+  const size_t asm_ = attention_smem<T>(N, d / H);
+  const size_t absm = sizeof(T) * (size_t)(5 * N * (d / H) + 2 * N * N + N);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_head_bwd<T, T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         220 * 1024);
+    cudaFuncSetAttribute(k_attention<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_attn_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ln_bwd<T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const HeadOffsets hoff{dsc.off_det_logw, dsc.off_jas_c_same, dsc.off_jas_c_opp,
+                         dsc.off_jastrow_loga, dsc.off_dW};
+  for (int w0 = 0; w0 < W; w0 += nwc) {
+    const int nw = std::min(nwc, W - w0);
+    const int nt = nw * N;
+    JobBatch jb{JOB_VALUE, nw, N, 1, 0, 0, w0, R, S, nullptr};
+    // ---------------- forward with saved activations ----------------
+    T* x = b.xin[0] ? b.xin[0] : b.xL;
+    k_embed<T><<<(nt + 7) / 8, 256, 0, st>>>(jb, mc, w.emb_w, w.emb_b, mc.depth ? b.xin[0] : b.xL);
+    NQS_CHECK_LAUNCH("k_embed");
+    for (int l = 0; l < mc.depth; ++l) {
+      const BlockW<T>& bw = w.blk[l];
+      x = b.xin[l];
+      k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[l]);
+      NQS_CHECK_LAUNCH("k_layernorm");
+      GemmArgs<T> g{};
+      g.X = b.h0[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+      g.Y = b.qkv[l]; g.ldy = 3 * d; g.nseg = 3;
+      g.seg[0] = GemmSeg<T>{bw.wq, bw.bq, d, d, 0, 0};
+      g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
+      g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+      k_attention<T><<<nw * H, 128, asm_, st>>>(nw, N, 1, 0, 0, d, H, b.qkv[l], b.ao[l]);
+      NQS_CHECK_LAUNCH("k_attention");
+      g = GemmArgs<T>{};
+      g.X = b.ao[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+      g.Y = b.xmid[l]; g.ldy = d; g.Res = x; g.ldr = d; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+      k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, b.xmid[l], bw.ln1_s, bw.ln1_b,
+                                                   b.h1[l]);
+      NQS_CHECK_LAUNCH("k_layernorm");
+      g = GemmArgs<T>{};
+      g.X = b.h1[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+      g.Y = b.a0[l]; g.ldy = D; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+      cudaMemcpyAsync(b.g0[l], b.a0[l], sizeof(T) * (size_t)nt * D, cudaMemcpyDeviceToDevice, st);
+      const size_t nel = (size_t)nt * D;
+      k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, 1, 0, 0, D, b.g0[l]);
+      NQS_CHECK_LAUNCH("k_gelu");
+      g = GemmArgs<T>{};
+      g.X = b.g0[l]; g.ldx = D; g.rows = nt; g.K = D; g.C = 1;
+      g.Y = (l + 1 < mc.depth) ? b.xin[l + 1] : b.xL; g.ldy = d; g.Res = b.xmid[l]; g.ldr = d;
+      g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+    }
+    k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, b.xL, w.lnf_s, w.lnf_b, b.hf);
+    NQS_CHECK_LAUNCH("k_layernorm");
+    {
+      GemmArgs<T> g{};
+      g.X = b.hf; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+      g.Y = b.bf; g.ldy = 2 * KN; g.nseg = 2;
+      g.seg[0] = GemmSeg<T>{w.bf_w_re, w.bf_b_re, KN, KN, 0, 0};
+      g.seg[1] = GemmSeg<T>{w.bf_w_im, w.bf_b_im, KN, KN, KN, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+    }
+    // ---------------- reverse ----------------
+    k_head_bwd<T, T, TO><<<nw, 256, hsm, st>>>(jb, mc, b.bf, 2 * KN, hp, b.X1, b.X2, orows, hoff);
+    NQS_CHECK_LAUNCH("k_head_bwd");
+    // backflow: hbar = X1 Wr^T + X2 Wi^T ; O of the complex kernel / bias
+    {
+      GemmArgs<T> g{};
+      g.X = b.X1; g.ldx = KN; g.rows = 2 * nt; g.K = KN; g.C = 2; g.trans_w = 1;
+      g.Y = b.hb; g.ldy = d; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{w.bf_w_re, nullptr, KN, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+      g.X = b.X2; g.Res = b.hb; g.ldr = d;
+      g.seg[0] = GemmSeg<T>{w.bf_w_im, nullptr, KN, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+    }
+    NQS_TRY(launch_wgrad<T, TO>(nw, N, d, KN, b.hf, d, b.X1, KN, orows, w0,
+                                dsc.off_backflow_kernel, dsc.off_backflow_bias, 1, st));
+    // final LayerNorm
+    k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+        N, d, b.xL, b.hb, w.lnf_s, b.xb, 0, orows, w0, dsc.off_final_ln_scale,
+        dsc.off_final_ln_bias);
+    NQS_CHECK_LAUNCH("k_ln_bwd");
+    for (int l = mc.depth - 1; l >= 0; --l) {
+      const BlockW<T>& bw = w.blk[l];
+      const int64_t* of = dsc.off_block[l];
+      // MLP: x_out = xmid + g0 W1 + b1
+      GemmArgs<T> g{};
+      g.X = b.xb; g.ldx = d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
+      g.Y = b.big; g.ldy = D; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.w1, nullptr, d, D, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));  // gbar0 = xbar W1^T
+      NQS_TRY(launch_wgrad<T, TO>(nw, N, D, d, b.g0[l], D, b.xb, d, orows, w0,
+                                  of[NQS_B_DENSE1_KERNEL], of[NQS_B_DENSE1_BIAS], 0, st));
+      const size_t nel = (size_t)nt * D;
+      k_gelu_bwd<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, D, b.a0[l], b.big);
+      NQS_CHECK_LAUNCH("k_gelu_bwd");
+      g = GemmArgs<T>{};
+      g.X = b.big; g.ldx = D; g.rows = 2 * nt; g.K = D; g.C = 2; g.trans_w = 1;
+      g.Y = b.hb; g.ldy = d; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.w0, nullptr, D, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));  // hbar1 = abar0 W0^T
+      NQS_TRY(launch_wgrad<T, TO>(nw, N, d, D, b.h1[l], d, b.big, D, orows, w0,
+                                  of[NQS_B_DENSE0_KERNEL], of[NQS_B_DENSE0_BIAS], 0, st));
+      k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+          N, d, b.xmid[l], b.hb, bw.ln1_s, b.xb, 1, orows, w0, of[NQS_B_LN1_SCALE],
+          of[NQS_B_LN1_BIAS]);
+      NQS_CHECK_LAUNCH("k_ln_bwd");
+      // attention: xmid = xin + ao Wo + bo
+      g = GemmArgs<T>{};
+      g.X = b.xb; g.ldx = d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
+      g.Y = b.hb; g.ldy = d; g.nseg = 1;
+      g.seg[0] = GemmSeg<T>{bw.wo, nullptr, d, d, 0, 0};
+      NQS_TRY(launch_gemm<T>(g, st));  // aobar
+      NQS_TRY(launch_wgrad<T, TO>(nw, N, d, d, b.ao[l], d, b.xb, d, orows, w0,
+                                  of[NQS_B_O_KERNEL], of[NQS_B_O_BIAS], 0, st));
+      k_attn_bwd<T><<<nw * H, 128, absm, st>>>(N, d, H, b.qkv[l], b.hb, b.big);
+      NQS_CHECK_LAUNCH("k_attn_bwd");
+      // h0bar = qbar Wq^T + kbar Wk^T + vbar Wv^T
+      const T* wts[3] = {bw.wq, bw.wk, bw.wv};
+      for (int s = 0; s < 3; ++s) {
+        g = GemmArgs<T>{};
+        g.X = b.big + s * d; g.ldx = 3 * d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
+        g.Y = b.hb; g.ldy = d; g.Res = s ? b.hb : nullptr; g.ldr = d; g.nseg = 1;
+        g.seg[0] = GemmSeg<T>{wts[s], nullptr, d, d, 0, 0};
+        NQS_TRY(launch_gemm<T>(g, st));
+      }
+      const int kk[3] = {NQS_B_Q_KERNEL, NQS_B_K_KERNEL, NQS_B_V_KERNEL};
+      const int kb[3] = {NQS_B_Q_BIAS, NQS_B_K_BIAS, NQS_B_V_BIAS};
+      for (int s = 0; s < 3; ++s)
+        NQS_TRY(launch_wgrad<T, TO>(nw, N, d, d, b.h0[l], d, b.big + s * d, 3 * d, orows, w0,
+                                    of[kk[s]], of[kb[s]], 0, st));
+      k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+          N, d, b.xin[l], b.hb, bw.ln0_s, b.xb, 1, orows, w0, of[NQS_B_LN0_SCALE],
+          of[NQS_B_LN0_BIAS]);
+      NQS_CHECK_LAUNCH("k_ln_bwd");
+    }
+    // embedding
+    k_features<T><<<(nt * Fp + 255) / 256, 256, 0, st>>>(jb, mc, b.feat);
+    NQS_CHECK_LAUNCH("k_features");
+    NQS_TRY(launch_wgrad<T, TO>(nw, N, Fp, d, b.feat, Fp, b.xb, d, orows, w0,
+                                dsc.off_embed_kernel, dsc.off_embed_bias, 0, st));
+  }
+  ws.used = save;
+  return NQS_OK;
+}
+
+template size_t per_sample_O_scratch<double>(const ModelConst&, int);
+template size_t per_sample_O_scratch<float>(const ModelConst&, int);
+template int per_sample_O_run<double, double>(const HostModel&, const NetW<double>&,
+                                              const HeadParams&, const double*, const int32_t*,
+                                              int, double*, Arena&, cudaStream_t);
+template int per_sample_O_run<float, float>(const HostModel&, const NetW<float>&,
+                                            const HeadParams&, const double*, const int32_t*, int,
+                                            float*, Arena&, cudaStream_t);
+template int per_sample_O_run<float, double>(const HostModel&, const NetW<float>&,
+                                             const HeadParams&, const double*, const int32_t*,
+                                             int, double*, Arena&, cudaStream_t);
+template int per_sample_O_run<double, float>(const HostModel&, const NetW<double>&,
+                                             const HeadParams&, const double*, const int32_t*,
+                                             int, float*, Arena&, cudaStream_t);
+
+}  // namespace nqs

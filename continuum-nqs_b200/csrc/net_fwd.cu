@@ -12,910 +12,9 @@
 #include <cstdio>
 #include <algorithm>
 
-#include "net.cuh"
+#include "net_kernels.cuh"
 
 namespace nqs {
-
-constexpr double kPi = 3.141592653589793;
-constexpr double kLnEps = 1e-6;  // flax.linen.LayerNorm default epsilon
-
-// ============================================================================================
-// embed: periodic features + spin one-hot -> Dense "embed" (psiformer.py:84-97,127-131)
-// ============================================================================================
-template <typename T>
-__global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
-                                               const T* __restrict__ Wemb,
-                                               const T* __restrict__ bemb, T* __restrict__ X) {
-  __shared__ double sf[8][4][4 * NQS_MAX_FREQ];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
-  if (gw >= jb.n_jobs * jb.N) return;  // warp-uniform
-  const int j = gw / jb.N, tok = gw - j * jb.N;
-  const JobInfo ji = job_info(jb, j);
-  const double* r = jb.R + ((size_t)ji.walker * jb.N + tok) * 2;
-  const double r0 = r[0], r1 = r[1];
-  const int nf = mc.nf, F = 4 * nf, d = mc.d;
-  const int s = job_spin(jb, ji, tok);
-  const int te = tok - ji.tan_e0;
-  const bool is_tan = (te >= 0) && (2 * te < jb.n_tan);
-  for (int k = lane; k < F; k += 32) {
-    const int al = k / (2 * nf), rem = k - al * 2 * nf, tau = rem / nf, m = rem - tau * nf + 1;
-    const double sa = r0 * mc.Ainv[al * 2 + 0] + r1 * mc.Ainv[al * 2 + 1];
-    const double ph = (2.0 * kPi) * sa;
-    const double ang = ph * (double)m;
-    double sn, cs;
-    sincos(ang, &sn, &cs);
-    const double val = tau == 0 ? sn : cs;
-    const double der = tau == 0 ? cs : -sn;
-    const double c0 = 2.0 * kPi * m * mc.Ainv[al * 2 + 0], c1 = 2.0 * kPi * m * mc.Ainv[al * 2 + 1];
-    sf[wib][0][k] = val;
-    sf[wib][1][k] = c0 * der;
-    sf[wib][2][k] = c1 * der;
-    sf[wib][3][k] = -(c0 * c0 + c1 * c1) * val;
-  }
-  __syncwarp();
-  T* xrow = X + ((size_t)j * jb.N + tok) * jb.C * d;
-  for (int n = lane; n < d; n += 32) {
-    double v = 0, dx = 0, dy = 0, lp = 0;
-    for (int k = 0; k < F; ++k) {
-      const double w = (double)Wemb[(size_t)k * d + n];
-      v = fma(sf[wib][0][k], w, v);
-      dx = fma(sf[wib][1][k], w, dx);
-      dy = fma(sf[wib][2][k], w, dy);
-      lp = fma(sf[wib][3][k], w, lp);
-    }
-    v += (double)Wemb[(size_t)(F + s) * d + n];
-    v += (double)bemb[n];
-    xrow[n] = (T)v;
-    for (int t = 0; t < jb.n_tan; ++t) {
-      double o = 0;
-      if (is_tan && t == 2 * te) o = dx;
-      if (is_tan && t == 2 * te + 1) o = dy;
-      xrow[(size_t)(1 + t) * d + n] = (T)o;
-    }
-    if (jb.has_lap) xrow[(size_t)(jb.C - 1) * d + n] = (T)(is_tan ? lp : 0.0);
-  }
-}
-
-// ============================================================================================
-// LayerNorm with tangent and Laplacian channels (flax LayerNorm: eps 1e-6, scale, bias)
-//   u = x - mean(x), v = mean(u^2), rho = (v+eps)^-1/2, y = u rho g + b
-//   d_t y = g (d_t u rho + u d_t rho),  d_t rho = -rho^3 mean(u d_t u)
-//   Lap y = g (Lap u rho + 2 sum_t d_t u d_t rho + u Lap rho),
-//   Lap rho = 3/4 rho^5 sum_t (d_t v)^2 - 1/2 rho^3 Lap v,  Lap v = 2 mean(u Lap u) + 2 sum_t mean((d_t u)^2)
-// ============================================================================================
-template <typename T>
-__global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, int has_lap, int d,
-                                                   const T* __restrict__ X,
-                                                   const T* __restrict__ g,
-                                                   const T* __restrict__ b, T* __restrict__ Y) {
-  constexpr int Q = NQS_MAX_EMBED / 32;
-  const int lane = threadIdx.x & 31;
-  const int tok = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (tok >= n_tok) return;
-  const T* x = X + (size_t)tok * C * d;
-  T* y = Y + (size_t)tok * C * d;
-  const T inv_d = T(1) / T(d);
-  T u[Q], gm[Q];
-  T s = 0;
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int f = lane + 32 * q;
-    u[q] = f < d ? x[f] : T(0);
-    gm[q] = f < d ? g[f] : T(0);
-    s += u[q];
-  }
-  const T mu = warp_sum(s) * inv_d;
-  s = 0;
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int f = lane + 32 * q;
-    if (f < d) {
-      u[q] -= mu;
-      s += u[q] * u[q];
-    }
-  }
-  const T var = warp_sum(s) * inv_d;
-  const T rho = T(1) / sqrt(var + T(kLnEps));
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int f = lane + 32 * q;
-    if (f < d) y[f] = (u[q] * rho) * gm[q] + b[f];
-  }
-  T S1 = 0, S2 = 0, acc[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) acc[q] = 0;
-  const T rho3 = rho * rho * rho;
-  for (int t = 0; t < n_tan; ++t) {
-    const T* xt = x + (size_t)(1 + t) * d;
-    T du[Q];
-    s = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      du[q] = f < d ? xt[f] : T(0);
-      s += du[q];
-    }
-    const T mt = warp_sum(s) * inv_d;
-    T s2 = 0, s3 = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) {
-        du[q] -= mt;
-        s2 += u[q] * du[q];
-        s3 += du[q] * du[q];
-      }
-    }
-    const T dv = T(2) * warp_sum(s2) * inv_d;
-    const T drho = T(-0.5) * rho3 * dv;
-    T* yt = y + (size_t)(1 + t) * d;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) {
-        yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
-        acc[q] += du[q] * drho;
-      }
-    }
-    S1 += dv * dv;
-    S2 += warp_sum(s3) * inv_d;
-  }
-  if (has_lap) {
-    const T* xl = x + (size_t)(C - 1) * d;
-    T dl[Q];
-    s = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      dl[q] = f < d ? xl[f] : T(0);
-      s += dl[q];
-    }
-    const T ml = warp_sum(s) * inv_d;
-    T s2 = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) {
-        dl[q] -= ml;
-        s2 += u[q] * dl[q];
-      }
-    }
-    const T dvl = T(2) * warp_sum(s2) * inv_d + T(2) * S2;
-    const T d2rho = T(0.75) * rho3 * rho * rho * S1 - T(0.5) * rho3 * dvl;
-    T* yl = y + (size_t)(C - 1) * d;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) yl[f] = (dl[q] * rho + T(2) * acc[q] + u[q] * d2rho) * gm[q];
-    }
-  }
-}
-
-// ============================================================================================
-// Row GEMM: Y[r, off+n] = sum_k X[r,k] W[k,n] (+ bias[n] on value rows r % C == 0) (+ Res)
-// Up to 3 column segments with their own weights (q|k|v, re|im backflow). SIMT, 64x64 tiles.
-// ============================================================================================
-template <typename T>
-struct GemmSeg {
-  const T* W;
-  const T* b;
-  int ldw, ncols, out_off, tile0;
-};
-template <typename T>
-struct GemmArgs {
-  const T* X;
-  int ldx, rows, K, C;
-  T* Y;
-  int ldy;
-  const T* Res;
-  int ldr;
-  int nseg, trans_w;
-  GemmSeg<T> seg[3];
-};
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_gemm(GemmArgs<T> g) {
-  constexpr int BM = 64, BN = 64, BK = 16;
-  __shared__ T As[BK][BM + 1];
-  __shared__ T Bs[BK][BN + 1];
-  const int ct = blockIdx.y;
-  int sidx = 0;
-  while (sidx + 1 < g.nseg && ct >= g.seg[sidx + 1].tile0) ++sidx;
-  const GemmSeg<T> sg = g.seg[sidx];
-  const int n0 = (ct - sg.tile0) * BN;
-  const int m0 = blockIdx.x * BM;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  T acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) acc[i][jj] = T(0);
-  for (int k0 = 0; k0 < g.K; k0 += BK) {
-    for (int idx = threadIdx.x; idx < BM * BK; idx += 256) {
-      const int r = idx / BK, kk = idx - r * BK;
-      const int gr = m0 + r, gk = k0 + kk;
-      As[kk][r] = (gr < g.rows && gk < g.K) ? g.X[(size_t)gr * g.ldx + gk] : T(0);
-    }
-    for (int idx = threadIdx.x; idx < BK * BN; idx += 256) {
-      int kk, n;
-      if (!g.trans_w) {
-        kk = idx / BN;
-        n = idx - kk * BN;
-      } else {
-        n = idx / BK;
-        kk = idx - n * BK;
-      }
-      const int gk = k0 + kk, gn = n0 + n;
-      T v = T(0);
-      if (gk < g.K && gn < sg.ncols)
-        v = g.trans_w ? sg.W[(size_t)gn * sg.ldw + gk] : sg.W[(size_t)gk * sg.ldw + gn];
-      Bs[kk][n] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      T a[4], bb[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) bb[jj] = Bs[kk][tx + 16 * jj];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[i][jj] = fma(a[i], bb[jj], acc[i][jj]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = m0 + ty + 16 * i;
-    if (r >= g.rows) continue;
-    const bool val = (r % g.C) == 0;
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const int n = n0 + tx + 16 * jj;
-      if (n >= sg.ncols) continue;
-      T v = acc[i][jj];
-      if (val && sg.b) v += sg.b[n];
-      const size_t o = (size_t)r * g.ldy + sg.out_off + n;
-      if (g.Res) v = g.Res[(size_t)r * g.ldr + sg.out_off + n] + v;
-      g.Y[o] = v;
-    }
-  }
-}
-
-template <typename T>
-static int launch_gemm(GemmArgs<T> g, cudaStream_t st) {
-  int tiles = 0;
-  for (int s = 0; s < g.nseg; ++s) {
-    g.seg[s].tile0 = tiles;
-    tiles += (g.seg[s].ncols + 63) / 64;
-  }
-  if (g.rows <= 0 || tiles == 0) return NQS_OK;
-  k_gemm<T><<<dim3((g.rows + 63) / 64, tiles), 256, 0, st>>>(g);
-  NQS_CHECK_LAUNCH("k_gemm");
-  return NQS_OK;
-}
-
-// ============================================================================================
-// Multi-head attention with tangent / Laplacian channels, one CTA per (job, head).
-//   s = q.k/sqrt(hd), a = softmax_j(s), o = a v
-//   d_t s = (d_t q.k + q.d_t k) sc, d_t lse_i = sum_l a_il d_t s_il, d_t a = a (d_t s - d_t lse)
-//   d_t o = d_t a v + a d_t v
-//   Lap s = (Lap q.k + q.Lap k + 2 P_qk) sc,  P_qk = sum_t d_t q . d_t k
-//   Lap a = a (P_sq + Lap s - Lap lse), Lap lse_i = sum_l a_il (Lap s_il + P_sq_il),
-//           P_sq = sum_t (d_t s - d_t lse)^2
-//   Lap o = Lap a v + a Lap v + 2 P_av,  P_av = sum_t d_t a d_t v
-// ============================================================================================
-template <typename T>
-__global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int n_tan, int has_lap,
-                                                   int d, int H, const T* __restrict__ QKV,
-                                                   T* __restrict__ OUT) {
-  const int job = blockIdx.x / H, h = blockIdx.x - job * H;
-  const int hd = d / H;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* q = reinterpret_cast<T*>(smraw);
-  T* k = q + N * hd;
-  T* v = k + N * hd;
-  T* a = v + N * hd;
-  T* qt = a + N * N;
-  T* kt = qt + N * hd;
-  T* vt = kt + N * hd;
-  T* st = vt + N * hd;
-  T* lt = st + N * N;
-  T* Pqk = lt + N;
-  T* Psq = Pqk + N * N;
-  T* Pav = Psq + N * N;
-  const T sc = T(1) / sqrt(T(hd));
-  const int ld = 3 * d;
-  auto row = [&](int i, int c) -> size_t { return ((size_t)job * N + i) * C + c; };
-  const int tid = threadIdx.x, nth = blockDim.x;
-  for (int idx = tid; idx < N * hd; idx += nth) {
-    const int i = idx / hd, e = idx - i * hd;
-    const T* p = QKV + row(i, 0) * ld + h * hd + e;
-    q[idx] = p[0];
-    k[idx] = p[d];
-    v[idx] = p[2 * d];
-  }
-  if (has_lap)
-    for (int idx = tid; idx < N * N; idx += nth) Pqk[idx] = Psq[idx] = T(0);
-  if (has_lap)
-    for (int idx = tid; idx < N * hd; idx += nth) Pav[idx] = T(0);
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
-    const int i = idx / N, jj = idx - i * N;
-    T sacc = 0;
-    for (int e = 0; e < hd; ++e) sacc = fma(q[i * hd + e], k[jj * hd + e], sacc);
-    a[idx] = sacc * sc;
-  }
-  __syncthreads();
-  for (int i = tid; i < N; i += nth) {
-    T mx = a[i * N];
-    for (int jj = 1; jj < N; ++jj) mx = max(mx, a[i * N + jj]);
-    T ssum = 0;
-    for (int jj = 0; jj < N; ++jj) {
-      const T e = exp(a[i * N + jj] - mx);
-      a[i * N + jj] = e;
-      ssum += e;
-    }
-    for (int jj = 0; jj < N; ++jj) a[i * N + jj] = a[i * N + jj] / ssum;
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
-    const int i = idx / hd, e = idx - i * hd;
-    T o = 0;
-    for (int jj = 0; jj < N; ++jj) o = fma(a[i * N + jj], v[jj * hd + e], o);
-    OUT[row(i, 0) * d + h * hd + e] = o;
-  }
-  for (int t = 0; t < n_tan; ++t) {
-    __syncthreads();
-    for (int idx = tid; idx < N * hd; idx += nth) {
-      const int i = idx / hd, e = idx - i * hd;
-      const T* p = QKV + row(i, 1 + t) * ld + h * hd + e;
-      qt[idx] = p[0];
-      kt[idx] = p[d];
-      vt[idx] = p[2 * d];
-    }
-    __syncthreads();
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int i = idx / N, jj = idx - i * N;
-      T s1 = 0, s2 = 0;
-      for (int e = 0; e < hd; ++e) {
-        s1 = fma(qt[i * hd + e], k[jj * hd + e], s1);
-        s1 = fma(q[i * hd + e], kt[jj * hd + e], s1);
-        s2 = fma(qt[i * hd + e], kt[jj * hd + e], s2);
-      }
-      st[idx] = s1 * sc;
-      if (has_lap) Pqk[idx] += s2;
-    }
-    __syncthreads();
-    for (int i = tid; i < N; i += nth) {
-      T l = 0;
-      for (int jj = 0; jj < N; ++jj) l = fma(a[i * N + jj], st[i * N + jj], l);
-      lt[i] = l;
-    }
-    __syncthreads();
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int i = idx / N;
-      const T ds = st[idx] - lt[i];
-      if (has_lap) Psq[idx] += ds * ds;
-      st[idx] = a[idx] * ds;
-    }
-    __syncthreads();
-    for (int idx = tid; idx < N * hd; idx += nth) {
-      const int i = idx / hd, e = idx - i * hd;
-      T o = 0, pav = 0;
-      for (int jj = 0; jj < N; ++jj) {
-        o = fma(st[i * N + jj], v[jj * hd + e], o);
-        o = fma(a[i * N + jj], vt[jj * hd + e], o);
-        pav = fma(st[i * N + jj], vt[jj * hd + e], pav);
-      }
-      OUT[row(i, 1 + t) * d + h * hd + e] = o;
-      if (has_lap) Pav[idx] += pav;
-    }
-  }
-  if (!has_lap) return;
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
-    const int i = idx / hd, e = idx - i * hd;
-    const T* p = QKV + row(i, C - 1) * ld + h * hd + e;
-    qt[idx] = p[0];
-    kt[idx] = p[d];
-    vt[idx] = p[2 * d];
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
-    const int i = idx / N, jj = idx - i * N;
-    T s1 = 0;
-    for (int e = 0; e < hd; ++e) {
-      s1 = fma(qt[i * hd + e], k[jj * hd + e], s1);
-      s1 = fma(q[i * hd + e], kt[jj * hd + e], s1);
-    }
-    st[idx] = (s1 + T(2) * Pqk[idx]) * sc;
-  }
-  __syncthreads();
-  for (int i = tid; i < N; i += nth) {
-    T l = 0;
-    for (int jj = 0; jj < N; ++jj) l = fma(a[i * N + jj], st[i * N + jj] + Psq[i * N + jj], l);
-    lt[i] = l;
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
-    const int i = idx / N;
-    st[idx] = a[idx] * (Psq[idx] + st[idx] - lt[i]);
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
-    const int i = idx / hd, e = idx - i * hd;
-    T o = 0;
-    for (int jj = 0; jj < N; ++jj) {
-      o = fma(st[i * N + jj], v[jj * hd + e], o);
-      o = fma(a[i * N + jj], vt[jj * hd + e], o);
-    }
-    OUT[row(i, C - 1) * d + h * hd + e] = o + T(2) * Pav[idx];
-  }
-}
-
-template <typename T>
-static size_t attention_smem(int N, int hd) {
-  return sizeof(T) * (size_t)(6 * N * hd + 4 * N * N + N + N * hd);
-}
-
-// ============================================================================================
-// tanh-GELU (jax.nn.gelu, approximate=True) with tangent / Laplacian channels, in place.
-//   g = x cdf, cdf = 0.5 (1 + tanh(w)), w = c (x + 0.044715 x^3)
-//   g' = cdf + 0.5 x sech^2 w',  g'' = sech^2 (w' - x tanh(w) w'^2 + 0.5 x w'')
-// ============================================================================================
-template <typename T>
-__global__ void __launch_bounds__(256) k_gelu(size_t n_tok, int C, int n_tan, int has_lap, int D,
-                                              T* __restrict__ X) {
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_tok * (size_t)D) return;
-  const size_t tok = idx / D;
-  const int f = (int)(idx - tok * D);
-  T* x = X + tok * (size_t)C * D + f;
-  const T xv = x[0];
-  const T c = T(0.7978845608028654);  // sqrt(2/pi)
-  const T b3 = T(0.044715);
-  const T th = tanh(c * (xv + b3 * (xv * xv * xv)));
-  const T cdf = T(0.5) * (T(1) + th);
-  const T sech2 = T(1) - th * th;
-  const T w1 = c * (T(1) + T(3) * b3 * xv * xv);
-  const T w2 = c * T(6) * b3 * xv;
-  const T g1 = cdf + T(0.5) * xv * sech2 * w1;
-  const T g2 = sech2 * (w1 - xv * th * w1 * w1 + T(0.5) * xv * w2);
-  x[0] = xv * cdf;
-  T acc = 0;
-  for (int t = 0; t < n_tan; ++t) {
-    T* p = x + (size_t)(1 + t) * D;
-    const T xt = *p;
-    *p = g1 * xt;
-    acc += xt * xt;
-  }
-  if (has_lap) {
-    T* p = x + (size_t)(C - 1) * D;
-    *p = g1 * (*p) + g2 * acc;
-  }
-}
-
-// ============================================================================================
-// Head: envelope, K generalized spinor determinants (complex, partial pivoting, float64),
-// complex log-sum-exp over dets with det_logw, optional pair Jastrow; with tangents:
-//   d_t log det M = tr(M^-1 d_t M),   Lap log det M = tr(M^-1 Lap M) - sum_t tr((M^-1 d_t M)^2)
-//   LSE: d L = sum_k p_k d L_k,  Lap L = sum_k p_k (Lap L_k + sum_t (d_t L_k)^2) - sum_t (d_t L)^2
-// (psiformer.py:139-189). One CTA per job.
-// ============================================================================================
-// Shared-memory plan of k_head (complex entries unless noted):
-//   env[N*N] Wk[N*N] (inv[N*N] Bm[N*N] when tangents) ph[nG*N] G[n_tan] dLk[n_tan] fcol[N]
-//   red[40] | rx[N] ry[N] (double) | sp[N] piv sing (int)
-__host__ __device__ inline size_t head_smem_bytes(int N, int nG, int n_tan, bool tan) {
-  const size_t n2 = (size_t)N * N;
-  const size_t nc = (tan ? 4 : 2) * n2 + (size_t)nG * N + 2 * (size_t)n_tan + N + 40;
-  return nc * sizeof(cplx) + 2 * N * sizeof(double) + (N + 2) * sizeof(int);
-}
-
-__device__ __forceinline__ double cabs1(cplx z) { return fabs(z.re) + fabs(z.im); }
-
-// Block-wide complex sum; red needs >= 32 entries. All threads must call it.
-__device__ cplx block_sum_c(cplx v, cplx* red) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  v.re = warp_sum(v.re);
-  v.im = warp_sum(v.im);
-  __syncthreads();
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    cplx r = threadIdx.x < nw ? red[threadIdx.x] : mk(0, 0);
-    r.re = warp_sum(r.re);
-    r.im = warp_sum(r.im);
-    if (threadIdx.x == 0) red[0] = r;
-  }
-  __syncthreads();
-  const cplx r = red[0];
-  __syncthreads();
-  return r;
-}
-
-// Gauss-Jordan (inv != nullptr) or LU (value only) with partial pivoting (largest |re|+|im|,
-// first index on ties, as LAPACK getrf) on Wk (N x N row-major, rows = orbitals a,
-// cols = electrons j). Writes log det (principal arg) to *out_logdet and a singular flag;
-// inv receives M^-1 indexed [j][a]. All threads must call it.
-__device__ void det_factor(cplx* Wk, cplx* inv, int N, int* piv_s, cplx* fcol, cplx* out_logdet,
-                           int* out_sing) {
-  const int tid = threadIdx.x, nth = blockDim.x;
-  if (inv)
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int r = idx / N, c = idx - r * N;
-      inv[idx] = mk(r == c ? 1.0 : 0.0, 0.0);
-    }
-  double logabs = 0.0;
-  cplx sgn = mk(1.0, 0.0);
-  int sing = 0;
-  __syncthreads();
-  for (int c = 0; c < N; ++c) {
-    if (tid < 32) {
-      double best = -1.0;
-      int bi = c;
-      for (int r = c + tid; r < N; r += 32) {
-        const double v = cabs1(Wk[r * N + c]);
-        if (v > best) {
-          best = v;
-          bi = r;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      if (tid == 0) *piv_s = bi;
-    }
-    __syncthreads();
-    const int p = *piv_s;
-    if (p != c) {
-      for (int col = tid; col < N; col += nth) {
-        cplx t = Wk[c * N + col];
-        Wk[c * N + col] = Wk[p * N + col];
-        Wk[p * N + col] = t;
-        if (inv) {
-          t = inv[c * N + col];
-          inv[c * N + col] = inv[p * N + col];
-          inv[p * N + col] = t;
-        }
-      }
-      sgn = mk(-sgn.re, -sgn.im);
-    }
-    __syncthreads();
-    const cplx pv = Wk[c * N + c];
-    const double apv = hypot(pv.re, pv.im);
-    if (apv == 0.0) {
-      sing = 1;
-    } else {
-      logabs += log(apv);
-      sgn = cmul(sgn, mk(pv.re / apv, pv.im / apv));
-    }
-    const cplx ipv = (apv == 0.0) ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
-    for (int r = tid; r < N; r += nth) {
-      if (r == c || (!inv && r < c)) continue;
-      fcol[r] = cmul(Wk[r * N + c], ipv);
-    }
-    __syncthreads();
-    const int ncol = N - c - 1;
-    if (inv) {
-      const int wdt = ncol + N;
-      const int tot = N * wdt;
-      for (int idx = tid; idx < tot; idx += nth) {
-        const int r = idx / wdt, cc = idx - r * wdt;
-        if (r == c) continue;
-        const cplx f = fcol[r];
-        if (cc < ncol) {
-          const int col = c + 1 + cc;
-          Wk[r * N + col] = csub(Wk[r * N + col], cmul(f, Wk[c * N + col]));
-        } else {
-          const int col = cc - ncol;
-          inv[r * N + col] = csub(inv[r * N + col], cmul(f, inv[c * N + col]));
-        }
-      }
-      __syncthreads();
-      for (int col = tid; col < N; col += nth) {
-        if (col > c) Wk[c * N + col] = cmul(Wk[c * N + col], ipv);
-        inv[c * N + col] = cmul(inv[c * N + col], ipv);
-      }
-    } else {
-      const int tot = (N - c - 1) * ncol;
-      for (int idx = tid; idx < tot; idx += nth) {
-        const int rr = idx / ncol, cc = idx - rr * ncol;
-        const int r = c + 1 + rr, col = c + 1 + cc;
-        Wk[r * N + col] = csub(Wk[r * N + col], cmul(fcol[r], Wk[c * N + col]));
-      }
-    }
-    __syncthreads();
-  }
-  if (tid == 0) {
-    *out_logdet = sing ? mk(-INFINITY, 0.0) : mk(logabs, atan2(sgn.im, sgn.re));
-    *out_sing = sing;
-  }
-  __syncthreads();
-}
-
-// Pair Jastrow u(r), u'(r), u''(r) (psiformer.py:168-186).
-__device__ __forceinline__ void jastrow_u(const ModelConst& mc, const HeadParams& hp, double r,
-                                          bool same, double* u, double* u1, double* u2) {
-  if (mc.jastrow_kind == 0) {
-    const double* c = same ? hp.jas_same : hp.jas_opp;
-    double a0 = 0, a1 = 0, a2 = 0;
-    const double iw = 1.0 / mc.wdt;
-    for (int k = 0; k < mc.n_knots; ++k) {
-      const double z = (r - mc.knots[k]) / mc.wdt;
-      const double ce = c[k] * exp(-(z * z));
-      a0 += ce;
-      a1 += ce * (-2.0 * z * iw);
-      a2 += ce * (4.0 * z * z - 2.0) * iw * iw;
-    }
-    *u = a0;
-    *u1 = a1;
-    *u2 = a2;
-  } else {
-    const double la = hp.jas_loga[0];
-    const double a = (la > 0 ? la + log1p(exp(-la)) : log1p(exp(la))) + 0.05;  // softplus + .05
-    const double al = same ? mc.cusp / 3.0 : mc.cusp;
-    const double e = exp(-r / a);
-    *u = al * a * (1.0 - e);
-    *u1 = al * e;
-    *u2 = -(al / a) * e;
-  }
-}
-
-// Nearest-image displacement (psiformer.py:164-166): round-half-even as jnp.round.
-__device__ __forceinline__ void min_image(const ModelConst& mc, double dx, double dy, double* ox,
-                                          double* oy) {
-  double f0 = dx * mc.Ainv[0] + dy * mc.Ainv[1];
-  double f1 = dx * mc.Ainv[2] + dy * mc.Ainv[3];
-  f0 -= rint(f0);
-  f1 -= rint(f1);
-  *ox = f0 * mc.A[0] + f1 * mc.A[1];
-  *oy = f0 * mc.A[2] + f1 * mc.A[3];
-}
-
-template <typename TIN, bool TAN>
-__global__ void __launch_bounds__(256) k_head(JobBatch jb, ModelConst mc, const TIN* __restrict__ BF,
-                                              int ldbf, HeadParams hp, HeadOut out, int j_out0) {
-  const int job = blockIdx.x;
-  const int N = jb.N, C = jb.C, nG = mc.nG, K = mc.K;
-  const int n_tan = TAN ? jb.n_tan : 0;
-  const bool has_lap = TAN && jb.has_lap;
-  const JobInfo ji = job_info(jb, job);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* env = reinterpret_cast<cplx*>(smraw);
-  cplx* Wk = env + N * N;
-  cplx* inv = TAN ? Wk + N * N : nullptr;
-  cplx* Bm = TAN ? inv + N * N : nullptr;
-  cplx* ph = (TAN ? Bm : Wk) + N * N;
-  cplx* G = ph + nG * N;
-  cplx* dLk = G + n_tan;
-  cplx* fcol = dLk + n_tan;
-  cplx* red = fcol + N;  // 40 entries: [0..31] reductions, [33] logdet
-  double* rx = reinterpret_cast<double*>(red + 40);
-  double* ry = rx + N;
-  int* sp = reinterpret_cast<int*>(ry + N);
-  int* piv_s = sp + N;
-  int* sing_s = piv_s + 1;
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int te_lo = ji.tan_e0, te_hi = ji.tan_e0 + n_tan / 2;  // tangent electrons [lo, hi)
-
-  for (int i = tid; i < N; i += nth) {
-    const double* r = jb.R + ((size_t)ji.walker * N + i) * 2;
-    rx[i] = r[0];
-    ry[i] = r[1];
-    sp[i] = job_spin(jb, ji, i);
-  }
-  for (int t = tid; t < n_tan; t += nth) G[t] = mk(0, 0);
-  __syncthreads();
-  for (int idx = tid; idx < nG * N; idx += nth) {  // exp(i G.r) (psiformer.py:146)
-    const int g = idx / N, i = idx - g * N;
-    const double x = mc.Gs[2 * g] * rx[i] + mc.Gs[2 * g + 1] * ry[i];
-    double s, c;
-    sincos(x, &s, &c);
-    ph[idx] = mk(c, s);
-  }
-  __syncthreads();
-  auto Weff = [&](int a, int g, int s) -> cplx {
-    const size_t o = ((size_t)a * nG + g) * 2 + s;
-    cplx w = mk(mc.W[2 * o], mc.W[2 * o + 1]);
-    if (mc.learnable_env) w = cadd(w, mk(hp.dW[o], hp.dW[(size_t)N * nG * 2 + o]));
-    return w;
-  };
-  for (int idx = tid; idx < N * N; idx += nth) {  // env[a,i] (psiformer.py:147-148)
-    const int a = idx / N, i = idx - a * N;
-    cplx e = mk(0, 0);
-    for (int g = 0; g < nG; ++g) cfma(e, ph[g * N + i], Weff(a, g, sp[i]));
-    env[idx] = e;
-  }
-  __syncthreads();
-
-  // ---- Jastrow value and Laplacian ----
-  double J = 0.0, lapJ = 0.0;
-  if (mc.use_jastrow) {
-    double accJ = 0.0, accL = 0.0;
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int i = idx / N, jj = idx - i * N;
-      if (jj <= i) continue;
-      double dx, dy;
-      min_image(mc, rx[i] - rx[jj], ry[i] - ry[jj], &dx, &dy);
-      const double d2 = dx * dx + dy * dy;
-      const double r = sqrt(d2 + 1e-12);
-      double u, u1, u2;
-      jastrow_u(mc, hp, r, sp[i] == sp[jj], &u, &u1, &u2);
-      accJ += u;
-      if (has_lap) {
-        const double l = u2 * d2 / (r * r) + u1 * (2.0 / r - d2 / (r * r * r));
-        const int cnt = (i >= te_lo && i < te_hi) + (jj >= te_lo && jj < te_hi);
-        accL += l * cnt;
-      }
-    }
-    const cplx s = block_sum_c(mk(accJ, accL), red);
-    J = s.re;
-    lapJ = s.im;
-  }
-
-  auto bfval = [&](int c, int k, int a, int i) -> cplx {
-    const TIN* p = BF + (((size_t)job * N + i) * C + c) * ldbf;
-    return mk((double)p[k * N + a], (double)p[K * N + k * N + a]);
-  };
-
-  // ---- determinants with an online complex log-sum-exp (max-Re shift) ----
-  double m_run = -INFINITY;
-  cplx ssum = mk(0, 0), Lam = mk(0, 0), L_first = mk(0, 0), lap_first = mk(0, 0);
-  for (int k = 0; k < K; ++k) {
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int a = idx / N, i = idx - a * N;
-      const cplx b0 = bfval(0, k, a, i);
-      Wk[idx] = cmul(env[idx], mk(1.0 + b0.re, b0.im));  // M = env (1 + bf)
-    }
-    __syncthreads();
-    det_factor(Wk, inv, N, piv_s, fcol, red + 33, sing_s);
-    const cplx logdet = red[33];
-    const int sing = *sing_s;
-    cplx lapk = mk(0, 0), sq = mk(0, 0);
-    if (TAN) {
-      if (has_lap) {  // tr(M^-1 Lap M)
-        cplx acc = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {
-          const int a = idx / N, i = idx - a * N;
-          cplx lm = cmul(env[idx], bfval(C - 1, k, a, i));
-          if (i >= te_lo && i < te_hi) {
-            cplx dxe = mk(0, 0), dye = mk(0, 0), le = mk(0, 0);
-            for (int g = 0; g < nG; ++g) {
-              const cplx pw = cmul(ph[g * N + i], Weff(a, g, sp[i]));
-              const double gx = mc.Gs[2 * g], gy = mc.Gs[2 * g + 1];
-              cfma(dxe, pw, mk(0, gx));
-              cfma(dye, pw, mk(0, gy));
-              le = cadd(le, cscale(pw, -(gx * gx + gy * gy)));
-            }
-            const cplx b0 = bfval(0, k, a, i);
-            const int tx = 2 * (i - te_lo);
-            lm = cadd(lm, cmul(le, mk(1.0 + b0.re, b0.im)));
-            lm = cadd(lm, cscale(cmul(dxe, bfval(1 + tx, k, a, i)), 2.0));
-            lm = cadd(lm, cscale(cmul(dye, bfval(2 + tx, k, a, i)), 2.0));
-          }
-          cfma(acc, inv[i * N + a], lm);
-        }
-        lapk = block_sum_c(acc, red);
-      }
-      for (int t = 0; t < n_tan; ++t) {
-        const int e = te_lo + t / 2, bax = t & 1;
-        for (int idx = tid; idx < N * N; idx += nth) {  // D_t = d_t M
-          const int a = idx / N, i = idx - a * N;
-          cplx dm = cmul(env[idx], bfval(1 + t, k, a, i));
-          if (i == e) {
-            cplx de = mk(0, 0);
-            for (int g = 0; g < nG; ++g)
-              cfma(de, cmul(ph[g * N + i], Weff(a, g, sp[i])), mk(0, mc.Gs[2 * g + bax]));
-            const cplx b0 = bfval(0, k, a, i);
-            dm = cadd(dm, cmul(de, mk(1.0 + b0.re, b0.im)));
-          }
-          Wk[idx] = dm;
-        }
-        __syncthreads();
-        cplx trb = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {  // B = M^-1 D_t
-          const int i = idx / N, i2 = idx - i * N;
-          cplx s = mk(0, 0);
-          for (int a = 0; a < N; ++a) cfma(s, inv[i * N + a], Wk[a * N + i2]);
-          Bm[idx] = s;
-          if (i == i2) trb = cadd(trb, s);
-        }
-        __syncthreads();
-        cplx trb2 = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {
-          const int i = idx / N, i2 = idx - i * N;
-          cfma(trb2, Bm[idx], Bm[i2 * N + i]);
-        }
-        const cplx tr1 = block_sum_c(trb, red);
-        const cplx tr2 = block_sum_c(trb2, red);
-        if (tid == 0) dLk[t] = tr1;
-        lapk = csub(lapk, tr2);
-        cfma(sq, tr1, tr1);
-      }
-      __syncthreads();
-    }
-    if (k == 0) {
-      L_first = logdet;
-      lap_first = lapk;
-    }
-    const cplx wk = (K > 1 && hp.det_logw) ? mk(hp.det_logw[k], hp.det_logw[K + k]) : mk(0, 0);
-    const cplx z = cadd(logdet, wk);
-    if (!sing) {
-      if (z.re > m_run) {
-        const double sc = (m_run == -INFINITY) ? 0.0 : exp(m_run - z.re);
-        ssum = cscale(ssum, sc);
-        Lam = cscale(Lam, sc);
-        for (int t = tid; t < n_tan; t += nth) G[t] = cscale(G[t], sc);
-        m_run = z.re;
-      }
-      const cplx e = cexp_(mk(z.re - m_run, z.im));
-      ssum = cadd(ssum, e);
-      Lam = cadd(Lam, cmul(e, cadd(lapk, sq)));
-      for (int t = tid; t < n_tan; t += nth) cfma(G[t], e, dLk[t]);
-    }
-    __syncthreads();
-  }
-
-  // ---- combine, add Jastrow, write ----
-  const int jo = j_out0 + job;
-  const bool all_sing = (m_run == -INFINITY);
-  cplx L;
-  if (K == 1) {
-    L = L_first;
-  } else {
-    L = all_sing ? mk(-INFINITY, 0.0)
-                 : mk(m_run + log(hypot(ssum.re, ssum.im)), atan2(ssum.im, ssum.re));
-  }
-  cplx sumsq_local = mk(0, 0);
-  for (int t = tid; t < n_tan; t += nth) {
-    cplx g = all_sing ? mk(NAN, NAN) : (K == 1 ? dLk[t] : cdiv(G[t], ssum));
-    cfma(sumsq_local, g, g);
-    if (mc.use_jastrow) {
-      const int e = te_lo + t / 2, bax = t & 1;
-      double gj = 0.0;
-      for (int jj = 0; jj < N; ++jj) {
-        if (jj == e) continue;
-        double dx, dy;
-        min_image(mc, rx[e] - rx[jj], ry[e] - ry[jj], &dx, &dy);
-        const double r = sqrt(dx * dx + dy * dy + 1e-12);
-        double u, u1, u2;
-        jastrow_u(mc, hp, r, sp[e] == sp[jj], &u, &u1, &u2);
-        gj += u1 * (bax == 0 ? dx : dy) / r;
-      }
-      g.re += gj;
-    }
-    if (out.dL) out.dL[(size_t)jo * jb.n_tan + t] = g;
-  }
-  cplx sumsq = mk(0, 0);
-  if (has_lap && K > 1) sumsq = block_sum_c(sumsq_local, red);
-  if (tid == 0) {
-    if (mc.use_jastrow) L.re += J;
-    if (out.L) out.L[jo] = L;
-    if (has_lap && out.lap) {
-      cplx lap;
-      if (K == 1)
-        lap = lap_first;
-      else
-        lap = all_sing ? mk(NAN, NAN) : csub(cdiv(Lam, ssum), sumsq);
-      lap.re += lapJ;
-      out.lap[jo] = lap;
-    }
-  }
-}
-
-static size_t head_smem(int N, int nG, int n_tan, bool tan) {
-  return head_smem_bytes(N, nG, n_tan, tan);
-}
 
 // ============================================================================================
 // host orchestration

@@ -23,9 +23,9 @@ int cuda_status(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return nqs::cuda_status(_e, what);               \
   } while (0)
 
-#define NQS_TRY(expr)                                                       \
+#define NQS_TRY(...)                                                        \
   do {                                                                      \
-    int _s = (expr);                                                        \
+    int _s = (__VA_ARGS__);                                                 \
     if (_s != NQS_OK) return _s;                                            \
   } while (0)
 

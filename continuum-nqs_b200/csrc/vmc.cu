@@ -405,6 +405,10 @@ size_t plan_bytes(const NqsModel* m, int op, int W, int prec) {
       p.add(sizeof(int32_t) * (size_t)W);         // flip indices
       p.add(net_bytes(mc, prec, chunk_rows(JOB_VALUE, W, N, 1, kMaxRows)));
       break;
+    case NQS_OP_PER_SAMPLE_O:
+      p.add(prec == NQS_PREC_FP64 ? per_sample_O_scratch<double>(mc, W)
+                                  : per_sample_O_scratch<float>(mc, W));
+      break;
     default:
       return 0;
   }
@@ -617,8 +621,22 @@ int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, dou
 extern "C" int nqs_per_sample_O(NqsModel* m, const double* theta, const double* R,
                                 const int32_t* S, int W, void* out_O, int out_dtype, int prec,
                                 void* wsp, size_t wsb, void* stream) {
-  (void)m; (void)theta; (void)R; (void)S; (void)W; (void)out_O; (void)out_dtype; (void)prec;
-  (void)wsp; (void)wsb; (void)stream;
-  set_error("nqs_per_sample_O: reverse-mode kernels not built yet");
-  return NQS_ERR_UNSUPPORTED;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (W < 0 || (W > 0 && (!R || !S || !out_O)) || (out_dtype != 0 && out_dtype != 1))
+    return NQS_ERR_INVALID_ARG;
+  if (W == 0) return NQS_OK;
+  NQS_TRY(check_ws(m, NQS_OP_PER_SAMPLE_O, W, prec, wsb));
+  Ctx c;
+  NQS_TRY(begin(m, theta, prec, wsp, wsb, st, &c));
+  const HeadParams hp = make_head_params(m->hm.desc, c.theta64);
+  if (prec == NQS_PREC_FP64) {
+    const NetW<double> w = make_netw<double>(m->hm.desc, c.theta64, c.theta64);
+    if (out_dtype == 0)
+      return per_sample_O_run<double, double>(m->hm, w, hp, R, S, W, (double*)out_O, c.ws, st);
+    return per_sample_O_run<double, float>(m->hm, w, hp, R, S, W, (float*)out_O, c.ws, st);
+  }
+  const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  if (out_dtype == 0)
+    return per_sample_O_run<float, double>(m->hm, w, hp, R, S, W, (double*)out_O, c.ws, st);
+  return per_sample_O_run<float, float>(m->hm, w, hp, R, S, W, (float*)out_O, c.ws, st);
 }

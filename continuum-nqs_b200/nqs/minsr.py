@@ -61,3 +61,127 @@ def real_ravel(pytree):
         return {"params": out} if wrapped else out
 
     return vec, unravel
+
+
+# ---------------------------------------------------------------------------------------------
+# per-sample Jacobian and the sample-space solve (libnqs)
+# ---------------------------------------------------------------------------------------------
+def per_sample_O_rows(model, theta, R, S, dtype=torch.float64, precision="fp64"):
+    """O as the [2W][P] real matrix (rows 0..W-1 = Re O, W..2W-1 = Im O) on the device."""
+    from . import _lib
+    from .psiformer import _prec, as_batch
+    R, S, _ = as_batch(R, S)
+    W = R.shape[0]
+    P = model.n_params()
+    theta = theta.to(R.device, F64).contiguous()
+    out = torch.empty(2 * W, P, dtype=dtype, device=R.device)
+    prec = _prec(precision)
+    h = model.native().handle
+    ws, _ = _lib.workspace_for(h, _lib.OP_PER_SAMPLE_O, W, prec)
+    _lib.check(_lib.lib().nqs_per_sample_O(
+        h, _lib.ptr(theta), _lib.ptr(R), _lib.ptr(S), W, _lib.ptr(out),
+        0 if dtype == torch.float64 else 1, prec, _lib.ptr(ws), ws.numel(), _lib.stream_ptr()),
+        "nqs_per_sample_O")
+    return out
+
+
+def per_sample_O(model, theta, unravel, R, S):
+    """O[s,k] = d log Psi(x_s) / d theta_k, complex (W, P) (minsr.py:56-65)."""
+    rows = per_sample_O_rows(model, theta, R, S)
+    W = rows.shape[0] // 2
+    return torch.complex(rows[:W], rows[W:])
+
+
+def _as_rows(O):
+    """Complex (W, P) -> real [2W][P] (copy); real [2W][P] passes through."""
+    if O.is_complex():
+        return torch.cat([O.real, O.imag], 0).contiguous()
+    return O
+
+
+_GRAM = {"fp64": 0, "bf16": 1, "tf32": 2}
+
+
+def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True):
+    """Sample-space natural gradient on the device. O_rows is [2W][P] (f64 or f32; a float64
+    O_rows is centred in place by the float64 Gram). Returns dtheta (P,) and updates theta in
+    place by -lr dtheta when given."""
+    from . import _lib
+    _lib.require_cuda()
+    dev = O_rows.device
+    n, P = O_rows.shape
+    W = n // 2
+    eps = torch.as_tensor(eps).to(dev, torch.complex128).contiguous()
+    od = 0 if O_rows.dtype == torch.float64 else 1
+    g = _GRAM[gram]
+    nb = ctypes_size(W, P, od, g)
+    ws = _lib.workspace.get(nb)
+    d = torch.empty(P, dtype=F64, device=dev) if want_direction else None
+    _lib.check(_lib.lib().nqs_minsr_direction(
+        _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, _lib.ptr(d), _lib.ptr(theta),
+        float(lr), None, _lib.ptr(ws), ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
+    return d
+
+
+def ctypes_size(W, P, od, g):
+    import ctypes
+    from . import _lib
+    n = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().nqs_minsr_workspace_size(W, P, od, g, ctypes.byref(n)),
+               "nqs_minsr_workspace_size")
+    return n.value
+
+
+def minsr_direction(O, eps, lam, gram="fp64"):
+    """Natural-gradient direction via the SAMPLE-space (2W x 2W) solve (minsr.py:76-81).
+    O: complex (W, P) or real [2W][P]; the input is not modified."""
+    rows = _as_rows(O)
+    if rows is O:
+        rows = rows.clone()
+    return minsr_step(rows, eps, lam, gram)
+
+
+def gram_solve(A, rhs, lam):
+    """x = (A A^T + lam I)^-1 rhs for a float64 row-major A (M x K) on the device, with the
+    library's float64 Gram and Cholesky (nqs_gram_solve)."""
+    from . import _lib
+    A = A.to(F64).contiguous()
+    M, K = A.shape
+    rhs = rhs.to(A.device, F64).contiguous()
+    x = torch.empty(M, dtype=F64, device=A.device)
+    import ctypes
+    n = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().nqs_gram_solve_workspace_size(M, K, ctypes.byref(n)),
+               "nqs_gram_solve_workspace_size")
+    ws = _lib.workspace.get(n.value)
+    _lib.check(_lib.lib().nqs_gram_solve(_lib.ptr(A), M, K, float(lam), _lib.ptr(rhs), _lib.ptr(x),
+                                         _lib.ptr(ws), ws.numel(), _lib.stream_ptr()),
+               "nqs_gram_solve")
+    return x
+
+
+def paramsr_direction(O, eps, lam):
+    """The same direction via the explicit PARAMETER-space (P x P) solve (minsr.py:84-88):
+    (Otil^T Otil + lam I)^-1 Otil^T etil, with Otil^T as the Gram operand (test-sized P)."""
+    rows = _as_rows(O).to(F64)
+    W = rows.shape[0] // 2
+    Ot = torch.cat([rows[:W] - rows[:W].mean(0, keepdim=True),
+                    rows[W:] - rows[W:].mean(0, keepdim=True)], 0)
+    eps = torch.as_tensor(eps).to(rows.device, torch.complex128)
+    ec = eps - eps.mean()
+    et = torch.cat([ec.real, ec.imag])
+    At = Ot.T.contiguous()
+    return gram_solve(At, At @ et, lam)
+
+
+def clip_energies(e, clip_k):
+    """median-MAD clip of Re e (minsr.py:145-148) and the energy statistics, on the device.
+    Returns (e_clip complex (W,), stats f64[5] = mean, err, var, median, mad)."""
+    from . import _lib
+    e = torch.as_tensor(e).to(torch.complex128).contiguous()
+    out = torch.empty_like(e)
+    stats = torch.empty(5, dtype=F64, device=e.device)
+    _lib.check(_lib.lib().nqs_clip_energies(_lib.ptr(e), e.shape[0], float(clip_k), _lib.ptr(out),
+                                            _lib.ptr(stats), _lib.stream_ptr()),
+               "nqs_clip_energies")
+    return out, stats

@@ -153,6 +153,34 @@ int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, cons
                      int n_walkers, void* out_O, int out_dtype, int precision,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* MinSR direction (src/nqs/minsr.py:68-81): O is the [2W][P] output of nqs_per_sample_O
+ * (o_dtype 0 = f64, 1 = f32), eps complex[W] the (clipped) local energies.
+ *   Otil = O - column mean (per half), etil = [Re; Im](eps - mean eps),
+ *   T = Otil Otil^T, (T + lam I) = L L^T (float64 Cholesky), y = (T + lam I)^-1 etil,
+ *   dtheta = Otil^T y;  out_dtheta (nullable) receives dtheta, theta_io (nullable) is updated
+ *   theta -= lr dtheta in the same pass.
+ * gram_prec: 0 = float64 SIMT Gram (a float64 O is centred IN PLACE), 1 = BF16 tcgen05 Gram,
+ * 2 = TF32 tcgen05 Gram (both float32 accumulation). status_dev (nullable, device int) is set
+ * non-zero when a Cholesky pivot was not positive. */
+int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int gram_prec,
+                             size_t* bytes);
+int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
+                        int64_t n_params, double lam, int gram_prec, double* out_dtheta,
+                        double* theta_io, double lr, int* status_dev, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* x = (A A^T + lam I)^-1 rhs for a float64 row-major A [M][K] (float64 Gram + Cholesky); used
+ * for the explicit parameter-space SR of src/nqs/minsr.py:84-88 (A = Otil^T). */
+int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes);
+int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* rhs, double* x,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Median-MAD clip of Re e (src/nqs/minsr.py:145-148): med = median(Re e),
+ * mad = median(|Re e - med|) + 1e-12, Re e clipped to med +- clip_k mad, Im kept.
+ * stats (nullable, f64[5]): mean Re e, std(Re e)/sqrt(W), var(Re e), med, mad. W <= 16384. */
+int nqs_clip_energies(const double* e, int n_walkers, double clip_k, double* out_eclip,
+                      double* stats, void* stream);
+
 /* Ewald (src/nqs/ewald.py:26-73): eta = ewald_alpha, or sqrt(pi/area) when ewald_alpha <= 0. */
 int nqs_ewald_create(const double A[4], double alpha, double ewald_alpha, int n_real,
                      int n_recip, NqsEwald** out);

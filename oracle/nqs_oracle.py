@@ -300,7 +300,7 @@ class Ewald:
 # ----------------------------------------------------------------------------------------------
 def wrap(R, A):
     """sampler.py:30-31 — mod(r A^-T, 1) A^T."""
-    At = _t(A)
+    At = _t(cell_matrix(A))
     Ainv = torch.linalg.inv(At)
     return torch.remainder(R @ Ainv.T, 1.0) @ At.T
 
