@@ -421,11 +421,18 @@ def paramsr_direction(O, eps, lam):
     return torch.linalg.solve(Otil.T @ Otil + lam * torch.eye(P, dtype=F64), Otil.T @ etil)
 
 
+def _median(x):
+    """jnp.median: midpoint of the two middle order statistics for an even count."""
+    v, _ = torch.sort(x)
+    n = v.numel()
+    return v[n // 2] if n % 2 == 1 else 0.5 * (v[n // 2 - 1] + v[n // 2])
+
+
 def clip_energies(e, clip_k):
     """minsr.py:145-148 — median-MAD clip of Re e (gradient only); Im kept."""
     e_re = e.real
-    med = torch.median(e_re) if e_re.numel() % 2 == 1 else torch.quantile(e_re, 0.5)
-    mad = (torch.quantile(torch.abs(e_re - med), 0.5)) + 1e-12
+    med = _median(e_re)
+    mad = _median(torch.abs(e_re - med)) + 1e-12
     return torch.clamp(e_re, med - clip_k * mad, med + clip_k * mad) + 1j * e.imag
 
 
