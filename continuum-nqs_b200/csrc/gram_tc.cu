@@ -1,19 +1,363 @@
-// gram_tc.cu — tensor-core (tcgen05) Gram of the centred per-sample Jacobian.
+// gram_tc.cu — tensor-core Gram T = Otil Otil^T (lower triangle) on sm_100a.
+//
+// Otil (2W x P) is the centred per-sample Jacobian converted to BF16 (kind::f16) or kept in
+// float32 (kind::tf32). One CTA computes one 128 x 256 tile of T:
+//   * warp 0 / lane 0 issues TMA loads (128B-swizzled 128-row x 128-byte boxes, no multicast)
+//     into a 4-stage shared-memory ring guarded by mbarriers;
+//   * warp 1 / lane 0 issues tcgen05.mma (M=128, N=256, K=16 BF16 or K=8 TF32) with the
+//     accumulator in tensor memory (256 float32 columns), and tcgen05.commit frees each stage;
+//   * all 4 warps drain TMEM with tcgen05.ld (32 lanes x 16 columns per load) and write the
+//     lower-triangular part of the tile to T in float64.
+// Every wait is bounded: on time-out the CTA records an error flag, stops issuing, drains what
+// it issued (bounded) and frees its tensor memory.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cstdio>
+#include <algorithm>
+
 #include "minsr.cuh"
 
 namespace nqs {
+namespace tc {
+
+constexpr int BM = 128, BN = 256, STAGES = 4;
+constexpr int ROW_BYTES = 128;                  // one 128B swizzle atom row per tile row
+constexpr int A_BYTES = BM * ROW_BYTES;         // 16 KB
+constexpr int B_BYTES = BN * ROW_BYTES;         // 32 KB
+constexpr int SMEM_BYTES = STAGES * (A_BYTES + B_BYTES) + 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false (and raises the CTA abort flag) when the limit runs out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 255u) == 255u && *abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// shared-memory matrix descriptor: K-major operand, 128B swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t make_desc(const void* p) {
+  const uint64_t start = (smem_u32(p) & 0x3FFFFu) >> 4;
+  return start | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+template <int KIND>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                    uint32_t acc) {
+  if constexpr (KIND == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+  }
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// instruction descriptor: D f32, A/B format (1 = BF16, 2 = TF32), both K-major, M=128, N=256
+template <int KIND>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | ((KIND == 0 ? 1u : 2u) << 7) | ((KIND == 0 ? 1u : 2u) << 10) |
+         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+// lower-triangular tile enumeration over 128-row x 256-col tiles: row tile ti needs col tiles
+// 0 .. floor(ti/2)
+__device__ __forceinline__ void tile_coords(int t, int* ti, int* tj) {
+  int i = 0, base = 0;
+  while (base + (i / 2 + 1) <= t) {
+    base += i / 2 + 1;
+    ++i;
+  }
+  *ti = i;
+  *tj = t - base;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUtensorMap tmap,
+                                                    int M, int64_t K, double* __restrict__ T,
+                                                    int64_t ldt, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~(uintptr_t)1023);
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + STAGES * A_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int ti, tj;
+  tile_coords(blockIdx.x, &ti, &tj);
+  const int i0 = ti * BM, j0 = tj * BN;
+  constexpr int KE = (KIND == 0) ? 64 : 32;  // elements per 128-byte row
+  const int nk = (int)((K + KE - 1) / KE);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort)) break;
+      mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
+      tma_load_2d(sA + s * A_BYTES, &tmap, kb * KE, i0, &full[s]);
+      tma_load_2d(sB + s * B_BYTES, &tmap, kb * KE, j0, &full[s]);
+      tma_load_2d(sB + s * B_BYTES + A_BYTES, &tmap, kb * KE, j0 + BM, &full[s]);
+      issued = kb + 1;
+    }
+    // drain: every issued stage's loads must have landed before the CTA may exit
+    for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
+      mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t id = idesc<KIND>();
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(&full[s], (kb / STAGES) & 1, abort)) break;
+      fence_after();
+      const uint8_t* a = sA + s * A_BYTES;
+      const uint8_t* b = sB + s * B_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes = one 128-byte row of K
+        mma<KIND>(tmem, make_desc(a + kk * 32), make_desc(b + kk * 32), id,
+                  (kb | kk) != 0 ? 1u : 0u);
+      mma_commit(&empty[s]);
+    }
+    mma_commit(done);  // tracks every MMA issued above, also on abort
+  }
+  // ---------------- epilogue (all 4 warps) ----------------
+  __syncwarp();
+  const bool ok = mbar_wait(done, 0, abort);
+  fence_after();
+  const bool go = __all_sync(0xffffffffu, ok && !*abort);  // tcgen05.ld is warp-collective
+  if (go) {
+    const int row = i0 + warp * 32 + lane;
+    const int wrow_max = i0 + warp * 32 + 31;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      if (j0 + c0 > wrow_max) break;  // warp-uniform: no column of this chunk is on/below diag
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+          "%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+            "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int col = j0 + c0 + q;
+          if (col <= row && col < M) T[(size_t)row * ldt + col] = (double)__uint_as_float(r[q]);
+        }
+      }
+    }
+  }
+  if (*abort && threadIdx.x == 0) atomicExch(err, 1);
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
+// centre and convert: D[r][p] = O[r][p] - mu[half][p] (p < P), zero padding up to ldd
+template <typename TO, typename TD>
+__global__ void k_center_cvt(const TO* __restrict__ O, int W, int64_t P, int64_t ldd,
+                             const double* __restrict__ mu, TD* __restrict__ D) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (p >= ldd) return;
+  const int half = r >= W;
+  double v = 0.0;
+  if (p < P) v = (double)O[(size_t)r * P + p] - mu[(size_t)half * P + p];
+  if constexpr (sizeof(TD) == 2)
+    D[(size_t)r * ldd + p] = __double2bfloat16(v);
+  else
+    D[(size_t)r * ldd + p] = (TD)v;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace tc
+
+static int64_t tc_ld(int64_t P, int prec) {
+  const int64_t a = prec == 1 ? 8 : 4;  // 16-byte row stride
+  return (P + a - 1) / a * a;
+}
 
 size_t gram_tc_workspace(int W, int64_t P, int prec) {
-  (void)W; (void)P; (void)prec;
-  return 0;
+  const size_t es = prec == 1 ? 2 : 4;
+  return (size_t)2 * W * tc_ld(P, prec) * es + 1024;
+}
+
+// Encode the tensor map and launch the Gram on an operand already in D (rows M, ld ldd).
+int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, double* T, int64_t ldt,
+                   int* err, cudaStream_t st) {
+  tc::EncodeTiledFn enc = tc::encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return NQS_ERR_CUDA;
+  }
+  const size_t es = prec == 1 ? 2 : 4;
+  if ((reinterpret_cast<uintptr_t>(D) & 15) || ((ldd * es) & 15)) {
+    set_error("gram_tc: operand not 16-byte aligned");
+    return NQS_ERR_INVALID_ARG;
+  }
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)M};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ldd * es)};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)tc::BM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(&map, prec == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, const_cast<void*>(D), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return NQS_ERR_CUDA;
+  }
+  const int nrt = (M + tc::BM - 1) / tc::BM;
+  int tiles = 0;
+  for (int i = 0; i < nrt; ++i) tiles += i / 2 + 1;
+  // every column tile must start inside the matrix: col tile tj <= floor(ti/2) => j0 <= i0
+  if (prec == 1) {
+    cudaFuncSetAttribute(tc::k_gram_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::SMEM_BYTES);
+    tc::k_gram_tc<0><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err);
+  } else {
+    cudaFuncSetAttribute(tc::k_gram_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::SMEM_BYTES);
+    tc::k_gram_tc<1><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err);
+  }
+  NQS_CHECK_LAUNCH("k_gram_tc");
+  return NQS_OK;
 }
 
 int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int prec, double* T,
-            Arena& ws, int nsm, cudaStream_t st) {
-  (void)O; (void)o_dtype; (void)mu; (void)W; (void)P; (void)prec; (void)T; (void)ws; (void)nsm;
-  (void)st;
-  set_error("tensor-core Gram not built yet");
-  return NQS_ERR_UNSUPPORTED;
+            Arena& ws, int nsm, cudaStream_t st, int* err) {
+  (void)nsm;
+  const int64_t ldd = tc_ld(P, prec);
+  const int M = 2 * W;
+  const dim3 g((unsigned)((ldd + 255) / 256), (unsigned)M);
+  void* D;
+  if (prec == 1) {
+    __nv_bfloat16* d = ws.take<__nv_bfloat16>((size_t)M * ldd);
+    if (!d) return NQS_ERR_WORKSPACE;
+    if (o_dtype == 0)
+      tc::k_center_cvt<double, __nv_bfloat16><<<g, 256, 0, st>>>((const double*)O, W, P, ldd, mu, d);
+    else
+      tc::k_center_cvt<float, __nv_bfloat16><<<g, 256, 0, st>>>((const float*)O, W, P, ldd, mu, d);
+    D = d;
+  } else {
+    float* d = ws.take<float>((size_t)M * ldd);
+    if (!d) return NQS_ERR_WORKSPACE;
+    if (o_dtype == 0)
+      tc::k_center_cvt<double, float><<<g, 256, 0, st>>>((const double*)O, W, P, ldd, mu, d);
+    else
+      tc::k_center_cvt<float, float><<<g, 256, 0, st>>>((const float*)O, W, P, ldd, mu, d);
+    D = d;
+  }
+  NQS_CHECK_LAUNCH("k_center_cvt");
+  return gram_tc_launch(D, prec, M, P, ldd, T, M, err, st);
 }
 
 }  // namespace nqs
+
+extern "C" int nqs_gram(const void* A, int a_dtype, int M, int64_t K, int64_t lda, double* T,
+                        int64_t ldt, int* err_dev, void* stream) {
+  using namespace nqs;
+  if (!A || !T || M < 1 || K < 1 || lda < K || ldt < M || (a_dtype != 1 && a_dtype != 2)) {
+    set_error("nqs_gram: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  return gram_tc_launch(A, a_dtype, M, K, lda, T, ldt, err_dev, (cudaStream_t)stream);
+}

@@ -403,27 +403,81 @@ __global__ void __launch_bounds__(1024) k_trsv_lower_t(const double* __restrict_
   }
 }
 
-// dtheta[p] = sum_r Otil[r][p] y[r] with Otil = O - mu (centred on the fly);
-// theta[p] -= lr dtheta[p] when theta != nullptr
+// out[k] = sum_m (O[m][k] - mu[m >= Mh][k]) x[m]   (mu nullable); theta[k] -= lr out[k] if theta
 template <typename TO>
-__global__ void k_pushthrough(const TO* __restrict__ O, int W, int64_t P,
-                              const double* __restrict__ mu, const double* __restrict__ y,
-                              double* __restrict__ dtheta, double* __restrict__ theta, double lr) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  double s0 = 0, s1 = 0;
-  const double m0 = mu[p], m1 = mu[P + p];
-  double ys0 = 0, ys1 = 0;
-  for (int w = 0; w < W; ++w) {
-    const double yr = y[w], yi = y[W + w];
-    s0 = fma((double)O[(size_t)w * P + p], yr, s0);
-    s1 = fma((double)O[((size_t)W + w) * P + p], yi, s1);
-    ys0 += yr;
-    ys1 += yi;
+__global__ void k_gemv_t(const TO* __restrict__ O, int M, int Mh, int64_t K,
+                         const double* __restrict__ mu, const double* __restrict__ x,
+                         double* __restrict__ out, double* __restrict__ theta, double lr) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double s0 = 0, s1 = 0, xs0 = 0, xs1 = 0;
+  for (int m = 0; m < Mh; ++m) {
+    s0 = fma((double)O[(size_t)m * K + k], x[m], s0);
+    xs0 += x[m];
   }
-  const double d = (s0 - m0 * ys0) + (s1 - m1 * ys1);
-  if (dtheta) dtheta[p] = d;
-  if (theta) theta[p] -= lr * d;
+  for (int m = Mh; m < M; ++m) {
+    s1 = fma((double)O[(size_t)m * K + k], x[m], s1);
+    xs1 += x[m];
+  }
+  double d = s0 + s1;
+  if (mu) d -= mu[k] * xs0 + mu[K + k] * xs1;
+  if (out) out[k] = d;
+  if (theta) theta[k] -= lr * d;
+}
+
+// r[m] = b[m] - lam x[m] - sum_k (O[m][k] - mu[m >= Mh][k]) v[k]   (one CTA per row)
+template <typename TO>
+__global__ void __launch_bounds__(256) k_gemv_n_resid(const TO* __restrict__ O, int M, int Mh,
+                                                      int64_t K, const double* __restrict__ mu,
+                                                      const double* __restrict__ v,
+                                                      const double* __restrict__ b, double lam,
+                                                      const double* __restrict__ x,
+                                                      double* __restrict__ r) {
+  const int m = blockIdx.x;
+  const TO* row = O + (size_t)m * K;
+  const double* mr = mu ? mu + (m >= Mh ? K : 0) : nullptr;
+  double s = 0;
+  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+    const double o = (double)row[k] - (mr ? mr[k] : 0.0);
+    s = fma(o, v[k], s);
+  }
+  __shared__ double red[32];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    r[m] = b[m] - lam * x[m] - t;
+  }
+}
+
+__global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a[i];
+}
+
+// Solve (A A^T + lam I) y = b given the Cholesky factor L of (A A^T + lam I), with n_refine
+// steps of iterative refinement against the exact operator y -> A (A^T y) + lam y, where
+// A = O - mu (centred on the fly). On return tmpK holds A^T y.
+template <typename TO>
+static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
+                         const double* mu, double lam, const double* b, double* y, double* r,
+                         double* tmpK, int n_refine, cudaStream_t st) {
+  cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
+  k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, y);
+  k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, y);
+  NQS_CHECK_LAUNCH("cholesky solve");
+  const unsigned gk = (unsigned)((K + 255) / 256);
+  for (int it = 0; it < n_refine; ++it) {
+    k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, nullptr, 0.0);
+    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, b, lam, y, r);
+    k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, r);
+    k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, r);
+    k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
+    NQS_CHECK_LAUNCH("refinement");
+  }
+  return NQS_OK;
 }
 
 // ============================================================================================
@@ -467,7 +521,9 @@ __global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W
   bitonic_sort(sa, n2);
   const double mad = median_sorted(sa, W) + 1e-12;
   __syncthreads();
-  const double lo = med - clip_k * mad, hi = med + clip_k * mad;
+  // two roundings, as the reference's `med - clip_k * mad` (no fused multiply-add)
+  const double kmad = __dmul_rn(clip_k, mad);
+  const double lo = __dsub_rn(med, kmad), hi = __dadd_rn(med, kmad);
   for (int i = threadIdx.x; i < W; i += blockDim.x) {
     const double r = e[i].re;
     out[i] = mk(fmin(fmax(r, lo), hi), e[i].im);
@@ -542,11 +598,11 @@ int nqs_minsr_workspace_size(int W, int64_t P, int o_dtype, int gram_prec, size_
 }
 
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t P, double lam,
-                        int gram_prec, double* out_dtheta, double* theta_io, double lr,
-                        int* status_dev, void* wsp, size_t wsb, void* stream) {
+                        int gram_prec, int n_refine, double* out_dtheta, double* theta_io,
+                        double lr, int* status_dev, void* wsp, size_t wsb, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   if (!O || !eps || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || gram_prec < 0 ||
-      gram_prec > 2 || (!out_dtheta && !theta_io)) {
+      gram_prec > 2 || n_refine < 0 || n_refine > 8 || (!out_dtheta && !theta_io)) {
     set_error("nqs_minsr_direction: invalid argument");
     return NQS_ERR_INVALID_ARG;
   }
@@ -558,11 +614,15 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   Arena ws{(char*)wsp, wsb, 0};
   const int n = 2 * W;
   double* mu = ws.take<double>(2 * P);
+  double* et = ws.take<double>(n);
   double* y = ws.take<double>(n);
+  double* r = ws.take<double>(n);
+  double* tmpK = ws.take<double>(P);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
   const size_t part_elems = minsr_part_elems(W);
   double* part = ws.take<double>(part_elems);
+  if (!part) return NQS_ERR_WORKSPACE;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -573,9 +633,12 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   else
     k_colmean<float><<<cg, 256, 0, st>>>((const float*)O, W, P, mu);
   NQS_CHECK_LAUNCH("k_colmean");
-  k_center_eps<<<1, 1024, 0, st>>>((const cplx*)eps, W, y);
+  k_center_eps<<<1, 1024, 0, st>>>((const cplx*)eps, W, et);
   NQS_CHECK_LAUNCH("k_center_eps");
   const dim3 ce((unsigned)((P + 255) / 256), (unsigned)n);
+  const void* Oop = O;        // operand of the refinement / push-through
+  int op_dtype = o_dtype;
+  const double* mu_op = mu;
   if (gram_prec == 0) {
     double* Ot;
     if (o_dtype == 0) {  // centre in place
@@ -583,38 +646,43 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
       Ot = (double*)O;
     } else {
       Ot = ws.take<double>((size_t)n * P);
+      if (!Ot) return NQS_ERR_WORKSPACE;
       k_center<float, double><<<ce, 256, 0, st>>>((const float*)O, W, P, mu, Ot, P);
     }
     NQS_CHECK_LAUNCH("k_center");
     NQS_TRY(dsyrk_lower(Ot, P, n, P, 1.0, 0.0, T, n, part, part_elems, nsm, st));
-    // mu is now zero for the push-through of an in-place centred float64 O
-    if (o_dtype == 0) cudaMemsetAsync(mu, 0, sizeof(double) * 2 * P, st);
+    Oop = Ot;
+    op_dtype = 0;
+    mu_op = nullptr;
   } else {
-    NQS_TRY(gram_tc(O, o_dtype, mu, W, P, gram_prec, T, ws, nsm, st));
+    NQS_TRY(gram_tc(O, o_dtype, mu, W, P, gram_prec, T, ws, nsm, st, bad + 1));
   }
   k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st));
-  k_trsv_lower<<<1, 1024, 0, st>>>(T, n, n, y);
-  NQS_CHECK_LAUNCH("k_trsv_lower");
-  k_trsv_lower_t<<<1, 1024, 0, st>>>(T, n, n, y);
-  NQS_CHECK_LAUNCH("k_trsv_lower_t");
-  const unsigned gp = (unsigned)((P + 255) / 256);
-  if (o_dtype == 0)
-    k_pushthrough<double><<<gp, 256, 0, st>>>((const double*)O, W, P, mu, y, out_dtheta, theta_io,
-                                              lr);
+  if (op_dtype == 0)
+    NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, tmpK,
+                                  n_refine, st));
   else
-    k_pushthrough<float><<<gp, 256, 0, st>>>((const float*)O, W, P, mu, y, out_dtheta, theta_io,
-                                             lr);
-  NQS_CHECK_LAUNCH("k_pushthrough");
-  if (status_dev) cudaMemcpyAsync(status_dev, bad, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, tmpK,
+                                 n_refine, st));
+  const unsigned gp = (unsigned)((P + 255) / 256);
+  if (op_dtype == 0)
+    k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)Oop, n, W, P, mu_op, y, out_dtheta,
+                                         theta_io, lr);
+  else
+    k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)Oop, n, W, P, mu_op, y, out_dtheta,
+                                        theta_io, lr);
+  NQS_CHECK_LAUNCH("k_gemv_t");
+  if (status_dev) cudaMemcpyAsync(status_dev, bad, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return NQS_OK;
 }
 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
-  *bytes = sizeof(double) * (m * m + m + std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 4096;
+  *bytes = sizeof(double) * (m * m + 2 * m + (size_t)K + std::min<size_t>(16 * m * m, (size_t)8 << 20)) +
+           8192;
   return NQS_OK;
 }
 
@@ -627,6 +695,8 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   if (wsb < need) return NQS_ERR_WORKSPACE;
   Arena ws{(char*)wsp, wsb, 0};
   double* T = ws.take<double>((size_t)M * M);
+  double* r = ws.take<double>(M);
+  double* tmpK = ws.take<double>(K);
   const size_t pe = std::min<size_t>(16 * (size_t)M * M, (size_t)8 << 20);
   double* part = ws.take<double>(pe);
   int* bad = ws.take<int>(4);
@@ -638,9 +708,7 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   NQS_TRY(dsyrk_lower(A, K, M, K, 1.0, 0.0, T, M, part, pe, nsm, st));
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
-  cudaMemcpyAsync(x, rhs, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
-  k_trsv_lower<<<1, 1024, 0, st>>>(T, M, M, x);
-  k_trsv_lower_t<<<1, 1024, 0, st>>>(T, M, M, x);
+  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, 2, st));
   NQS_CHECK_LAUNCH("nqs_gram_solve");
   return NQS_OK;
 }

@@ -13,6 +13,8 @@ int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, do
 // O - mu converted to the operand type of `prec` (1 = BF16, 2 = TF32), float32 accumulation.
 size_t gram_tc_workspace(int W, int64_t P, int prec);
 int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int prec, double* T,
-            Arena& ws, int nsm, cudaStream_t st);
+            Arena& ws, int nsm, cudaStream_t st, int* err);
+int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, double* T, int64_t ldt,
+                   int* err, cudaStream_t st);
 
 }  // namespace nqs

@@ -89,12 +89,13 @@ __global__ void k_propose_pos(McArgs a, const double* __restrict__ R, double* __
     n0 = rad * c;
     n1 = rad * s;
   }
-  const double x = R[(size_t)idx * 2] + a.step * n0;
-  const double y = R[(size_t)idx * 2 + 1] + a.step * n1;
-  const double f0 = jmod1(x * a.Ainv[0] + y * a.Ainv[1]);
-  const double f1 = jmod1(x * a.Ainv[2] + y * a.Ainv[3]);
-  Rp[(size_t)idx * 2] = f0 * a.A[0] + f1 * a.A[1];
-  Rp[(size_t)idx * 2 + 1] = f0 * a.A[2] + f1 * a.A[3];
+  // R + step*N(0,1), wrapped: mod(r A^-T, 1) A^T, every product rounded separately (no FMA)
+  const double x = __dadd_rn(R[(size_t)idx * 2], __dmul_rn(a.step, n0));
+  const double y = __dadd_rn(R[(size_t)idx * 2 + 1], __dmul_rn(a.step, n1));
+  const double f0 = jmod1(__dadd_rn(__dmul_rn(x, a.Ainv[0]), __dmul_rn(y, a.Ainv[1])));
+  const double f1 = jmod1(__dadd_rn(__dmul_rn(x, a.Ainv[2]), __dmul_rn(y, a.Ainv[3])));
+  Rp[(size_t)idx * 2] = __dadd_rn(__dmul_rn(f0, a.A[0]), __dmul_rn(f1, a.A[1]));
+  Rp[(size_t)idx * 2 + 1] = __dadd_rn(__dmul_rn(f0, a.A[2]), __dmul_rn(f1, a.A[3]));
 }
 
 __device__ __forceinline__ bool mh_accept(double d, double u) {
@@ -106,7 +107,7 @@ __global__ void k_accept_pos(McArgs a, double* __restrict__ R, const double* __r
                              double* __restrict__ acc_pos, double* __restrict__ out_d) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= a.W) return;
-  const double d = 2.0 * Lp[w].re - 2.0 * Lc[w].re;
+  const double d = __dsub_rn(2.0 * Lp[w].re, 2.0 * Lc[w].re);
   double u;
   if (a.inj_u_pos) {
     u = a.inj_u_pos[(size_t)a.s * a.W + w];
@@ -142,7 +143,7 @@ __global__ void k_accept_flip(McArgs a, int j, int32_t* __restrict__ S,
                               double* __restrict__ out_d) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= a.W) return;
-  const double d = 2.0 * Lp[w].re - 2.0 * Lc[w].re;
+  const double d = __dsub_rn(2.0 * Lp[w].re, 2.0 * Lc[w].re);
   double u;
   if (a.inj_u_flip) {
     u = a.inj_u_flip[((size_t)a.s * a.n_flips + j) * a.W + w];

@@ -102,7 +102,8 @@ def _as_rows(O):
 _GRAM = {"fp64": 0, "bf16": 1, "tf32": 2}
 
 
-def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True):
+def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True,
+               n_refine=1):
     """Sample-space natural gradient on the device. O_rows is [2W][P] (f64 or f32; a float64
     O_rows is centred in place by the float64 Gram). Returns dtheta (P,) and updates theta in
     place by -lr dtheta when given."""
@@ -118,7 +119,8 @@ def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction
     ws = _lib.workspace.get(nb)
     d = torch.empty(P, dtype=F64, device=dev) if want_direction else None
     _lib.check(_lib.lib().nqs_minsr_direction(
-        _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, _lib.ptr(d), _lib.ptr(theta),
+        _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, int(n_refine), _lib.ptr(d),
+        _lib.ptr(theta),
         float(lr), None, _lib.ptr(ws), ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
     return d
 
@@ -132,13 +134,13 @@ def ctypes_size(W, P, od, g):
     return n.value
 
 
-def minsr_direction(O, eps, lam, gram="fp64"):
+def minsr_direction(O, eps, lam, gram="fp64", n_refine=1):
     """Natural-gradient direction via the SAMPLE-space (2W x 2W) solve (minsr.py:76-81).
     O: complex (W, P) or real [2W][P]; the input is not modified."""
     rows = _as_rows(O)
     if rows is O:
         rows = rows.clone()
-    return minsr_step(rows, eps, lam, gram)
+    return minsr_step(rows, eps, lam, gram, n_refine=n_refine)
 
 
 def gram_solve(A, rhs, lam):
@@ -185,3 +187,28 @@ def clip_energies(e, clip_k):
                                             _lib.ptr(stats), _lib.stream_ptr()),
                "nqs_clip_energies")
     return out, stats
+
+
+def gram_lower(A, kind="bf16"):
+    """Lower triangle of A A^T (float64 out) on the tcgen05 tensor cores; A (M, K) float32 on
+    the device is rounded to BF16 (kind 'bf16') or read as TF32 (kind 'tf32')."""
+    from . import _lib
+    _lib.require_cuda()
+    M, K = A.shape
+    if kind == "bf16":
+        lda = (K + 7) // 8 * 8
+        Ad = torch.zeros(M, lda, dtype=torch.bfloat16, device=A.device)
+        Ad[:, :K] = A.to(torch.bfloat16)
+        code = 1
+    else:
+        lda = (K + 3) // 4 * 4
+        Ad = torch.zeros(M, lda, dtype=torch.float32, device=A.device)
+        Ad[:, :K] = A.to(torch.float32)
+        code = 2
+    T = torch.zeros(M, M, dtype=F64, device=A.device)
+    err = torch.zeros(1, dtype=torch.int32, device=A.device)
+    _lib.check(_lib.lib().nqs_gram(_lib.ptr(Ad), code, M, K, lda, _lib.ptr(T), M, _lib.ptr(err),
+                                   _lib.stream_ptr()), "nqs_gram")
+    if int(err.item()) != 0:
+        raise RuntimeError("nqs_gram: a tensor-core CTA hit its bounded-wait limit")
+    return T

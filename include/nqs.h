@@ -160,14 +160,24 @@ int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, cons
  *   dtheta = Otil^T y;  out_dtheta (nullable) receives dtheta, theta_io (nullable) is updated
  *   theta -= lr dtheta in the same pass.
  * gram_prec: 0 = float64 SIMT Gram (a float64 O is centred IN PLACE), 1 = BF16 tcgen05 Gram,
- * 2 = TF32 tcgen05 Gram (both float32 accumulation). status_dev (nullable, device int) is set
- * non-zero when a Cholesky pivot was not positive. */
+ * 2 = TF32 tcgen05 Gram (both float32 accumulation). n_refine (0..8) steps of iterative
+ * refinement of y against the exact operator Otil Otil^T + lam I (applied with O itself, never
+ * the rounded Gram). status_dev (nullable, device int) is set
+ * non-zero when a Cholesky pivot was not positive; status_dev[1] when a tensor-core Gram CTA hit
+ * its bounded-wait limit. */
 int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int gram_prec,
                              size_t* bytes);
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
-                        int64_t n_params, double lam, int gram_prec, double* out_dtheta,
+                        int64_t n_params, double lam, int gram_prec, int n_refine,
+                        double* out_dtheta,
                         double* theta_io, double lr, int* status_dev, void* workspace,
                         size_t workspace_bytes, void* stream);
+
+/* Lower triangle of T = A A^T on the tcgen05 tensor cores (float32 accumulation, float64 out):
+ * A row-major [M][lda] of BF16 (a_dtype 1) or float32 read as TF32 (a_dtype 2); lda * elem size
+ * a multiple of 16 bytes; err_dev (device int, nullable) set to 1 if a bounded wait ran out. */
+int nqs_gram(const void* A, int a_dtype, int M, int64_t K, int64_t lda, double* T, int64_t ldt,
+             int* err_dev, void* stream);
 
 /* x = (A A^T + lam I)^-1 rhs for a float64 row-major A [M][K] (float64 Gram + Cholesky); used
  * for the explicit parameter-space SR of src/nqs/minsr.py:84-88 (A = Otil^T). */
