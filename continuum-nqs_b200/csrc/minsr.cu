@@ -403,52 +403,91 @@ __global__ void __launch_bounds__(1024) k_trsv_lower_t(const double* __restrict_
   }
 }
 
-// out[k] = sum_m (O[m][k] - mu[m >= Mh][k]) x[m]   (mu nullable); theta[k] -= lr out[k] if theta
+// error-free transformations (Knuth TwoSum, FMA TwoProduct) for compensated dot products
+struct DD {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add_prod(double a, double b) {
+    const double p = a * b;
+    const double pe = fma(a, b, -p);
+    const double t = s + p;
+    const double z = t - s;
+    c += ((s - (t - z)) + (p - z)) + pe;
+    s = t;
+  }
+  __device__ __forceinline__ void add(double a) {
+    const double t = s + a;
+    const double z = t - s;
+    c += (s - (t - z)) + (a - z);
+    s = t;
+  }
+};
+
+// out[k] = sum_m (O[m][k] - mu[m >= Mh][k]) x[m]  (mu nullable), compensated; out_lo (nullable)
+// receives the low word of the double-double result; theta[k] -= lr out[k] when theta given
 template <typename TO>
 __global__ void k_gemv_t(const TO* __restrict__ O, int M, int Mh, int64_t K,
                          const double* __restrict__ mu, const double* __restrict__ x,
-                         double* __restrict__ out, double* __restrict__ theta, double lr) {
+                         double* __restrict__ out, double* __restrict__ out_lo,
+                         double* __restrict__ theta, double lr) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
-  double s0 = 0, s1 = 0, xs0 = 0, xs1 = 0;
-  for (int m = 0; m < Mh; ++m) {
-    s0 = fma((double)O[(size_t)m * K + k], x[m], s0);
-    xs0 += x[m];
+  const double m0 = mu ? mu[k] : 0.0, m1 = mu ? mu[K + k] : 0.0;
+  DD acc;
+  for (int m = 0; m < M; ++m) {
+    const double o = (double)O[(size_t)m * K + k] - (m < Mh ? m0 : m1);
+    acc.add_prod(o, x[m]);
   }
-  for (int m = Mh; m < M; ++m) {
-    s1 = fma((double)O[(size_t)m * K + k], x[m], s1);
-    xs1 += x[m];
-  }
-  double d = s0 + s1;
-  if (mu) d -= mu[k] * xs0 + mu[K + k] * xs1;
-  if (out) out[k] = d;
-  if (theta) theta[k] -= lr * d;
+  const double hi = acc.s + acc.c;
+  if (out) out[k] = hi;
+  if (out_lo) out_lo[k] = acc.c - (hi - acc.s);
+  if (theta) theta[k] -= lr * hi;
 }
 
-// r[m] = b[m] - lam x[m] - sum_k (O[m][k] - mu[m >= Mh][k]) v[k]   (one CTA per row)
+// r[m] = b[m] - lam x[m] - sum_k (O[m][k] - mu[m >= Mh][k]) (v[k] + v_lo[k]), compensated
+// (one CTA per row)
 template <typename TO>
 __global__ void __launch_bounds__(256) k_gemv_n_resid(const TO* __restrict__ O, int M, int Mh,
                                                       int64_t K, const double* __restrict__ mu,
                                                       const double* __restrict__ v,
+                                                      const double* __restrict__ v_lo,
                                                       const double* __restrict__ b, double lam,
                                                       const double* __restrict__ x,
                                                       double* __restrict__ r) {
   const int m = blockIdx.x;
   const TO* row = O + (size_t)m * K;
   const double* mr = mu ? mu + (m >= Mh ? K : 0) : nullptr;
-  double s = 0;
+  DD acc;
   for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
     const double o = (double)row[k] - (mr ? mr[k] : 0.0);
-    s = fma(o, v[k], s);
+    acc.add_prod(o, v[k]);
+    acc.add_prod(o, v_lo[k]);
   }
-  __shared__ double red[32];
-  s = warp_sum(s);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __shared__ double red_s[32], red_c[32];
+  // warp reduction of (s, c) pairs with TwoSum
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double os = __shfl_xor_sync(0xffffffffu, acc.s, off);
+    const double oc = __shfl_xor_sync(0xffffffffu, acc.c, off);
+    acc.add(os);
+    acc.c += oc;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red_s[threadIdx.x >> 5] = acc.s;
+    red_c[threadIdx.x >> 5] = acc.c;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t = 0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
-    r[m] = b[m] - lam * x[m] - t;
+    DD t;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      t.add(red_s[i]);
+      t.c += red_c[i];
+    }
+    DD q;  // b - lam x - t
+    q.add(b[m]);
+    q.add_prod(-lam, x[m]);
+    q.add(-t.s);
+    q.c -= t.c;
+    r[m] = q.s + q.c;
   }
 }
 
@@ -463,15 +502,15 @@ __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__
 template <typename TO>
 static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
                          const double* mu, double lam, const double* b, double* y, double* r,
-                         double* tmpK, int n_refine, cudaStream_t st) {
+                         double* tmpK, double* tmpK_lo, int n_refine, cudaStream_t st) {
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
   k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, y);
   k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, y);
   NQS_CHECK_LAUNCH("cholesky solve");
   const unsigned gk = (unsigned)((K + 255) / 256);
   for (int it = 0; it < n_refine; ++it) {
-    k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, nullptr, 0.0);
-    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, b, lam, y, r);
+    k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0);
+    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, y, r);
     k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, r);
     k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, r);
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
@@ -576,7 +615,10 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   size_t b = 0;
   auto add = [&](size_t x) { b += ((x + 255) / 256) * 256 + 256; };
   add(sizeof(double) * 2 * P);          // column means
-  add(sizeof(double) * n);              // etil -> y
+  add(sizeof(double) * n);              // etil
+  add(sizeof(double) * n);              // y
+  add(sizeof(double) * n);              // refinement residual
+  add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(int) * 4);                 // status
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
@@ -618,6 +660,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* y = ws.take<double>(n);
   double* r = ws.take<double>(n);
   double* tmpK = ws.take<double>(P);
+  double* tmpK_lo = ws.take<double>(P);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
   const size_t part_elems = minsr_part_elems(W);
@@ -662,17 +705,17 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st));
   if (op_dtype == 0)
     NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, tmpK,
-                                  n_refine, st));
+                                  tmpK_lo, n_refine, st));
   else
     NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, tmpK,
-                                 n_refine, st));
+                                 tmpK_lo, n_refine, st));
   const unsigned gp = (unsigned)((P + 255) / 256);
   if (op_dtype == 0)
     k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)Oop, n, W, P, mu_op, y, out_dtheta,
-                                         theta_io, lr);
+                                         nullptr, theta_io, lr);
   else
     k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)Oop, n, W, P, mu_op, y, out_dtheta,
-                                        theta_io, lr);
+                                        nullptr, theta_io, lr);
   NQS_CHECK_LAUNCH("k_gemv_t");
   if (status_dev) cudaMemcpyAsync(status_dev, bad, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return NQS_OK;
@@ -681,8 +724,8 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
-  *bytes = sizeof(double) * (m * m + 2 * m + (size_t)K + std::min<size_t>(16 * m * m, (size_t)8 << 20)) +
-           8192;
+  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K +
+                             std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 8192;
   return NQS_OK;
 }
 
@@ -697,6 +740,7 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   double* T = ws.take<double>((size_t)M * M);
   double* r = ws.take<double>(M);
   double* tmpK = ws.take<double>(K);
+  double* tmpK_lo = ws.take<double>(K);
   const size_t pe = std::min<size_t>(16 * (size_t)M * M, (size_t)8 << 20);
   double* part = ws.take<double>(pe);
   int* bad = ws.take<int>(4);
@@ -708,7 +752,7 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   NQS_TRY(dsyrk_lower(A, K, M, K, 1.0, 0.0, T, M, part, pe, nsm, st));
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
-  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, 2, st));
+  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, 3, st));
   NQS_CHECK_LAUNCH("nqs_gram_solve");
   return NQS_OK;
 }

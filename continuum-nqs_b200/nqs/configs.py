@@ -1,0 +1,63 @@
+"""The synthetic benchmark configurations of the VMC iteration.
+
+config1: N=2 electrons, r_s=2 (L = sqrt(pi N) r_s), Rashba 0.5, Zeeman 0.1; width 32, 2 blocks,
+         4 heads, 8 Fourier harmonics, K=1, no Jastrow; 256 walkers, Gaussian step 0.2 r_s,
+         10 sweeps, MinSR damping 1e-3, lr 0.05; flax-default initialisation, zero backflow.
+config2: N=16, r_s=5, Rashba 0.3, Zeeman 0.05; width 64, 4 blocks, 4 heads, 8 harmonics, K=4,
+         RBF pair Jastrow with 16 centres; Bloch envelopes of the non-interacting Rashba orbitals
+         (twist (0.1, 0.17), where the closed shell has a gap); Dense kernels ~N(0, 0.02^2),
+         backflow ~N(0, 1e-3^2), Jastrow ~N(0, 0.02^2); 4096 walkers; step 0.2 r_s; 10 sweeps.
+Both: Coulomb coupling 1 through the 2D Ewald sum with eta = 5/L, 7x7 real-space images
+(n_real = 3) and the |m| <= 8 reciprocal index box; 2 spin-flip proposals per sweep.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+from . import rashba
+from .psiformer import ContinuumSpinorPsiformer
+
+
+@dataclass
+class VMCSetup:
+    name: str
+    N: int
+    L: float
+    lambda_r: float
+    h_z: float
+    n_walkers: int
+    n_sweeps: int
+    step: float
+    lam: float
+    lr: float
+    ewald_eta: float
+    n_real: int = 3
+    n_recip: int = 8
+    E_gs: float = 0.0
+
+
+def config(n: int, n_walkers: int | None = None):
+    """(model, params, setup) of configuration n (1 or 2)."""
+    if n == 1:
+        N, rs, lr_soc, hz = 2, 2.0, 0.5, 0.1
+        L = math.sqrt(math.pi * N) * rs
+        env = rashba.cell_rashba_envelope(L, N, 1.0, lr_soc, hz, 10, (0.0, 0.0))
+        model = ContinuumSpinorPsiformer(N, env["Gs"], env["W"], L, embed_dim=32, depth=2,
+                                         n_heads=4, n_freq=8, n_dets=1)
+        params = model.init(0)
+        W = 256
+    elif n == 2:
+        N, rs, lr_soc, hz = 16, 5.0, 0.3, 0.05
+        L = math.sqrt(math.pi * N) * rs
+        env = rashba.cell_rashba_envelope(L, N, 1.0, lr_soc, hz, 10, (0.1, 0.17))
+        model = ContinuumSpinorPsiformer(N, env["Gs"], env["W"], L, embed_dim=64, depth=4,
+                                         n_heads=4, n_freq=8, n_dets=4, use_jastrow=True,
+                                         n_knots=16)
+        params = model.init_normal(0, std=0.02, backflow_std=1e-3, jastrow_std=0.02)
+        W = 4096
+    else:
+        raise ValueError(f"unknown configuration {n}")
+    setup = VMCSetup(f"config{n}", N, L, lr_soc, hz, n_walkers or W, 10, 0.2 * rs, 1e-3, 0.05,
+                     5.0 / L, E_gs=env["E_gs"])
+    return model, params, setup

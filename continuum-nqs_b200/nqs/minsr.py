@@ -134,7 +134,7 @@ def ctypes_size(W, P, od, g):
     return n.value
 
 
-def minsr_direction(O, eps, lam, gram="fp64", n_refine=1):
+def minsr_direction(O, eps, lam, gram="fp64", n_refine=2):
     """Natural-gradient direction via the SAMPLE-space (2W x 2W) solve (minsr.py:76-81).
     O: complex (W, P) or real [2W][P]; the input is not modified."""
     rows = _as_rows(O)
@@ -212,3 +212,143 @@ def gram_lower(A, kind="bf16"):
     if int(err.item()) != 0:
         raise RuntimeError("nqs_gram: a tensor-core CTA hit its bounded-wait limit")
     return T
+
+
+# ---------------------------------------------------------------------------------------------
+# the VMC iteration and the MinSR training loop (minsr.py:92-159)
+# ---------------------------------------------------------------------------------------------
+class VMCIteration:
+    """Device-resident state of one VMC run: theta, walkers, and the buffers of one iteration.
+
+    step() = n_sweeps Metropolis sweeps (nqs_mcmc_sweeps) -> local energies with the Ewald term
+    fused (nqs_local_energy) -> per-sample Jacobian (nqs_per_sample_O) -> median-MAD clip
+    (nqs_clip_energies) -> MinSR direction with the update theta -= lr dtheta fused
+    (nqs_minsr_direction). No host synchronisation happens inside step().
+
+    precision "fp64": every stage float64 (float64 O, float64 Gram).
+    precision "mixed": float32 network, float32 O, BF16 tcgen05 Gram ("gram" may override:
+    "bf16" or "tf32"); determinants, energies, Cholesky and solves stay float64."""
+
+    def __init__(self, model, theta, R, S, *, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
+                 lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, clip_k=5.0, n_spin_flips=2,
+                 seed=0, counter=0, precision="fp64", gram=None, n_refine=1):
+        from . import _lib
+        from .psiformer import _prec, as_batch
+        _lib.require_cuda()
+        self.model = model
+        self.theta = theta.to(_lib.device(), F64).contiguous().clone()
+        self.R, self.S, _ = as_batch(R, S)
+        self.R, self.S = self.R.clone(), self.S.clone()
+        self.W, self.N = self.S.shape
+        self.P = model.n_params()
+        self.m_star, self.lambda_r, self.h_z = float(m_star), float(lambda_r), float(h_z)
+        self.ewald = None
+        if coulomb is not None:
+            if not hasattr(coulomb, "ewald"):
+                raise NotImplementedError("coulomb must come from nqs.ewald.make_ewald")
+            self.ewald = coulomb.ewald
+        self.lr, self.lam, self.clip_k = float(lr), float(lam), float(clip_k)
+        self.n_sweeps, self.step_size, self.n_flips = int(n_sweeps), float(step_size), n_spin_flips
+        self.seed, self.counter = int(seed), int(counter)
+        self.prec_name = precision
+        self.prec = _prec(precision)
+        self.gram = gram or ("fp64" if self.prec == _lib.PREC_FP64 else "bf16")
+        self.n_refine = int(n_refine)
+        dev = self.R.device
+        self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
+        self.O = torch.empty(2 * self.W, self.P, dtype=self.o_dtype, device=dev)
+        self.e = torch.empty(self.W, dtype=torch.complex128, device=dev)
+        self.e_clip = torch.empty_like(self.e)
+        self.stats = torch.zeros(5, dtype=F64, device=dev)
+        self.acc_pos = torch.zeros(self.W, dtype=F64, device=dev)
+        self.acc_spin = torch.zeros(self.W, dtype=F64, device=dev)
+        self.status = torch.zeros(2, dtype=torch.int32, device=dev)
+        h = model.native().handle
+        self.h = h
+        sizes = [_lib.workspace_for(h, op, self.W, self.prec)[1]
+                 for op in (_lib.OP_MCMC, _lib.OP_LOCAL_E, _lib.OP_PER_SAMPLE_O)]
+        sizes.append(ctypes_size(self.W, self.P, 0 if self.o_dtype == torch.float64 else 1,
+                                 _GRAM[self.gram]))
+        self.ws = _lib.workspace.get(max(sizes))
+
+    def sample(self, n_sweeps=None):
+        from . import _lib
+        L = _lib.lib()
+        n = self.n_sweeps if n_sweeps is None else n_sweeps
+        _lib.check(L.nqs_mcmc_sweeps(
+            self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), None, self.W, n,
+            self.n_flips, self.step_size, self.seed, self.counter, None, None, None, None,
+            _lib.ptr(self.acc_pos), _lib.ptr(self.acc_spin), None, self.prec, _lib.ptr(self.ws),
+            self.ws.numel(), _lib.stream_ptr()), "nqs_mcmc_sweeps")
+        self.counter += n
+
+    def energies(self):
+        from . import _lib
+        _lib.check(_lib.lib().nqs_local_energy(
+            self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W, self.m_star,
+            self.lambda_r, self.h_z, self.ewald.handle if self.ewald else None, _lib.ptr(self.e),
+            None, self.prec, _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
+            "nqs_local_energy")
+
+    def jacobian(self):
+        from . import _lib
+        _lib.check(_lib.lib().nqs_per_sample_O(
+            self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W,
+            _lib.ptr(self.O), 0 if self.o_dtype == torch.float64 else 1, self.prec,
+            _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()), "nqs_per_sample_O")
+
+    def update(self):
+        from . import _lib
+        L = _lib.lib()
+        _lib.check(L.nqs_clip_energies(_lib.ptr(self.e), self.W, self.clip_k,
+                                       _lib.ptr(self.e_clip), _lib.ptr(self.stats),
+                                       _lib.stream_ptr()), "nqs_clip_energies")
+        _lib.check(L.nqs_minsr_direction(
+            _lib.ptr(self.O), 0 if self.o_dtype == torch.float64 else 1, _lib.ptr(self.e_clip),
+            self.W, self.P, self.lam, _GRAM[self.gram], self.n_refine, None, _lib.ptr(self.theta),
+            self.lr, _lib.ptr(self.status), _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
+            "nqs_minsr_direction")
+
+    def step(self):
+        self.sample()
+        self.energies()
+        self.jacobian()
+        self.update()
+
+
+def train_minsr(model, params, L, n_elec, key, *, m_star=1.0, lambda_r=1.0, h_z=0.0,
+                ext_field=None, coulomb=None, use_folx=False, n_walkers=256, n_steps=100,
+                lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, burn=80, clip_k=5.0,
+                log_every=20, history=None, R0=None, S0=None, return_walkers=False,
+                precision="fp64", gram=None):
+    """Optimise the Psiformer with MinSR on the device (minsr.py:92-159). Returns
+    (params, history) or (params, history, R, S) when return_walkers=True. Cold start draws
+    uniform walkers and `burn` sweeps; a warm ensemble (R0, S0) skips the burn stage."""
+    from .random import as_key, key_to_seed, split
+    from .sampler import init_walkers_uniform
+    if ext_field is not None:
+        raise NotImplementedError("ext_field is not implemented by the CUDA kernels")
+    theta, unravel = real_ravel(params)
+    kk, ks = split(as_key(key), 2)
+    if R0 is None:
+        R, S = init_walkers_uniform(kk, n_walkers, n_elec, L)
+    else:
+        R, S = torch.as_tensor(R0), torch.as_tensor(S0)
+    it = VMCIteration(model, theta, R, S, m_star=m_star, lambda_r=lambda_r, h_z=h_z,
+                      coulomb=coulomb, lr=lr, lam=lam, n_sweeps=n_sweeps, step_size=step_size,
+                      clip_k=clip_k, seed=key_to_seed(ks), precision=precision, gram=gram)
+    if R0 is None and burn > 0:
+        it.sample(burn)
+    hist = history if history is not None else {"E": [], "Eerr": []}
+    for i in range(n_steps):
+        it.step()
+        st = it.stats.cpu()
+        hist["E"].append(float(st[0]))
+        hist["Eerr"].append(float(st[1]))
+        if log_every and (i % log_every == 0 or i == n_steps - 1):
+            print(f"    minsr {i:4d}: E={float(st[0]):+.6f} +/- {float(st[1]):.1e} "
+                  f"acc={float(it.acc_pos.mean()):.2f}", flush=True)
+    out = unravel(it.theta.to(theta.device))
+    if return_walkers:
+        return out, hist, it.R, it.S
+    return out, hist

@@ -24,7 +24,8 @@ def test_gram_tc_matches_fp64_of_rounded_operands(M, K, kind):
     ref = torch.tril(Ar @ Ar.T)
     scale = (Ar.abs() @ Ar.abs().T).max()
     err = (T - ref).abs().max() / scale
-    assert err < 2e-6, float(err)
+    # float32 accumulation over K terms: relative error ~ sqrt(K) 2^-24, bounded by K 2^-24
+    assert err < 3e-5, float(err)
     assert torch.count_nonzero(torch.triu(T, 1)) == 0
 
 
