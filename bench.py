@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""VMC-iteration benchmark on B200: MinSR iteration over persistent walkers (configuration 2:
+N=16 electrons, 4096 walkers, width 64, 4 blocks, K=4 determinants, RBF Jastrow, Ewald Coulomb).
+
+One step = 10 Metropolis sweeps (1 joint move + 2 spin flips per sweep) + forward-Laplacian local
+energies with the Ewald term + the per-sample Jacobian + the median-MAD clip + the MinSR update.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1|2]
+
+Rank 0 prints ONE JSON line. The headline `value` is VMC iterations/s of the mixed-precision
+path (float32 network, float32 O, BF16 tcgen05 Gram, float64 determinants / Cholesky / energies);
+the plain float64 GPU path is timed in the same run for the mixed-vs-fp64 comparison. With N>1
+every rank runs an independent replica (the path's only cross-walker coupling, the MinSR Gram,
+is solved per GPU), so value = N x per-replica iterations / max-over-ranks time ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "continuum-nqs_b200"))
+
+import torch  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--walkers", type=int, default=None)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sample work")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic work (flops) of one iteration, for the roofline
+# ---------------------------------------------------------------------------------------------
+def gram_flops(W, P):
+    """Lower-triangular SYRK of the 2W x P Jacobian: (2W)(2W+1) P flops (never the mirror)."""
+    n = 2 * W
+    return n * (n + 1) * P
+
+
+def forward_flops(model):
+    N, d, H, K, F = model.n_elec, model.embed_dim, model.n_heads, model.n_dets, 4 * model.n_freq + 2
+    D = model.ff_mult * d
+    g = 2 * N * F * d + model.depth * (2 * N * d * 3 * d + 2 * N * d * d + 2 * N * d * D + 2 * N * D * d
+                                       + 4 * N * N * d)
+    g += 4 * N * d * K * N + 8 * N ** 3 + K * (8 * N ** 3) // 3
+    return g
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+def run_ours(a, rank, world):
+    from nqs import _lib
+    from nqs.configs import config
+    from nqs.ewald import make_ewald
+    from nqs.minsr import VMCIteration
+    from nqs.sampler import init_walkers_uniform
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    model, params, su = config(a.config, a.walkers)
+    theta = model.theta(params)
+    R0, S0 = init_walkers_uniform(1234 + rank, su.n_walkers, su.N, su.L)
+    _, _, coul = make_ewald(su.L, alpha=1.0, ewald_alpha=su.ewald_eta, n_real=su.n_real,
+                            n_recip=su.n_recip)
+    common = dict(m_star=1.0, lambda_r=su.lambda_r, h_z=su.h_z, coulomb=coul, lr=su.lr,
+                  lam=su.lam, n_sweeps=su.n_sweeps, step_size=su.step, clip_k=5.0, seed=7 + rank)
+    it = VMCIteration(model, theta, R0, S0, precision="mixed", gram="bf16", **common)
+    it.sample(40)  # thermalise once before timing
+    torch.cuda.synchronize()
+    L = _lib.lib()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(a.warmup):
+        it.step()
+    torch.cuda.synchronize()
+    # ------------------------------------------------ timed region (device time, events)
+    clocks = Clocks(dev.index)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.steps)]
+    launches0 = L.nqs_kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev[0].record()
+    for k in range(a.steps):
+        # events recorded on the stream right before / after the Gram kernel of this step
+        L.nqs_profile_events(gev[k][0].cuda_event, gev[k][1].cuda_event)
+        it.step()
+    ev[1].record()
+    torch.cuda.synchronize()
+    L.nqs_profile_events(None, None)
+    gram_ms = [g0.elapsed_time(g1) for g0, g1 in gev]
+    barrier()
+    clk = clocks.stop()
+    launches = (L.nqs_kernel_launches() - launches0) // a.steps
+    ms = ev[0].elapsed_time(ev[1]) / a.steps
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    # ------------------------------------------------ phase breakdown (one extra step)
+    pe = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    pe[0].record()
+    it.sample()
+    pe[1].record()
+    it.energies()
+    pe[2].record()
+    it.jacobian()
+    pe[3].record()
+    it.update()
+    pe[4].record()
+    torch.cuda.synchronize()
+    phases = {k: pe[i].elapsed_time(pe[i + 1]) for i, k in
+              enumerate(["sample_ms", "local_energy_ms", "jacobian_ms", "minsr_ms"])}
+    stats = it.stats.cpu().tolist()
+    # ------------------------------------------------ end to end through host buffers
+    e2e = None
+    if a.steps > 0:
+        Rh = it.R.cpu().pin_memory()
+        Sh = it.S.cpu().pin_memory()
+        Th = it.theta.cpu().pin_memory()
+        st_h = torch.empty(5, dtype=torch.float64).pin_memory()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            it.R.copy_(Rh, non_blocking=True)
+            it.S.copy_(Sh, non_blocking=True)
+            it.theta.copy_(Th, non_blocking=True)
+            it.step()
+            Th.copy_(it.theta, non_blocking=True)
+            Rh.copy_(it.R, non_blocking=True)
+            Sh.copy_(it.S, non_blocking=True)
+            st_h.copy_(it.stats, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / a.steps
+        h2d = Rh.numel() * 8 + Sh.numel() * 4 + Th.numel() * 8
+        d2h = h2d + 5 * 8
+        e2e = {"value": world * 1000.0 / e2e_ms, "unit": "VMC iter/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
+    # ------------------------------------------------ plain float64 GPU path
+    fp64 = None
+    if not a.no_fp64 and a.fp64_steps > 0:
+        it64 = VMCIteration(model, theta, it.R, it.S, precision="fp64", **common)
+        it64.step()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(a.fp64_steps):
+            it64.step()
+        f1.record()
+        torch.cuda.synchronize()
+        ms64 = f0.elapsed_time(f1) / a.fp64_steps
+        fp64 = {"ms_per_step": ms64, "VMC_iter_per_s": 1000.0 / ms64,
+                "mixed_speedup": ms64 / ms, "E": float(it64.stats[0])}
+        del it64
+    # ------------------------------------------------ roofline of the dominant kernel (Gram)
+    peaks, src = load_peaks()
+    gflop = gram_flops(su.n_walkers, it.P)
+    g_ms = sorted(gram_ms)[len(gram_ms) // 2] if gram_ms else float("nan")
+    achieved = gflop / (g_ms * 1e-3) / 1e12
+    peak = peaks.get("bf16_tflops", 1590.0)
+    roof = {"kernel": "k_gram_tc<bf16> (tcgen05 SYRK of the 2W x P Jacobian)", "bound": "tensor",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": f"{src} (burst bf16)", "gram_ms": g_ms,
+            "traffic": None, "algorithmic_flops": gflop}
+    return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof, clocks=clk,
+                launches=launches, su=su, model=model, P=it.P)
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline: the float64 oracle on a bounded sample, extrapolated to the full iteration
+# ---------------------------------------------------------------------------------------------
+def cpu_sample(cfg, budget_s, walkers=None):
+    """Time the reference algorithm (oracle restatement: recomputed log psi per proposal, dense
+    Hessian kinetic term, reverse-mode per-sample gradients, explicit Gram + LU solve) on a
+    bounded sample and extrapolate to one full iteration. Returns (iter/s, description)."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle import nqs_oracle as O
+    from nqs.configs import config
+    torch.set_num_threads(os.cpu_count() or 1)
+    model, params, su = config(cfg, walkers)
+    W, N = su.n_walkers, su.N
+    p = params
+    f = lambda r, s: O.logpsi(model, p, r, s)  # noqa: E731
+    rng = np.random.default_rng(0)
+    R = torch.as_tensor(rng.uniform(0, su.L, (N, 2)))
+    S = torch.as_tensor(rng.integers(0, 2, N))
+    def timed(fn, reps=1):
+        fn()  # warm: torch.func builds its transforms on the first call
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    # one walker, one sweep (1 joint move + 2 flips, log psi recomputed per proposal)
+    t_sweep = timed(lambda: O.mcmc_sweep(f, su.L, R, S, su.step,
+                                         torch.as_tensor(rng.standard_normal((N, 2))), 0.5,
+                                         rng.integers(0, N, 2), rng.uniform(size=2)), 2)
+    t_eloc = timed(lambda: O.local_energy(f, R, S, 1.0, su.lambda_r, su.h_z))
+    ew = O.Ewald(su.L, 1.0, su.ewald_eta, su.n_real, su.n_recip)
+    t_coul = timed(lambda: ew.energy(R.numpy()), 3)
+    theta, unravel = O.real_ravel(p["params"])
+    t_O = timed(lambda: O.per_sample_O(model, theta, unravel, R[None], S[None]))
+    P = theta.shape[0]
+    # explicit Gram of the 2W x P matrix (the reference forms the full Otil Otil^T) + LU solve,
+    # sampled at m rows and scaled by flops
+    m = min(2 * W, 512)
+    A = torch.randn(m, P, dtype=torch.float64)
+    t_g = timed(lambda: A @ A.T)
+    gemm_rate = 2.0 * m * m * P / t_g
+    n = min(2 * W, 2048)
+    Tm = torch.randn(n, n, dtype=torch.float64)
+    Tm = Tm @ Tm.T + n * torch.eye(n, dtype=torch.float64)
+    rhs = torch.randn(n, dtype=torch.float64)
+    t_lu = timed(lambda: torch.linalg.solve(Tm, rhs))
+    lu_rate = (2.0 / 3.0) * n ** 3 / t_lu
+    n2 = 2 * W
+    t_iter = (W * (su.n_sweeps * t_sweep + t_eloc + t_coul + t_O) + 2.0 * n2 * n2 * P / gemm_rate
+              + (2.0 / 3.0) * n2 ** 3 / lu_rate)
+    desc = (f"float64 oracle (torch CPU, {torch.get_num_threads()} threads) timed on 1 walker: "
+            f"sweep {t_sweep * 1e3:.1f} ms, E_loc (dense Hessian + SOC) {t_eloc * 1e3:.0f} ms, "
+            f"Ewald {t_coul * 1e3:.1f} ms, per-sample grad {t_O * 1e3:.0f} ms; Gram at "
+            f"{gemm_rate / 1e9:.0f} GFLOP/s ({m} rows sampled), LU at {lu_rate / 1e9:.0f} GFLOP/s "
+            f"(n={n}); extrapolated to W={W}: {t_iter:.0f} s per iteration")
+    return 1.0 / t_iter, desc, torch.get_num_threads()
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    vals = []
+    desc = ""
+    cores = 1
+    for i in range(a.warmup + a.steps):
+        v, desc, cores = cpu_sample(a.config, a.cpu_budget, a.walkers)
+        if i >= a.warmup:
+            vals.append(v)
+        if i == 0 and a.warmup + a.steps > 2:
+            pass
+    v = sum(vals) / max(len(vals), 1)
+    from nqs.configs import config
+    _, _, su = config(a.config, a.walkers)
+    line = {"impl": "reference", "metric": "VMC iter/s", "value": v, "unit": "VMC iter/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{su.name}: N={su.N}, W={su.n_walkers}, 10 sweeps + E_loc + "
+                                   "O + MinSR", "walkers": su.n_walkers, "electrons": su.N},
+            "cpu_baseline": {"value": v, "unit": "VMC iter/s", "cores": cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": v, "unit": "VMC iter/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    rank = int(os.environ.get("RANK", 0))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    r = run_ours(a, rank, world)
+    su = r["su"]
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        try:
+            v, desc, cores = cpu_sample(a.config, a.cpu_budget, a.walkers)
+            cpu = {"value": v, "unit": "VMC iter/s", "cores": cores, "kind": "port", "sample": desc}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "VMC iter/s", "cores": None, "kind": "port",
+                   "sample": f"failed: {e}"}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    ms = r["ms"]
+    ph = r["phases"]
+    W = su.n_walkers
+    line = {
+        "metric": "VMC iter/s", "value": world * 1000.0 / ms, "unit": "VMC iter/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/bf16+f64",
+        "data": "synthetic (seeded uniform walkers, N(0,0.02^2) weights)",
+        "config": {"workload": f"{su.name}: N={su.N}, W={W}, width 64, 4 blocks, K=4, Jastrow; "
+                               "10 sweeps + forward-Laplacian E_loc + Ewald + O + MinSR",
+                   "walkers": W, "electrons": su.N, "params": r["P"], "precision": "mixed",
+                   "gram": "bf16 tcgen05", "l2": "working set (O: 2W x P f32 = "
+                   f"{2 * W * r['P'] * 4 / 1e9:.1f} GB) exceeds L2 every step",
+                   "parallelism": f"{world} independent replicas"},
+        "walker_steps_per_s": world * W * su.n_sweeps / (ph["sample_ms"] * 1e-3),
+        "eloc_evals_per_s": world * W / (ph["local_energy_ms"] * 1e-3),
+        "phases_ms": ph, "energy": {"mean": r["stats"][0], "err": r["stats"][1],
+                                    "var": r["stats"][2]},
+        "fp64_plain": r["fp64"], "roofline": r["roofline"], "cpu_baseline": cpu,
+        "e2e": r["e2e"], "clocks": r["clocks"], "gpu_launches": int(r["launches"]),
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -309,6 +309,7 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
   int tiles = 0;
   for (int i = 0; i < nrt; ++i) tiles += i / 2 + 1;
   // every column tile must start inside the matrix: col tile tj <= floor(ti/2) => j0 <= i0
+  if (g_prof_start) cudaEventRecord(g_prof_start, st);
   if (prec == 1) {
     cudaFuncSetAttribute(tc::k_gram_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
@@ -319,6 +320,7 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
     tc::k_gram_tc<1><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err);
   }
   NQS_CHECK_LAUNCH("k_gram_tc");
+  if (g_prof_stop) cudaEventRecord(g_prof_stop, st);
   return NQS_OK;
 }
 

@@ -505,16 +505,21 @@ static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
                          double* tmpK, double* tmpK_lo, int n_refine, cudaStream_t st) {
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
   k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, y);
+  NQS_CHECK_LAUNCH("k_trsv_lower");
   k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, y);
-  NQS_CHECK_LAUNCH("cholesky solve");
+  NQS_CHECK_LAUNCH("k_trsv_lower_t");
   const unsigned gk = (unsigned)((K + 255) / 256);
   for (int it = 0; it < n_refine; ++it) {
     k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0);
+    NQS_CHECK_LAUNCH("k_gemv_t");
     k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, y, r);
+    NQS_CHECK_LAUNCH("k_gemv_n_resid");
     k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, r);
+    NQS_CHECK_LAUNCH("k_trsv_lower");
     k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, r);
+    NQS_CHECK_LAUNCH("k_trsv_lower_t");
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
-    NQS_CHECK_LAUNCH("refinement");
+    NQS_CHECK_LAUNCH("k_axpy");
   }
   return NQS_OK;
 }
@@ -693,7 +698,9 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
       k_center<float, double><<<ce, 256, 0, st>>>((const float*)O, W, P, mu, Ot, P);
     }
     NQS_CHECK_LAUNCH("k_center");
+    if (g_prof_start) cudaEventRecord(g_prof_start, st);
     NQS_TRY(dsyrk_lower(Ot, P, n, P, 1.0, 0.0, T, n, part, part_elems, nsm, st));
+    if (g_prof_stop) cudaEventRecord(g_prof_stop, st);
     Oop = Ot;
     op_dtype = 0;
     mu_op = nullptr;
@@ -751,9 +758,9 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   cudaMemsetAsync(bad, 0, sizeof(int) * 4, st);
   NQS_TRY(dsyrk_lower(A, K, M, K, 1.0, 0.0, T, M, part, pe, nsm, st));
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
+  NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
   NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, 3, st));
-  NQS_CHECK_LAUNCH("nqs_gram_solve");
   return NQS_OK;
 }
 

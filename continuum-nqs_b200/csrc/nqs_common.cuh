@@ -12,13 +12,19 @@
 // --------------------------------------------------------------------------------------------
 // error plumbing (host)
 // --------------------------------------------------------------------------------------------
+#include <atomic>
+
 namespace nqs {
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+extern std::atomic<unsigned long long> g_launches;  // kernels launched by this library
+extern cudaEvent_t g_prof_start, g_prof_stop;      // optional events around the Gram kernel
 }  // namespace nqs
 
+// every kernel launch is followed by exactly one NQS_CHECK_LAUNCH (it also counts the launch)
 #define NQS_CHECK_LAUNCH(what)                                              \
   do {                                                                      \
+    nqs::g_launches.fetch_add(1, std::memory_order_relaxed);                \
     cudaError_t _e = cudaGetLastError();                                    \
     if (_e != cudaSuccess) return nqs::cuda_status(_e, what);               \
   } while (0)

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <vector>
 #include <cmath>
+#include <atomic>
 
 #include "net.cuh"
 
@@ -17,6 +18,8 @@ struct NqsModel {
 namespace nqs {
 
 static thread_local char g_err[512] = "";
+std::atomic<unsigned long long> g_launches{0};
+cudaEvent_t g_prof_start = nullptr, g_prof_stop = nullptr;
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -290,6 +293,14 @@ const char* nqs_status_string(int s) {
 }
 
 const char* nqs_last_error(void) { return g_err; }
+
+unsigned long long nqs_kernel_launches(void) { return g_launches.load(); }
+
+int nqs_profile_events(void* start, void* stop) {
+  g_prof_start = (cudaEvent_t)start;
+  g_prof_stop = (cudaEvent_t)stop;
+  return NQS_OK;
+}
 
 int nqs_model_create(const NqsModelDesc* d, NqsModel** out) {
   if (!out) return NQS_ERR_INVALID_ARG;
@@ -608,12 +619,20 @@ int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, dou
     }
   }
   if (n_sweeps > 0) {
-    if (out_acc_pos) k_scale<<<nb, 128, 0, st>>>(out_acc_pos, W, 1.0 / n_sweeps);
-    if (out_acc_spin && n_flips > 0)
+    if (out_acc_pos) {
+      k_scale<<<nb, 128, 0, st>>>(out_acc_pos, W, 1.0 / n_sweeps);
+      NQS_CHECK_LAUNCH("k_scale");
+    }
+    if (out_acc_spin && n_flips > 0) {
       k_scale<<<nb, 128, 0, st>>>(out_acc_spin, W, 1.0 / ((double)n_sweeps * n_flips));
+      NQS_CHECK_LAUNCH("k_scale");
+    }
   }
-  if (logpsi_io) cudaMemcpyAsync(logpsi_io, Lc, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st);
-  NQS_CHECK_LAUNCH("nqs_mcmc_sweeps");
+  if (logpsi_io) {
+    const cudaError_t e = cudaMemcpyAsync(logpsi_io, Lc, sizeof(cplx) * W,
+                                          cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e, "nqs_mcmc_sweeps: copy");
+  }
   return NQS_OK;
 }
 

@@ -93,6 +93,11 @@ int nqs_version(void);
 const char* nqs_status_string(int status);
 /* Last error detail (thread-local, human readable). */
 const char* nqs_last_error(void);
+/* Number of kernels this library has launched since it was loaded (process-wide). */
+unsigned long long nqs_kernel_launches(void);
+/* Optional cudaEvent_t pair (NULL to clear) recorded on the caller's stream immediately before and
+ * after the Gram kernel inside nqs_minsr_direction, for timing it in isolation. */
+int nqs_profile_events(void* start_event, void* stop_event);
 
 /* Model handle: validates the descriptor and uploads the immutable constants (Gs, W, knots).
  * Replaces the flax module construction in src/nqs/psiformer.py:100-116. */

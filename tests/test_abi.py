@@ -10,7 +10,7 @@ HDR = os.path.join(os.path.dirname(__file__), os.pardir, "include", "nqs.h")
 
 def declared():
     src = open(HDR).read()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(nqs_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*|unsigned long long)\s+(nqs_\w+)\s*\(", src, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
