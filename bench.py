@@ -154,6 +154,9 @@ def run_ours(a, rank, world):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(a.steps)]
+    for e0_, e1_ in gev:  # create the CUDA events now; the library re-records them
+        e0_.record()
+        e1_.record()
     launches0 = L.nqs_kernel_launches()
     barrier()
     torch.cuda.synchronize()

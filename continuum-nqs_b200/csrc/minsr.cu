@@ -237,10 +237,15 @@ constexpr int CB = 64;
 
 // factor the diagonal block in place (lower), one CTA of 256 threads; adds lam to the diagonal
 // first if add_lam; sets *bad when a pivot is not positive
+// factor the diagonal block in place (lower), one CTA of 256 threads. A pivot d <= *floor_p is
+// replaced by *floor_p (modified Cholesky with a pivot floor; bad[2] counts the replacements) when
+// floor_p is given, else flagged in bad[0] (not positive definite).
 __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int64_t lda, int k0,
-                                                    int n, double lam, int* __restrict__ bad) {
+                                                    int n, const double* __restrict__ floor_p,
+                                                    int* __restrict__ bad) {
   __shared__ double L[CB][CB + 1];
   const int b = min(CB, n - k0);
+  const double fl = floor_p ? *floor_p : 0.0;
   for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
     const int i = idx / b, j = idx - i * b;
     L[i][j] = (j <= i) ? A[(size_t)(k0 + i) * lda + k0 + j] : 0.0;
@@ -248,9 +253,13 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int6
   __syncthreads();
   for (int j = 0; j < b; ++j) {
     if (threadIdx.x == 0) {
-      const double d = L[j][j];
+      double d = L[j][j];
+      if (floor_p && !(d > fl)) {
+        d = fl;
+        atomicAdd(bad + 2, 1);
+      }
       if (!(d > 0.0)) {
-        *bad = 1;
+        bad[0] = 1;
         L[j][j] = NAN;
       } else {
         L[j][j] = sqrt(d);
@@ -260,7 +269,6 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int6
     const double piv = L[j][j];
     for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) L[i][j] /= piv;
     __syncthreads();
-    // trailing update of the block
     for (int idx = threadIdx.x; idx < (b - j - 1) * (b - j - 1); idx += blockDim.x) {
       const int ii = j + 1 + idx / (b - j - 1), jj = j + 1 + idx % (b - j - 1);
       if (jj <= ii) L[ii][jj] -= L[ii][j] * L[jj][j];
@@ -271,7 +279,23 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int6
     const int i = idx / b, j = idx - i * b;
     if (j <= i) A[(size_t)(k0 + i) * lda + k0 + j] = L[i][j];
   }
-  (void)lam;
+}
+
+// *floor = rel * max_i A[i][i]  (one CTA)
+__global__ void k_pivot_floor(const double* __restrict__ A, int64_t lda, int n, double rel,
+                              double* __restrict__ floor_out) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, A[(size_t)i * lda + i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t = fmax(t, red[i]);
+    *floor_out = rel * t;
+  }
 }
 
 // panel: rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L_kk^-T  (one warp per row)
@@ -313,10 +337,10 @@ __global__ void k_add_diag(double* A, int64_t lda, int n, double lam) {
 }
 
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
-                   int nsm, cudaStream_t st) {
+                   int nsm, cudaStream_t st, const double* floor_p = nullptr) {
   for (int k0 = 0; k0 < n; k0 += CB) {
     const int b = std::min(CB, n - k0);
-    k_potrf_diag<<<1, 256, 0, st>>>(A, lda, k0, n, 0.0, bad);
+    k_potrf_diag<<<1, 256, 0, st>>>(A, lda, k0, n, floor_p, bad);
     NQS_CHECK_LAUNCH("k_potrf_diag");
     const int rest = n - k0 - b;
     if (rest <= 0) break;
@@ -491,6 +515,26 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid(const TO* __restrict__ O, 
   }
 }
 
+__global__ void k_scale_vec(double* x, int64_t n, double s) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= s;
+}
+
+// Adam (Kingma & Ba 2015) with bias correction, as optax.adam: m <- b1 m + (1-b1) g,
+// v <- b2 v + (1-b2) g^2, theta <- theta - lr (m/c1) / (sqrt(v/c2) + eps)
+__global__ void k_adam(double* __restrict__ th, const double* __restrict__ g, double* __restrict__ m,
+                       double* __restrict__ v, int64_t n, double lr, double b1, double b2,
+                       double eps, double c1, double c2) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double gi = g[i];
+  const double mi = b1 * m[i] + (1.0 - b1) * gi;
+  const double vi = b2 * v[i] + (1.0 - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  th[i] -= lr * (mi / c1) / (sqrt(vi / c2) + eps);
+}
+
 __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__ y) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += a[i];
@@ -626,6 +670,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(int) * 4);                 // status
+  add(sizeof(double));                  // pivot floor
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
   if (gram == 0 && odtype == 1) add(sizeof(double) * n * P);  // float64 Otil from float32 O
   if (gram != 0) add(gram_tc_workspace(W, P, gram));
@@ -709,7 +754,18 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   }
   k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
-  NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st));
+  // A tensor-core Gram carries rounding noise ~ u sqrt(Tii Tjj) (u = 2^-8 BF16, 2^-11 TF32)
+  // that can exceed lam along the null directions the centring creates, so its factor is a
+  // preconditioner built with a pivot floor; the refinement below solves the exact system.
+  const double* floor_p = nullptr;
+  if (gram_prec != 0) {
+    double* fl = ws.take<double>(1);
+    if (!fl) return NQS_ERR_WORKSPACE;
+    k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-8 : 0x1p-11, fl);
+    NQS_CHECK_LAUNCH("k_pivot_floor");
+    floor_p = fl;
+  }
+  NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
   if (op_dtype == 0)
     NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, tmpK,
                                   tmpK_lo, n_refine, st));
@@ -724,7 +780,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
     k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)Oop, n, W, P, mu_op, y, out_dtheta,
                                         nullptr, theta_io, lr);
   NQS_CHECK_LAUNCH("k_gemv_t");
-  if (status_dev) cudaMemcpyAsync(status_dev, bad, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (status_dev) cudaMemcpyAsync(status_dev, bad, 3 * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return NQS_OK;
 }
 
@@ -761,6 +817,39 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
   NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, 3, st));
+  return NQS_OK;
+}
+
+int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int W, int64_t P,
+                        double* out_grad, void* wsp, size_t wsb, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!O || !e || !out_grad || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || !wsp ||
+      wsb < sizeof(double) * 2 * (size_t)W + 256)
+    return NQS_ERR_INVALID_ARG;
+  double* x = (double*)wsp;
+  k_center_eps<<<1, 1024, 0, st>>>((const cplx*)e, W, x);
+  NQS_CHECK_LAUNCH("k_center_eps");
+  const unsigned gp = (unsigned)((P + 255) / 256);
+  // g = (2/W) sum_w Re(conj(e_w - mean e) O_w) = (2/W) O_rows^T [Re eps; Im eps]
+  if (o_dtype == 0)
+    k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)O, 2 * W, 2 * W, P, nullptr, x, out_grad,
+                                         nullptr, nullptr, 0.0);
+  else
+    k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)O, 2 * W, 2 * W, P, nullptr, x, out_grad,
+                                        nullptr, nullptr, 0.0);
+  NQS_CHECK_LAUNCH("k_gemv_t");
+  k_scale_vec<<<gp, 256, 0, st>>>(out_grad, P, 2.0 / W);
+  NQS_CHECK_LAUNCH("k_scale_vec");
+  return NQS_OK;
+}
+
+int nqs_adam_update(double* theta, const double* grad, double* m, double* v, int64_t P, double lr,
+                    double b1, double b2, double eps, int t, void* stream) {
+  if (!theta || !grad || !m || !v || P < 1 || t < 1) return NQS_ERR_INVALID_ARG;
+  const double c1 = 1.0 - pow(b1, (double)t), c2 = 1.0 - pow(b2, (double)t);
+  k_adam<<<(unsigned)((P + 255) / 256), 256, 0, (cudaStream_t)stream>>>(theta, grad, m, v, P, lr,
+                                                                         b1, b2, eps, c1, c2);
+  NQS_CHECK_LAUNCH("k_adam");
   return NQS_OK;
 }
 

@@ -170,6 +170,10 @@ _SIGS.update({
                              c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_size_t, c_void_p],
                             c_int),
     "nqs_clip_energies": ([c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p], c_int),
+    "nqs_energy_gradient": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_size_t,
+                             c_void_p], c_int),
+    "nqs_adam_update": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_double,
+                         c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),
     "nqs_profile_events": ([c_void_p, c_void_p], c_int),
     "nqs_gram": ([c_void_p, c_int, c_int, c_int64, c_int64, c_void_p, c_int64, c_void_p, c_void_p],

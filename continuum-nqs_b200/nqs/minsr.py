@@ -231,7 +231,7 @@ class VMCIteration:
 
     def __init__(self, model, theta, R, S, *, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
                  lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, clip_k=5.0, n_spin_flips=2,
-                 seed=0, counter=0, precision="fp64", gram=None, n_refine=1):
+                 seed=0, counter=0, precision="fp64", gram=None, n_refine=None):
         from . import _lib
         from .psiformer import _prec, as_batch
         _lib.require_cuda()
@@ -253,7 +253,7 @@ class VMCIteration:
         self.prec_name = precision
         self.prec = _prec(precision)
         self.gram = gram or ("fp64" if self.prec == _lib.PREC_FP64 else "bf16")
-        self.n_refine = int(n_refine)
+        self.n_refine = int(n_refine if n_refine is not None else (1 if self.gram == "fp64" else 3))
         dev = self.R.device
         self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
         self.O = torch.empty(2 * self.W, self.P, dtype=self.o_dtype, device=dev)
@@ -262,7 +262,7 @@ class VMCIteration:
         self.stats = torch.zeros(5, dtype=F64, device=dev)
         self.acc_pos = torch.zeros(self.W, dtype=F64, device=dev)
         self.acc_spin = torch.zeros(self.W, dtype=F64, device=dev)
-        self.status = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(3, dtype=torch.int32, device=dev)
         h = model.native().handle
         self.h = h
         sizes = [_lib.workspace_for(h, op, self.W, self.prec)[1]

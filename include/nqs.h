@@ -169,7 +169,9 @@ int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, cons
  * refinement of y against the exact operator Otil Otil^T + lam I (applied with O itself, never
  * the rounded Gram). status_dev (nullable, device int) is set
  * non-zero when a Cholesky pivot was not positive; status_dev[1] when a tensor-core Gram CTA hit
- * its bounded-wait limit. */
+ * its bounded-wait limit; status_dev[2] counts pivots raised to the floor u * max T_ii
+ * (u = 2^-8 BF16, 2^-11 TF32) in the factor of a tensor-core Gram, which only preconditions the
+ * refinement against the exact operator (3 ints). */
 int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int gram_prec,
                              size_t* bytes);
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
@@ -189,6 +191,17 @@ int nqs_gram(const void* A, int a_dtype, int M, int64_t K, int64_t lda, double* 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes);
 int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* rhs, double* x,
                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Energy gradient of the surrogate 2 mean_w Re[conj(e_w - mean e) log psi_theta(x_w)]
+ * (src/nqs/train.py:53-59): grad = (2/W) sum_w Re(conj(e_w - mean e) O_w), with O the [2W][P]
+ * rows of nqs_per_sample_O. The workspace needs 2W doubles. */
+int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int n_walkers,
+                        int64_t n_params, double* out_grad, void* workspace,
+                        size_t workspace_bytes, void* stream);
+/* Adam step (optax.adam defaults b1 0.9, b2 0.999, eps 1e-8) on the real ravel theta; t >= 1 is
+ * the step count used for bias correction. m, v: float64[P] moment buffers (start at 0). */
+int nqs_adam_update(double* theta, const double* grad, double* m, double* v, int64_t n_params,
+                    double lr, double b1, double b2, double eps, int t, void* stream);
 
 /* Median-MAD clip of Re e (src/nqs/minsr.py:145-148): med = median(Re e),
  * mad = median(|Re e - med|) + 1e-12, Re e clipped to med +- clip_k mad, Im kept.

@@ -39,6 +39,6 @@ def test_minsr_bf16_gram_close_to_fp64():
     eps = torch.as_tensor(rng.normal(size=W) + 1j * rng.normal(size=W))
     d64 = minsr_direction(Oc.cuda(), eps, 1e-3, gram="fp64")
     for kind in ("bf16", "tf32"):
-        d = minsr_direction(Oc.cuda(), eps, 1e-3, gram=kind, n_refine=2)
+        d = minsr_direction(Oc.cuda(), eps, 1e-3, gram=kind, n_refine=4)
         rel = float((d - d64).norm() / d64.norm())
         assert rel < 1e-6, (kind, rel)

@@ -20,3 +20,29 @@ def test_minsr_descends_to_Egs(precision):
     assert E_final < g["E_gs"] + 1e-2, (E_final, g["E_gs"])
     assert E_final > g["E_gs"] - 2e-2
     assert hist["E"][0] > E_final
+
+
+def test_adam_training_descends_to_Egs():
+    """tests/test_nqs_train.py:36-72: Adam removes >= 95% of the perturbation's energy excess."""
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import make_logpsi
+    from nqs.sampler import run_chain, vmc_energy
+    from nqs.train import train
+    g, model = build(N=5, L=7.0, hz=0.5, embed=16, heads=4)
+    params = perturb(model.init(0), 0.15, 2, only="backflow")
+
+    def energy_now(p):
+        lp = make_logpsi(model, p)
+        R, S, _, _ = run_chain(lp, 7.0, 5, 7, n_walkers=256, n_sweeps=80, burn=80, step=0.5)
+        return vmc_energy(make_local_energy(lp, 1.0, 1.0, 0.5), R, S)[0]
+
+    E_init = energy_now(params)
+    params, hist = train(model, params, 7.0, 5, 3, m_star=1.0, lambda_r=1.0, h_z=0.5,
+                         n_walkers=256, n_steps=120, lr=3e-3, n_sweeps=8, step_size=0.5, burn=40,
+                         log_every=0)
+    E_final = energy_now(params)
+    excess = E_init - g["E_gs"]
+    assert excess > 1e-2
+    assert E_final < E_init - 1e-3
+    assert (E_final - g["E_gs"]) / excess < 0.05, (E_init, E_final, g["E_gs"])
+    assert E_final > g["E_gs"] - 0.02
