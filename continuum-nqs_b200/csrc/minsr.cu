@@ -12,7 +12,11 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 #include "minsr.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace nqs {
 
@@ -356,75 +360,159 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
   return NQS_OK;
 }
 
-// forward solve L z = v (in place), one CTA (1024 threads), blocked by 64: x_blk via a warp,
-// then the remaining rows are updated in parallel.
-__global__ void __launch_bounds__(1024) k_trsv_lower(const double* __restrict__ L, int64_t ldl,
-                                                     int n, double* __restrict__ v) {
-  __shared__ double xb[CB];
-  for (int k0 = 0; k0 < n; k0 += CB) {
-    const int b = min(CB, n - k0);
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
-      for (int j = 0; j < b; ++j) {
-        const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
-                          L[(size_t)(k0 + j) * ldl + k0 + j];
-        if (lane == (j & 31)) {
-          if (j < 32) x0 = xj; else x1 = xj;
-        }
-        if (lane > j && lane < b) x0 -= xj * L[(size_t)(k0 + lane) * ldl + k0 + j];
-        if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[(size_t)(k0 + lane + 32) * ldl + k0 + j];
+// Triangular solves on the whole GPU (cooperative launch, grid.sync between block steps):
+// per 64-wide block the first CTA solves the diagonal block with one warp, then every warp of the
+// grid updates the remaining rows (forward) / columns (transposed) against that block.
+__device__ __forceinline__ void diag_solve_warp(const double* __restrict__ L, int64_t ldl, int k0,
+                                                int b, double* __restrict__ v,
+                                                double* __restrict__ xb, bool transposed) {
+  const int lane = threadIdx.x & 31;
+  double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
+  if (!transposed) {
+    for (int j = 0; j < b; ++j) {
+      const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
+                        L[(size_t)(k0 + j) * ldl + k0 + j];
+      if (lane == (j & 31)) {
+        if (j < 32) x0 = xj; else x1 = xj;
       }
-      if (lane < b) xb[lane] = x0;
-      if (lane + 32 < b) xb[lane + 32] = x1;
+      if (lane > j && lane < b) x0 -= xj * L[(size_t)(k0 + lane) * ldl + k0 + j];
+      if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[(size_t)(k0 + lane + 32) * ldl + k0 + j];
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < b; i += blockDim.x) v[k0 + i] = xb[i];
-    // update rows below: v[r] -= sum_j L[r][k0+j] xb[j]  (one warp per row)
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r = k0 + b + wid; r < n; r += nw) {
-      double s = 0;
-      for (int j = lane; j < b; j += 32) s += L[(size_t)r * ldl + k0 + j] * xb[j];
-      s = warp_sum(s);
-      if (lane == 0) v[r] -= s;
+  } else {
+    for (int j = b - 1; j >= 0; --j) {
+      const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
+                        L[(size_t)(k0 + j) * ldl + k0 + j];
+      if (lane == (j & 31)) {
+        if (j < 32) x0 = xj; else x1 = xj;
+      }
+      if (lane < j) x0 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane];
+      if (lane + 32 < j) x1 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane + 32];
     }
-    __syncthreads();
+  }
+  if (lane < b) {
+    v[k0 + lane] = x0;
+    xb[lane] = x0;
+  }
+  if (lane + 32 < b) {
+    v[k0 + lane + 32] = x1;
+    xb[lane + 32] = x1;
   }
 }
 
-// backward solve L^T y = z (in place)
-__global__ void __launch_bounds__(1024) k_trsv_lower_t(const double* __restrict__ L, int64_t ldl,
-                                                       int n, double* __restrict__ v) {
-  __shared__ double xb[CB];
+// solves L x = v (transposed = 0) or L^T x = v (transposed = 1) in place; xb: 64 doubles scratch
+__global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L, int64_t ldl,
+                                                   int n, double* __restrict__ v,
+                                                   double* __restrict__ xb, int transposed) {
+  cg::grid_group grid = cg::this_grid();
   const int nblk = (n + CB - 1) / CB;
-  for (int bi = nblk - 1; bi >= 0; --bi) {
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  __shared__ double xs[CB];
+  for (int s = 0; s < nblk; ++s) {
+    const int bi = transposed ? nblk - 1 - s : s;
     const int k0 = bi * CB, b = min(CB, n - k0);
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
-      for (int j = b - 1; j >= 0; --j) {
-        const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
-                          L[(size_t)(k0 + j) * ldl + k0 + j];
-        if (lane == (j & 31)) {
-          if (j < 32) x0 = xj; else x1 = xj;
-        }
-        // L^T[m][j] = L[j][m]: rows m < j get x_m -= L[j][m] x_j
-        if (lane < j) x0 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane];
-        if (lane + 32 < j) x1 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane + 32];
+    if (blockIdx.x == 0 && threadIdx.x < 32) diag_solve_warp(L, ldl, k0, b, v, xb, transposed);
+    grid.sync();
+    for (int i = threadIdx.x; i < b; i += blockDim.x) xs[i] = xb[i];
+    __syncthreads();
+    if (!transposed) {
+      // rows r >= k0 + b: v[r] -= sum_j L[r][k0 + j] x_j   (one warp per row)
+      for (int r = k0 + b + gwarp; r < n; r += nwarps) {
+        const double* lr = L + (size_t)r * ldl + k0;
+        double acc = 0.0;
+        for (int j = lane; j < b; j += 32) acc = fma(lr[j], xs[j], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) v[r] -= acc;
       }
-      if (lane < b) xb[lane] = x0;
-      if (lane + 32 < b) xb[lane + 32] = x1;
+    } else {
+      // columns m < k0: v[m] -= sum_j L[k0 + j][m] x_j   (one thread per column, coalesced)
+      for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < k0; m += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < b; ++j) acc = fma(L[(size_t)(k0 + j) * ldl + m], xs[j], acc);
+        v[m] -= acc;
+      }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < b; i += blockDim.x) v[k0 + i] = xb[i];
-    // rows above: v[m] -= sum_j L[k0+j][m] xb[j], m < k0  (threads over m: coalesced along m)
-    for (int m = threadIdx.x; m < k0; m += blockDim.x) {
-      double s = 0;
-      for (int j = 0; j < b; ++j) s += L[(size_t)(k0 + j) * ldl + m] * xb[j];
-      v[m] -= s;
-    }
-    __syncthreads();
+    grid.sync();
   }
+}
+
+static int trsv_grid(const double* L, int64_t ldl, int n, double* v, double* xb, int transposed,
+                     cudaStream_t st) {
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trsv_grid, 256, 0);
+    grid = nsm * std::max(1, std::min(per, 4));
+  }
+  void* args[] = {(void*)&L, (void*)&ldl, (void*)&n, (void*)&v, (void*)&xb, (void*)&transposed};
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_trsv_grid, grid, 256, args, 0, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_trsv_grid");
+  NQS_CHECK_LAUNCH("k_trsv_grid");
+  return NQS_OK;
+}
+
+// Double centring of a symmetric Gram held in its lower triangle, per walker half:
+//   T <- C T C,  C = blockdiag(I - 1 1^T / W, I - 1 1^T / W)
+// (makes the two null vectors created by centring O exact again after a low-precision Gram).
+__global__ void k_gram_rowsums(const double* __restrict__ T, int n, int W,
+                               double* __restrict__ rs) {
+  const int i = blockIdx.x;
+  double s0 = 0.0, s1 = 0.0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double t = j <= i ? T[(size_t)i * n + j] : T[(size_t)j * n + i];
+    if (j < W) s0 += t; else s1 += t;
+  }
+  __shared__ double r0[32], r1[32];
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  if ((threadIdx.x & 31) == 0) {
+    r0[threadIdx.x >> 5] = s0;
+    r1[threadIdx.x >> 5] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += r0[w];
+      b += r1[w];
+    }
+    rs[2 * i] = a / W;
+    rs[2 * i + 1] = b / W;
+  }
+}
+
+__global__ void k_gram_blocksums(const double* __restrict__ rs, int n, int W,
+                                 double* __restrict__ S) {
+  // S[2a + b] = mean over rows i in half a of rs[i][b]
+  __shared__ double red[4][32];
+  double acc[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int a = i >= W;
+    acc[2 * a] += rs[2 * i];
+    acc[2 * a + 1] += rs[2 * i + 1];
+  }
+  for (int q = 0; q < 4; ++q) {
+    const double v = warp_sum(acc[q]);
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+    S[threadIdx.x] = t / W;
+  }
+}
+
+__global__ void k_gram_center(double* __restrict__ T, int n, int W, const double* __restrict__ rs,
+                              const double* __restrict__ S) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > i) return;
+  const int a = i >= W, b = j >= W;
+  T[(size_t)i * n + j] += -rs[2 * i + b] - rs[2 * j + a] + S[2 * a + b];
 }
 
 // error-free transformations (Knuth TwoSum, FMA TwoProduct) for compensated dot products
@@ -546,22 +634,19 @@ __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__
 template <typename TO>
 static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
                          const double* mu, double lam, const double* b, double* y, double* r,
-                         double* tmpK, double* tmpK_lo, int n_refine, cudaStream_t st) {
+                         double* tmpK, double* tmpK_lo, double* xb, int n_refine,
+                         cudaStream_t st) {
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
-  k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, y);
-  NQS_CHECK_LAUNCH("k_trsv_lower");
-  k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, y);
-  NQS_CHECK_LAUNCH("k_trsv_lower_t");
+  NQS_TRY(trsv_grid(L, M, M, y, xb, 0, st));
+  NQS_TRY(trsv_grid(L, M, M, y, xb, 1, st));
   const unsigned gk = (unsigned)((K + 255) / 256);
   for (int it = 0; it < n_refine; ++it) {
     k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0);
     NQS_CHECK_LAUNCH("k_gemv_t");
     k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, y, r);
     NQS_CHECK_LAUNCH("k_gemv_n_resid");
-    k_trsv_lower<<<1, 1024, 0, st>>>(L, M, M, r);
-    NQS_CHECK_LAUNCH("k_trsv_lower");
-    k_trsv_lower_t<<<1, 1024, 0, st>>>(L, M, M, r);
-    NQS_CHECK_LAUNCH("k_trsv_lower_t");
+    NQS_TRY(trsv_grid(L, M, M, r, xb, 0, st));
+    NQS_TRY(trsv_grid(L, M, M, r, xb, 1, st));
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
     NQS_CHECK_LAUNCH("k_axpy");
   }
@@ -669,6 +754,8 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * n);              // refinement residual
   add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
+  add(sizeof(double) * (2 * n + 4));    // Gram row sums (double centring)
+  add(sizeof(double) * CB);             // triangular-solve block
   add(sizeof(int) * 4);                 // status
   add(sizeof(double));                  // pivot floor
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
@@ -711,6 +798,8 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* r = ws.take<double>(n);
   double* tmpK = ws.take<double>(P);
   double* tmpK_lo = ws.take<double>(P);
+  double* xb = ws.take<double>(CB);
+  double* rsum = ws.take<double>(2 * (size_t)n + 4);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
   const size_t part_elems = minsr_part_elems(W);
@@ -751,6 +840,12 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
     mu_op = nullptr;
   } else {
     NQS_TRY(gram_tc(O, o_dtype, mu, W, P, gram_prec, T, ws, nsm, st, bad + 1));
+    k_gram_rowsums<<<n, 256, 0, st>>>(T, n, W, rsum);
+    NQS_CHECK_LAUNCH("k_gram_rowsums");
+    k_gram_blocksums<<<1, 1024, 0, st>>>(rsum, n, W, rsum + 2 * n);
+    NQS_CHECK_LAUNCH("k_gram_blocksums");
+    k_gram_center<<<dim3((n + 255) / 256, n), 256, 0, st>>>(T, n, W, rsum, rsum + 2 * n);
+    NQS_CHECK_LAUNCH("k_gram_center");
   }
   k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
@@ -768,10 +863,10 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
   if (op_dtype == 0)
     NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, tmpK,
-                                  tmpK_lo, n_refine, st));
+                                  tmpK_lo, xb, n_refine, st));
   else
     NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, tmpK,
-                                 tmpK_lo, n_refine, st));
+                                 tmpK_lo, xb, n_refine, st));
   const unsigned gp = (unsigned)((P + 255) / 256);
   if (op_dtype == 0)
     k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)Oop, n, W, P, mu_op, y, out_dtheta,
@@ -787,7 +882,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
-  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K +
+  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + CB +
                              std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 8192;
   return NQS_OK;
 }
@@ -816,7 +911,9 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
-  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, 3, st));
+  double* xb = ws.take<double>(CB);
+  if (!xb) return NQS_ERR_WORKSPACE;
+  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, xb, 3, st));
   return NQS_OK;
 }
 
