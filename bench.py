@@ -219,10 +219,29 @@ def run_ours(a, rank, world):
         d2h = h2d + 5 * 8
         e2e = {"value": world * 1000.0 / e2e_ms, "unit": "VMC iter/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
-    # ------------------------------------------------ plain float64 GPU path
+    # ------------------------------------------------ plain float64 GPU path + accuracy gates
     fp64 = None
+    acc = None
     if not a.no_fp64 and a.fp64_steps > 0:
-        it64 = VMCIteration(model, theta, it.R, it.S, precision="fp64", **common)
+        from nqs.minsr import minsr_step
+        it64 = VMCIteration(model, it.theta, it.R, it.S, precision="fp64", **common)
+        # accuracy of the mixed path against float64 on identical walkers and parameters
+        it.energies()
+        it64.energies()
+        em, e64 = it.e.real.double(), it64.e.real.double()
+        it.jacobian()
+        it64.jacobian()
+        d_mixed = minsr_step(it.O.clone(), it.e, su.lam, "bf16", n_refine=it.n_refine)
+        d_gram = minsr_step(it.O.double(), it64.e, su.lam, "fp64")
+        d_64 = minsr_step(it64.O.clone(), it64.e, su.lam, "fp64")
+        n64 = float(d_64.norm())
+        acc = {"dE_per_electron": float((em.mean() - e64.mean()).abs()) / su.N,
+               "dE_target": 1e-4,
+               "dvar_rel": float((em.var() - e64.var()).abs() / e64.var()),
+               "dvar_target": 0.05,
+               "dtheta_rel": float((d_mixed - d_64).norm()) / n64,
+               "dtheta_rel_network_only": float((d_gram - d_64).norm()) / n64,
+               "E_fp64": float(e64.mean()), "E_mixed": float(em.mean())}
         it64.step()
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -246,7 +265,7 @@ def run_ours(a, rank, world):
             "peak_source": f"{src} (burst bf16)", "gram_ms": g_ms,
             "traffic": None, "algorithmic_flops": gflop}
     return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof, clocks=clk,
-                launches=launches, su=su, model=model, P=it.P)
+                launches=launches, su=su, model=model, P=it.P, acc=acc)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -381,7 +400,8 @@ def main():
         "eloc_evals_per_s": world * W / (ph["local_energy_ms"] * 1e-3),
         "phases_ms": ph, "energy": {"mean": r["stats"][0], "err": r["stats"][1],
                                     "var": r["stats"][2]},
-        "fp64_plain": r["fp64"], "roofline": r["roofline"], "cpu_baseline": cpu,
+        "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "roofline": r["roofline"],
+        "cpu_baseline": cpu,
         "e2e": r["e2e"], "clocks": r["clocks"], "gpu_launches": int(r["launches"]),
     }
     print(json.dumps(line), flush=True)

@@ -506,13 +506,33 @@ __global__ void k_gram_blocksums(const double* __restrict__ rs, int n, int W,
   }
 }
 
+// T <- C T C + (alpha / W) [same half]: alpha = mean diagonal of T (from S[4]) lifts the two
+// exact null directions of the centred Gram to a well-conditioned eigenvalue, so the factor of a
+// low-precision Gram is a uniform preconditioner there (the energies are centred, so the
+// solution has no component along them and dtheta = Otil^T y ignores them).
 __global__ void k_gram_center(double* __restrict__ T, int n, int W, const double* __restrict__ rs,
                               const double* __restrict__ S) {
   const int i = blockIdx.y;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > i) return;
   const int a = i >= W, b = j >= W;
-  T[(size_t)i * n + j] += -rs[2 * i + b] - rs[2 * j + a] + S[2 * a + b];
+  double t = T[(size_t)i * n + j] - rs[2 * i + b] - rs[2 * j + a] + S[2 * a + b];
+  if (a == b) t += S[4] / W;
+  T[(size_t)i * n + j] = t;
+}
+
+__global__ void k_mean_diag(const double* __restrict__ T, int n, double* __restrict__ out) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += T[(size_t)i * n + i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    *out = t / n;
+  }
 }
 
 // error-free transformations (Knuth TwoSum, FMA TwoProduct) for compensated dot products
@@ -754,7 +774,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * n);              // refinement residual
   add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
-  add(sizeof(double) * (2 * n + 4));    // Gram row sums (double centring)
+  add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
   add(sizeof(double) * CB);             // triangular-solve block
   add(sizeof(int) * 4);                 // status
   add(sizeof(double));                  // pivot floor
@@ -799,7 +819,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* tmpK = ws.take<double>(P);
   double* tmpK_lo = ws.take<double>(P);
   double* xb = ws.take<double>(CB);
-  double* rsum = ws.take<double>(2 * (size_t)n + 4);
+  double* rsum = ws.take<double>(2 * (size_t)n + 5);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
   const size_t part_elems = minsr_part_elems(W);
@@ -844,19 +864,22 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
     NQS_CHECK_LAUNCH("k_gram_rowsums");
     k_gram_blocksums<<<1, 1024, 0, st>>>(rsum, n, W, rsum + 2 * n);
     NQS_CHECK_LAUNCH("k_gram_blocksums");
+    k_mean_diag<<<1, 1024, 0, st>>>(T, n, rsum + 2 * n + 4);
+    NQS_CHECK_LAUNCH("k_mean_diag");
     k_gram_center<<<dim3((n + 255) / 256, n), 256, 0, st>>>(T, n, W, rsum, rsum + 2 * n);
     NQS_CHECK_LAUNCH("k_gram_center");
   }
   k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
-  // A tensor-core Gram carries rounding noise ~ u sqrt(Tii Tjj) (u = 2^-8 BF16, 2^-11 TF32)
-  // that can exceed lam along the null directions the centring creates, so its factor is a
-  // preconditioner built with a pivot floor; the refinement below solves the exact system.
+  // A tensor-core Gram carries rounding noise ~ u sqrt(Tii Tjj) (u = 2^-8 BF16, 2^-11 TF32); its
+  // factor only preconditions the refinement below, which solves the exact system. The null
+  // directions of the centring were lifted above; a small pivot floor guards against noise that
+  // still makes a pivot non-positive.
   const double* floor_p = nullptr;
   if (gram_prec != 0) {
     double* fl = ws.take<double>(1);
     if (!fl) return NQS_ERR_WORKSPACE;
-    k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-8 : 0x1p-11, fl);
+    k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-16 : 0x1p-20, fl);
     NQS_CHECK_LAUNCH("k_pivot_floor");
     floor_p = fl;
   }

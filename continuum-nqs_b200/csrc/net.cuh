@@ -14,8 +14,19 @@ struct BlockW {
   const T *w0, *b0, *w1, *b1;
 };
 
+// K-major float32 weight copies for the tensor-core row GEMMs of the mixed path.
+struct TcNet {
+  int on;
+  const float *wqkv[NQS_MAX_DEPTH], *bqkv[NQS_MAX_DEPTH], *wo[NQS_MAX_DEPTH];
+  const float *w0[NQS_MAX_DEPTH], *w1[NQS_MAX_DEPTH];
+  const float *wbf;
+  int npad_qkv, npad_bf;
+  int* err;
+};
+
 template <typename T>
 struct NetW {
+  TcNet tc;
   const T *emb_w, *emb_b;
   BlockW<T> blk[NQS_MAX_DEPTH];
   const T *lnf_s, *lnf_b;
@@ -86,6 +97,15 @@ size_t per_sample_O_scratch(const ModelConst& mc, int W);
 template <typename T, typename TO>
 int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
                      const double* R, const int32_t* S, int W, TO* O, Arena& ws,
+                     cudaStream_t st);
+
+// tensor-core row GEMM (gemm_tc.cu)
+bool rowgemm_tc_ok(int K, int ldx, int Nout);
+int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
+               const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
+               cudaStream_t st);
+size_t tc_weights_bytes(const NqsModelDesc& d);
+int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,
                      cudaStream_t st);
 
 // Default row budget of one network chunk.

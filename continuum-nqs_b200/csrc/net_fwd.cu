@@ -48,13 +48,13 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
     return NQS_ERR_WORKSPACE;
   }
   const bool tan = jb.n_tan > 0;
-  const size_t hsm = head_smem(N, mc.nG, jb.n_tan, tan);
+  const bool tcn = sizeof(T) == 4 && w.tc.on;
   const size_t asm_ = attention_smem<T>(N, d / mc.H);
   static bool attr_set = false;  // per-instantiation one-time opt-in to large shared memory
   if (!attr_set) {
     cudaFuncSetAttribute(k_attention<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_head<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(k_head<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_head<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+    cudaFuncSetAttribute(k_head<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
     attr_set = true;
   }
   for (int j0 = 0; j0 < jb.n_jobs; j0 += jobs_per_chunk) {
@@ -76,54 +76,86 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
                                                      bw.ln0_s, bw.ln0_b, Hb);
       NQS_CHECK_LAUNCH("k_layernorm");
       GemmArgs<T> g{};
-      g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
-      g.Y = Big; g.ldy = 3 * d; g.Res = nullptr; g.ldr = 0; g.trans_w = 0; g.nseg = 3;
-      g.seg[0] = GemmSeg<T>{bw.wq, bw.bq, d, d, 0, 0};
-      g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
-      g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      if (tcn) {
+        NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wqkv[b], w.tc.npad_qkv, 3 * d,
+                           w.tc.bqkv[b], C, nullptr, 0, (float*)Big, 3 * d, w.tc.err, st));
+      } else {
+        g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
+        g.Y = Big; g.ldy = 3 * d; g.Res = nullptr; g.ldr = 0; g.trans_w = 0; g.nseg = 3;
+        g.seg[0] = GemmSeg<T>{bw.wq, bw.bq, d, d, 0, 0};
+        g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
+        g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
+        NQS_TRY(launch_gemm<T>(g, st));
+      }
       k_attention<T><<<cb.n_jobs * mc.H, 128, asm_, st>>>(cb.n_jobs, N, C, cb.n_tan, cb.has_lap,
                                                           d, mc.H, Big, Att);
       NQS_CHECK_LAUNCH("k_attention");
-      g = GemmArgs<T>{};
-      g.X = Att; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
-      g.Y = X; g.ldy = d; g.Res = X; g.ldr = d; g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      if (tcn) {
+        NQS_TRY(rowgemm_tc((const float*)Att, d, rows, d, w.tc.wo[b], d, d, (const float*)bw.bo,
+                           C, (const float*)X, d, (float*)X, d, w.tc.err, st));
+      } else {
+        g = GemmArgs<T>{};
+        g.X = Att; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
+        g.Y = X; g.ldy = d; g.Res = X; g.ldr = d; g.nseg = 1;
+        g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
+        NQS_TRY(launch_gemm<T>(g, st));
+      }
       k_layernorm<T><<<(ntok + 7) / 8, 256, 0, st>>>(ntok, C, cb.n_tan, cb.has_lap, d, X,
                                                      bw.ln1_s, bw.ln1_b, Hb);
       NQS_CHECK_LAUNCH("k_layernorm");
       const int D = mc.ff * d;
-      g = GemmArgs<T>{};
-      g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
-      g.Y = Big; g.ldy = D; g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      if (tcn) {
+        NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.w0[b], D, D, (const float*)bw.b0, C,
+                           nullptr, 0, (float*)Big, D, w.tc.err, st));
+      } else {
+        g = GemmArgs<T>{};
+        g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
+        g.Y = Big; g.ldy = D; g.nseg = 1;
+        g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
+        NQS_TRY(launch_gemm<T>(g, st));
+      }
       const size_t nel = (size_t)ntok * D;
       k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)ntok, C, cb.n_tan,
                                                                cb.has_lap, D, Big);
       NQS_CHECK_LAUNCH("k_gelu");
-      g = GemmArgs<T>{};
-      g.X = Big; g.ldx = D; g.rows = rows; g.K = D; g.C = C;
-      g.Y = X; g.ldy = d; g.Res = X; g.ldr = d; g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      if (tcn) {
+        NQS_TRY(rowgemm_tc((const float*)Big, D, rows, D, w.tc.w1[b], d, d, (const float*)bw.b1,
+                           C, (const float*)X, d, (float*)X, d, w.tc.err, st));
+      } else {
+        g = GemmArgs<T>{};
+        g.X = Big; g.ldx = D; g.rows = rows; g.K = D; g.C = C;
+        g.Y = X; g.ldy = d; g.Res = X; g.ldr = d; g.nseg = 1;
+        g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
+        NQS_TRY(launch_gemm<T>(g, st));
+      }
     }
     k_layernorm<T><<<(ntok + 7) / 8, 256, 0, st>>>(ntok, C, cb.n_tan, cb.has_lap, d, X, w.lnf_s,
                                                    w.lnf_b, Hb);
     NQS_CHECK_LAUNCH("k_layernorm");
     const int KN = mc.K * N;
-    GemmArgs<T> g{};
-    g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
-    g.Y = Big; g.ldy = 2 * KN; g.nseg = 2;
-    g.seg[0] = GemmSeg<T>{w.bf_w_re, w.bf_b_re, KN, KN, 0, 0};
-    g.seg[1] = GemmSeg<T>{w.bf_w_im, w.bf_b_im, KN, KN, KN, 0};
-    NQS_TRY(launch_gemm<T>(g, st));
-    const int jout = j0;
-    if (tan) {
-      k_head<T, true><<<cb.n_jobs, 256, hsm, st>>>(cb, mc, Big, 2 * KN, hp, out, jout);
+    if (tcn) {
+      NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wbf, w.tc.npad_bf, 2 * KN,
+                         (const float*)w.bf_b_re, C, nullptr, 0, (float*)Big, 2 * KN, w.tc.err,
+                         st));
     } else {
-      k_head<T, false><<<cb.n_jobs, 256, hsm, st>>>(cb, mc, Big, 2 * KN, hp, out, jout);
+      GemmArgs<T> g{};
+      g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
+      g.Y = Big; g.ldy = 2 * KN; g.nseg = 2;
+      g.seg[0] = GemmSeg<T>{w.bf_w_re, w.bf_b_re, KN, KN, 0, 0};
+      g.seg[1] = GemmSeg<T>{w.bf_w_im, w.bf_b_im, KN, KN, KN, 0};
+      NQS_TRY(launch_gemm<T>(g, st));
+    }
+    const int jout = j0;
+    const HeadPlan hpl = head_plan(N, mc.nG, mc.K, cb.n_tan, tan);
+    const unsigned hgrid = (unsigned)((cb.n_jobs + hpl.jpc - 1) / hpl.jpc);
+    if (tan) {
+      k_head<T, true><<<hgrid, 32 * hpl.wpc, hpl.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
+                                                              hpl.jpc, hpl.job_bytes,
+                                                              hpl.warp_bytes);
+    } else {
+      k_head<T, false><<<hgrid, 32 * hpl.wpc, hpl.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
+                                                               hpl.jpc, hpl.job_bytes,
+                                                               hpl.warp_bytes);
     }
     NQS_CHECK_LAUNCH("k_head");
   }

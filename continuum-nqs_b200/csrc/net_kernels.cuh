@@ -673,46 +673,170 @@ __device__ __forceinline__ void min_image(const ModelConst& mc, double dx, doubl
   *oy = f0 * mc.A[2] + f1 * mc.A[3];
 }
 
+// --------------------------------------------------------------------------------------------
+// warp-synchronous complex LU (value) / Gauss-Jordan (with inverse) on one N x N matrix in shared
+// memory; partial pivoting on |re|+|im| with the first index on ties (as LAPACK getrf).
+// M rows = orbitals a, columns = electrons j; inv (nullable) receives M^-1 indexed [j][a].
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ void warp_factor(cplx* M, cplx* inv, int N, cplx* fcol, cplx* logdet,
+                                            int* singular) {
+  const int lane = threadIdx.x & 31;
+  if (inv)
+    for (int idx = lane; idx < N * N; idx += 32) {
+      const int r = idx / N, c = idx - r * N;
+      inv[idx] = mk(r == c ? 1.0 : 0.0, 0.0);
+    }
+  double logabs = 0.0;
+  cplx sgn = mk(1.0, 0.0);
+  int sing = 0;
+  __syncwarp();
+  for (int c = 0; c < N; ++c) {
+    double best = -1.0;
+    int bi = c;
+    for (int r = c + lane; r < N; r += 32) {
+      const double v = cabs1(M[r * N + c]);
+      if (v > best) {
+        best = v;
+        bi = r;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (bi != c) {
+      for (int col = lane; col < N; col += 32) {
+        cplx t = M[c * N + col];
+        M[c * N + col] = M[bi * N + col];
+        M[bi * N + col] = t;
+        if (inv) {
+          t = inv[c * N + col];
+          inv[c * N + col] = inv[bi * N + col];
+          inv[bi * N + col] = t;
+        }
+      }
+      sgn = mk(-sgn.re, -sgn.im);
+    }
+    __syncwarp();
+    const cplx pv = M[c * N + c];
+    const double apv = hypot(pv.re, pv.im);
+    if (apv == 0.0) {
+      sing = 1;
+    } else {
+      logabs += log(apv);
+      sgn = cmul(sgn, mk(pv.re / apv, pv.im / apv));
+    }
+    const cplx ipv = (apv == 0.0) ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
+    for (int r = lane; r < N; r += 32)
+      if (r != c && (inv || r > c)) fcol[r] = cmul(M[r * N + c], ipv);
+    __syncwarp();
+    const int nc = N - c - 1;
+    if (inv) {
+      const int wd = nc + N;
+      for (int idx = lane; idx < N * wd; idx += 32) {
+        const int r = idx / wd, cc = idx - r * wd;
+        if (r == c) continue;
+        if (cc < nc) {
+          const int col = c + 1 + cc;
+          M[r * N + col] = csub(M[r * N + col], cmul(fcol[r], M[c * N + col]));
+        } else {
+          const int col = cc - nc;
+          inv[r * N + col] = csub(inv[r * N + col], cmul(fcol[r], inv[c * N + col]));
+        }
+      }
+      __syncwarp();
+      for (int col = lane; col < N; col += 32) {
+        if (col > c) M[c * N + col] = cmul(M[c * N + col], ipv);
+        inv[c * N + col] = cmul(inv[c * N + col], ipv);
+      }
+    } else {
+      for (int idx = lane; idx < nc * nc; idx += 32) {
+        const int r = c + 1 + idx / nc, col = c + 1 + idx % nc;
+        M[r * N + col] = csub(M[r * N + col], cmul(fcol[r], M[c * N + col]));
+      }
+    }
+    __syncwarp();
+  }
+  *logdet = sing ? mk(-INFINITY, 0.0) : mk(logabs, atan2(sgn.im, sgn.re));
+  *singular = sing;
+}
+
+// Shared-memory plan of k_head: per job slot env[N*N], ph[nG*N], per-det results
+// (logdet, lap part, sum of squares, singular flag) and dL_k[K][n_tan]; per warp M[N*N]
+// (+ inv[N*N], B[N*N] with tangents) and fcol[N].
+struct HeadPlan {
+  int wpc, jpc;
+  size_t job_bytes, warp_bytes, bytes;
+};
+__host__ __device__ inline size_t head_job_bytes(int N, int nG, int K, int n_tan) {
+  return 16 * ((size_t)N * N + (size_t)nG * N + 3 * (size_t)K + (size_t)K * n_tan) +
+         8 * 2 * (size_t)N + 4 * ((size_t)N + K) + 16;
+}
+__host__ __device__ inline size_t head_warp_bytes(int N, bool tan) {
+  return 16 * ((tan ? 3 : 1) * (size_t)N * N + (size_t)N);
+}
+inline HeadPlan head_plan(int N, int nG, int K, int n_tan, bool tan) {
+  HeadPlan p;
+  p.wpc = tan ? 4 : 8;
+  p.job_bytes = head_job_bytes(N, nG, K, tan ? n_tan : 0);
+  p.warp_bytes = head_warp_bytes(N, tan);
+  for (;;) {
+    p.jpc = std::max(1, p.wpc / K);
+    p.bytes = p.jpc * p.job_bytes + p.wpc * p.warp_bytes;
+    if (p.bytes <= 200 * 1024 || p.wpc == 1) break;
+    p.wpc /= 2;
+  }
+  return p;
+}
+
 template <typename TIN, bool TAN>
 __global__ void __launch_bounds__(256) k_head(JobBatch jb, ModelConst mc, const TIN* __restrict__ BF,
-                                              int ldbf, HeadParams hp, HeadOut out, int j_out0) {
-  const int job = blockIdx.x;
+                                              int ldbf, HeadParams hp, HeadOut out, int j_out0,
+                                              int jpc, size_t job_bytes, size_t warp_bytes) {
   const int N = jb.N, C = jb.C, nG = mc.nG, K = mc.K;
   const int n_tan = TAN ? jb.n_tan : 0;
   const bool has_lap = TAN && jb.has_lap;
-  const JobInfo ji = job_info(jb, job);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int job0 = blockIdx.x * jpc;
+  const int njob = min(jpc, jb.n_jobs - job0);
   extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* env = reinterpret_cast<cplx*>(smraw);
-  cplx* Wk = env + N * N;
-  cplx* inv = TAN ? Wk + N * N : nullptr;
-  cplx* Bm = TAN ? inv + N * N : nullptr;
-  cplx* ph = (TAN ? Bm : Wk) + N * N;
-  cplx* G = ph + nG * N;
-  cplx* dLk = G + n_tan;
-  cplx* fcol = dLk + n_tan;
-  cplx* red = fcol + N;  // 40 entries: [0..31] reductions, [33] logdet
-  double* rx = reinterpret_cast<double*>(red + 40);
-  double* ry = rx + N;
-  int* sp = reinterpret_cast<int*>(ry + N);
-  int* piv_s = sp + N;
-  int* sing_s = piv_s + 1;
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int te_lo = ji.tan_e0, te_hi = ji.tan_e0 + n_tan / 2;  // tangent electrons [lo, hi)
-
-  for (int i = tid; i < N; i += nth) {
+  // ---- carve ----
+  auto jbase = [&](int j) -> unsigned char* { return smraw + (size_t)j * job_bytes; };
+  auto j_env = [&](int j) { return reinterpret_cast<cplx*>(jbase(j)); };
+  auto j_ph = [&](int j) { return j_env(j) + N * N; };
+  auto j_ld = [&](int j) { return j_ph(j) + nG * N; };     // K
+  auto j_lapk = [&](int j) { return j_ld(j) + K; };         // K
+  auto j_sq = [&](int j) { return j_lapk(j) + K; };         // K
+  auto j_dLk = [&](int j) { return j_sq(j) + K; };          // K * n_tan
+  auto j_rx = [&](int j) { return reinterpret_cast<double*>(j_dLk(j) + K * n_tan); };
+  auto j_ry = [&](int j) { return j_rx(j) + N; };
+  auto j_sp = [&](int j) { return reinterpret_cast<int*>(j_ry(j) + N); };
+  auto j_sing = [&](int j) { return j_sp(j) + N; };         // K
+  unsigned char* wbase = smraw + (size_t)jpc * job_bytes + (size_t)warp * warp_bytes;
+  cplx* Mw = reinterpret_cast<cplx*>(wbase);
+  cplx* Iw = TAN ? Mw + N * N : nullptr;
+  cplx* Bw = TAN ? Iw + N * N : nullptr;
+  cplx* fw = (TAN ? Bw : Mw) + N * N;
+  // ---- phase 1: positions, spins, phases, envelopes of this CTA's jobs ----
+  for (int idx = threadIdx.x; idx < njob * N; idx += blockDim.x) {
+    const int j = idx / N, i = idx - j * N;
+    const JobInfo ji = job_info(jb, job0 + j);
     const double* r = jb.R + ((size_t)ji.walker * N + i) * 2;
-    rx[i] = r[0];
-    ry[i] = r[1];
-    sp[i] = job_spin(jb, ji, i);
+    j_rx(j)[i] = r[0];
+    j_ry(j)[i] = r[1];
+    j_sp(j)[i] = job_spin(jb, ji, i);
   }
-  for (int t = tid; t < n_tan; t += nth) G[t] = mk(0, 0);
   __syncthreads();
-  for (int idx = tid; idx < nG * N; idx += nth) {  // exp(i G.r) (psiformer.py:146)
-    const int g = idx / N, i = idx - g * N;
-    const double x = mc.Gs[2 * g] * rx[i] + mc.Gs[2 * g + 1] * ry[i];
-    double s, c;
-    sincos(x, &s, &c);
-    ph[idx] = mk(c, s);
+  for (int idx = threadIdx.x; idx < njob * nG * N; idx += blockDim.x) {
+    const int j = idx / (nG * N), r = idx - j * nG * N, g = r / N, i = r - g * N;
+    double sn, cs;
+    sincos(mc.Gs[2 * g] * j_rx(j)[i] + mc.Gs[2 * g + 1] * j_ry(j)[i], &sn, &cs);
+    j_ph(j)[r] = mk(cs, sn);
   }
   __syncthreads();
   auto Weff = [&](int a, int g, int s) -> cplx {
@@ -721,64 +845,44 @@ __global__ void __launch_bounds__(256) k_head(JobBatch jb, ModelConst mc, const 
     if (mc.learnable_env) w = cadd(w, mk(hp.dW[o], hp.dW[(size_t)N * nG * 2 + o]));
     return w;
   };
-  for (int idx = tid; idx < N * N; idx += nth) {  // env[a,i] (psiformer.py:147-148)
-    const int a = idx / N, i = idx - a * N;
+  for (int idx = threadIdx.x; idx < njob * N * N; idx += blockDim.x) {
+    const int j = idx / (N * N), r = idx - j * N * N, a = r / N, i = r - a * N;
+    const int s = j_sp(j)[i];
+    const cplx* ph = j_ph(j);
     cplx e = mk(0, 0);
-    for (int g = 0; g < nG; ++g) cfma(e, ph[g * N + i], Weff(a, g, sp[i]));
-    env[idx] = e;
+    for (int g = 0; g < nG; ++g) cfma(e, ph[g * N + i], Weff(a, g, s));
+    j_env(j)[r] = e;
   }
   __syncthreads();
-
-  // ---- Jastrow value and Laplacian ----
-  double J = 0.0, lapJ = 0.0;
-  if (mc.use_jastrow) {
-    double accJ = 0.0, accL = 0.0;
-    for (int idx = tid; idx < N * N; idx += nth) {
-      const int i = idx / N, jj = idx - i * N;
-      if (jj <= i) continue;
-      double dx, dy;
-      min_image(mc, rx[i] - rx[jj], ry[i] - ry[jj], &dx, &dy);
-      const double d2 = dx * dx + dy * dy;
-      const double r = sqrt(d2 + 1e-12);
-      double u, u1, u2;
-      jastrow_u(mc, hp, r, sp[i] == sp[jj], &u, &u1, &u2);
-      accJ += u;
-      if (has_lap) {
-        const double l = u2 * d2 / (r * r) + u1 * (2.0 / r - d2 / (r * r * r));
-        const int cnt = (i >= te_lo && i < te_hi) + (jj >= te_lo && jj < te_hi);
-        accL += l * cnt;
-      }
-    }
-    const cplx s = block_sum_c(mk(accJ, accL), red);
-    J = s.re;
-    lapJ = s.im;
-  }
-
-  auto bfval = [&](int c, int k, int a, int i) -> cplx {
-    const TIN* p = BF + (((size_t)job * N + i) * C + c) * ldbf;
-    return mk((double)p[k * N + a], (double)p[K * N + k * N + a]);
-  };
-
-  // ---- determinants with an online complex log-sum-exp (max-Re shift) ----
-  double m_run = -INFINITY;
-  cplx ssum = mk(0, 0), Lam = mk(0, 0), L_first = mk(0, 0), lap_first = mk(0, 0);
-  for (int k = 0; k < K; ++k) {
-    for (int idx = tid; idx < N * N; idx += nth) {
+  // ---- phase 2: one warp per (job, determinant) ----
+  for (int q = warp; q < njob * K; q += nwarp) {
+    const int j = q / K, k = q - j * K;
+    const int job = job0 + j;
+    const JobInfo ji = job_info(jb, job);
+    const int te_lo = ji.tan_e0, te_hi = ji.tan_e0 + n_tan / 2;
+    const cplx* env = j_env(j);
+    const cplx* ph = j_ph(j);
+    const int* sp = j_sp(j);
+    auto bfval = [&](int c, int a, int i) -> cplx {
+      const TIN* p = BF + (((size_t)job * N + i) * C + c) * ldbf;
+      return mk((double)p[k * N + a], (double)p[K * N + k * N + a]);
+    };
+    for (int idx = lane; idx < N * N; idx += 32) {
       const int a = idx / N, i = idx - a * N;
-      const cplx b0 = bfval(0, k, a, i);
-      Wk[idx] = cmul(env[idx], mk(1.0 + b0.re, b0.im));  // M = env (1 + bf)
+      const cplx b0 = bfval(0, a, i);
+      Mw[idx] = cmul(env[idx], mk(1.0 + b0.re, b0.im));
     }
-    __syncthreads();
-    det_factor(Wk, inv, N, piv_s, fcol, red + 33, sing_s);
-    const cplx logdet = red[33];
-    const int sing = *sing_s;
+    __syncwarp();
+    cplx logdet;
+    int sing;
+    warp_factor(Mw, Iw, N, fw, &logdet, &sing);
     cplx lapk = mk(0, 0), sq = mk(0, 0);
-    if (TAN) {
+    if (TAN && !sing) {
       if (has_lap) {  // tr(M^-1 Lap M)
         cplx acc = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {
+        for (int idx = lane; idx < N * N; idx += 32) {
           const int a = idx / N, i = idx - a * N;
-          cplx lm = cmul(env[idx], bfval(C - 1, k, a, i));
+          cplx lm = cmul(env[idx], bfval(C - 1, a, i));
           if (i >= te_lo && i < te_hi) {
             cplx dxe = mk(0, 0), dye = mk(0, 0), le = mk(0, 0);
             for (int g = 0; g < nG; ++g) {
@@ -788,124 +892,180 @@ __global__ void __launch_bounds__(256) k_head(JobBatch jb, ModelConst mc, const 
               cfma(dye, pw, mk(0, gy));
               le = cadd(le, cscale(pw, -(gx * gx + gy * gy)));
             }
-            const cplx b0 = bfval(0, k, a, i);
+            const cplx b0 = bfval(0, a, i);
             const int tx = 2 * (i - te_lo);
             lm = cadd(lm, cmul(le, mk(1.0 + b0.re, b0.im)));
-            lm = cadd(lm, cscale(cmul(dxe, bfval(1 + tx, k, a, i)), 2.0));
-            lm = cadd(lm, cscale(cmul(dye, bfval(2 + tx, k, a, i)), 2.0));
+            lm = cadd(lm, cscale(cmul(dxe, bfval(1 + tx, a, i)), 2.0));
+            lm = cadd(lm, cscale(cmul(dye, bfval(2 + tx, a, i)), 2.0));
           }
-          cfma(acc, inv[i * N + a], lm);
+          cfma(acc, Iw[i * N + a], lm);
         }
-        lapk = block_sum_c(acc, red);
+        acc.re = warp_sum(acc.re);
+        acc.im = warp_sum(acc.im);
+        lapk = acc;
       }
       for (int t = 0; t < n_tan; ++t) {
         const int e = te_lo + t / 2, bax = t & 1;
-        for (int idx = tid; idx < N * N; idx += nth) {  // D_t = d_t M
+        for (int idx = lane; idx < N * N; idx += 32) {  // D_t = d_t M
           const int a = idx / N, i = idx - a * N;
-          cplx dm = cmul(env[idx], bfval(1 + t, k, a, i));
+          cplx dm = cmul(env[idx], bfval(1 + t, a, i));
           if (i == e) {
             cplx de = mk(0, 0);
             for (int g = 0; g < nG; ++g)
               cfma(de, cmul(ph[g * N + i], Weff(a, g, sp[i])), mk(0, mc.Gs[2 * g + bax]));
-            const cplx b0 = bfval(0, k, a, i);
+            const cplx b0 = bfval(0, a, i);
             dm = cadd(dm, cmul(de, mk(1.0 + b0.re, b0.im)));
           }
-          Wk[idx] = dm;
+          Mw[idx] = dm;
         }
-        __syncthreads();
+        __syncwarp();
         cplx trb = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {  // B = M^-1 D_t
+        for (int idx = lane; idx < N * N; idx += 32) {  // B = M^-1 D_t
           const int i = idx / N, i2 = idx - i * N;
-          cplx s = mk(0, 0);
-          for (int a = 0; a < N; ++a) cfma(s, inv[i * N + a], Wk[a * N + i2]);
-          Bm[idx] = s;
-          if (i == i2) trb = cadd(trb, s);
+          cplx s2 = mk(0, 0);
+          for (int a = 0; a < N; ++a) cfma(s2, Iw[i * N + a], Mw[a * N + i2]);
+          Bw[idx] = s2;
+          if (i == i2) trb = cadd(trb, s2);
         }
-        __syncthreads();
+        __syncwarp();
         cplx trb2 = mk(0, 0);
-        for (int idx = tid; idx < N * N; idx += nth) {
+        for (int idx = lane; idx < N * N; idx += 32) {
           const int i = idx / N, i2 = idx - i * N;
-          cfma(trb2, Bm[idx], Bm[i2 * N + i]);
+          cfma(trb2, Bw[idx], Bw[i2 * N + i]);
         }
-        const cplx tr1 = block_sum_c(trb, red);
-        const cplx tr2 = block_sum_c(trb2, red);
-        if (tid == 0) dLk[t] = tr1;
-        lapk = csub(lapk, tr2);
-        cfma(sq, tr1, tr1);
+        trb.re = warp_sum(trb.re);
+        trb.im = warp_sum(trb.im);
+        trb2.re = warp_sum(trb2.re);
+        trb2.im = warp_sum(trb2.im);
+        if (lane == 0) j_dLk(j)[k * n_tan + t] = trb;
+        lapk = csub(lapk, trb2);
+        cfma(sq, trb, trb);
+        __syncwarp();
       }
-      __syncthreads();
     }
-    if (k == 0) {
-      L_first = logdet;
-      lap_first = lapk;
+    if (lane == 0) {
+      j_ld(j)[k] = logdet;
+      j_lapk(j)[k] = lapk;
+      j_sq(j)[k] = sq;
+      j_sing(j)[k] = sing;
     }
-    const cplx wk = (K > 1 && hp.det_logw) ? mk(hp.det_logw[k], hp.det_logw[K + k]) : mk(0, 0);
-    const cplx z = cadd(logdet, wk);
-    if (!sing) {
-      if (z.re > m_run) {
-        const double sc = (m_run == -INFINITY) ? 0.0 : exp(m_run - z.re);
-        ssum = cscale(ssum, sc);
-        Lam = cscale(Lam, sc);
-        for (int t = tid; t < n_tan; t += nth) G[t] = cscale(G[t], sc);
-        m_run = z.re;
+    __syncwarp();
+  }
+  __syncthreads();
+  // ---- phase 3: one warp per job: log-sum-exp over dets (max-Re shift), Jastrow, outputs ----
+  for (int j = warp; j < njob; j += nwarp) {
+    const int job = job0 + j;
+    const JobInfo ji = job_info(jb, job);
+    const int te_lo = ji.tan_e0, te_hi = ji.tan_e0 + n_tan / 2;
+    const int jo = j_out0 + job;
+    const cplx* ld = j_ld(j);
+    const int* sg = j_sing(j);
+    const double* rx = j_rx(j);
+    const double* ry = j_ry(j);
+    const int* sp = j_sp(j);
+    double m = -INFINITY;
+    for (int k = 0; k < K; ++k) {
+      const double zr = ld[k].re + ((K > 1 && hp.det_logw) ? hp.det_logw[k] : 0.0);
+      if (!sg[k] && zr > m) m = zr;
+    }
+    const bool all_sing = (m == -INFINITY);
+    cplx ssum = mk(0, 0);
+    cplx p[NQS_MAX_DETS];
+    for (int k = 0; k < K; ++k) {
+      if (sg[k]) {
+        p[k] = mk(0, 0);
+        continue;
       }
-      const cplx e = cexp_(mk(z.re - m_run, z.im));
-      ssum = cadd(ssum, e);
-      Lam = cadd(Lam, cmul(e, cadd(lapk, sq)));
-      for (int t = tid; t < n_tan; t += nth) cfma(G[t], e, dLk[t]);
+      const cplx wk = (K > 1 && hp.det_logw) ? mk(hp.det_logw[k], hp.det_logw[K + k]) : mk(0, 0);
+      p[k] = cexp_(mk(ld[k].re + wk.re - m, ld[k].im + wk.im));
+      ssum = cadd(ssum, p[k]);
     }
-    __syncthreads();
-  }
-
-  // ---- combine, add Jastrow, write ----
-  const int jo = j_out0 + job;
-  const bool all_sing = (m_run == -INFINITY);
-  cplx L;
-  if (K == 1) {
-    L = L_first;
-  } else {
-    L = all_sing ? mk(-INFINITY, 0.0)
-                 : mk(m_run + log(hypot(ssum.re, ssum.im)), atan2(ssum.im, ssum.re));
-  }
-  cplx sumsq_local = mk(0, 0);
-  for (int t = tid; t < n_tan; t += nth) {
-    cplx g = all_sing ? mk(NAN, NAN) : (K == 1 ? dLk[t] : cdiv(G[t], ssum));
-    cfma(sumsq_local, g, g);
+    cplx L;
+    if (K == 1) {
+      L = ld[0];
+    } else {
+      L = all_sing ? mk(-INFINITY, 0.0)
+                   : mk(m + log(hypot(ssum.re, ssum.im)), atan2(ssum.im, ssum.re));
+      if (!all_sing) {
+        const cplx inv_s = cdiv(mk(1.0, 0.0), ssum);
+        for (int k = 0; k < K; ++k) p[k] = cmul(p[k], inv_s);
+      }
+    }
+    if (K == 1) p[0] = mk(1.0, 0.0);
+    // Jastrow value and Laplacian
+    double J = 0.0, lapJ = 0.0;
     if (mc.use_jastrow) {
-      const int e = te_lo + t / 2, bax = t & 1;
-      double gj = 0.0;
-      for (int jj = 0; jj < N; ++jj) {
-        if (jj == e) continue;
+      for (int idx = lane; idx < N * N; idx += 32) {
+        const int i = idx / N, jj = idx - i * N;
+        if (jj <= i) continue;
         double dx, dy;
-        min_image(mc, rx[e] - rx[jj], ry[e] - ry[jj], &dx, &dy);
-        const double r = sqrt(dx * dx + dy * dy + 1e-12);
+        min_image(mc, rx[i] - rx[jj], ry[i] - ry[jj], &dx, &dy);
+        const double d2 = dx * dx + dy * dy;
+        const double r = sqrt(d2 + 1e-12);
         double u, u1, u2;
-        jastrow_u(mc, hp, r, sp[e] == sp[jj], &u, &u1, &u2);
-        gj += u1 * (bax == 0 ? dx : dy) / r;
+        jastrow_u(mc, hp, r, sp[i] == sp[jj], &u, &u1, &u2);
+        J += u;
+        if (has_lap) {
+          const int cnt = (i >= te_lo && i < te_hi) + (jj >= te_lo && jj < te_hi);
+          lapJ += (u2 * d2 / (r * r) + u1 * (2.0 / r - d2 / (r * r * r))) * cnt;
+        }
       }
-      g.re += gj;
+      J = warp_sum(J);
+      lapJ = warp_sum(lapJ);
     }
-    if (out.dL) out.dL[(size_t)jo * jb.n_tan + t] = g;
-  }
-  cplx sumsq = mk(0, 0);
-  if (has_lap && K > 1) sumsq = block_sum_c(sumsq_local, red);
-  if (tid == 0) {
-    if (mc.use_jastrow) L.re += J;
-    if (out.L) out.L[jo] = L;
-    if (has_lap && out.lap) {
-      cplx lap;
-      if (K == 1)
-        lap = lap_first;
-      else
-        lap = all_sing ? mk(NAN, NAN) : csub(cdiv(Lam, ssum), sumsq);
-      lap.re += lapJ;
-      out.lap[jo] = lap;
+    cplx sumsq = mk(0, 0);
+    for (int t = lane; t < n_tan; t += 32) {
+      cplx g = mk(0, 0);
+      if (all_sing) {
+        g = mk(NAN, NAN);
+      } else {
+        for (int k = 0; k < K; ++k)
+          if (!sg[k]) cfma(g, p[k], j_dLk(j)[k * n_tan + t]);
+      }
+      cfma(sumsq, g, g);
+      if (mc.use_jastrow) {
+        const int e = te_lo + t / 2, bax = t & 1;
+        double gj = 0.0;
+        for (int jj = 0; jj < N; ++jj) {
+          if (jj == e) continue;
+          double dx, dy;
+          min_image(mc, rx[e] - rx[jj], ry[e] - ry[jj], &dx, &dy);
+          const double r = sqrt(dx * dx + dy * dy + 1e-12);
+          double u, u1, u2;
+          jastrow_u(mc, hp, r, sp[e] == sp[jj], &u, &u1, &u2);
+          gj += u1 * (bax == 0 ? dx : dy) / r;
+        }
+        g.re += gj;
+      }
+      if (out.dL) out.dL[(size_t)jo * jb.n_tan + t] = g;
+    }
+    sumsq.re = warp_sum(sumsq.re);
+    sumsq.im = warp_sum(sumsq.im);
+    if (lane == 0) {
+      if (mc.use_jastrow) L.re += J;
+      if (out.L) out.L[jo] = L;
+      if (has_lap && out.lap) {
+        cplx lap;
+        if (all_sing) {
+          lap = mk(NAN, NAN);
+        } else if (K == 1) {
+          lap = j_lapk(j)[0];
+        } else {
+          lap = mk(0, 0);
+          for (int k = 0; k < K; ++k)
+            if (!sg[k]) cfma(lap, p[k], cadd(j_lapk(j)[k], j_sq(j)[k]));
+          lap = csub(lap, sumsq);
+        }
+        lap.re += lapJ;
+        out.lap[jo] = lap;
+      }
     }
   }
 }
 
 inline size_t head_smem(int N, int nG, int n_tan, bool tan) {
-  return head_smem_bytes(N, nG, n_tan, tan);
+  (void)N; (void)nG; (void)n_tan; (void)tan;
+  return 0;
 }
 
 

@@ -8,7 +8,7 @@
 #include <cmath>
 #include <atomic>
 
-#include "net.cuh"
+#include "net_kernels.cuh"
 
 struct NqsModel {
   nqs::HostModel hm;
@@ -33,10 +33,8 @@ int cuda_status(cudaError_t e, const char* what) {
   return NQS_ERR_CUDA;
 }
 
-size_t head_smem_host(int N, int nG, int n_tan, bool tan) {
-  const size_t n2 = (size_t)N * N;
-  const size_t nc = (tan ? 4 : 2) * n2 + (size_t)nG * N + 2 * (size_t)n_tan + N + 40;
-  return nc * 16 + 2 * N * sizeof(double) + (N + 2) * sizeof(int);
+size_t head_smem_host(int N, int nG, int K, int n_tan, bool tan) {
+  return head_job_bytes(N, nG, K, tan ? n_tan : 0) + head_warp_bytes(N, tan);
 }
 
 // rows of one chunk for a batch (whole jobs; SOC chunks hold whole walkers)
@@ -266,7 +264,7 @@ static int validate_desc(const NqsModelDesc* d) {
     set_error("model descriptor: singular cell");
     return NQS_ERR_INVALID_ARG;
   }
-  if (head_smem_host(d->n_elec, d->n_g, 0, false) > 227 * 1024) {
+  if (head_smem_host(d->n_elec, d->n_g, d->n_dets, 0, false) > 210 * 1024) {
     set_error("model: N=%d, n_g=%d exceeds the determinant kernel's shared memory", d->n_elec,
               d->n_g);
     return NQS_ERR_UNSUPPORTED;
@@ -360,7 +358,7 @@ int nqs_model_create(const NqsModelDesc* d, NqsModel** out) {
   mc.Gs = hm.d_Gs;
   mc.W = hm.d_W;
   mc.knots = hm.d_knots;
-  m->fl_ok = head_smem_host(d->n_elec, d->n_g, 2 * d->n_elec, true) <= 227 * 1024;
+  m->fl_ok = head_smem_host(d->n_elec, d->n_g, d->n_dets, 2 * d->n_elec, true) <= 210 * 1024;
   *out = m;
   return NQS_OK;
 }
@@ -397,7 +395,8 @@ size_t plan_bytes(const NqsModel* m, int op, int W, int prec) {
   const ModelConst& mc = m->hm.mc;
   const int N = mc.N;
   Plan p;
-  if (prec == NQS_PREC_MIXED) p.add(sizeof(float) * m->hm.desc.n_params);
+  if (prec != NQS_PREC_FP64) p.add(sizeof(float) * m->hm.desc.n_params);
+  if (prec == NQS_PREC_MIXED) p.add(tc_weights_bytes(m->hm.desc));
   switch (op) {
     case NQS_OP_LOGPSI:
       p.add(net_bytes(mc, prec, chunk_rows(JOB_VALUE, W, N, 1, kMaxRows)));
@@ -431,6 +430,7 @@ struct Ctx {
   Arena ws;
   const double* theta64;
   const float* theta32;
+  TcNet tc;
 };
 
 int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cudaStream_t st,
@@ -439,14 +439,14 @@ int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cud
     set_error("null model or theta");
     return NQS_ERR_INVALID_ARG;
   }
-  if (prec != NQS_PREC_FP64 && prec != NQS_PREC_MIXED) {
+  if (prec != NQS_PREC_FP64 && prec != NQS_PREC_MIXED && prec != NQS_PREC_MIXED_SIMT) {
     set_error("unknown precision %d", prec);
     return NQS_ERR_INVALID_ARG;
   }
   c->ws = Arena{(char*)wsp, wsb, 0};
   c->theta64 = theta;
   c->theta32 = nullptr;
-  if (prec == NQS_PREC_MIXED) {
+  if (prec != NQS_PREC_FP64) {
     float* t32 = c->ws.take<float>(m->hm.desc.n_params);
     if (!t32) {
       set_error("workspace too small");
@@ -455,6 +455,8 @@ int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cud
     NQS_TRY(theta_to_f32(theta, t32, m->hm.desc.n_params, st));
     c->theta32 = t32;
   }
+  c->tc = TcNet{};
+  if (prec == NQS_PREC_MIXED) NQS_TRY(build_tc_weights(m->hm.desc, c->theta32, c->ws, &c->tc, st));
   return NQS_OK;
 }
 
@@ -464,7 +466,8 @@ int run_net(NqsModel* m, Ctx& c, int prec, const JobBatch& jb, HeadOut out, cuda
     const NetW<double> w = make_netw<double>(m->hm.desc, c.theta64, c.theta64);
     return net_forward<double>(m->hm, w, hp, jb, out, c.ws, kMaxRows, st);
   }
-  const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  w.tc = c.tc;
   return net_forward<float>(m->hm, w, hp, jb, out, c.ws, kMaxRows, st);
 }
 

@@ -23,6 +23,7 @@ NQS_ERR_WORKSPACE = 3
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_MIXED_SIMT = 2
 
 OP_LOGPSI, OP_LOCAL_E, OP_MCMC, OP_PER_SAMPLE_O = 0, 1, 2, 3
 

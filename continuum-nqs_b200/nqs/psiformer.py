@@ -238,8 +238,10 @@ class _NativeModel:
 def _prec(precision) -> int:
     if precision in (0, "fp64", "float64"):
         return _lib.PREC_FP64
-    if precision in (1, "mixed", "bf16", "fp32"):
+    if precision in (1, "mixed", "tf32"):
         return _lib.PREC_MIXED
+    if precision in (2, "mixed_simt", "fp32"):
+        return _lib.PREC_MIXED_SIMT
     raise ValueError(f"unknown precision {precision!r}")
 
 

@@ -47,8 +47,10 @@ extern "C" {
 
 /* ---- precision of the wavefunction network ------------------------------------------------ */
 #define NQS_PREC_FP64   0   /* every stage in float64                                         */
-#define NQS_PREC_MIXED  1   /* network in float32 (tensor-core BF16 GEMMs where available);
-                               determinants, LU pivots, log-space sums, energies in float64   */
+#define NQS_PREC_MIXED  1   /* network in float32 with its Dense GEMMs on the tcgen05 tensor
+                               cores (TF32 operands, float32 accumulation) where the shapes
+                               allow; determinants, LU pivots, log-space sums, energies float64 */
+#define NQS_PREC_MIXED_SIMT 2  /* as NQS_PREC_MIXED with every GEMM on the float32 SIMT cores  */
 
 /* ---- compiled limits ---------------------------------------------------------------------- */
 #define NQS_MAX_DEPTH     16
@@ -170,7 +172,7 @@ int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, cons
  * the rounded Gram). status_dev (nullable, device int) is set
  * non-zero when a Cholesky pivot was not positive; status_dev[1] when a tensor-core Gram CTA hit
  * its bounded-wait limit; status_dev[2] counts pivots raised to the floor u * max T_ii
- * (u = 2^-8 BF16, 2^-11 TF32) in the factor of a tensor-core Gram, which only preconditions the
+ * (u = 2^-16 BF16, 2^-20 TF32) in the factor of a tensor-core Gram, which only preconditions the
  * refinement against the exact operator (3 ints). */
 int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int gram_prec,
                              size_t* bytes);

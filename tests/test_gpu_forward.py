@@ -67,3 +67,20 @@ def test_antisymmetry():
     L1 = f(R[:, perm], S[:, perm]).cpu()
     ratio = torch.exp(L1 - L0)
     assert (ratio + 1).abs().max() < 1e-9
+
+
+def test_tensor_core_network_matches_simt_and_fp64():
+    """Width-64 model: the mixed path runs its Dense layers on tcgen05 (TF32 operands); compare
+    log psi and E_loc with the float32-SIMT network and with float64."""
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import make_logpsi
+    g, model = build(N=6, L=7.5, embed=64, heads=4, n_dets=2, use_jastrow=True, n_freq=8)
+    p = model.init_normal(3, std=0.05, backflow_std=0.02, jastrow_std=0.02)
+    R, S = configs(6, 7.5, 300, 9)   # 300 walkers x 6 tokens: several 128-row tiles + a ragged one
+    lp = {k: make_logpsi(model, p, precision=k) for k in ("fp64", "mixed", "mixed_simt")}
+    L = {k: f(R, S).cpu() for k, f in lp.items()}
+    assert (L["mixed"] - L["fp64"]).real.abs().max() < 2e-3
+    assert (L["mixed_simt"] - L["fp64"]).real.abs().max() < 1e-4
+    E = {k: make_local_energy(f, 1.0, 1.0, 0.5)(R[:64], S[:64]).cpu() for k, f in lp.items()}
+    assert (E["mixed"] - E["fp64"]).real.abs().max() < 5e-3
+    assert abs(float(E["mixed"].real.mean() - E["fp64"].real.mean())) < 5e-4
