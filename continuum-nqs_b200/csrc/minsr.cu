@@ -399,38 +399,72 @@ __device__ __forceinline__ void diag_solve_warp(const double* __restrict__ L, in
   }
 }
 
-// solves L x = v (transposed = 0) or L^T x = v (transposed = 1) in place; xb: 64 doubles scratch
+// Solves L x = v (transposed = 0) or L^T x = v (transposed = 1) in place with one grid barrier
+// per 64-block (look-ahead): in step s the first CTA applies x_s to block s+1 and solves that
+// diagonal block, while every other CTA applies x_s to the blocks beyond it. xb: 2 x 64 doubles.
 __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L, int64_t ldl,
                                                    int n, double* __restrict__ v,
                                                    double* __restrict__ xb, int transposed) {
   cg::grid_group grid = cg::this_grid();
   const int nblk = (n + CB - 1) / CB;
   const int lane = threadIdx.x & 31;
-  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   __shared__ double xs[CB];
+  auto blk = [&](int s) { return transposed ? nblk - 1 - s : s; };
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    const int k0 = blk(0) * CB;
+    diag_solve_warp(L, ldl, k0, min(CB, n - k0), v, xb, transposed);
+  }
+  grid.sync();
   for (int s = 0; s < nblk; ++s) {
-    const int bi = transposed ? nblk - 1 - s : s;
-    const int k0 = bi * CB, b = min(CB, n - k0);
-    if (blockIdx.x == 0 && threadIdx.x < 32) diag_solve_warp(L, ldl, k0, b, v, xb, transposed);
-    grid.sync();
-    for (int i = threadIdx.x; i < b; i += blockDim.x) xs[i] = xb[i];
+    const int k0 = blk(s) * CB, b = min(CB, n - k0);
+    const double* xcur = xb + (s & 1) * CB;
+    for (int i = threadIdx.x; i < b; i += blockDim.x) xs[i] = xcur[i];
     __syncthreads();
-    if (!transposed) {
-      // rows r >= k0 + b: v[r] -= sum_j L[r][k0 + j] x_j   (one warp per row)
-      for (int r = k0 + b + gwarp; r < n; r += nwarps) {
-        const double* lr = L + (size_t)r * ldl + k0;
-        double acc = 0.0;
-        for (int j = lane; j < b; j += 32) acc = fma(lr[j], xs[j], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) v[r] -= acc;
+    const bool more = s + 1 < nblk;
+    const int k1 = more ? blk(s + 1) * CB : 0, b1 = more ? min(CB, n - k1) : 0;
+    if (blockIdx.x == 0) {
+      if (more) {
+        // apply x_s to block s+1, then solve it
+        const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (!transposed) {
+          for (int r = k1 + w; r < k1 + b1; r += nw) {
+            const double* lr = L + (size_t)r * ldl + k0;
+            double acc = 0.0;
+            for (int jj = lane; jj < b; jj += 32) acc = fma(lr[jj], xs[jj], acc);
+            acc = warp_sum(acc);
+            if (lane == 0) v[r] -= acc;
+          }
+        } else {
+          for (int m = k1 + threadIdx.x; m < k1 + b1; m += blockDim.x) {
+            double acc = 0.0;
+            for (int jj = 0; jj < b; ++jj) acc = fma(L[(size_t)(k0 + jj) * ldl + m], xs[jj], acc);
+            v[m] -= acc;
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x < 32)
+          diag_solve_warp(L, ldl, k1, b1, v, xb + ((s + 1) & 1) * CB, transposed);
       }
     } else {
-      // columns m < k0: v[m] -= sum_j L[k0 + j][m] x_j   (one thread per column, coalesced)
-      for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < k0; m += gridDim.x * blockDim.x) {
-        double acc = 0.0;
-        for (int j = 0; j < b; ++j) acc = fma(L[(size_t)(k0 + j) * ldl + m], xs[j], acc);
-        v[m] -= acc;
+      // every other CTA: apply x_s to the rows (columns) beyond block s+1
+      const int gw = ((blockIdx.x - 1) * blockDim.x + threadIdx.x) >> 5;
+      const int nwk = ((gridDim.x - 1) * blockDim.x) >> 5;
+      if (!transposed) {
+        for (int r = k0 + b + b1 + gw; r < n; r += nwk) {
+          const double* lr = L + (size_t)r * ldl + k0;
+          double acc = 0.0;
+          for (int jj = lane; jj < b; jj += 32) acc = fma(lr[jj], xs[jj], acc);
+          acc = warp_sum(acc);
+          if (lane == 0) v[r] -= acc;
+        }
+      } else {
+        const int lim = more ? k1 : 0;  // columns below block s+1's start
+        for (int m = (blockIdx.x - 1) * blockDim.x + threadIdx.x; m < lim;
+             m += (gridDim.x - 1) * blockDim.x) {
+          double acc = 0.0;
+          for (int jj = 0; jj < b; ++jj) acc = fma(L[(size_t)(k0 + jj) * ldl + m], xs[jj], acc);
+          v[m] -= acc;
+        }
       }
     }
     grid.sync();
@@ -445,7 +479,7 @@ static int trsv_grid(const double* L, int64_t ldl, int n, double* v, double* xb,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trsv_grid, 256, 0);
-    grid = nsm * std::max(1, std::min(per, 4));
+    grid = per >= 1 ? nsm : 1;  // one CTA per SM keeps the grid barrier cheap
   }
   void* args[] = {(void*)&L, (void*)&ldl, (void*)&n, (void*)&v, (void*)&xb, (void*)&transposed};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_trsv_grid, grid, 256, args, 0, st);
@@ -775,7 +809,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
-  add(sizeof(double) * CB);             // triangular-solve block
+  add(sizeof(double) * 2 * CB);         // triangular-solve blocks (double-buffered)
   add(sizeof(int) * 4);                 // status
   add(sizeof(double));                  // pivot floor
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
@@ -818,7 +852,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* r = ws.take<double>(n);
   double* tmpK = ws.take<double>(P);
   double* tmpK_lo = ws.take<double>(P);
-  double* xb = ws.take<double>(CB);
+  double* xb = ws.take<double>(2 * CB);
   double* rsum = ws.take<double>(2 * (size_t)n + 5);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
@@ -905,7 +939,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
-  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + CB +
+  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + 2 * CB +
                              std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 8192;
   return NQS_OK;
 }
@@ -934,7 +968,7 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
-  double* xb = ws.take<double>(CB);
+  double* xb = ws.take<double>(2 * CB);
   if (!xb) return NQS_ERR_WORKSPACE;
   NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, xb, 3, st));
   return NQS_OK;

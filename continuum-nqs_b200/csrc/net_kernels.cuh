@@ -773,12 +773,15 @@ struct HeadPlan {
   int wpc, jpc;
   size_t job_bytes, warp_bytes, bytes;
 };
+// slot sizes are rounded to 128 bytes so every job / warp slot (and the complex arrays at its
+// start) stays 16-byte aligned for vector shared-memory access
+__host__ __device__ inline size_t round128(size_t b) { return (b + 127) & ~(size_t)127; }
 __host__ __device__ inline size_t head_job_bytes(int N, int nG, int K, int n_tan) {
-  return 16 * ((size_t)N * N + (size_t)nG * N + 3 * (size_t)K + (size_t)K * n_tan) +
-         8 * 2 * (size_t)N + 4 * ((size_t)N + K) + 16;
+  return round128(16 * ((size_t)N * N + (size_t)nG * N + 3 * (size_t)K + (size_t)K * n_tan) +
+                  8 * 2 * (size_t)N + 4 * ((size_t)N + K) + 16);
 }
 __host__ __device__ inline size_t head_warp_bytes(int N, bool tan) {
-  return 16 * ((tan ? 3 : 1) * (size_t)N * N + (size_t)N);
+  return round128(16 * ((tan ? 3 : 1) * (size_t)N * N + (size_t)N));
 }
 inline HeadPlan head_plan(int N, int nG, int K, int n_tan, bool tan) {
   HeadPlan p;
