@@ -231,16 +231,21 @@ def run_ours(a, rank, world):
         em, e64 = it.e.real.double(), it64.e.real.double()
         it.jacobian()
         it64.jacobian()
-        d_mixed = minsr_step(it.O.clone(), it.e, su.lam, "bf16", n_refine=it.n_refine)
-        d_gram = minsr_step(it.O.double(), it64.e, su.lam, "fp64")
+        delta = torch.zeros(1, dtype=torch.float64, device=dev)
+        d_mixed = minsr_step(it.O.clone(), it.e, su.lam, "bf16", n_refine=it.n_refine,
+                             damping_out=delta)
+        dl = float(delta.item())
         d_64 = minsr_step(it64.O.clone(), it64.e, su.lam, "fp64")
-        n64 = float(d_64.norm())
+        d_64d = minsr_step(it64.O.clone(), it64.e, su.lam + dl, "fp64")
+        n64, n64d = float(d_64.norm()), float(d_64d.norm())
         acc = {"dE_per_electron": float((em.mean() - e64.mean()).abs()) / su.N,
                "dE_target": 1e-4,
                "dvar_rel": float((em.var() - e64.var()).abs() / e64.var()),
                "dvar_target": 0.05,
-               "dtheta_rel": float((d_mixed - d_64).norm()) / n64,
-               "dtheta_rel_network_only": float((d_gram - d_64).norm()) / n64,
+               "bf16_gram_extra_damping": dl,
+               "dtheta_rel_vs_fp64_same_damping": float((d_mixed - d_64d).norm()) / n64d,
+               "dtheta_rel_vs_fp64_lam": float((d_mixed - d_64).norm()) / n64,
+               "dtheta_cos_vs_fp64_lam": float((d_mixed * d_64).sum()) / (float(d_mixed.norm()) * n64),
                "E_fp64": float(e64.mean()), "E_mixed": float(em.mean())}
         it64.step()
         torch.cuda.synchronize()

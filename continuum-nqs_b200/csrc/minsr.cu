@@ -340,6 +340,15 @@ __global__ void k_add_diag(double* A, int64_t lda, int n, double lam) {
   if (i < n) A[(size_t)i * lda + i] += lam;
 }
 
+// extra[0] = u * (mean diagonal), added to the diagonal together with lam
+__global__ void k_add_diag_noise(double* A, int64_t lda, int n, double lam, double u,
+                                 const double* __restrict__ mean_diag, double* __restrict__ extra) {
+  const double x = u * (*mean_diag);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[(size_t)i * lda + i] += lam + x;
+  if (i == 0 && extra) *extra = x;
+}
+
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
   for (int k0 = 0; k0 < n; k0 += CB) {
@@ -616,9 +625,11 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid(const TO* __restrict__ O, 
                                                       int64_t K, const double* __restrict__ mu,
                                                       const double* __restrict__ v,
                                                       const double* __restrict__ v_lo,
-                                                      const double* __restrict__ b, double lam,
+                                                      const double* __restrict__ b, double lam0,
+                                                      const double* __restrict__ lam_extra,
                                                       const double* __restrict__ x,
                                                       double* __restrict__ r) {
+  const double lam = lam0 + (lam_extra ? *lam_extra : 0.0);
   const int m = blockIdx.x;
   const TO* row = O + (size_t)m * K;
   const double* mr = mu ? mu + (m >= Mh ? K : 0) : nullptr;
@@ -687,7 +698,8 @@ __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__
 // A = O - mu (centred on the fly). On return tmpK holds A^T y.
 template <typename TO>
 static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
-                         const double* mu, double lam, const double* b, double* y, double* r,
+                         const double* mu, double lam, const double* lam_extra, const double* b,
+                         double* y, double* r,
                          double* tmpK, double* tmpK_lo, double* xb, int n_refine,
                          cudaStream_t st) {
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
@@ -697,7 +709,8 @@ static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
   for (int it = 0; it < n_refine; ++it) {
     k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0);
     NQS_CHECK_LAUNCH("k_gemv_t");
-    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, y, r);
+    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, lam_extra, y,
+                                          r);
     NQS_CHECK_LAUNCH("k_gemv_n_resid");
     NQS_TRY(trsv_grid(L, M, M, r, xb, 0, st));
     NQS_TRY(trsv_grid(L, M, M, r, xb, 1, st));
@@ -811,7 +824,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
   add(sizeof(double) * 2 * CB);         // triangular-solve blocks (double-buffered)
   add(sizeof(int) * 4);                 // status
-  add(sizeof(double));                  // pivot floor
+  add(sizeof(double) * 2);              // pivot floor, extra damping
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
   if (gram == 0 && odtype == 1) add(sizeof(double) * n * P);  // float64 Otil from float32 O
   if (gram != 0) add(gram_tc_workspace(W, P, gram));
@@ -832,7 +845,8 @@ int nqs_minsr_workspace_size(int W, int64_t P, int o_dtype, int gram_prec, size_
 
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t P, double lam,
                         int gram_prec, int n_refine, double* out_dtheta, double* theta_io,
-                        double lr, int* status_dev, void* wsp, size_t wsb, void* stream) {
+                        double lr, int* status_dev, double* damping_out, void* wsp, size_t wsb,
+                        void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   if (!O || !eps || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || gram_prec < 0 ||
       gram_prec > 2 || n_refine < 0 || n_refine > 8 || (!out_dtheta && !theta_io)) {
@@ -903,26 +917,35 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
     k_gram_center<<<dim3((n + 255) / 256, n), 256, 0, st>>>(T, n, W, rsum, rsum + 2 * n);
     NQS_CHECK_LAUNCH("k_gram_center");
   }
-  k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
-  NQS_CHECK_LAUNCH("k_add_diag");
-  // A tensor-core Gram carries rounding noise ~ u sqrt(Tii Tjj) (u = 2^-8 BF16, 2^-11 TF32); its
-  // factor only preconditions the refinement below, which solves the exact system. The null
-  // directions of the centring were lifted above; a small pivot floor guards against noise that
-  // still makes a pivot non-positive.
+  // A tensor-core Gram accumulated in float32 carries absolute errors ~ u T_ii (u = 2^-8 BF16
+  // operands, 2^-11 TF32), far above a small lam along the Jacobian's near-null directions. Its
+  // solve therefore uses the damping lam + delta, delta = u mean(T_ii) (written to damping_out),
+  // and the refinement below solves that system exactly against the true operator.
   const double* floor_p = nullptr;
-  if (gram_prec != 0) {
-    double* fl = ws.take<double>(1);
+  const double* lam_x = nullptr;
+  if (gram_prec == 0) {
+    k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
+    NQS_CHECK_LAUNCH("k_add_diag");
+    if (damping_out) cudaMemsetAsync(damping_out, 0, sizeof(double), st);
+  } else {
+    double* fl = ws.take<double>(2);
     if (!fl) return NQS_ERR_WORKSPACE;
+    k_add_diag_noise<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam,
+                                                       gram_prec == 1 ? 0x1p-8 : 0x1p-11,
+                                                       rsum + 2 * n + 4, fl + 1);
+    NQS_CHECK_LAUNCH("k_add_diag_noise");
     k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-16 : 0x1p-20, fl);
     NQS_CHECK_LAUNCH("k_pivot_floor");
     floor_p = fl;
+    lam_x = fl + 1;
+    if (damping_out) cudaMemcpyAsync(damping_out, fl + 1, sizeof(double), cudaMemcpyDeviceToDevice, st);
   }
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
   if (op_dtype == 0)
-    NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, tmpK,
+    NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
                                   tmpK_lo, xb, n_refine, st));
   else
-    NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, tmpK,
+    NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
                                  tmpK_lo, xb, n_refine, st));
   const unsigned gp = (unsigned)((P + 255) / 256);
   if (op_dtype == 0)
@@ -970,7 +993,8 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
   double* xb = ws.take<double>(2 * CB);
   if (!xb) return NQS_ERR_WORKSPACE;
-  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, rhs, x, r, tmpK, tmpK_lo, xb, 3, st));
+  NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, nullptr, rhs, x, r, tmpK, tmpK_lo, xb,
+                                3, st));
   return NQS_OK;
 }
 

@@ -168,8 +168,8 @@ def workspace_for(model_handle, op: int, n_walkers: int, prec: int) -> tuple[tor
 _SIGS.update({
     "nqs_minsr_workspace_size": ([c_int, c_int64, c_int, c_int, POINTER(c_size_t)], c_int),
     "nqs_minsr_direction": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_double, c_int, c_int,
-                             c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_size_t, c_void_p],
-                            c_int),
+                             c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_size_t,
+                             c_void_p], c_int),
     "nqs_clip_energies": ([c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p], c_int),
     "nqs_energy_gradient": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_size_t,
                              c_void_p], c_int),

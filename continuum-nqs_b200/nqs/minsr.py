@@ -103,7 +103,7 @@ _GRAM = {"fp64": 0, "bf16": 1, "tf32": 2}
 
 
 def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True,
-               n_refine=1):
+               n_refine=1, damping_out=None):
     """Sample-space natural gradient on the device. O_rows is [2W][P] (f64 or f32; a float64
     O_rows is centred in place by the float64 Gram). Returns dtheta (P,) and updates theta in
     place by -lr dtheta when given."""
@@ -121,7 +121,8 @@ def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction
     _lib.check(_lib.lib().nqs_minsr_direction(
         _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, int(n_refine), _lib.ptr(d),
         _lib.ptr(theta),
-        float(lr), None, _lib.ptr(ws), ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
+        float(lr), None, _lib.ptr(damping_out), _lib.ptr(ws), ws.numel(), _lib.stream_ptr()),
+        "nqs_minsr_direction")
     return d
 
 
@@ -253,7 +254,7 @@ class VMCIteration:
         self.prec_name = precision
         self.prec = _prec(precision)
         self.gram = gram or ("fp64" if self.prec == _lib.PREC_FP64 else "bf16")
-        self.n_refine = int(n_refine if n_refine is not None else (1 if self.gram == "fp64" else 3))
+        self.n_refine = int(n_refine if n_refine is not None else (1 if self.gram == "fp64" else 2))
         dev = self.R.device
         self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
         self.O = torch.empty(2 * self.W, self.P, dtype=self.o_dtype, device=dev)
@@ -263,6 +264,7 @@ class VMCIteration:
         self.acc_pos = torch.zeros(self.W, dtype=F64, device=dev)
         self.acc_spin = torch.zeros(self.W, dtype=F64, device=dev)
         self.status = torch.zeros(3, dtype=torch.int32, device=dev)
+        self.damping = torch.zeros(1, dtype=F64, device=dev)  # extra damping of a TC Gram
         h = model.native().handle
         self.h = h
         sizes = [_lib.workspace_for(h, op, self.W, self.prec)[1]
@@ -306,8 +308,8 @@ class VMCIteration:
         _lib.check(L.nqs_minsr_direction(
             _lib.ptr(self.O), 0 if self.o_dtype == torch.float64 else 1, _lib.ptr(self.e_clip),
             self.W, self.P, self.lam, _GRAM[self.gram], self.n_refine, None, _lib.ptr(self.theta),
-            self.lr, _lib.ptr(self.status), _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
-            "nqs_minsr_direction")
+            self.lr, _lib.ptr(self.status), _lib.ptr(self.damping), _lib.ptr(self.ws),
+            self.ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
 
     def step(self):
         self.sample()

@@ -167,9 +167,11 @@ int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, cons
  *   dtheta = Otil^T y;  out_dtheta (nullable) receives dtheta, theta_io (nullable) is updated
  *   theta -= lr dtheta in the same pass.
  * gram_prec: 0 = float64 SIMT Gram (a float64 O is centred IN PLACE), 1 = BF16 tcgen05 Gram,
- * 2 = TF32 tcgen05 Gram (both float32 accumulation). n_refine (0..8) steps of iterative
- * refinement of y against the exact operator Otil Otil^T + lam I (applied with O itself, never
- * the rounded Gram). status_dev (nullable, device int) is set
+ * 2 = TF32 tcgen05 Gram (both float32 accumulation). A tensor-core Gram solves with the damping
+ * lam + delta, delta = u mean(diag T) (u = 2^-8 BF16, 2^-11 TF32: its absolute rounding level);
+ * damping_out (nullable, device double) receives delta (0 for the float64 Gram). n_refine (0..8)
+ * steps of iterative refinement of y against the exact operator Otil Otil^T + (lam + delta) I
+ * (applied with O itself, never the rounded Gram). status_dev (nullable, device int) is set
  * non-zero when a Cholesky pivot was not positive; status_dev[1] when a tensor-core Gram CTA hit
  * its bounded-wait limit; status_dev[2] counts pivots raised to the floor u * max T_ii
  * (u = 2^-16 BF16, 2^-20 TF32) in the factor of a tensor-core Gram, which only preconditions the
@@ -178,9 +180,9 @@ int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int g
                              size_t* bytes);
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
                         int64_t n_params, double lam, int gram_prec, int n_refine,
-                        double* out_dtheta,
-                        double* theta_io, double lr, int* status_dev, void* workspace,
-                        size_t workspace_bytes, void* stream);
+                        double* out_dtheta, double* theta_io, double lr, int* status_dev,
+                        double* damping_out, void* workspace, size_t workspace_bytes,
+                        void* stream);
 
 /* Lower triangle of T = A A^T on the tcgen05 tensor cores (float32 accumulation, float64 out):
  * A row-major [M][lda] of BF16 (a_dtype 1) or float32 read as TF32 (a_dtype 2); lda * elem size

@@ -29,16 +29,19 @@ def test_gram_tc_matches_fp64_of_rounded_operands(M, K, kind):
     assert torch.count_nonzero(torch.triu(T, 1)) == 0
 
 
-def test_minsr_bf16_gram_close_to_fp64():
-    """The BF16 Gram plus refinement against the exact operator gives a direction close to the
-    float64 one on a well-conditioned problem."""
-    from nqs.minsr import minsr_direction
+def test_minsr_tensor_core_gram_refined_to_fp64():
+    """With a tensor-core Gram the solve uses lam + delta (delta = u mean diag T, u its rounding
+    level); refinement against the exact operator reproduces the float64 solve at that damping."""
+    from nqs.minsr import minsr_direction, minsr_step, _as_rows
     rng = np.random.default_rng(2)
     W, P = 256, 4000
     Oc = torch.as_tensor(rng.normal(size=(W, P)) + 1j * rng.normal(size=(W, P)))
     eps = torch.as_tensor(rng.normal(size=W) + 1j * rng.normal(size=W))
-    d64 = minsr_direction(Oc.cuda(), eps, 1e-3, gram="fp64")
     for kind in ("bf16", "tf32"):
-        d = minsr_direction(Oc.cuda(), eps, 1e-3, gram=kind, n_refine=4)
+        delta = torch.zeros(1, dtype=torch.float64, device="cuda")
+        d = minsr_step(_as_rows(Oc).cuda(), eps, 1e-3, kind, n_refine=3, damping_out=delta)
+        dl = float(delta.item())
+        assert dl > 0
+        d64 = minsr_direction(Oc.cuda(), eps, 1e-3 + dl, gram="fp64")
         rel = float((d - d64).norm() / d64.norm())
-        assert rel < 1e-6, (kind, rel)
+        assert rel < 1e-8, (kind, rel)
