@@ -20,7 +20,7 @@ constexpr int RG_BM = 128;
 constexpr int RG_KB = 32;  // float32 per 128-byte swizzle row
 
 struct RowGemmArgs {
-  int rows, K, Nout, Npad, C;
+  int rows, K, Nout, Npad, C, vec4;
   const float* bias;
   const float* Res;
   int ldr;
@@ -88,32 +88,65 @@ __global__ void __launch_bounds__(128, 1) k_rowgemm_tc(const __grid_constant__ C
   fence_after();
   const bool go = __all_sync(0xffffffffu, ok && !*abort);
   if (go) {
-    const int row = m0 + warp * 32 + lane;
-    const bool vrow = row < g.rows;
-    const bool val = vrow && (row % g.C) == 0;
+    // Drain TMEM 32 columns at a time into a per-warp staging tile in the (now idle) operand
+    // buffer, then write 4 rows x 128 bytes per warp instruction (coalesced float4 when every
+    // row start is 16-byte aligned, scalar otherwise).
+    float* stage = reinterpret_cast<float*>(sA) + warp * (32 * 33);
+    const int r0 = m0 + warp * 32;
 #pragma unroll 1
-    for (int c0 = 0; c0 < g.Nout; c0 += 16) {
-      uint32_t r[16];
+    for (int c0 = 0; c0 < g.Nout; c0 += 32) {
+      uint32_t r[32];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
       asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-          "%14,%15}, [%16];"
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+          "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
           : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
             "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-            "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+            "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+            "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+            "=r"(r[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (vrow) {
+      const int row_l = r0 + lane;
+      const bool val = row_l < g.rows && (row_l % g.C) == 0;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int col = c0 + q;
-          if (col >= g.Nout) break;
-          float v = __uint_as_float(r[q]);
-          if (val && g.bias) v += g.bias[col];
-          if (g.Res) v = g.Res[(size_t)row * g.ldr + col] + v;
-          g.Y[(size_t)row * g.ldy + col] = v;
+      for (int q = 0; q < 32; ++q) {
+        const int col = c0 + q;
+        float v = __uint_as_float(r[q]);
+        if (val && g.bias && col < g.Nout) v += g.bias[col];
+        stage[lane * 33 + q] = v;
+      }
+      __syncwarp();
+      const int ncol = min(32, g.Nout - c0);
+      if (g.vec4 && ncol == 32) {
+#pragma unroll
+        for (int rr = 0; rr < 32; rr += 4) {
+          const int lr = rr + (lane >> 3), cg = (lane & 7) * 4;
+          const int row = r0 + lr;
+          if (row < g.rows) {
+            const float* sv = stage + lr * 33 + cg;
+            float4 v = make_float4(sv[0], sv[1], sv[2], sv[3]);
+            if (g.Res) {
+              const float4 rv =
+                  *reinterpret_cast<const float4*>(g.Res + (size_t)row * g.ldr + c0 + cg);
+              v = make_float4(rv.x + v.x, rv.y + v.y, rv.z + v.z, rv.w + v.w);
+            }
+            *reinterpret_cast<float4*>(g.Y + (size_t)row * g.ldy + c0 + cg) = v;
+          }
+        }
+      } else {
+        for (int rr = 0; rr < 32; ++rr) {
+          const int row = r0 + rr;
+          if (row >= g.rows) break;
+          for (int q = lane; q < ncol; q += 32) {
+            float v = stage[rr * 33 + q];
+            if (g.Res) v = g.Res[(size_t)row * g.ldr + c0 + q] + v;
+            g.Y[(size_t)row * g.ldy + c0 + q] = v;
+          }
         }
       }
+      __syncwarp();
     }
   }
   if (*abort && threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
@@ -178,7 +211,12 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     cudaFuncSetAttribute(tc::k_rowgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  tc::RowGemmArgs a{rows, K, Nout, Npad, C, bias, Res, ldr, Y, ldy, err};
+  // float4 row writes only when every row start of Y and Res is 16-byte aligned
+  const int vec4 = ((reinterpret_cast<uintptr_t>(Y) & 15) == 0 && (ldy % 4) == 0 &&
+                    (!Res || ((reinterpret_cast<uintptr_t>(Res) & 15) == 0 && (ldr % 4) == 0)))
+                       ? 1
+                       : 0;
+  tc::RowGemmArgs a{rows, K, Nout, Npad, C, vec4, bias, Res, ldr, Y, ldy, err};
   tc::k_rowgemm_tc<<<(rows + tc::RG_BM - 1) / tc::RG_BM, 128, sm, st>>>(ta, tb, a);
   NQS_CHECK_LAUNCH("k_rowgemm_tc");
   return NQS_OK;

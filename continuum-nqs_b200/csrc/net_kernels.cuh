@@ -300,13 +300,18 @@ inline int launch_gemm(GemmArgs<T> g, cudaStream_t st) {
 //   Lap o = Lap a v + a Lap v + 2 P_av,  P_av = sum_t d_t a d_t v
 // ============================================================================================
 template <typename T>
-__global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int n_tan, int has_lap,
+__global__ void __launch_bounds__(256) k_attention(int n_jobs, int N, int C, int n_tan, int has_lap,
                                                    int d, int H, const T* __restrict__ QKV,
                                                    T* __restrict__ OUT) {
-  const int job = blockIdx.x / H, h = blockIdx.x - job * H;
+  // one warp per (job, head); every phase is warp-synchronous
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int pair = blockIdx.x * nwarp + wib;
+  if (pair >= n_jobs * H) return;  // whole warp
+  const int job = pair / H, h = pair - job * H;
   const int hd = d / H;
+  const int per = 6 * N * hd + 4 * N * N + N + N * hd;  // elements of this warp's slot
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* q = reinterpret_cast<T*>(smraw);
+  T* q = reinterpret_cast<T*>(smraw) + (size_t)wib * per;
   T* k = q + N * hd;
   T* v = k + N * hd;
   T* a = v + N * hd;
@@ -321,27 +326,26 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
   const T sc = T(1) / sqrt(T(hd));
   const int ld = 3 * d;
   auto row = [&](int i, int c) -> size_t { return ((size_t)job * N + i) * C + c; };
-  const int tid = threadIdx.x, nth = blockDim.x;
-  for (int idx = tid; idx < N * hd; idx += nth) {
+  for (int idx = lane; idx < N * hd; idx += 32) {
     const int i = idx / hd, e = idx - i * hd;
     const T* p = QKV + row(i, 0) * ld + h * hd + e;
     q[idx] = p[0];
     k[idx] = p[d];
     v[idx] = p[2 * d];
   }
-  if (has_lap)
-    for (int idx = tid; idx < N * N; idx += nth) Pqk[idx] = Psq[idx] = T(0);
-  if (has_lap)
-    for (int idx = tid; idx < N * hd; idx += nth) Pav[idx] = T(0);
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
+  if (has_lap) {
+    for (int idx = lane; idx < N * N; idx += 32) Pqk[idx] = Psq[idx] = T(0);
+    for (int idx = lane; idx < N * hd; idx += 32) Pav[idx] = T(0);
+  }
+  __syncwarp();
+  for (int idx = lane; idx < N * N; idx += 32) {
     const int i = idx / N, jj = idx - i * N;
     T sacc = 0;
     for (int e = 0; e < hd; ++e) sacc = fma(q[i * hd + e], k[jj * hd + e], sacc);
     a[idx] = sacc * sc;
   }
-  __syncthreads();
-  for (int i = tid; i < N; i += nth) {
+  __syncwarp();
+  for (int i = lane; i < N; i += 32) {
     T mx = a[i * N];
     for (int jj = 1; jj < N; ++jj) mx = max(mx, a[i * N + jj]);
     T ssum = 0;
@@ -352,24 +356,24 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
     }
     for (int jj = 0; jj < N; ++jj) a[i * N + jj] = a[i * N + jj] / ssum;
   }
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
+  __syncwarp();
+  for (int idx = lane; idx < N * hd; idx += 32) {
     const int i = idx / hd, e = idx - i * hd;
     T o = 0;
     for (int jj = 0; jj < N; ++jj) o = fma(a[i * N + jj], v[jj * hd + e], o);
     OUT[row(i, 0) * d + h * hd + e] = o;
   }
   for (int t = 0; t < n_tan; ++t) {
-    __syncthreads();
-    for (int idx = tid; idx < N * hd; idx += nth) {
+    __syncwarp();
+    for (int idx = lane; idx < N * hd; idx += 32) {
       const int i = idx / hd, e = idx - i * hd;
       const T* p = QKV + row(i, 1 + t) * ld + h * hd + e;
       qt[idx] = p[0];
       kt[idx] = p[d];
       vt[idx] = p[2 * d];
     }
-    __syncthreads();
-    for (int idx = tid; idx < N * N; idx += nth) {
+    __syncwarp();
+    for (int idx = lane; idx < N * N; idx += 32) {
       const int i = idx / N, jj = idx - i * N;
       T s1 = 0, s2 = 0;
       for (int e = 0; e < hd; ++e) {
@@ -380,21 +384,21 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
       st[idx] = s1 * sc;
       if (has_lap) Pqk[idx] += s2;
     }
-    __syncthreads();
-    for (int i = tid; i < N; i += nth) {
+    __syncwarp();
+    for (int i = lane; i < N; i += 32) {
       T l = 0;
       for (int jj = 0; jj < N; ++jj) l = fma(a[i * N + jj], st[i * N + jj], l);
       lt[i] = l;
     }
-    __syncthreads();
-    for (int idx = tid; idx < N * N; idx += nth) {
+    __syncwarp();
+    for (int idx = lane; idx < N * N; idx += 32) {
       const int i = idx / N;
       const T ds = st[idx] - lt[i];
       if (has_lap) Psq[idx] += ds * ds;
       st[idx] = a[idx] * ds;
     }
-    __syncthreads();
-    for (int idx = tid; idx < N * hd; idx += nth) {
+    __syncwarp();
+    for (int idx = lane; idx < N * hd; idx += 32) {
       const int i = idx / hd, e = idx - i * hd;
       T o = 0, pav = 0;
       for (int jj = 0; jj < N; ++jj) {
@@ -407,16 +411,16 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
     }
   }
   if (!has_lap) return;
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
+  __syncwarp();
+  for (int idx = lane; idx < N * hd; idx += 32) {
     const int i = idx / hd, e = idx - i * hd;
     const T* p = QKV + row(i, C - 1) * ld + h * hd + e;
     qt[idx] = p[0];
     kt[idx] = p[d];
     vt[idx] = p[2 * d];
   }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
+  __syncwarp();
+  for (int idx = lane; idx < N * N; idx += 32) {
     const int i = idx / N, jj = idx - i * N;
     T s1 = 0;
     for (int e = 0; e < hd; ++e) {
@@ -425,19 +429,19 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
     }
     st[idx] = (s1 + T(2) * Pqk[idx]) * sc;
   }
-  __syncthreads();
-  for (int i = tid; i < N; i += nth) {
+  __syncwarp();
+  for (int i = lane; i < N; i += 32) {
     T l = 0;
     for (int jj = 0; jj < N; ++jj) l = fma(a[i * N + jj], st[i * N + jj] + Psq[i * N + jj], l);
     lt[i] = l;
   }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nth) {
+  __syncwarp();
+  for (int idx = lane; idx < N * N; idx += 32) {
     const int i = idx / N;
     st[idx] = a[idx] * (Psq[idx] + st[idx] - lt[i]);
   }
-  __syncthreads();
-  for (int idx = tid; idx < N * hd; idx += nth) {
+  __syncwarp();
+  for (int idx = lane; idx < N * hd; idx += 32) {
     const int i = idx / hd, e = idx - i * hd;
     T o = 0;
     for (int jj = 0; jj < N; ++jj) {
@@ -448,9 +452,21 @@ __global__ void __launch_bounds__(128) k_attention(int n_jobs, int N, int C, int
   }
 }
 
+// warps per CTA and dynamic shared memory of k_attention (each warp's slot rounded to 16 bytes)
+template <typename T>
+inline size_t attention_warp_bytes(int N, int hd) {
+  return ((sizeof(T) * (size_t)(6 * N * hd + 4 * N * N + N + N * hd)) + 15) & ~(size_t)15;
+}
+template <typename T>
+inline int attention_wpc(int N, int hd) {
+  const size_t wb = attention_warp_bytes<T>(N, hd);
+  int w = 8;
+  while (w > 1 && (size_t)w * wb > 96 * 1024) w /= 2;
+  return w;
+}
 template <typename T>
 inline size_t attention_smem(int N, int hd) {
-  return sizeof(T) * (size_t)(6 * N * hd + 4 * N * N + N + N * hd);
+  return (size_t)attention_wpc<T>(N, hd) * attention_warp_bytes<T>(N, hd);
 }
 
 // ============================================================================================
