@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include <cooperative_groups.h>
 
@@ -1009,6 +1010,76 @@ int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int W, int6
   NQS_CHECK_LAUNCH("k_center_eps");
   const unsigned gp = (unsigned)((P + 255) / 256);
   // g = (2/W) sum_w Re(conj(e_w - mean e) O_w) = (2/W) O_rows^T [Re eps; Im eps]
+  if (o_dtype == 0)
+    k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)O, 2 * W, 2 * W, P, nullptr, x, out_grad,
+                                         nullptr, nullptr, 0.0);
+  else
+    k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)O, 2 * W, 2 * W, P, nullptr, x, out_grad,
+                                        nullptr, nullptr, 0.0);
+  NQS_CHECK_LAUNCH("k_gemv_t");
+  k_scale_vec<<<gp, 256, 0, st>>>(out_grad, P, 2.0 / W);
+  NQS_CHECK_LAUNCH("k_scale_vec");
+  return NQS_OK;
+}
+
+// ---- nqs_energy_gradient_noalloc: the same computation with its 2W-double scratch in a
+// file-scope device array instead of a caller workspace. Every call on a device shares the one
+// array; the centred energies are written in full by k_center_eps before k_gemv_t reads them,
+// so nothing in it has to start at zero. Calls that overlap in time on one device race.
+static __device__ __align__(256) double g_eg_scratch[2 * NQS_NOALLOC_MAX_WALKERS];
+
+namespace {
+constexpr int kScratchDevices = 64;
+std::mutex g_eg_scratch_mu;
+double* g_eg_scratch_ptr[kScratchDevices];  // address of g_eg_scratch per device ordinal
+}  // namespace
+
+// Resolves the scratch address of the current device once (cudaGetSymbolAddress with that
+// device current) and caches it per ordinal.
+static int eg_scratch(double** out) {
+  int dev = -1;
+  cudaError_t rc = cudaGetDevice(&dev);
+  if (rc != cudaSuccess) {
+    set_error("nqs_energy_gradient_noalloc: cudaGetDevice: %s", cudaGetErrorString(rc));
+    return NQS_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kScratchDevices) {
+    set_error("nqs_energy_gradient_noalloc: device ordinal %d >= %d", dev, kScratchDevices);
+    return NQS_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_eg_scratch_mu);
+  if (!g_eg_scratch_ptr[dev]) {
+    void* p = nullptr;
+    rc = cudaGetSymbolAddress(&p, g_eg_scratch);
+    if (rc != cudaSuccess || !p) {
+      set_error("nqs_energy_gradient_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+                cudaGetErrorString(rc));
+      return NQS_ERR_CUDA;
+    }
+    g_eg_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_eg_scratch_ptr[dev];
+  return NQS_OK;
+}
+
+int nqs_energy_gradient_noalloc(const void* O, int o_dtype, const double* e, int W, int64_t P,
+                                double* out_grad, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!O || !e || !out_grad || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1)) {
+    set_error("nqs_energy_gradient_noalloc: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  if (W > NQS_NOALLOC_MAX_WALKERS) {
+    set_error("nqs_energy_gradient_noalloc: n_walkers=%d exceeds the static scratch limit of %d "
+              "walkers; use nqs_energy_gradient with a workspace",
+              W, NQS_NOALLOC_MAX_WALKERS);
+    return NQS_ERR_UNSUPPORTED;
+  }
+  double* x = nullptr;
+  NQS_TRY(eg_scratch(&x));
+  k_center_eps<<<1, 1024, 0, st>>>((const cplx*)e, W, x);
+  NQS_CHECK_LAUNCH("k_center_eps");
+  const unsigned gp = (unsigned)((P + 255) / 256);
   if (o_dtype == 0)
     k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)O, 2 * W, 2 * W, P, nullptr, x, out_grad,
                                          nullptr, nullptr, 0.0);

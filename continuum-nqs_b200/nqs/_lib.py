@@ -173,6 +173,8 @@ _SIGS.update({
     "nqs_clip_energies": ([c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p], c_int),
     "nqs_energy_gradient": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_size_t,
                              c_void_p], c_int),
+    "nqs_energy_gradient_noalloc": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p,
+                                     c_void_p], c_int),
     "nqs_adam_update": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_double,
                          c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),

@@ -202,6 +202,18 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
 int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int n_walkers,
                         int64_t n_params, double* out_grad, void* workspace,
                         size_t workspace_bytes, void* stream);
+/* nqs_energy_gradient for callers that hold no workspace and must not allocate device memory.
+ * No counterpart in the reference: it exists for callers such as a framework's custom-call
+ * handler whose allocator owns the device memory. Same result as nqs_energy_gradient; its 2W
+ * doubles of scratch are a file-scope device array inside libnqs (512 KiB per device), so it
+ * allocates nothing and n_walkers is limited to NQS_NOALLOC_MAX_WALKERS (larger: returns
+ * NQS_ERR_UNSUPPORTED with the reason in nqs_last_error). The first call on each device resolves
+ * that array's address with the device current; make it before any stream capture. All calls on
+ * a device share the array: calls that overlap in time (other streams, other host threads) race
+ * and must be serialised by the caller. */
+#define NQS_NOALLOC_MAX_WALKERS 32768
+int nqs_energy_gradient_noalloc(const void* O, int o_dtype, const double* e, int n_walkers,
+                                int64_t n_params, double* out_grad, void* stream);
 /* Adam step (optax.adam defaults b1 0.9, b2 0.999, eps 1e-8) on the real ravel theta; t >= 1 is
  * the step count used for bias correction. m, v: float64[P] moment buffers (start at 0). */
 int nqs_adam_update(double* theta, const double* grad, double* m, double* v, int64_t n_params,
