@@ -370,94 +370,161 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
   return NQS_OK;
 }
 
-// Triangular solves on the whole GPU (cooperative launch, grid.sync between block steps):
-// per 64-wide block the first CTA solves the diagonal block with one warp, then every warp of the
-// grid updates the remaining rows (forward) / columns (transposed) against that block.
-__device__ __forceinline__ void diag_solve_warp(const double* __restrict__ L, int64_t ldl, int k0,
-                                                int b, double* __restrict__ v,
-                                                double* __restrict__ xb, bool transposed) {
-  const int lane = threadIdx.x & 31;
-  double x0 = lane < b ? v[k0 + lane] : 0.0, x1 = lane + 32 < b ? v[k0 + lane + 32] : 0.0;
-  if (!transposed) {
-    for (int j = 0; j < b; ++j) {
-      const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
-                        L[(size_t)(k0 + j) * ldl + k0 + j];
-      if (lane == (j & 31)) {
-        if (j < 32) x0 = xj; else x1 = xj;
+// Inverses of the 64x64 diagonal blocks of a lower-triangular L: dinv[s] = L_ss^-1 (row-major
+// 64x64 per block, zero-padded past n). One CTA per block, one thread per column of the inverse
+// (forward substitution against e_j in shared memory).
+__global__ void __launch_bounds__(CB) k_trtri_diag(const double* __restrict__ L, int64_t ldl, int n,
+                                                   double* __restrict__ dinv) {
+  extern __shared__ double trtri_sm[];
+  double(*Ls)[CB + 1] = reinterpret_cast<double(*)[CB + 1]>(trtri_sm);
+  double(*X)[CB + 1] = Ls + CB;
+  const int s = blockIdx.x, k0 = s * CB, b = min(CB, n - k0);
+  for (int idx = threadIdx.x; idx < CB * CB; idx += blockDim.x) {
+    const int i = idx / CB, j = idx - i * CB;
+    Ls[i][j] = (i < b && j <= i) ? L[(size_t)(k0 + i) * ldl + k0 + j] : 0.0;
+    X[i][j] = 0.0;
+  }
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j < b) {
+    X[j][j] = 1.0 / Ls[j][j];
+    for (int i = j + 1; i < b; ++i) {
+      double a0 = 0.0, a1 = 0.0;
+      int k = j;
+      for (; k + 1 < i; k += 2) {
+        a0 = fma(Ls[i][k], X[k][j], a0);
+        a1 = fma(Ls[i][k + 1], X[k + 1][j], a1);
       }
-      if (lane > j && lane < b) x0 -= xj * L[(size_t)(k0 + lane) * ldl + k0 + j];
-      if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[(size_t)(k0 + lane + 32) * ldl + k0 + j];
-    }
-  } else {
-    for (int j = b - 1; j >= 0; --j) {
-      const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31) /
-                        L[(size_t)(k0 + j) * ldl + k0 + j];
-      if (lane == (j & 31)) {
-        if (j < 32) x0 = xj; else x1 = xj;
-      }
-      if (lane < j) x0 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane];
-      if (lane + 32 < j) x1 -= xj * L[(size_t)(k0 + j) * ldl + k0 + lane + 32];
+      if (k < i) a0 = fma(Ls[i][k], X[k][j], a0);
+      X[i][j] = -(a0 + a1) / Ls[i][i];
     }
   }
-  if (lane < b) {
-    v[k0 + lane] = x0;
-    xb[lane] = x0;
-  }
-  if (lane + 32 < b) {
-    v[k0 + lane + 32] = x1;
-    xb[lane + 32] = x1;
+  __syncthreads();
+  double* D = dinv + (size_t)s * CB * CB;
+  for (int idx = threadIdx.x; idx < CB * CB; idx += blockDim.x) {
+    const int i = idx / CB, jj = idx - i * CB;
+    D[idx] = X[i][jj];
   }
 }
 
-// Solves L x = v (transposed = 0) or L^T x = v (transposed = 1) in place with one grid barrier
-// per 64-block (look-ahead): in step s the first CTA applies x_s to block s+1 and solves that
-// diagonal block, while every other CTA applies x_s to the blocks beyond it. xb: 2 x 64 doubles.
+// doubles of the triangular-solve scratch for order n: 2 x 64 exchange + one 64x64 inverse per block
+inline size_t trsv_elems(size_t n) { return 2 * CB + ((n + CB - 1) / CB) * CB * CB; }
+
+static int trtri_diag(const double* L, int64_t ldl, int n, double* dinv, cudaStream_t st) {
+  const size_t sm = sizeof(double) * 2 * CB * (CB + 1);
+  cudaFuncSetAttribute(k_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_trtri_diag<<<(n + CB - 1) / CB, CB, sm, st>>>(L, ldl, n, dinv);
+  NQS_CHECK_LAUNCH("k_trtri_diag");
+  return NQS_OK;
+}
+
+// Triangular solves on the whole GPU (cooperative launch, one grid barrier per 64-block):
+//   forward   L x = v:   x_s = D_s (v_s - sum_{t<s} L_st x_t)
+//   transposed L^T x = v: x_s = D_s^T (v_s - sum_{t>s} L_ts^T x_t),   D_s = L_ss^-1 (k_trtri_diag)
+// In step s the first CTA applies x_s to block s+1 and multiplies by D_{s+1} (two 64x64 mat-vecs
+// whose operands it loaded into registers before the previous barrier), while every other CTA
+// applies x_s to the blocks beyond s+1. v is overwritten with x; xb: 2 x 64 doubles.
 __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L, int64_t ldl,
-                                                   int n, double* __restrict__ v,
+                                                   int n, const double* __restrict__ dinv,
+                                                   double* __restrict__ v,
                                                    double* __restrict__ xb, int transposed) {
   cg::grid_group grid = cg::this_grid();
   const int nblk = (n + CB - 1) / CB;
-  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, lane = tid & 31;
   __shared__ double xs[CB];
+  __shared__ double vs[CB];
+  __shared__ double red[4][CB];
   auto blk = [&](int s) { return transposed ? nblk - 1 - s : s; };
-  if (blockIdx.x == 0 && threadIdx.x < 32) {
-    const int k0 = blk(0) * CB;
-    diag_solve_warp(L, ldl, k0, min(CB, n - k0), v, xb, transposed);
+  // CTA 0's thread layout for a 64x64 mat-vec y = A x: forward (row-major A): row = tid / 4,
+  // columns q*16 .. q*16+15 (q = tid % 4); transposed: column m = tid % 64, rows q*16.. (q = tid / 64)
+  double lreg[16], dreg[16];
+  auto load_next = [&](int s1) {  // operands of step s1-1 -> block s1 (L panel) and D_{s1}
+    const int kb = blk(s1) * CB, bb = min(CB, n - kb);
+    const double* D = dinv + (size_t)blk(s1) * CB * CB;
+    if (!transposed) {
+      const int r = tid >> 2, q = tid & 3;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) dreg[c] = D[r * CB + q * 16 + c];
+      if (s1 > 0) {
+        const int kp = blk(s1 - 1) * CB, bp = min(CB, n - kp);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int col = q * 16 + c;
+          lreg[c] = (r < bb && col < bp) ? L[(size_t)(kb + r) * ldl + kp + col] : 0.0;
+        }
+      }
+    } else {
+      const int m = tid & 63, q = tid >> 6;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) dreg[c] = D[(q * 16 + c) * CB + m];
+      if (s1 > 0) {
+        const int kp = blk(s1 - 1) * CB, bp = min(CB, n - kp);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int row = q * 16 + c;
+          lreg[c] = (m < bb && row < bp) ? L[(size_t)(kp + row) * ldl + kb + m] : 0.0;
+        }
+      }
+    }
+  };
+  // y = A_reg . x (x in shared memory, 64 long) reduced over the 4 partial sums -> out[64]
+  auto matvec = [&](const double* reg, const double* x, double* out) {
+    double acc = 0.0;
+    if (!transposed) {
+      const int q = tid & 3;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) acc = fma(reg[c], x[q * 16 + c], acc);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      if (q == 0) out[tid >> 2] = acc;
+    } else {
+      const int q = tid >> 6;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) acc = fma(reg[c], x[q * 16 + c], acc);
+      red[q][tid & 63] = acc;
+      __syncthreads();
+      if (tid < CB) out[tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    }
+  };
+  if (blockIdx.x == 0) {
+    const int k0 = blk(0) * CB, b = min(CB, n - k0);
+    load_next(0);
+    if (tid < CB) vs[tid] = tid < b ? v[k0 + tid] : 0.0;
+    __syncthreads();
+    matvec(dreg, vs, xs);
+    __syncthreads();
+    if (tid < b) {
+      v[k0 + tid] = xs[tid];
+      xb[tid] = xs[tid];
+    }
+    if (nblk > 1) load_next(1);
   }
   grid.sync();
   for (int s = 0; s < nblk; ++s) {
     const int k0 = blk(s) * CB, b = min(CB, n - k0);
     const double* xcur = xb + (s & 1) * CB;
-    for (int i = threadIdx.x; i < b; i += blockDim.x) xs[i] = xcur[i];
+    if (tid < CB) xs[tid] = tid < b ? xcur[tid] : 0.0;
     __syncthreads();
     const bool more = s + 1 < nblk;
     const int k1 = more ? blk(s + 1) * CB : 0, b1 = more ? min(CB, n - k1) : 0;
     if (blockIdx.x == 0) {
       if (more) {
-        // apply x_s to block s+1, then solve it
-        const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (!transposed) {
-          for (int r = k1 + w; r < k1 + b1; r += nw) {
-            const double* lr = L + (size_t)r * ldl + k0;
-            double acc = 0.0;
-            for (int jj = lane; jj < b; jj += 32) acc = fma(lr[jj], xs[jj], acc);
-            acc = warp_sum(acc);
-            if (lane == 0) v[r] -= acc;
-          }
-        } else {
-          for (int m = k1 + threadIdx.x; m < k1 + b1; m += blockDim.x) {
-            double acc = 0.0;
-            for (int jj = 0; jj < b; ++jj) acc = fma(L[(size_t)(k0 + jj) * ldl + m], xs[jj], acc);
-            v[m] -= acc;
-          }
-        }
+        matvec(lreg, xs, vs);  // vs = L-panel . x_s
         __syncthreads();
-        if (threadIdx.x < 32)
-          diag_solve_warp(L, ldl, k1, b1, v, xb + ((s + 1) & 1) * CB, transposed);
+        if (tid < CB) vs[tid] = tid < b1 ? v[k1 + tid] - vs[tid] : 0.0;
+        __syncthreads();
+        matvec(dreg, vs, xs);  // x_{s+1} = D_{s+1} v
+        __syncthreads();
+        double* xn = xb + ((s + 1) & 1) * CB;
+        if (tid < b1) {
+          v[k1 + tid] = xs[tid];
+          xn[tid] = xs[tid];
+        }
+        if (s + 2 < nblk) load_next(s + 2);
       }
     } else {
       // every other CTA: apply x_s to the rows (columns) beyond block s+1
-      const int gw = ((blockIdx.x - 1) * blockDim.x + threadIdx.x) >> 5;
+      const int gw = ((blockIdx.x - 1) * blockDim.x + tid) >> 5;
       const int nwk = ((gridDim.x - 1) * blockDim.x) >> 5;
       if (!transposed) {
         for (int r = k0 + b + b1 + gw; r < n; r += nwk) {
@@ -469,7 +536,7 @@ __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L,
         }
       } else {
         const int lim = more ? k1 : 0;  // columns below block s+1's start
-        for (int m = (blockIdx.x - 1) * blockDim.x + threadIdx.x; m < lim;
+        for (int m = (blockIdx.x - 1) * blockDim.x + tid; m < lim;
              m += (gridDim.x - 1) * blockDim.x) {
           double acc = 0.0;
           for (int jj = 0; jj < b; ++jj) acc = fma(L[(size_t)(k0 + jj) * ldl + m], xs[jj], acc);
@@ -481,8 +548,8 @@ __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L,
   }
 }
 
-static int trsv_grid(const double* L, int64_t ldl, int n, double* v, double* xb, int transposed,
-                     cudaStream_t st) {
+static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, double* v,
+                     double* xb, int transposed, cudaStream_t st) {
   static int grid = 0;
   if (!grid) {
     int dev = 0, nsm = 0, per = 0;
@@ -491,7 +558,8 @@ static int trsv_grid(const double* L, int64_t ldl, int n, double* v, double* xb,
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trsv_grid, 256, 0);
     grid = per >= 1 ? nsm : 1;  // one CTA per SM keeps the grid barrier cheap
   }
-  void* args[] = {(void*)&L, (void*)&ldl, (void*)&n, (void*)&v, (void*)&xb, (void*)&transposed};
+  void* args[] = {(void*)&L,  (void*)&ldl, (void*)&n, (void*)&dinv,
+                  (void*)&v, (void*)&xb,  (void*)&transposed};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_trsv_grid, grid, 256, args, 0, st);
   if (e != cudaSuccess) return cuda_status(e, "k_trsv_grid");
   NQS_CHECK_LAUNCH("k_trsv_grid");
@@ -619,54 +687,198 @@ __global__ void k_gemv_t(const TO* __restrict__ O, int M, int Mh, int64_t K,
   if (theta) theta[k] -= lr * hi;
 }
 
-// r[m] = b[m] - lam x[m] - sum_k (O[m][k] - mu[m >= Mh][k]) (v[k] + v_lo[k]), compensated
-// (one CTA per row)
-template <typename TO>
-__global__ void __launch_bounds__(256) k_gemv_n_resid(const TO* __restrict__ O, int M, int Mh,
+// Split form of k_gemv_t for the large solves: each thread owns 4 consecutive columns and one
+// slice of rows (blockIdx.y), writes the double-double partial (s, c) of its slice to
+// part[y][k][2]; k_gemv_t_reduce adds the slices. VEC: K % 4 == 0 (16-byte row starts).
+template <typename TO, bool VEC>
+__global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, int M, int Mh,
                                                       int64_t K, const double* __restrict__ mu,
-                                                      const double* __restrict__ v,
-                                                      const double* __restrict__ v_lo,
-                                                      const double* __restrict__ b, double lam0,
-                                                      const double* __restrict__ lam_extra,
-                                                      const double* __restrict__ x,
-                                                      double* __restrict__ r) {
-  const double lam = lam0 + (lam_extra ? *lam_extra : 0.0);
-  const int m = blockIdx.x;
-  const TO* row = O + (size_t)m * K;
-  const double* mr = mu ? mu + (m >= Mh ? K : 0) : nullptr;
-  DD acc;
-  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-    const double o = (double)row[k] - (mr ? mr[k] : 0.0);
-    acc.add_prod(o, v[k]);
-    acc.add_prod(o, v_lo[k]);
-  }
-  __shared__ double red_s[32], red_c[32];
-  // warp reduction of (s, c) pairs with TwoSum
+                                                      const double* __restrict__ x, int mchunk,
+                                                      double* __restrict__ part) {
+  const int64_t k0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (k0 >= K) return;
+  const int m_lo = blockIdx.y * mchunk, m_hi = min(M, m_lo + mchunk);
+  double m0[4], m1[4];
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const double os = __shfl_xor_sync(0xffffffffu, acc.s, off);
-    const double oc = __shfl_xor_sync(0xffffffffu, acc.c, off);
-    acc.add(os);
-    acc.c += oc;
+  for (int c = 0; c < 4; ++c) {
+    const bool in = k0 + c < K;
+    m0[c] = (mu && in) ? mu[k0 + c] : 0.0;
+    m1[c] = (mu && in) ? mu[K + k0 + c] : 0.0;
   }
-  if ((threadIdx.x & 31) == 0) {
-    red_s[threadIdx.x >> 5] = acc.s;
-    red_c[threadIdx.x >> 5] = acc.c;
+  DD acc[4];
+  for (int m = m_lo; m < m_hi; ++m) {
+    const TO* row = O + (size_t)m * K + k0;
+    double o[4];
+    if (VEC) {
+      if (sizeof(TO) == 4) {
+        const float4 f = *reinterpret_cast<const float4*>(row);
+        o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+      } else {
+        const double2 a = reinterpret_cast<const double2*>(row)[0];
+        const double2 b = reinterpret_cast<const double2*>(row)[1];
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) o[c] = k0 + c < K ? (double)row[c] : 0.0;
+    }
+    const double xm = x[m];
+    const bool lo_half = m < Mh;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c].add_prod(o[c] - (lo_half ? m0[c] : m1[c]), xm);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (k0 + c < K) {
+      double* pp = part + ((size_t)blockIdx.y * K + k0 + c) * 2;
+      pp[0] = acc[c].s;
+      pp[1] = acc[c].c;
+    }
+}
+
+template <typename TO>
+__global__ void k_gemv_t_reduce(const double* __restrict__ part, int nsplit, int64_t K,
+                                double* __restrict__ out, double* __restrict__ out_lo,
+                                double* __restrict__ theta, double lr) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  DD acc;
+  for (int z = 0; z < nsplit; ++z) {
+    const double* pp = part + ((size_t)z * K + k) * 2;
+    acc.add(pp[0]);
+    acc.c += pp[1];
+  }
+  const double hi = acc.s + acc.c;
+  if (out) out[k] = hi;
+  if (out_lo) out_lo[k] = acc.c - (hi - acc.s);
+  if (theta) theta[k] -= lr * hi;
+}
+
+// out = (O - mu)^T x through the split kernel when the scratch holds the slices, else k_gemv_t
+template <typename TO>
+static int gemv_t(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* x,
+                  double* out, double* out_lo, double* theta, double lr, double* part,
+                  size_t part_elems, cudaStream_t st) {
+  int nsplit = std::max(1, std::min(16, M / 512));
+  while (nsplit > 1 && (size_t)nsplit * K * 2 > part_elems) --nsplit;
+  if (nsplit <= 1 || !part) {
+    k_gemv_t<TO><<<(unsigned)((K + 255) / 256), 256, 0, st>>>(O, M, Mh, K, mu, x, out, out_lo,
+                                                               theta, lr);
+    NQS_CHECK_LAUNCH("k_gemv_t");
+    return NQS_OK;
+  }
+  const int mchunk = (M + nsplit - 1) / nsplit;
+  const dim3 g((unsigned)((K + 1023) / 1024), (unsigned)nsplit);
+  if (K % 4 == 0)
+    k_gemv_t_split<TO, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part);
+  else
+    k_gemv_t_split<TO, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part);
+  NQS_CHECK_LAUNCH("k_gemv_t_split");
+  k_gemv_t_reduce<TO><<<(unsigned)((K + 255) / 256), 256, 0, st>>>(part, nsplit, K, out, out_lo,
+                                                                   theta, lr);
+  NQS_CHECK_LAUNCH("k_gemv_t_reduce");
+  return NQS_OK;
+}
+
+// Residual r = b - lam x - (O - mu)(v + v_lo) for RB rows per CTA (v, v_lo and mu read once per
+// CTA for all its rows), double-double accumulation; 4 consecutive columns per thread when VEC.
+template <typename TO, int RB, bool VEC>
+__global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
+    const TO* __restrict__ O, int M, int Mh, int64_t K, const double* __restrict__ mu,
+    const double* __restrict__ v, const double* __restrict__ v_lo, const double* __restrict__ b,
+    double lam0, const double* __restrict__ lam_extra, const double* __restrict__ x,
+    double* __restrict__ r) {
+  const double lam = lam0 + (lam_extra ? *lam_extra : 0.0);
+  const int m0 = blockIdx.x * RB;
+  const int nr = min(RB, M - m0);
+  DD acc[RB];
+  bool hi_half[RB];
+#pragma unroll
+  for (int i = 0; i < RB; ++i) hi_half[i] = m0 + i >= Mh;
+  const int64_t step = (int64_t)blockDim.x * 4;
+  for (int64_t k = (int64_t)threadIdx.x * 4; k < K; k += step) {
+    double vv[4], vl[4], u0[4], u1[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const bool in = VEC || k + c < K;
+      vv[c] = in ? v[k + c] : 0.0;
+      vl[c] = in ? v_lo[k + c] : 0.0;
+      u0[c] = (mu && in) ? mu[k + c] : 0.0;
+      u1[c] = (mu && in) ? mu[K + k + c] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < RB; ++i) {
+      if (i >= nr) break;
+      const TO* row = O + (size_t)(m0 + i) * K + k;
+      double o[4];
+      if (VEC) {
+        if (sizeof(TO) == 4) {
+          const float4 f = *reinterpret_cast<const float4*>(row);
+          o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+        } else {
+          const double2 a = reinterpret_cast<const double2*>(row)[0];
+          const double2 bb = reinterpret_cast<const double2*>(row)[1];
+          o[0] = a.x; o[1] = a.y; o[2] = bb.x; o[3] = bb.y;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) o[c] = k + c < K ? (double)row[c] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double oc = o[c] - (hi_half[i] ? u1[c] : u0[c]);
+        acc[i].add_prod(oc, vv[c]);
+        acc[i].add_prod(oc, vl[c]);
+      }
+    }
+  }
+  __shared__ double red_s[RB][8], red_c[RB][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < RB; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double os = __shfl_xor_sync(0xffffffffu, acc[i].s, off);
+      const double oc = __shfl_xor_sync(0xffffffffu, acc[i].c, off);
+      acc[i].add(os);
+      acc[i].c += oc;
+    }
+    if (lane == 0) {
+      red_s[i][w] = acc[i].s;
+      red_c[i][w] = acc[i].c;
+    }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < nr) {
+    const int i = threadIdx.x, m = m0 + i;
     DD t;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-      t.add(red_s[i]);
-      t.c += red_c[i];
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      t.add(red_s[i][q]);
+      t.c += red_c[i][q];
     }
-    DD q;  // b - lam x - t
-    q.add(b[m]);
-    q.add_prod(-lam, x[m]);
-    q.add(-t.s);
-    q.c -= t.c;
-    r[m] = q.s + q.c;
+    DD qd;  // b - lam x - t
+    qd.add(b[m]);
+    qd.add_prod(-lam, x[m]);
+    qd.add(-t.s);
+    qd.c -= t.c;
+    r[m] = qd.s + qd.c;
   }
+}
+
+template <typename TO>
+static int gemv_n_resid(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* v,
+                        const double* v_lo, const double* b, double lam0, const double* lam_extra,
+                        const double* x, double* r, cudaStream_t st) {
+  constexpr int RB = 4;
+  const unsigned g = (unsigned)((M + RB - 1) / RB);
+  if (K % 4 == 0)
+    k_gemv_n_resid_rows<TO, RB, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, v_lo, b, lam0,
+                                                         lam_extra, x, r);
+  else
+    k_gemv_n_resid_rows<TO, RB, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, v_lo, b, lam0,
+                                                          lam_extra, x, r);
+  NQS_CHECK_LAUNCH("k_gemv_n_resid_rows");
+  return NQS_OK;
 }
 
 __global__ void k_scale_vec(double* x, int64_t n, double s) {
@@ -702,19 +914,17 @@ static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
                          const double* mu, double lam, const double* lam_extra, const double* b,
                          double* y, double* r,
                          double* tmpK, double* tmpK_lo, double* xb, int n_refine,
-                         cudaStream_t st) {
+                         double* part, size_t part_elems, cudaStream_t st) {
+  double* dinv = xb + 2 * CB;  // the diagonal-block inverses follow the 2 x 64 exchange buffer
+  NQS_TRY(trtri_diag(L, M, M, dinv, st));
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
-  NQS_TRY(trsv_grid(L, M, M, y, xb, 0, st));
-  NQS_TRY(trsv_grid(L, M, M, y, xb, 1, st));
-  const unsigned gk = (unsigned)((K + 255) / 256);
+  NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 0, st));
+  NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 1, st));
   for (int it = 0; it < n_refine; ++it) {
-    k_gemv_t<TO><<<gk, 256, 0, st>>>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0);
-    NQS_CHECK_LAUNCH("k_gemv_t");
-    k_gemv_n_resid<TO><<<M, 256, 0, st>>>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, lam_extra, y,
-                                          r);
-    NQS_CHECK_LAUNCH("k_gemv_n_resid");
-    NQS_TRY(trsv_grid(L, M, M, r, xb, 0, st));
-    NQS_TRY(trsv_grid(L, M, M, r, xb, 1, st));
+    NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0, part, part_elems, st));
+    NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, lam_extra, y, r, st));
+    NQS_TRY(trsv_grid(L, M, M, dinv, r, xb, 0, st));
+    NQS_TRY(trsv_grid(L, M, M, dinv, r, xb, 1, st));
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
     NQS_CHECK_LAUNCH("k_axpy");
   }
@@ -823,7 +1033,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
-  add(sizeof(double) * 2 * CB);         // triangular-solve blocks (double-buffered)
+  add(sizeof(double) * trsv_elems(n));  // triangular-solve exchange + diagonal-block inverses
   add(sizeof(int) * 4);                 // status
   add(sizeof(double) * 2);              // pivot floor, extra damping
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
@@ -867,7 +1077,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* r = ws.take<double>(n);
   double* tmpK = ws.take<double>(P);
   double* tmpK_lo = ws.take<double>(P);
-  double* xb = ws.take<double>(2 * CB);
+  double* xb = ws.take<double>(trsv_elems(n));
   double* rsum = ws.take<double>(2 * (size_t)n + 5);
   double* T = ws.take<double>((size_t)n * n);
   int* bad = ws.take<int>(4);
@@ -944,18 +1154,16 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
   if (op_dtype == 0)
     NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
-                                  tmpK_lo, xb, n_refine, st));
+                                  tmpK_lo, xb, n_refine, part, part_elems, st));
   else
     NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
-                                 tmpK_lo, xb, n_refine, st));
-  const unsigned gp = (unsigned)((P + 255) / 256);
+                                 tmpK_lo, xb, n_refine, part, part_elems, st));
   if (op_dtype == 0)
-    k_gemv_t<double><<<gp, 256, 0, st>>>((const double*)Oop, n, W, P, mu_op, y, out_dtheta,
-                                         nullptr, theta_io, lr);
+    NQS_TRY(gemv_t<double>((const double*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io,
+                           lr, part, part_elems, st));
   else
-    k_gemv_t<float><<<gp, 256, 0, st>>>((const float*)Oop, n, W, P, mu_op, y, out_dtheta,
-                                        nullptr, theta_io, lr);
-  NQS_CHECK_LAUNCH("k_gemv_t");
+    NQS_TRY(gemv_t<float>((const float*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io, lr,
+                          part, part_elems, st));
   if (status_dev) cudaMemcpyAsync(status_dev, bad, 3 * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return NQS_OK;
 }
@@ -963,7 +1171,7 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
-  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + 2 * CB +
+  *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + trsv_elems(m) +
                              std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 8192;
   return NQS_OK;
 }
@@ -992,10 +1200,10 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
   NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
-  double* xb = ws.take<double>(2 * CB);
+  double* xb = ws.take<double>(trsv_elems(M));
   if (!xb) return NQS_ERR_WORKSPACE;
   NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, nullptr, rhs, x, r, tmpK, tmpK_lo, xb,
-                                3, st));
+                                3, part, pe, st));
   return NQS_OK;
 }
 

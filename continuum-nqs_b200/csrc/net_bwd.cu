@@ -574,14 +574,11 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
   }
   ORows<TO> orows{O, dsc.n_params, W};
   const size_t hsm = head_bwd_smem(N, mc.nG, mc.K, mc.learnable_env);
-  const size_t asm_ = attention_smem<T>(N, d / H);
-  const int awpc = attention_wpc<T>(N, d / H);
   const size_t absm = sizeof(T) * (size_t)(5 * N * (d / H) + 2 * N * N + N);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_head_bwd<T, T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          220 * 1024);
-    cudaFuncSetAttribute(k_attention<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_attn_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_ln_bwd<T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
@@ -608,9 +605,7 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
       g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
       NQS_TRY(launch_gemm<T>(g, st));
-      k_attention<T><<<(nw * H + awpc - 1) / awpc, 32 * awpc, asm_, st>>>(nw, N, 1, 0, 0, d, H,
-                                                                         b.qkv[l], b.ao[l]);
-      NQS_CHECK_LAUNCH("k_attention");
+      NQS_TRY(launch_attention<T>(nw, N, 1, 0, 0, d, H, b.qkv[l], b.ao[l], st));
       g = GemmArgs<T>{};
       g.X = b.ao[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
       g.Y = b.xmid[l]; g.ldy = d; g.Res = x; g.ldr = d; g.nseg = 1;

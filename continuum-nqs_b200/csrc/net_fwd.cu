@@ -49,11 +49,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
   }
   const bool tan = jb.n_tan > 0;
   const bool tcn = sizeof(T) == 4 && w.tc.on;
-  const size_t asm_ = attention_smem<T>(N, d / mc.H);
-  const int awpc = attention_wpc<T>(N, d / mc.H);
   static bool attr_set = false;  // per-instantiation one-time opt-in to large shared memory
   if (!attr_set) {
-    cudaFuncSetAttribute(k_attention<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_head<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
     cudaFuncSetAttribute(k_head<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
     attr_set = true;
@@ -88,10 +85,7 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
         NQS_TRY(launch_gemm<T>(g, st));
       }
-      k_attention<T><<<(cb.n_jobs * mc.H + awpc - 1) / awpc, 32 * awpc, asm_, st>>>(
-          cb.n_jobs, N, C, cb.n_tan, cb.has_lap,
-                                                          d, mc.H, Big, Att);
-      NQS_CHECK_LAUNCH("k_attention");
+      NQS_TRY(launch_attention<T>(cb.n_jobs, N, C, cb.n_tan, cb.has_lap, d, mc.H, Big, Att, st));
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Att, d, rows, d, w.tc.wo[b], d, d, (const float*)bw.bo,
                            C, (const float*)X, d, (float*)X, d, w.tc.err, st));

@@ -452,6 +452,290 @@ __global__ void __launch_bounds__(256) k_attention(int n_jobs, int N, int C, int
   }
 }
 
+// --------------------------------------------------------------------------------------------
+// Register-tiled attention for N <= 16 tokens and head width HD in {4, 8, 16}: same arithmetic as
+// k_attention, one warp per (job, head). Lane pair (2i, 2i+1) owns query row i; lane parity hh
+// owns keys j = 2m + hh (m < 8) for scores / probabilities / P_qk / P_sq, and output features
+// hh*HD/2 .. hh*HD/2 + HD/2-1 for outputs / P_av. Each channel's Q, K, V head tiles (16 x HD) are
+// staged into shared memory with cp.async, double-buffered one channel ahead; the value channel's
+// K, V stay resident. Interleaving the keys between the lanes of a pair keeps the two rows that a
+// warp reads at one time in different banks, and every other lane reads the same address
+// (broadcast).
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+// NEL contiguous elements from shared memory; 16-byte loads when the row allows them
+template <typename T, int NEL>
+__device__ __forceinline__ void lds_row(const T* __restrict__ p, T* r) {
+  if constexpr ((NEL * sizeof(T)) % 16 == 0) {
+    constexpr int V = 16 / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < NEL / V; ++c) {
+      const int4 v = reinterpret_cast<const int4*>(p)[c];
+      const T* t = reinterpret_cast<const T*>(&v);
+#pragma unroll
+      for (int e = 0; e < V; ++e) r[c * V + e] = t[e];
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < NEL; ++e) r[e] = p[e];
+  }
+}
+template <typename T, int NEL>
+__device__ __forceinline__ void stg_row(T* __restrict__ p, const T* r) {
+  if constexpr ((NEL * sizeof(T)) % 16 == 0) {
+    constexpr int V = 16 / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < NEL / V; ++c) {
+      int4 v;
+      T* t = reinterpret_cast<T*>(&v);
+#pragma unroll
+      for (int e = 0; e < V; ++e) t[e] = r[c * V + e];
+      reinterpret_cast<int4*>(p)[c] = v;
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < NEL; ++e) p[e] = r[e];
+  }
+}
+
+constexpr int kAttnTok = 16;  // token slots of k_attention_rt
+
+template <typename T, int HD>
+__host__ __device__ constexpr size_t attention_rt_warp_bytes() {
+  return sizeof(T) * 8 * kAttnTok * HD;  // resident K, V + two buffers of Q, K, V
+}
+
+template <typename T, int HD, bool LAP>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(int n_jobs, int N, int C, int n_tan,
+                                                         int d, int H, const T* __restrict__ QKV,
+                                                         T* __restrict__ OUT) {
+  constexpr bool has_lap = LAP;
+  constexpr int NT = kAttnTok, HE = HD / 2, V = 16 / sizeof(T), CH = HD / V;  // 16-B chunks/row
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int pair = blockIdx.x * nwarp + wib;
+  if (pair >= n_jobs * H) return;  // whole warp; no block-level barrier below
+  const int job = pair / H, h = pair - job * H;
+  const int i = lane >> 1, hh = lane & 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Kv = reinterpret_cast<T*>(smraw + (size_t)wib * attention_rt_warp_bytes<T, HD>());
+  T* Vv = Kv + NT * HD;
+  T* buf = Vv + NT * HD;  // buf + b * 3 * NT * HD: Q, K, V tiles of one channel
+  const int ld = 3 * d;
+  const T sc = T(1) / sqrt(T(HD));
+  // rows >= N are never copied: zero them once (zero probabilities times zero values)
+  for (int idx = lane; idx < 8 * NT * HD; idx += 32) Kv[idx] = T(0);
+  __syncwarp();
+  auto issue = [&](int c, int b) {
+    if (c < C) {
+      T* dst = buf + b * 3 * NT * HD;
+      for (int q = lane; q < 3 * N * CH; q += 32) {
+        const int t = q / (N * CH), r = q - t * (N * CH), tok = r / CH, ch = r - tok * CH;
+        const T* src = QKV + (((size_t)job * N + tok) * C + c) * ld + t * d + h * HD + ch * V;
+        cp_async16(dst + (t * NT + tok) * HD + ch * V, src);
+      }
+    }
+    cp_async_commit();
+  };
+  auto out_row = [&](int c) { return OUT + (((size_t)job * N + i) * C + c) * d + h * HD + hh * HE; };
+  const bool live = i < N;
+  // ---- value channel ----
+  issue(0, 0);
+  issue(1, 1);
+  cp_async_wait<1>();
+  __syncwarp();
+  T q[HD], a[8], ao[8];
+  {
+    const T* Q0 = buf;
+    const T* K0 = buf + NT * HD;
+    const T* V0 = buf + 2 * NT * HD;
+    lds_row<T, HD>(Q0 + i * HD, q);
+    T s[8];
+    T mx = T(-INFINITY);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int j = 2 * m + hh;
+      T k[HD];
+      lds_row<T, HD>(K0 + j * HD, k);
+      T acc = 0;
+#pragma unroll
+      for (int e = 0; e < HD; ++e) acc = fma(q[e], k[e], acc);
+      s[m] = j < N ? acc * sc : T(-INFINITY);
+      mx = max(mx, s[m]);
+    }
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    T ssum = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      a[m] = (2 * m + hh < N) ? exp(s[m] - mx) : T(0);
+      ssum += a[m];
+    }
+    ssum += __shfl_xor_sync(0xffffffffu, ssum, 1);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      a[m] = a[m] / ssum;
+      ao[m] = __shfl_xor_sync(0xffffffffu, a[m], 1);
+    }
+    T o[HE];
+#pragma unroll
+    for (int e = 0; e < HE; ++e) o[e] = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      T v0[HE], v1[HE];
+      lds_row<T, HE>(V0 + (2 * m + hh) * HD + hh * HE, v0);
+      lds_row<T, HE>(V0 + (2 * m + 1 - hh) * HD + hh * HE, v1);
+#pragma unroll
+      for (int e = 0; e < HE; ++e) o[e] = fma(a[m], v0[e], fma(ao[m], v1[e], o[e]));
+    }
+    if (live) stg_row<T, HE>(out_row(0), o);
+    // keep the value channel's K, V resident
+    for (int idx = lane; idx < N * HD; idx += 32) {
+      Kv[idx] = K0[idx];
+      Vv[idx] = V0[idx];
+    }
+  }
+  __syncwarp();
+  issue(2, 0);
+  T Pqk[8], Psq[8], Pav[HE];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) Pqk[m] = Psq[m] = T(0);
+#pragma unroll
+  for (int e = 0; e < HE; ++e) Pav[e] = T(0);
+  // ---- tangent channels ----
+  for (int t = 0; t < n_tan; ++t) {
+    const int c = 1 + t, b = c & 1;
+    cp_async_wait<1>();
+    __syncwarp();
+    const T* Qt = buf + b * 3 * NT * HD;
+    const T* Kt = Qt + NT * HD;
+    const T* Vt = Kt + NT * HD;
+    T qt[HD], st[8];
+    lds_row<T, HD>(Qt + i * HD, qt);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int j = 2 * m + hh;
+      T k[HD], kt[HD];
+      lds_row<T, HD>(Kv + j * HD, k);
+      lds_row<T, HD>(Kt + j * HD, kt);
+      T s1 = 0, s2 = 0;
+#pragma unroll
+      for (int e = 0; e < HD; ++e) {
+        s1 = fma(qt[e], k[e], s1);
+        s1 = fma(q[e], kt[e], s1);
+        s2 = fma(qt[e], kt[e], s2);
+      }
+      st[m] = s1 * sc;
+      if (has_lap) Pqk[m] += s2;
+    }
+    T lt = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lt = fma(a[m], st[m], lt);
+    lt += __shfl_xor_sync(0xffffffffu, lt, 1);
+    T sto[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const T ds = st[m] - lt;
+      if (has_lap) Psq[m] += ds * ds;
+      st[m] = a[m] * ds;
+      sto[m] = __shfl_xor_sync(0xffffffffu, st[m], 1);
+    }
+    T o[HE];
+#pragma unroll
+    for (int e = 0; e < HE; ++e) o[e] = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int j0 = 2 * m + hh, j1 = 2 * m + 1 - hh;
+      T v0[HE], v1[HE], w0[HE], w1[HE];
+      lds_row<T, HE>(Vv + j0 * HD + hh * HE, v0);
+      lds_row<T, HE>(Vv + j1 * HD + hh * HE, v1);
+      lds_row<T, HE>(Vt + j0 * HD + hh * HE, w0);
+      lds_row<T, HE>(Vt + j1 * HD + hh * HE, w1);
+#pragma unroll
+      for (int e = 0; e < HE; ++e) {
+        o[e] = fma(st[m], v0[e], o[e]);
+        o[e] = fma(a[m], w0[e], o[e]);
+        o[e] = fma(sto[m], v1[e], o[e]);
+        o[e] = fma(ao[m], w1[e], o[e]);
+        if (has_lap) Pav[e] = fma(st[m], w0[e], fma(sto[m], w1[e], Pav[e]));
+      }
+    }
+    if (live) stg_row<T, HE>(out_row(c), o);
+    __syncwarp();
+    issue(c + 2, b);
+  }
+  if (!has_lap) {
+    cp_async_wait<0>();
+    return;
+  }
+  // ---- Laplacian channel (C - 1 = 1 + n_tan) ----
+  {
+    const int c = C - 1, b = c & 1;
+    cp_async_wait<0>();
+    __syncwarp();
+    const T* Ql = buf + b * 3 * NT * HD;
+    const T* Kl = Ql + NT * HD;
+    const T* Vl = Kl + NT * HD;
+    T ql[HD], sl[8];
+    lds_row<T, HD>(Ql + i * HD, ql);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int j = 2 * m + hh;
+      T k[HD], kl[HD];
+      lds_row<T, HD>(Kv + j * HD, k);
+      lds_row<T, HD>(Kl + j * HD, kl);
+      T s1 = 0;
+#pragma unroll
+      for (int e = 0; e < HD; ++e) {
+        s1 = fma(ql[e], k[e], s1);
+        s1 = fma(q[e], kl[e], s1);
+      }
+      sl[m] = (s1 + T(2) * Pqk[m]) * sc;
+    }
+    T ll = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) ll = fma(a[m], sl[m] + Psq[m], ll);
+    ll += __shfl_xor_sync(0xffffffffu, ll, 1);
+    T slo[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      sl[m] = a[m] * (Psq[m] + sl[m] - ll);
+      slo[m] = __shfl_xor_sync(0xffffffffu, sl[m], 1);
+    }
+    T o[HE];
+#pragma unroll
+    for (int e = 0; e < HE; ++e) o[e] = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int j0 = 2 * m + hh, j1 = 2 * m + 1 - hh;
+      T v0[HE], v1[HE], w0[HE], w1[HE];
+      lds_row<T, HE>(Vv + j0 * HD + hh * HE, v0);
+      lds_row<T, HE>(Vv + j1 * HD + hh * HE, v1);
+      lds_row<T, HE>(Vl + j0 * HD + hh * HE, w0);
+      lds_row<T, HE>(Vl + j1 * HD + hh * HE, w1);
+#pragma unroll
+      for (int e = 0; e < HE; ++e) {
+        o[e] = fma(sl[m], v0[e], o[e]);
+        o[e] = fma(a[m], w0[e], o[e]);
+        o[e] = fma(slo[m], v1[e], o[e]);
+        o[e] = fma(ao[m], w1[e], o[e]);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < HE; ++e) o[e] += T(2) * Pav[e];
+    if (live) stg_row<T, HE>(out_row(c), o);
+  }
+}
+
 // warps per CTA and dynamic shared memory of k_attention (each warp's slot rounded to 16 bytes)
 template <typename T>
 inline size_t attention_warp_bytes(int N, int hd) {
@@ -467,6 +751,58 @@ inline int attention_wpc(int N, int hd) {
 template <typename T>
 inline size_t attention_smem(int N, int hd) {
   return (size_t)attention_wpc<T>(N, hd) * attention_warp_bytes<T>(N, hd);
+}
+
+// k_attention_rt when N <= 16, the head width is 4, 8 or 16 and rows are 16-byte aligned,
+// else k_attention
+template <typename T, int HD>
+inline int launch_attention_rt(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
+                               const T* QKV, T* OUT, cudaStream_t st) {
+  const size_t wb = attention_rt_warp_bytes<T, HD>();
+  int wpc = 8;
+  while (wpc > 1 && wpc * wb > 96 * 1024) wpc /= 2;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_attention_rt<T, HD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         96 * 1024);
+    cudaFuncSetAttribute(k_attention_rt<T, HD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         96 * 1024);
+    attr = true;
+  }
+  const long long pairs = (long long)n_jobs * H;
+  const unsigned grid = (unsigned)((pairs + wpc - 1) / wpc);
+  if (has_lap)
+    k_attention_rt<T, HD, true><<<grid, 32 * wpc, wpc * wb, st>>>(n_jobs, N, C, n_tan, d, H, QKV,
+                                                                   OUT);
+  else
+    k_attention_rt<T, HD, false><<<grid, 32 * wpc, wpc * wb, st>>>(n_jobs, N, C, n_tan, d, H, QKV,
+                                                                    OUT);
+  NQS_CHECK_LAUNCH("k_attention_rt");
+  return NQS_OK;
+}
+
+template <typename T>
+inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
+                            const T* QKV, T* OUT, cudaStream_t st) {
+  const int hd = d / H;
+  const bool aligned = ((uintptr_t)QKV % 16 == 0) && ((uintptr_t)OUT % 16 == 0) &&
+                       ((size_t)d * sizeof(T)) % 16 == 0;
+  if (N <= kAttnTok && aligned && C == 1 + n_tan + has_lap) {
+    if (hd == 16) return launch_attention_rt<T, 16>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+    if (hd == 8) return launch_attention_rt<T, 8>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+    if (hd == 4)
+      return launch_attention_rt<T, 4>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_attention<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const int awpc = attention_wpc<T>(N, hd);
+  k_attention<T><<<(unsigned)(((long long)n_jobs * H + awpc - 1) / awpc), 32 * awpc,
+                   attention_smem<T>(N, hd), st>>>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT);
+  NQS_CHECK_LAUNCH("k_attention");
+  return NQS_OK;
 }
 
 // ============================================================================================
@@ -923,7 +1259,28 @@ __global__ void __launch_bounds__(256) k_head(JobBatch jb, ModelConst mc, const 
         acc.im = warp_sum(acc.im);
         lapk = acc;
       }
-      for (int t = 0; t < n_tan; ++t) {
+      for (int t = 0; t < n_tan && !has_lap; ++t) {
+        // without the Laplacian only tr(M^-1 D_t) = sum_{a,i} M^-1[i][a] D_t[a][i] is needed
+        const int e = te_lo + t / 2, bax = t & 1;
+        cplx trb = mk(0, 0);
+        for (int idx = lane; idx < N * N; idx += 32) {
+          const int a = idx / N, i = idx - a * N;
+          cplx dm = cmul(env[idx], bfval(1 + t, a, i));
+          if (i == e) {
+            cplx de = mk(0, 0);
+            for (int g = 0; g < nG; ++g)
+              cfma(de, cmul(ph[g * N + i], Weff(a, g, sp[i])), mk(0, mc.Gs[2 * g + bax]));
+            const cplx b0 = bfval(0, a, i);
+            dm = cadd(dm, cmul(de, mk(1.0 + b0.re, b0.im)));
+          }
+          cfma(trb, Iw[i * N + a], dm);
+        }
+        trb.re = warp_sum(trb.re);
+        trb.im = warp_sum(trb.im);
+        if (lane == 0) j_dLk(j)[k * n_tan + t] = trb;
+        cfma(sq, trb, trb);
+      }
+      for (int t = 0; t < n_tan && has_lap; ++t) {
         const int e = te_lo + t / 2, bax = t & 1;
         for (int idx = lane; idx < N * N; idx += 32) {  // D_t = d_t M
           const int a = idx / N, i = idx - a * N;
