@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "net_kernels.cuh"
+#include "head_rt.cuh"
 
 namespace nqs {
 
@@ -53,6 +54,12 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
   if (!attr_set) {
     cudaFuncSetAttribute(k_head<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
     cudaFuncSetAttribute(k_head<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+    cudaFuncSetAttribute(k_head_rt<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(k_head_rt<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(k_head_rt<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
     attr_set = true;
   }
   for (int j0 = 0; j0 < jb.n_jobs; j0 += jobs_per_chunk) {
@@ -142,6 +149,26 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       NQS_TRY(launch_gemm<T>(g, st));
     }
     const int jout = j0;
+    if (N <= kHeadTok) {
+      const bool lap = tan && cb.has_lap;
+      const HeadRtPlan rp = head_rt_plan(N, mc.nG, mc.K, cb.n_tan, tan, lap);
+      const unsigned rg = (unsigned)((cb.n_jobs + rp.jpc - 1) / rp.jpc);
+      if (rp.bytes > 200 * 1024) {
+        set_error("head: %zu bytes of shared memory per CTA", rp.bytes);
+        return NQS_ERR_UNSUPPORTED;
+      }
+      if (lap)
+        k_head_rt<T, true, true><<<rg, 64, rp.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
+                                                           rp.jpc, rp.job_bytes, rp.hw_bytes);
+      else if (tan)
+        k_head_rt<T, true, false><<<rg, 64, rp.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
+                                                            rp.jpc, rp.job_bytes, rp.hw_bytes);
+      else
+        k_head_rt<T, false, false><<<rg, 64, rp.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
+                                                             rp.jpc, rp.job_bytes, rp.hw_bytes);
+      NQS_CHECK_LAUNCH("k_head_rt");
+      continue;
+    }
     const HeadPlan hpl = head_plan(N, mc.nG, mc.K, cb.n_tan, tan);
     const unsigned hgrid = (unsigned)((cb.n_jobs + hpl.jpc - 1) / hpl.jpc);
     if (tan) {
