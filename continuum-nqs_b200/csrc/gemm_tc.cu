@@ -2,10 +2,10 @@
 //
 // Y[r, n] = sum_k X[r, k] W[k, n] (+ bias[n] on value rows r % C == 0) (+ Res[r, n]) with X the
 // float32 activations read by TMA as TF32 operands (kind::tf32, float32 accumulation in TMEM) and W
-// pre-transposed to K-major W^T[n][k] once per call. One CTA = one 128-row tile and the whole
-// output width (N <= 256, padded to a multiple of 16); K <= 128 fits in shared memory at once, so
-// each CTA issues all its TMA loads on one mbarrier, one thread issues the MMAs, and four warps
-// drain TMEM. Waits are bounded (tc_common.cuh); an abort is recorded in *err.
+// pre-transposed to K-major W^T[n][k] once per call. Persistent CTAs (one per SM) keep W^T
+// resident in shared memory and stream 128-row tiles of X through a TMA ring; each tile's MMA
+// covers the whole output width (N <= 256, padded to a multiple of 16) and K <= 128. Waits are
+// bounded (tc_common.cuh); an abort is recorded in *err.
 #include <cstdio>
 #include <algorithm>
 #include <vector>
@@ -20,43 +20,72 @@ constexpr int RG_BM = 128;
 constexpr int RG_KB = 32;  // float32 per 128-byte swizzle row
 
 struct RowGemmArgs {
-  int rows, K, Nout, Npad, C, vec4;
+  int rows, K, Nout, Npad, C, res_inplace, stages;
   const float* bias;
-  const float* Res;
-  int ldr;
-  float* Y;
-  int ldy;
   int* err;
 };
 
-__global__ void __launch_bounds__(128, 1) k_rowgemm_tc(const __grid_constant__ CUtensorMap tA,
-                                                       const __grid_constant__ CUtensorMap tB,
-                                                       RowGemmArgs g) {
+// Persistent, warp-specialised: warp 0 streams 128-row A tiles through an S-stage TMA ring (the
+// weight panel W^T is loaded once per CTA and stays resident), warp 1 issues the MMAs into one of
+// two TMEM accumulators, warps 2..5 drain the other accumulator (epilogue of tile i overlaps the
+// MMAs of tile i+1). Tiles are dealt round-robin over the grid.
+constexpr int RG_THREADS = 192;
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_constant__ CUtensorMap tA,
+                                                              const __grid_constant__ CUtensorMap tB,
+                                                              const __grid_constant__ CUtensorMap tY,
+                                                              RowGemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~(uintptr_t)1023);
-  const int nkb = g.K / RG_KB;
+  const int nkb = g.K / RG_KB, S = g.stages;
   const int a_bytes = RG_BM * 128, b_bytes = g.Npad * 128;
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + nkb * a_bytes;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sB + nkb * b_bytes);
-  uint64_t* done = full + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int stage_bytes = nkb * a_bytes;
+  uint8_t* sB = smem;
+  uint8_t* sA = smem + nkb * b_bytes;  // S stages
+  uint8_t* stage_out = sA + S * stage_bytes;  // 4 warps x 2 x (32 x 32 floats, 128B-swizzled)
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(stage_out + 4 * 2 * 4096);
+  uint64_t* afull = bfull + 1;
+  uint64_t* aempty = afull + S;
+  uint64_t* accfull = aempty + S;
+  uint64_t* accempty = accfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accempty + 2);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * RG_BM;
   const uint32_t ncols = g.Npad <= 32 ? 32u : g.Npad <= 64 ? 64u : g.Npad <= 128 ? 128u : 256u;
+  const int ntiles = (g.rows + RG_BM - 1) / RG_BM;
+  const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
   if (threadIdx.x == 0) {
-    mbar_init(full, 1);
-    mbar_init(done, 1);
+    mbar_init(bfull, 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&afull[s], 1);
+      mbar_init(&aempty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accfull[b], 1);
+      mbar_init(&accempty[b], 4);
+    }
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(ncols));
+                 "r"(2 * ncols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   fence_before();
@@ -64,97 +93,120 @@ __global__ void __launch_bounds__(128, 1) k_rowgemm_tc(const __grid_constant__ C
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
-    mbar_expect_tx(full, (uint32_t)(nkb * (a_bytes + b_bytes)));
-    for (int kb = 0; kb < nkb; ++kb) {
-      tma_load_2d(sA + kb * a_bytes, &tA, kb * RG_KB, m0, full);
-      tma_load_2d(sB + kb * b_bytes, &tB, kb * RG_KB, 0, full);
+  if (warp == 0) {
+    if (lane == 0) {
+      mbar_expect_tx(bfull, (uint32_t)(nkb * b_bytes));
+      for (int kb = 0; kb < nkb; ++kb) tma_load_2d(sB + kb * b_bytes, &tB, kb * RG_KB, 0, bfull);
+      int issued = 0;
+      for (int i = 0; i < my_tiles; ++i) {
+        const int s = i % S;
+        if (i >= S && !mbar_wait(&aempty[s], ((i / S) - 1) & 1, abort)) break;
+        const int m0 = (blockIdx.x + i * gridDim.x) * RG_BM;
+        mbar_expect_tx(&afull[s], (uint32_t)stage_bytes);
+        for (int kb = 0; kb < nkb; ++kb)
+          tma_load_2d(sA + s * stage_bytes + kb * a_bytes, &tA, kb * RG_KB, m0, &afull[s]);
+        issued = i + 1;
+      }
+      // drain: no bulk copy may still be writing shared memory when the CTA exits
+      mbar_wait(bfull, 0, abort);
+      for (int i = max(0, issued - S); i < issued; ++i)
+        mbar_wait(&afull[i % S], (i / S) & 1, abort);
     }
-    mbar_wait(full, 0, abort);  // drain before the CTA may exit
-  } else if (warp == 1 && lane == 0) {
-    const uint32_t id = make_idesc(1, RG_BM, g.Npad);
-    if (mbar_wait(full, 0, abort)) {
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t id = make_idesc(1, RG_BM, g.Npad);
+      if (mbar_wait(bfull, 0, abort)) {
+        for (int i = 0; i < my_tiles; ++i) {
+          const int s = i % S, b = i & 1;
+          if (!mbar_wait(&afull[s], (i / S) & 1, abort)) break;
+          if (i >= 2 && !mbar_wait(&accempty[b], ((i >> 1) - 1) & 1, abort)) break;
+          fence_after();
+          const uint32_t td = tmem + (uint32_t)b * ncols;
+          const uint8_t* sa = sA + s * stage_bytes;
+          for (int kb = 0; kb < nkb; ++kb)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)  // 4 x (K=8 TF32 = 32 bytes) per 128-byte row
+              mma<1>(td, make_desc(sa + kb * a_bytes + kk * 32), make_desc(sB + kb * b_bytes + kk * 32),
+                     id, (kb | kk) != 0 ? 1u : 0u);
+          mma_commit(&aempty[s]);
+          mma_commit(&accfull[b]);
+        }
+      }
+    }
+  } else {
+    // epilogue warps: TMEM lanes (warp % 4) * 32 .. +31 = tile rows. Each 32 x 32 chunk goes
+    // registers (+ bias on value rows) -> 128B-swizzled shared staging -> one TMA bulk store, or a
+    // bulk add-reduction into Y when Y already holds the residual (in-place Y += X W).
+    const int ew = warp & 3;
+    uint8_t* sbuf = stage_out + (warp - 2) * 8192;
+    int nst = 0;
+    for (int i = 0; i < my_tiles; ++i) {
+      const int b = i & 1;
+      const bool ok = mbar_wait(&accfull[b], (i >> 1) & 1, abort);
       fence_after();
-      for (int kb = 0; kb < nkb; ++kb)
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk)  // 4 x (K=8 TF32 = 32 bytes) per 128-byte row
-          mma<1>(tmem, make_desc(sA + kb * a_bytes + kk * 32), make_desc(sB + kb * b_bytes + kk * 32),
-                 id, (kb | kk) != 0 ? 1u : 0u);
-    }
-    mma_commit(done);
-  }
-  __syncwarp();
-  const bool ok = mbar_wait(done, 0, abort);
-  fence_after();
-  const bool go = __all_sync(0xffffffffu, ok && !*abort);
-  if (go) {
-    // Drain TMEM 32 columns at a time into a per-warp staging tile in the (now idle) operand
-    // buffer, then write 4 rows x 128 bytes per warp instruction (coalesced float4 when every
-    // row start is 16-byte aligned, scalar otherwise).
-    float* stage = reinterpret_cast<float*>(sA) + warp * (32 * 33);
-    const int r0 = m0 + warp * 32;
+      if (!__all_sync(0xffffffffu, ok && !*abort)) break;
+      const int r0 = (blockIdx.x + i * gridDim.x) * RG_BM + ew * 32;
+      const uint32_t tbase = tmem + (uint32_t)b * ncols + ((uint32_t)(ew * 32) << 16);
+      const bool val = ((r0 + lane) % g.C) == 0;
 #pragma unroll 1
-    for (int c0 = 0; c0 < g.Nout; c0 += 32) {
-      uint32_t r[32];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-          "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-            "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-            "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-            "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-            "=r"(r[31])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int row_l = r0 + lane;
-      const bool val = row_l < g.rows && (row_l % g.C) == 0;
-#pragma unroll
-      for (int q = 0; q < 32; ++q) {
-        const int col = c0 + q;
-        float v = __uint_as_float(r[q]);
-        if (val && g.bias && col < g.Nout) v += g.bias[col];
-        stage[lane * 33 + q] = v;
-      }
-      __syncwarp();
-      const int ncol = min(32, g.Nout - c0);
-      if (g.vec4 && ncol == 32) {
-#pragma unroll
-        for (int rr = 0; rr < 32; rr += 4) {
-          const int lr = rr + (lane >> 3), cg = (lane & 7) * 4;
-          const int row = r0 + lr;
-          if (row < g.rows) {
-            const float* sv = stage + lr * 33 + cg;
-            float4 v = make_float4(sv[0], sv[1], sv[2], sv[3]);
-            if (g.Res) {
-              const float4 rv =
-                  *reinterpret_cast<const float4*>(g.Res + (size_t)row * g.ldr + c0 + cg);
-              v = make_float4(rv.x + v.x, rv.y + v.y, rv.z + v.z, rv.w + v.w);
-            }
-            *reinterpret_cast<float4*>(g.Y + (size_t)row * g.ldy + c0 + cg) = v;
-          }
+      for (int c0 = 0; c0 < g.Nout; c0 += 32) {
+        uint32_t r[32];
+        tmem_ld32(tbase + (uint32_t)c0, r);
+        if (c0 + 32 >= g.Nout) {
+          // last TMEM read of this accumulator: hand it back to the MMA warp
+          fence_before();
+          __syncwarp();
+          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                          smem_u32(&accempty[b]))
+                                      : "memory");
         }
-      } else {
-        for (int rr = 0; rr < 32; ++rr) {
-          const int row = r0 + rr;
-          if (row >= g.rows) break;
-          for (int q = lane; q < ncol; q += 32) {
-            float v = stage[rr * 33 + q];
-            if (g.Res) v = g.Res[(size_t)row * g.ldr + c0 + q] + v;
-            g.Y[(size_t)row * g.ldy + c0 + q] = v;
-          }
+        uint8_t* buf = sbuf + (nst & 1) * 4096;
+        if (nst >= 2) {  // the store that last read this buffer must be done reading it
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+          __syncwarp();
         }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          float4 v;
+          float* pv = reinterpret_cast<float*>(&v);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int col = c0 + 4 * j + e;
+            pv[e] = __uint_as_float(r[4 * j + e]);
+            if (val && g.bias && col < g.Nout) pv[e] += g.bias[col];
+          }
+          *reinterpret_cast<float4*>(buf + lane * 128 + ((j ^ (lane & 7)) << 4)) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0 && r0 < g.rows) {  // rows past the end are clipped by the tensor map
+          if (g.res_inplace)
+            asm volatile(
+                "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(&tY)),
+                "r"(c0), "r"(r0), "r"(smem_u32(buf))
+                : "memory");
+          else
+            asm volatile(
+                "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(&tY)),
+                "r"(c0), "r"(r0), "r"(smem_u32(buf))
+                : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        ++nst;
       }
-      __syncwarp();
     }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
   }
-  if (*abort && threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
   fence_before();
   __syncthreads();
+  if (*abort && threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
   if (warp == 0) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * ncols));
   }
 }
 
@@ -202,22 +254,51 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
       return NQS_ERR_CUDA;
     }
   }
+  // the residual, when given, is Y itself (Y += X W in place): the epilogue adds into Y with a
+  // bulk reduction; Y rows must start on 16 bytes for the store tensor map
+  if (Res && (Res != Y || ldr != ldy)) {
+    set_error("rowgemm_tc: the residual must be the output itself (in-place Y += X W)");
+    return NQS_ERR_INVALID_ARG;
+  }
+  if ((reinterpret_cast<uintptr_t>(Y) & 15) || (ldy % 4)) {
+    set_error("rowgemm_tc: output rows not 16-byte aligned");
+    return NQS_ERR_INVALID_ARG;
+  }
+  CUtensorMap ty;
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)Nout, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldy * 4};
+    const cuuint32_t box[2] = {32, 32};
+    if (enc(&ty, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, Y, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      set_error("rowgemm_tc: tensor map (output)");
+      return NQS_ERR_CUDA;
+    }
+  }
   const int nkb = K / tc::RG_KB;
-  // at least 80 KB so at most two CTAs share an SM (2 x 256 TMEM columns <= 512)
-  const size_t sm = std::max<size_t>((size_t)80 * 1024,
-                                     (size_t)nkb * (tc::RG_BM * 128 + Npad * 128) + 1024 + 64);
+  // shared memory: resident W^T, S stages of A tiles, epilogue staging, barriers
+  const size_t fixed = (size_t)nkb * Npad * 128 + 4 * 2 * 4096 + 256 + 1024;
+  const size_t stage = (size_t)nkb * tc::RG_BM * 128;
+  const size_t cap = 200 * 1024;
+  int S = (int)std::min<size_t>(4, (cap - fixed) / stage);
+  if (S < 2) {
+    set_error("rowgemm_tc: K=%d, N=%d leave room for %d pipeline stages", K, Npad, S);
+    return NQS_ERR_UNSUPPORTED;
+  }
+  const size_t sm = fixed + (size_t)S * stage;
   static bool attr = false;
+  static int nsm = 0;
   if (!attr) {
-    cudaFuncSetAttribute(tc::k_rowgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(tc::k_rowgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     attr = true;
   }
-  // float4 row writes only when every row start of Y and Res is 16-byte aligned
-  const int vec4 = ((reinterpret_cast<uintptr_t>(Y) & 15) == 0 && (ldy % 4) == 0 &&
-                    (!Res || ((reinterpret_cast<uintptr_t>(Res) & 15) == 0 && (ldr % 4) == 0)))
-                       ? 1
-                       : 0;
-  tc::RowGemmArgs a{rows, K, Nout, Npad, C, vec4, bias, Res, ldr, Y, ldy, err};
-  tc::k_rowgemm_tc<<<(rows + tc::RG_BM - 1) / tc::RG_BM, 128, sm, st>>>(ta, tb, a);
+  tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, bias, err};
+  const int ntiles = (rows + tc::RG_BM - 1) / tc::RG_BM;
+  tc::k_rowgemm_tc<<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(ta, tb, ty, a);
   NQS_CHECK_LAUNCH("k_rowgemm_tc");
   return NQS_OK;
 }
