@@ -20,7 +20,7 @@ constexpr int RG_BM = 128;
 constexpr int RG_KB = 32;  // float32 per 128-byte swizzle row
 
 struct RowGemmArgs {
-  int rows, K, Nout, Npad, C, res_inplace, stages;
+  int rows, K, Nout, Npad, C, res_inplace, stages, act;
   const float* bias;
   int* err;
 };
@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
             const int col = c0 + 4 * j + e;
             pv[e] = __uint_as_float(r[4 * j + e]);
             if (val && g.bias && col < g.Nout) pv[e] += g.bias[col];
+            if (g.act) pv[e] = gelu_value(pv[e], gelu_tanh_w(pv[e]));
           }
           *reinterpret_cast<float4*>(buf + lane * 128 + ((j ^ (lane & 7)) << 4)) = v;
         }
@@ -218,8 +219,12 @@ bool rowgemm_tc_ok(int K, int ldx, int Nout) {
 
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
-               cudaStream_t st) {
+               cudaStream_t st, int act) {
   if (rows <= 0) return NQS_OK;
+  if (act && C != 1) {
+    set_error("rowgemm_tc: the fused activation needs single-channel rows");
+    return NQS_ERR_INVALID_ARG;
+  }
   tc::EncodeTiledFn enc = tc::encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -296,7 +301,7 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     attr = true;
   }
-  tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, bias, err};
+  tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, act, bias, err};
   const int ntiles = (rows + tc::RG_BM - 1) / tc::RG_BM;
   tc::k_rowgemm_tc<<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(ta, tb, ty, a);
   NQS_CHECK_LAUNCH("k_rowgemm_tc");

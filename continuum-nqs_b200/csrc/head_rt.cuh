@@ -49,7 +49,8 @@ inline HeadRtPlan head_rt_plan(int N, int nG, int K, int n_tan, bool tan, bool l
   HeadRtPlan p;
   p.jpc = std::max(1, 4 / K);
   p.job_bytes = head_rt_job_bytes(N, nG, K, tan ? n_tan : 0, tan, lap);
-  p.hw_bytes = round128(16 * (size_t)kHeadTok * kHeadLd);
+  // per half-warp: pivot-row broadcast (and, with tangents, the D_t / B_t matrix), pivot order
+  p.hw_bytes = round128(16 * (size_t)(tan ? kHeadTok * kHeadLd : 2 * kHeadTok) + 4 * kHeadTok);
   p.bytes = p.jpc * p.job_bytes + 4 * p.hw_bytes;
   return p;
 }
@@ -247,17 +248,17 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
         mr[i] = mk(i == l ? 1.0 : 0.0, 0.0);
       }
     }
-    // ---- elimination ----
-    int piv[NP];
+    // ---- elimination: register 0 always holds the current column (the row rotates left by one
+    // register per step), so the step loop is not unrolled ----
+    int* piv = reinterpret_cast<int*>(hbuf + (TAN ? NP * LD : 2 * NP));  // pivot row per column
     bool used = false;
     int step = l;  // the column this lane's row pivots (padding rows keep their own index)
     double logabs = 0.0;
     cplx sgn = mk(1.0, 0.0);
     int sing = 0;
-#pragma unroll
-    for (int c = 0; c < NP; ++c) {
-      if (c >= N) break;
-      double best = used ? -1.0 : cabs1(mr[c]);
+#pragma unroll 1
+    for (int c = 0; c < N; ++c) {
+      double best = used ? -1.0 : cabs1(mr[0]);
       int bi = l;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) {
@@ -269,10 +270,10 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
         }
       }
       const int p = bi;
-      piv[c] = p;
+      if (l == 0) piv[c] = p;
       const int src = (lane & 16) | p;
-      const cplx pv = mk(__shfl_sync(0xffffffffu, mr[c].re, src),
-                         __shfl_sync(0xffffffffu, mr[c].im, src));
+      const cplx pv = mk(__shfl_sync(0xffffffffu, mr[0].re, src),
+                         __shfl_sync(0xffffffffu, mr[0].im, src));
       const double apv = hypot(pv.re, pv.im);
       if (apv == 0.0) {
         sing = 1;
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
       cplx* prow = hbuf + (c & 1) * NP;  // double-buffered broadcast of the scaled pivot row
       if (TAN) {
         if (me) {
-          mr[c] = mk(1.0, 0.0);
+          mr[0] = mk(1.0, 0.0);
 #pragma unroll
           for (int col = 0; col < NP; ++col) {
             mr[col] = cmul(mr[col], ipv);
@@ -298,30 +299,44 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
         }
         __syncwarp();
         if (!me) {
-          const cplx f = mr[c];
-          mr[c] = mk(0.0, 0.0);
+          const cplx f = mr[0];
+          mr[0] = mk(0.0, 0.0);
 #pragma unroll
           for (int col = 0; col < NP; ++col) mr[col] = csub(mr[col], cmul(f, prow[col]));
         }
       } else {
         if (me) {
 #pragma unroll
-          for (int col = c + 1; col < NP; ++col) prow[col] = cmul(mr[col], ipv);
+          for (int col = 1; col < NP; ++col) prow[col] = cmul(mr[col], ipv);
         }
         __syncwarp();
         if (!used) {
-          const cplx f = mr[c];
+          const cplx f = mr[0];
 #pragma unroll
-          for (int col = c + 1; col < NP; ++col) mr[col] = csub(mr[col], cmul(f, prow[col]));
+          for (int col = 1; col < NP; ++col) mr[col] = csub(mr[col], cmul(f, prow[col]));
         }
       }
+      const cplx t0 = mr[0];
+#pragma unroll
+      for (int col = 0; col < NP - 1; ++col) mr[col] = mr[col + 1];
+      mr[NP - 1] = t0;
     }
+    if (TAN) {  // complete the rotation to NP registers: mr[c'] = slot c' of the in-place inverse
+#pragma unroll 1
+      for (int r = N; r < NP; ++r) {
+        const cplx t0 = mr[0];
+#pragma unroll
+        for (int col = 0; col < NP - 1; ++col) mr[col] = mr[col + 1];
+        mr[NP - 1] = t0;
+      }
+    }
+    __syncwarp();
     // parity of the pivot order: inversions (c < c', piv[c] > piv[c']) counted by the row
     // pivoting column c
     int inv_cnt = 0;
-#pragma unroll
-    for (int c2 = 0; c2 < NP; ++c2)
-      if (c2 < N && c2 > step && l < N && piv[c2] < l) ++inv_cnt;
+    if (l < N)
+      for (int c2 = step + 1; c2 < N; ++c2)
+        if (piv[c2] < l) ++inv_cnt;
 #pragma unroll
     for (int o = 8; o > 0; o >>= 1) inv_cnt += __shfl_xor_sync(0xffffffffu, inv_cnt, o);
     if (inv_cnt & 1) sgn = mk(-sgn.re, -sgn.im);

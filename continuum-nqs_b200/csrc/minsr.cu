@@ -232,59 +232,10 @@ int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, do
   return NQS_OK;
 }
 
-// general C[i][j] -= sum_k A[i][k] B[j][k] for a rectangular block (used by the Cholesky panel
-// update when the trailing matrix is lower triangular we use dsyrk_lower on the panel itself)
-
 // ============================================================================================
 // Cholesky (right-looking, block 64) and triangular solves, float64
 // ============================================================================================
 constexpr int CB = 64;
-
-// factor the diagonal block in place (lower), one CTA of 256 threads; adds lam to the diagonal
-// first if add_lam; sets *bad when a pivot is not positive
-// factor the diagonal block in place (lower), one CTA of 256 threads. A pivot d <= *floor_p is
-// replaced by *floor_p (modified Cholesky with a pivot floor; bad[2] counts the replacements) when
-// floor_p is given, else flagged in bad[0] (not positive definite).
-__global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int64_t lda, int k0,
-                                                    int n, const double* __restrict__ floor_p,
-                                                    int* __restrict__ bad) {
-  __shared__ double L[CB][CB + 1];
-  const int b = min(CB, n - k0);
-  const double fl = floor_p ? *floor_p : 0.0;
-  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
-    const int i = idx / b, j = idx - i * b;
-    L[i][j] = (j <= i) ? A[(size_t)(k0 + i) * lda + k0 + j] : 0.0;
-  }
-  __syncthreads();
-  for (int j = 0; j < b; ++j) {
-    if (threadIdx.x == 0) {
-      double d = L[j][j];
-      if (floor_p && !(d > fl)) {
-        d = fl;
-        atomicAdd(bad + 2, 1);
-      }
-      if (!(d > 0.0)) {
-        bad[0] = 1;
-        L[j][j] = NAN;
-      } else {
-        L[j][j] = sqrt(d);
-      }
-    }
-    __syncthreads();
-    const double piv = L[j][j];
-    for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) L[i][j] /= piv;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < (b - j - 1) * (b - j - 1); idx += blockDim.x) {
-      const int ii = j + 1 + idx / (b - j - 1), jj = j + 1 + idx % (b - j - 1);
-      if (jj <= ii) L[ii][jj] -= L[ii][j] * L[jj][j];
-    }
-    __syncthreads();
-  }
-  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
-    const int i = idx / b, j = idx - i * b;
-    if (j <= i) A[(size_t)(k0 + i) * lda + k0 + j] = L[i][j];
-  }
-}
 
 // *floor = rel * max_i A[i][i]  (one CTA)
 __global__ void k_pivot_floor(const double* __restrict__ A, int64_t lda, int n, double rel,
@@ -303,39 +254,6 @@ __global__ void k_pivot_floor(const double* __restrict__ A, int64_t lda, int n, 
   }
 }
 
-// panel: rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L_kk^-T  (one warp per row)
-__global__ void __launch_bounds__(256) k_trsm_panel(double* __restrict__ A, int64_t lda, int k0,
-                                                    int n) {
-  __shared__ double L[CB][CB + 1];
-  const int b = min(CB, n - k0);
-  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
-    const int i = idx / b, j = idx - i * b;
-    L[i][j] = (j <= i) ? A[(size_t)(k0 + i) * lda + k0 + j] : 0.0;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int r = k0 + b + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (r >= n) return;
-  double* row = A + (size_t)r * lda + k0;
-  // x L^T = a  -> forward substitution over columns: x_j = (a_j - sum_{m<j} x_m L[j][m]) / L[j][j]
-  double x0 = lane < b ? row[lane] : 0.0, x1 = lane + 32 < b ? row[lane + 32] : 0.0;
-  for (int j = 0; j < b; ++j) {
-    const double xj_raw = __shfl_sync(0xffffffffu, j < 32 ? x0 : x1, j & 31);
-    const double xj = xj_raw / L[j][j];
-    if (lane == (j & 31)) {
-      if (j < 32)
-        x0 = xj;
-      else
-        x1 = xj;
-    }
-    // eliminate from later columns
-    if (lane > j && lane < b) x0 -= xj * L[lane][j];
-    if (lane + 32 > j && lane + 32 < b) x1 -= xj * L[lane + 32][j];
-  }
-  if (lane < b) row[lane] = x0;
-  if (lane + 32 < b) row[lane + 32] = x1;
-}
-
 __global__ void k_add_diag(double* A, int64_t lda, int n, double lam) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) A[(size_t)i * lda + i] += lam;
@@ -350,23 +268,179 @@ __global__ void k_add_diag_noise(double* A, int64_t lda, int n, double lam, doub
   if (i == 0 && extra) *extra = x;
 }
 
+// Diagonal-block Cholesky + panel solve of one right-looking step, fused. Every CTA factors the
+// b x b diagonal block [k0, k0+b) redundantly: each thread owns a fixed set of lower-triangle
+// elements in registers (element e of the row-major lower triangle -> thread e % 256); in step j
+// the owners of column j publish it (double-buffered) and every owner of (i, k), k > j, applies
+// a_ik -= a_ij a_kj / d_j with the unscaled column, so one barrier per column suffices. The CTA
+// then solves its share of the panel rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L^-T,
+// four rows per warp side by side. The factor is written to Ld rather than into A (other CTAs may
+// still be reading the block); the next step's CTA 0 (or k_store_diag after the last step) copies
+// it into A. Pivots d_j below *floor_p are raised to it (counted in bad[2]); a non-positive pivot
+// sets bad[0] (CTA 0 records both).
+constexpr int kCholElems = (CB * (CB + 1) / 2 + 255) / 256;  // lower-triangle elements per thread
+
+__global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int64_t lda, int k0,
+                                                    int n, const double* __restrict__ floor_p,
+                                                    int* __restrict__ bad, int rpc,
+                                                    double* __restrict__ Ld, int prev_k0) {
+  __shared__ double col[2][CB];
+  __shared__ double L[CB][CB + 1];
+  __shared__ double rdiag[CB];
+  const int b = min(CB, n - k0);
+  const int tid = threadIdx.x;
+  if (blockIdx.x == 0 && prev_k0 >= 0) {  // previous step's diagonal factor into A
+    const int bp = min(CB, n - prev_k0);
+    for (int idx = tid; idx < bp * bp; idx += blockDim.x) {
+      const int i = idx / bp, j = idx - i * bp;
+      if (j <= i) A[(size_t)(prev_k0 + i) * lda + prev_k0 + j] = Ld[idx];
+    }
+    __syncthreads();  // Ld is rewritten below by this CTA
+  }
+  const double fl = floor_p ? *floor_p : 0.0;
+  __shared__ double dval[CB], dinv[CB];
+  // pivot d_j (raised to the floor when below it) and its reciprocal, set by the owner of (j, j)
+  auto set_pivot = [&](int j, double d) {
+    const bool floored = floor_p && !(d > fl);
+    if (floored) d = fl;
+    const bool pos = d > 0.0;
+    if (blockIdx.x == 0) {
+      if (floored) atomicAdd(bad + 2, 1);
+      if (!pos) bad[0] = 1;
+    }
+    dval[j] = d;
+    dinv[j] = pos ? 1.0 / d : NAN;
+  };
+  // owned elements: e = tid + 256 q of the row-major lower triangle of the b x b block
+  double v[kCholElems];
+  int ei[kCholElems], ek[kCholElems];
+  const int ne = b * (b + 1) / 2;
+#pragma unroll
+  for (int q = 0; q < kCholElems; ++q) {
+    const int e = tid + 256 * q;
+    int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= e) ++i;
+    while (i * (i + 1) / 2 > e) --i;
+    const int k = e - i * (i + 1) / 2;
+    const bool own = e < ne;
+    ei[q] = own ? i : 0;
+    ek[q] = own ? k : -1;  // not owned: never updated, never published
+    v[q] = own ? A[(size_t)(k0 + i) * lda + k0 + k] : 0.0;
+    if (own && k == 0) col[0][i] = v[q];
+    if (own && e == 0) set_pivot(0, v[q]);
+  }
+  __syncthreads();
+  // elimination with the unscaled columns (a_ik -= a_ij a_kj / d_j); square roots deferred
+  for (int j = 0; j < b; ++j) {
+    const double* cj = col[j & 1];
+    double* cn = col[(j + 1) & 1];
+    const double inv = dinv[j];
+#pragma unroll
+    for (int q = 0; q < kCholElems; ++q) {
+      const int i = ei[q], k = ek[q];
+      const double u = cj[i] * cj[k > 0 ? k : 0] * inv;
+      if (k > j) v[q] -= u;
+      if (k == j + 1) {
+        cn[i] = v[q];
+        if (i == k) set_pivot(k, v[q]);
+      }
+    }
+    __syncthreads();
+  }
+  // L[i][k] = a_ik / sqrt(d_k) (i > k), L[k][k] = sqrt(d_k)
+#pragma unroll
+  for (int q = 0; q < kCholElems; ++q) {
+    const int i = ei[q], k = ek[q];
+    if (k >= 0) {
+      const double d = dval[k];
+      const bool pos = d > 0.0;
+      const double sd = pos ? sqrt(d) : NAN;
+      L[i][k] = (i == k) ? sd : v[q] / sd;
+      if (i == k) rdiag[k] = pos ? 1.0 / sd : NAN;
+    }
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int idx = tid; idx < b * b; idx += blockDim.x) {
+      const int i = idx / b, j = idx - i * b;
+      Ld[idx] = j <= i ? L[i][j] : 0.0;
+    }
+  // panel rows of this CTA, four per warp at once: x L^T = a ->
+  //   x_j = (a_j - sum_{m<j} x_m L[j][m]) / L[j][j]
+  const int lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  const int r_lo = k0 + b + blockIdx.x * rpc, r_hi = min(n, r_lo + rpc);
+  for (int r0 = r_lo + 4 * w; r0 < r_hi; r0 += 4 * nw) {
+    double x0[4], x1[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + u;
+      const double* row = A + (size_t)r * lda + k0;
+      x0[u] = (r < r_hi && lane < b) ? row[lane] : 0.0;
+      x1[u] = (r < r_hi && lane + 32 < b) ? row[lane + 32] : 0.0;
+    }
+    for (int j = 0; j < b; ++j) {
+      const double rd = rdiag[j];
+      const double l0 = (lane > j && lane < b) ? L[lane][j] : 0.0;
+      const double l1 = (lane + 32 > j && lane + 32 < b) ? L[lane + 32][j] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? x0[u] : x1[u], j & 31) * rd;
+        if (lane == (j & 31)) {
+          if (j < 32)
+            x0[u] = xj;
+          else
+            x1[u] = xj;
+        }
+        x0[u] -= xj * l0;
+        x1[u] -= xj * l1;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + u;
+      if (r >= r_hi) break;
+      double* row = A + (size_t)r * lda + k0;
+      if (lane < b) row[lane] = x0[u];
+      if (lane + 32 < b) row[lane + 32] = x1[u];
+    }
+  }
+}
+
+__global__ void k_store_diag(double* __restrict__ A, int64_t lda, int k0, int n,
+                             const double* __restrict__ Ld) {
+  const int b = min(CB, n - k0);
+  for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, j = idx - i * b;
+    if (j <= i) A[(size_t)(k0 + i) * lda + k0 + j] = Ld[idx];
+  }
+}
+
+// Right-looking blocked Cholesky A = L L^T (lower triangle, in place), 64-column panels.
+// part: scratch of at least 64 x 64 doubles for the diagonal factor.
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
+  if (!part || part_elems < (size_t)CB * CB) {
+    set_error("cholesky_lower: scratch of %zu doubles < %d", part_elems, CB * CB);
+    return NQS_ERR_WORKSPACE;
+  }
+  int prev = -1;
   for (int k0 = 0; k0 < n; k0 += CB) {
     const int b = std::min(CB, n - k0);
-    k_potrf_diag<<<1, 256, 0, st>>>(A, lda, k0, n, floor_p, bad);
-    NQS_CHECK_LAUNCH("k_potrf_diag");
     const int rest = n - k0 - b;
+    // panel rows per CTA: about two CTAs per SM, at least four rows per warp
+    const int rpc = rest > 0 ? std::max(32, (rest + 2 * nsm - 1) / (2 * nsm)) : 1;
+    const int grid = rest > 0 ? (rest + rpc - 1) / rpc : 1;
+    k_potrf_trsm<<<grid, 256, 0, st>>>(A, lda, k0, n, floor_p, bad, rpc, part, prev);
+    NQS_CHECK_LAUNCH("k_potrf_trsm");
+    prev = k0;
     if (rest <= 0) break;
-    k_trsm_panel<<<(rest + 7) / 8, 256, 0, st>>>(A, lda, k0, n);
-    NQS_CHECK_LAUNCH("k_trsm_panel");
     // trailing: A[k0+b:, k0+b:] -= P P^T, P = A[k0+b:, k0:k0+b]
     double* P = A + (size_t)(k0 + b) * lda + k0;
     double* C = A + (size_t)(k0 + b) * lda + k0 + b;
     NQS_TRY(dsyrk_lower(P, lda, rest, b, -1.0, 1.0, C, lda, nullptr, 0, nsm, st));
-    (void)part;
-    (void)part_elems;
   }
+  k_store_diag<<<1, 256, 0, st>>>(A, lda, prev, n, part);
+  NQS_CHECK_LAUNCH("k_store_diag");
   return NQS_OK;
 }
 
@@ -1019,7 +1093,7 @@ __global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W
 // ============================================================================================
 size_t minsr_part_elems(int W) {
   const size_t n = 2 * (size_t)W;
-  return std::min<size_t>(16 * n * n, (size_t)8 << 20);
+  return std::max<size_t>(std::min<size_t>(16 * n * n, (size_t)8 << 20), (size_t)CB * CB);
 }
 
 size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
@@ -1172,7 +1246,8 @@ int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {
   if (!bytes || M < 1 || K < 1) return NQS_ERR_INVALID_ARG;
   const size_t m = (size_t)M;
   *bytes = sizeof(double) * (m * m + 2 * m + 2 * (size_t)K + trsv_elems(m) +
-                             std::min<size_t>(16 * m * m, (size_t)8 << 20)) + 8192;
+                             std::max<size_t>(std::min<size_t>(16 * m * m, (size_t)8 << 20),
+                                              (size_t)CB * CB)) + 8192;
   return NQS_OK;
 }
 
@@ -1188,7 +1263,8 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   double* r = ws.take<double>(M);
   double* tmpK = ws.take<double>(K);
   double* tmpK_lo = ws.take<double>(K);
-  const size_t pe = std::min<size_t>(16 * (size_t)M * M, (size_t)8 << 20);
+  const size_t pe = std::max<size_t>(std::min<size_t>(16 * (size_t)M * M, (size_t)8 << 20),
+                                     (size_t)CB * CB);
   double* part = ws.take<double>(pe);
   int* bad = ws.take<int>(4);
   if (!bad) return NQS_ERR_WORKSPACE;

@@ -103,7 +103,7 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
 bool rowgemm_tc_ok(int K, int ldx, int Nout);
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
-               cudaStream_t st);
+               cudaStream_t st, int act = 0);  // act 1: tanh-GELU on the output (C == 1 only)
 size_t tc_weights_bytes(const NqsModelDesc& d);
 int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,
                      cudaStream_t st);

@@ -596,8 +596,7 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
     for (int l = 0; l < mc.depth; ++l) {
       const BlockW<T>& bw = w.blk[l];
       x = b.xin[l];
-      k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[l]);
-      NQS_CHECK_LAUNCH("k_layernorm");
+      NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[l], st));
       GemmArgs<T> g{};
       g.X = b.h0[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
       g.Y = b.qkv[l]; g.ldy = 3 * d; g.nseg = 3;
@@ -611,9 +610,7 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       g.Y = b.xmid[l]; g.ldy = d; g.Res = x; g.ldr = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));
-      k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, b.xmid[l], bw.ln1_s, bw.ln1_b,
-                                                   b.h1[l]);
-      NQS_CHECK_LAUNCH("k_layernorm");
+      NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xmid[l], bw.ln1_s, bw.ln1_b, b.h1[l], st));
       g = GemmArgs<T>{};
       g.X = b.h1[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
       g.Y = b.a0[l]; g.ldy = D; g.nseg = 1;
@@ -630,8 +627,7 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));
     }
-    k_layernorm<T><<<(nt + 7) / 8, 256, 0, st>>>(nt, 1, 0, 0, d, b.xL, w.lnf_s, w.lnf_b, b.hf);
-    NQS_CHECK_LAUNCH("k_layernorm");
+    NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xL, w.lnf_s, w.lnf_b, b.hf, st));
     {
       GemmArgs<T> g{};
       g.X = b.hf; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;

@@ -77,9 +77,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
     NQS_CHECK_LAUNCH("k_embed");
     for (int b = 0; b < mc.depth; ++b) {
       const BlockW<T>& bw = w.blk[b];
-      k_layernorm<T><<<(ntok + 7) / 8, 256, 0, st>>>(ntok, C, cb.n_tan, cb.has_lap, d, X,
-                                                     bw.ln0_s, bw.ln0_b, Hb);
-      NQS_CHECK_LAUNCH("k_layernorm");
+      NQS_TRY(launch_layernorm<T>(ntok, C, cb.n_tan, cb.has_lap, d, X, bw.ln0_s, bw.ln0_b, Hb,
+                                  st));
       GemmArgs<T> g{};
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wqkv[b], w.tc.npad_qkv, 3 * d,
@@ -103,13 +102,14 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
         NQS_TRY(launch_gemm<T>(g, st));
       }
-      k_layernorm<T><<<(ntok + 7) / 8, 256, 0, st>>>(ntok, C, cb.n_tan, cb.has_lap, d, X,
-                                                     bw.ln1_s, bw.ln1_b, Hb);
-      NQS_CHECK_LAUNCH("k_layernorm");
+      NQS_TRY(launch_layernorm<T>(ntok, C, cb.n_tan, cb.has_lap, d, X, bw.ln1_s, bw.ln1_b, Hb,
+                                  st));
       const int D = mc.ff * d;
+      // single-channel rows: the GELU runs in the GEMM epilogue
+      const bool fuse_act = tcn && C == 1;
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.w0[b], D, D, (const float*)bw.b0, C,
-                           nullptr, 0, (float*)Big, D, w.tc.err, st));
+                           nullptr, 0, (float*)Big, D, w.tc.err, st, fuse_act ? 1 : 0));
       } else {
         g = GemmArgs<T>{};
         g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
@@ -117,10 +117,12 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
         NQS_TRY(launch_gemm<T>(g, st));
       }
-      const size_t nel = (size_t)ntok * D;
-      k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)ntok, C, cb.n_tan,
-                                                               cb.has_lap, D, Big);
-      NQS_CHECK_LAUNCH("k_gelu");
+      if (!fuse_act) {
+        const size_t nel = (size_t)ntok * D;
+        k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)ntok, C, cb.n_tan,
+                                                                 cb.has_lap, D, Big);
+        NQS_CHECK_LAUNCH("k_gelu");
+      }
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Big, D, rows, D, w.tc.w1[b], d, d, (const float*)bw.b1,
                            C, (const float*)X, d, (float*)X, d, w.tc.err, st));
@@ -132,9 +134,7 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         NQS_TRY(launch_gemm<T>(g, st));
       }
     }
-    k_layernorm<T><<<(ntok + 7) / 8, 256, 0, st>>>(ntok, C, cb.n_tan, cb.has_lap, d, X, w.lnf_s,
-                                                   w.lnf_b, Hb);
-    NQS_CHECK_LAUNCH("k_layernorm");
+    NQS_TRY(launch_layernorm<T>(ntok, C, cb.n_tan, cb.has_lap, d, X, w.lnf_s, w.lnf_b, Hb, st));
     const int KN = mc.K * N;
     if (tcn) {
       NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wbf, w.tc.npad_bf, 2 * KN,

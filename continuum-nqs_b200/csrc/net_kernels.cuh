@@ -805,6 +805,68 @@ inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, in
   return NQS_OK;
 }
 
+// LayerNorm of single-channel rows (no tangents): R tokens per warp with every load issued
+// before the reductions. Same arithmetic as the value channel of k_layernorm.
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_layernorm1(int n_tok, int d, const T* __restrict__ X,
+                                                    const T* __restrict__ g,
+                                                    const T* __restrict__ b, T* __restrict__ Y) {
+  constexpr int Q = NQS_MAX_EMBED / 32;
+  const int lane = threadIdx.x & 31;
+  const int tok0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * R;
+  if (tok0 >= n_tok) return;
+  const T inv_d = T(1) / T(d);
+  T u[R][Q];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      u[r][q] = (f < d && tok0 + r < n_tok) ? X[(size_t)(tok0 + r) * d + f] : T(0);
+    }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    T s = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s += u[r][q];
+    const T mu = warp_sum(s) * inv_d;
+    s = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      if (f < d) {
+        u[r][q] -= mu;
+        s += u[r][q] * u[r][q];
+      }
+    }
+    const T var = warp_sum(s) * inv_d;
+    const T rho = T(1) / sqrt(var + T(kLnEps));
+    if (tok0 + r < n_tok) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        if (f < d) Y[(size_t)(tok0 + r) * d + f] = (u[r][q] * rho) * g[f] + b[f];
+      }
+    }
+  }
+}
+
+// LayerNorm launcher: single-channel rows take k_layernorm1
+template <typename T>
+inline int launch_layernorm(int n_tok, int C, int n_tan, int has_lap, int d, const T* X,
+                            const T* g, const T* b, T* Y, cudaStream_t st) {
+  if (C == 1) {
+    constexpr int R = 4;
+    const int nw = (n_tok + R - 1) / R;
+    k_layernorm1<T, R><<<(nw + 7) / 8, 256, 0, st>>>(n_tok, d, X, g, b, Y);
+    NQS_CHECK_LAUNCH("k_layernorm1");
+  } else {
+    k_layernorm<T><<<(n_tok + 7) / 8, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
+    NQS_CHECK_LAUNCH("k_layernorm");
+  }
+  return NQS_OK;
+}
+
 // ============================================================================================
 // tanh-GELU (jax.nn.gelu, approximate=True) with tangent / Laplacian channels, in place.
 //   g = x cdf, cdf = 0.5 (1 + tanh(w)), w = c (x + 0.044715 x^3)
@@ -821,20 +883,50 @@ __global__ void __launch_bounds__(256) k_gelu(size_t n_tok, int C, int n_tan, in
   const T xv = x[0];
   const T c = T(0.7978845608028654);  // sqrt(2/pi)
   const T b3 = T(0.044715);
-  const T th = tanh(c * (xv + b3 * (xv * xv * xv)));
+  const T th = gelu_tanh_w(xv);
   const T cdf = T(0.5) * (T(1) + th);
   const T sech2 = T(1) - th * th;
   const T w1 = c * (T(1) + T(3) * b3 * xv * xv);
   const T w2 = c * T(6) * b3 * xv;
   const T g1 = cdf + T(0.5) * xv * sech2 * w1;
   const T g2 = sech2 * (w1 - xv * th * w1 * w1 + T(0.5) * xv * w2);
-  x[0] = xv * cdf;
+  // pass 1: independent loads of the tangents (sum of squares for the Laplacian); pass 2 rescales
+  // them in place (the second reads hit L1)
   T acc = 0;
-  for (int t = 0; t < n_tan; ++t) {
-    T* p = x + (size_t)(1 + t) * D;
-    const T xt = *p;
-    *p = g1 * xt;
-    acc += xt * xt;
+  if (has_lap) {
+    T a4[4] = {0, 0, 0, 0};
+    int t = 0;
+    for (; t + 3 < n_tan; t += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const T xt = x[(size_t)(1 + t + u) * D];
+        a4[u] += xt * xt;
+      }
+    }
+    for (; t < n_tan; ++t) {
+      const T xt = x[(size_t)(1 + t) * D];
+      a4[0] += xt * xt;
+    }
+    acc = (a4[0] + a4[1]) + (a4[2] + a4[3]);
+  }
+  x[0] = gelu_value(xv, th);
+  int t = 0;
+  for (; t + 3 < n_tan; t += 4) {
+    T v4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v4[u] = x[(size_t)(1 + t + u) * D];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[(size_t)(1 + t + u) * D] = g1 * v4[u];
+  }
+  {
+    T v4[4];
+    const int nr = n_tan - t;
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+      if (u < nr) v4[u] = x[(size_t)(1 + t + u) * D];
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+      if (u < nr) x[(size_t)(1 + t + u) * D] = g1 * v4[u];
   }
   if (has_lap) {
     T* p = x + (size_t)(C - 1) * D;

@@ -154,6 +154,17 @@ struct ModelConst {
   const double* knots;  // device [n_knots]
 };
 
+// tanh(w) of the tanh-GELU (jax.nn.gelu, approximate=True): w = sqrt(2/pi) (x + 0.044715 x^3);
+// gelu(x) = x * 0.5 (1 + tanh(w))
+template <typename T>
+__device__ __forceinline__ T gelu_tanh_w(T x) {
+  return tanh(T(0.7978845608028654) * (x + T(0.044715) * (x * x * x)));
+}
+template <typename T>
+__device__ __forceinline__ T gelu_value(T x, T th) {
+  return x * (T(0.5) * (T(1) + th));
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
