@@ -62,20 +62,52 @@ __global__ void __launch_bounds__(256) k_wgrad(int N, int d_in, int d_out, const
     ys[idx] = Yw[((size_t)t * 2 + ch) * ldy + o0 + oo];
   }
   __syncthreads();
+  // register blocks of 4 inputs x 4 outputs x 2 channels: lane -> outputs lane + 32 u, warp ->
+  // inputs w + 8 (4 c + v) of chunk c; accumulation in T (the activations' type)
   const int64_t nK = (int64_t)d_in * d_out;
-  for (int idx = threadIdx.x; idx < d_in * ot; idx += blockDim.x) {
-    const int i = idx / ot, oo = idx - i * ot;
-    double gr = 0, gi = 0;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nwp = blockDim.x >> 5;
+  for (int i0 = wp; i0 < d_in; i0 += 4 * nwp) {
+    T ar[4][4], ai[4][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) ar[v][u] = ai[v][u] = T(0);
     for (int t = 0; t < N; ++t) {
-      const double xv = (double)xs[t * d_in + i];
-      gr = fma(xv, (double)ys[(t * 2) * ot + oo], gr);
-      gi = fma(xv, (double)ys[(t * 2 + 1) * ot + oo], gi);
+      T xv[4], yr[4], yi[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int i = i0 + v * nwp;
+        xv[v] = i < d_in ? xs[t * d_in + i] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int oo = lane + 32 * u;
+        yr[u] = oo < ot ? ys[(t * 2) * ot + oo] : T(0);
+        yi[u] = oo < ot ? ys[(t * 2 + 1) * ot + oo] : T(0);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          ar[v][u] = fma(xv[v], yr[u], ar[v][u]);
+          ai[v][u] = fma(xv[v], yi[u], ai[v][u]);
+        }
     }
-    const int64_t e = (int64_t)i * d_out + o0 + oo;
-    if (is_complex)
-      o.put_c(w, off_k, nK, e, gr, gi);
-    else
-      o.put(w, off_k + e, gr, gi);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + v * nwp;
+      if (i >= d_in) continue;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int oo = lane + 32 * u;
+        if (oo >= ot) continue;
+        const int64_t e = (int64_t)i * d_out + o0 + oo;
+        if (is_complex)
+          o.put_c(w, off_k, nK, e, (double)ar[v][u], (double)ai[v][u]);
+        else
+          o.put(w, off_k + e, (double)ar[v][u], (double)ai[v][u]);
+      }
+    }
   }
   if (off_b >= 0) {
     for (int oo = threadIdx.x; oo < ot; oo += blockDim.x) {

@@ -17,6 +17,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
                                                const T* __restrict__ Wemb,
                                                const T* __restrict__ bemb, T* __restrict__ X) {
+  // With tangent / Laplacian channels: features and sums in float64. Value-only batches on the
+  // float path: the angle is reduced to [-pi, pi] in float64, then sincosf and float sums.
   __shared__ double sf[8][4][4 * NQS_MAX_FREQ];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -29,6 +31,29 @@ __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
   const int s = job_spin(jb, ji, tok);
   const int te = tok - ji.tan_e0;
   const bool is_tan = (te >= 0) && (2 * te < jb.n_tan);
+  const bool derivs = jb.n_tan > 0 || jb.has_lap;  // uniform over the launch
+  T* xrow = X + ((size_t)j * jb.N + tok) * jb.C * d;
+  if (!derivs && sizeof(T) == 4) {
+    T* sv = reinterpret_cast<T*>(&sf[wib][0][0]);
+    for (int k = lane; k < F; k += 32) {
+      const int al = k / (2 * nf), rem = k - al * 2 * nf, tau = rem / nf, m = rem - tau * nf + 1;
+      const double sa = r0 * mc.Ainv[al * 2 + 0] + r1 * mc.Ainv[al * 2 + 1];
+      const double ang = ((2.0 * kPi) * sa) * (double)m;
+      const double red = ang - (2.0 * kPi) * rint(ang * (0.5 / kPi));
+      float fs, fc;
+      sincosf((float)red, &fs, &fc);
+      sv[k] = (T)(tau == 0 ? fs : fc);
+    }
+    __syncwarp();
+    for (int n = lane; n < d; n += 32) {
+      T v = 0;
+      for (int k = 0; k < F; ++k) v = fma(sv[k], Wemb[(size_t)k * d + n], v);
+      v += Wemb[(size_t)(F + s) * d + n];
+      v += bemb[n];
+      xrow[n] = v;
+    }
+    return;
+  }
   for (int k = lane; k < F; k += 32) {
     const int al = k / (2 * nf), rem = k - al * 2 * nf, tau = rem / nf, m = rem - tau * nf + 1;
     const double sa = r0 * mc.Ainv[al * 2 + 0] + r1 * mc.Ainv[al * 2 + 1];
@@ -45,15 +70,18 @@ __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
     sf[wib][3][k] = -(c0 * c0 + c1 * c1) * val;
   }
   __syncwarp();
-  T* xrow = X + ((size_t)j * jb.N + tok) * jb.C * d;
   for (int n = lane; n < d; n += 32) {
     double v = 0, dx = 0, dy = 0, lp = 0;
-    for (int k = 0; k < F; ++k) {
-      const double w = (double)Wemb[(size_t)k * d + n];
-      v = fma(sf[wib][0][k], w, v);
-      dx = fma(sf[wib][1][k], w, dx);
-      dy = fma(sf[wib][2][k], w, dy);
-      lp = fma(sf[wib][3][k], w, lp);
+    if (derivs) {
+      for (int k = 0; k < F; ++k) {
+        const double w = (double)Wemb[(size_t)k * d + n];
+        v = fma(sf[wib][0][k], w, v);
+        dx = fma(sf[wib][1][k], w, dx);
+        dy = fma(sf[wib][2][k], w, dy);
+        lp = fma(sf[wib][3][k], w, lp);
+      }
+    } else {
+      for (int k = 0; k < F; ++k) v = fma(sf[wib][0][k], (double)Wemb[(size_t)k * d + n], v);
     }
     v += (double)Wemb[(size_t)(F + s) * d + n];
     v += (double)bemb[n];
