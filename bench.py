@@ -16,6 +16,7 @@ is solved per GPU), so value = N x per-replica iterations / max-over-ranks time 
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -158,17 +159,26 @@ def run_ours(a, rank, world):
         e0_.record()
         e1_.record()
     launches0 = L.nqs_kernel_launches()
+    L.nqs_profile_gemm_read(None, None, None)  # clear
     barrier()
     torch.cuda.synchronize()
     clocks.start()
+    L.nqs_profile_gemm(1)  # event pair around every tensor-core row GEMM launch of the timed steps
+    torch.cuda.nvtx.range_push("timed")  # lets ncu --nvtx-include "timed/" select these launches
     ev[0].record()
     for k in range(a.steps):
         # events recorded on the stream right before / after the Gram kernel of this step
         L.nqs_profile_events(gev[k][0].cuda_event, gev[k][1].cuda_event)
         it.step()
     ev[1].record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
+    L.nqs_profile_gemm(0)
     L.nqs_profile_events(None, None)
+    g_ms_c, g_bytes_c, g_n_c = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+    _lib.check(L.nqs_profile_gemm_read(ctypes.byref(g_ms_c), ctypes.byref(g_bytes_c),
+                                       ctypes.byref(g_n_c)), "nqs_profile_gemm_read")
+    gemm_prof = (g_ms_c.value, g_bytes_c.value, g_n_c.value)
     gram_ms = [g0.elapsed_time(g1) for g0, g1 in gev]
     barrier()
     clk = clocks.stop()
@@ -259,18 +269,48 @@ def run_ours(a, rank, world):
         fp64 = {"ms_per_step": ms64, "VMC_iter_per_s": 1000.0 / ms64,
                 "mixed_speedup": ms64 / ms, "E": float(it64.stats[0])}
         del it64
-    # ------------------------------------------------ roofline of the dominant kernel (Gram)
+    # ------------------------------------------------ roofline of the dominant kernel: the
+    # tensor-core row GEMMs of the network (HBM-bound), timed per launch over the timed steps
     peaks, src = load_peaks()
+    t_ms, t_bytes, t_n = gemm_prof
+    per_launch_bytes = t_bytes / max(t_n, 1)
+    per_launch_ms = t_ms / max(t_n, 1)
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if t_n else float("nan")
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    ratio = traffic_ratio()
+    roof = {"kernel": "k_rowgemm_tc (persistent tcgen05 TF32 row GEMMs of the network)",
+            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": f"{src} (HBM copy)",
+            "traffic": per_launch_bytes * ratio if ratio else None,
+            "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_ms,
+            "launches_per_step": t_n / a.steps, "share_of_step": t_ms / a.steps / ms,
+            "traffic_source": "ncu dram bytes / algorithmic bytes of the same launches, "
+                              "profiles/k_rowgemm_tc_config2.md" if ratio else None}
+    # the MinSR Gram on the tensor cores, for reference
     gflop = gram_flops(su.n_walkers, it.P)
     g_ms = sorted(gram_ms)[len(gram_ms) // 2] if gram_ms else float("nan")
-    achieved = gflop / (g_ms * 1e-3) / 1e12
-    peak = peaks.get("bf16_tflops", 1590.0)
-    roof = {"kernel": "k_gram_tc<bf16> (tcgen05 SYRK of the 2W x P Jacobian)", "bound": "tensor",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_source": f"{src} (burst bf16)", "gram_ms": g_ms,
-            "traffic": None, "algorithmic_flops": gflop}
-    return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof, clocks=clk,
-                launches=launches, su=su, model=model, P=it.P, acc=acc)
+    g_ach = gflop / (g_ms * 1e-3) / 1e12
+    g_peak = peaks.get("bf16_tflops", 1590.0)
+    roof_gram = {"kernel": "k_gram_tc<bf16> (tcgen05 SYRK of the 2W x P Jacobian)",
+                 "bound": "tensor", "achieved": g_ach, "peak": g_peak, "unit": "TFLOP/s",
+                 "frac": g_ach / g_peak, "peak_source": f"{src} (burst bf16)", "gram_ms": g_ms,
+                 "algorithmic_flops": gflop}
+    return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof,
+                roofline_gram=roof_gram, clocks=clk, launches=launches, su=su, model=model,
+                P=it.P, acc=acc)
+
+
+def traffic_ratio():
+    """DRAM bytes per algorithmic byte of the row GEMM launches, from the committed ncu summary
+    (profiles/k_rowgemm_tc_config2.md, line 'dram_per_algorithmic: <x>'), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_rowgemm_tc_config2.md")) as f:
+            for line in f:
+                if line.strip().startswith("dram_per_algorithmic:"):
+                    return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -406,6 +446,7 @@ def main():
         "phases_ms": ph, "energy": {"mean": r["stats"][0], "err": r["stats"][1],
                                     "var": r["stats"][2]},
         "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "roofline": r["roofline"],
+        "roofline_gram": r["roofline_gram"],
         "cpu_baseline": cpu,
         "e2e": r["e2e"], "clocks": r["clocks"], "gpu_launches": int(r["launches"]),
     }

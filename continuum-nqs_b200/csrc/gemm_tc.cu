@@ -213,6 +213,15 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
 
 }  // namespace tc
 
+// ---- optional per-launch timing (nqs_profile_gemm) ----
+namespace {
+constexpr int kGemmProfCap = 16384;
+bool g_gemm_prof = false;
+std::vector<cudaEvent_t> g_gemm_ev;  // pairs
+int g_gemm_n = 0;
+double g_gemm_bytes = 0.0;
+}  // namespace
+
 bool rowgemm_tc_ok(int K, int ldx, int Nout) {
   return K % tc::RG_KB == 0 && K <= 128 && ldx % 4 == 0 && Nout >= 1 && Nout <= 256;
 }
@@ -303,8 +312,49 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
   }
   tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, act, bias, err};
   const int ntiles = (rows + tc::RG_BM - 1) / tc::RG_BM;
+  const bool prof = g_gemm_prof && g_gemm_n < kGemmProfCap;
+  if (prof) {
+    if ((int)g_gemm_ev.size() < 2 * (g_gemm_n + 1)) {
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      g_gemm_ev.push_back(e0);
+      g_gemm_ev.push_back(e1);
+    }
+    cudaEventRecord(g_gemm_ev[2 * g_gemm_n], st);
+  }
   tc::k_rowgemm_tc<<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(ta, tb, ty, a);
+  if (prof) {
+    cudaEventRecord(g_gemm_ev[2 * g_gemm_n + 1], st);
+    ++g_gemm_n;
+    // operand rows, weight panel, output rows (read again and written when accumulating in place)
+    g_gemm_bytes += 4.0 * ((double)rows * K + (double)Npad * K + (double)rows * Nout * (Res ? 2 : 1));
+  }
   NQS_CHECK_LAUNCH("k_rowgemm_tc");
+  return NQS_OK;
+}
+
+extern "C" int nqs_profile_gemm(int enable) {
+  g_gemm_prof = enable != 0;
+  return NQS_OK;
+}
+
+extern "C" int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches) {
+  double t = 0.0;
+  for (int i = 0; i < g_gemm_n; ++i) {
+    float e = 0.f;
+    if (cudaEventSynchronize(g_gemm_ev[2 * i + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&e, g_gemm_ev[2 * i], g_gemm_ev[2 * i + 1]) != cudaSuccess) {
+      set_error("nqs_profile_gemm_read: event %d", i);
+      return NQS_ERR_CUDA;
+    }
+    t += e;
+  }
+  if (ms) *ms = t;
+  if (bytes) *bytes = g_gemm_bytes;
+  if (launches) *launches = g_gemm_n;
+  g_gemm_n = 0;
+  g_gemm_bytes = 0.0;
   return NQS_OK;
 }
 

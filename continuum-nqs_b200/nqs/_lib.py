@@ -178,6 +178,8 @@ _SIGS.update({
     "nqs_adam_update": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_double,
                          c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),
+    "nqs_profile_gemm": ([c_int], c_int),
+    "nqs_profile_gemm_read": ([c_void_p, c_void_p, c_void_p], c_int),
     "nqs_profile_events": ([c_void_p, c_void_p], c_int),
     "nqs_gram": ([c_void_p, c_int, c_int, c_int64, c_int64, c_void_p, c_int64, c_void_p, c_void_p],
                  c_int),

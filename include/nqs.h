@@ -100,6 +100,13 @@ unsigned long long nqs_kernel_launches(void);
 /* Optional cudaEvent_t pair (NULL to clear) recorded on the caller's stream immediately before and
  * after the Gram kernel inside nqs_minsr_direction, for timing it in isolation. */
 int nqs_profile_events(void* start_event, void* stop_event);
+/* Per-launch timing of the tensor-core row GEMMs of the float32 network (profiling aid, no
+ * reference counterpart): while enabled, every launch is bracketed by a pair of CUDA events (up to
+ * 16384 launches are kept) and its algorithmic bytes (operand rows, weights, output, residual)
+ * are summed. nqs_profile_gemm_read waits for the recorded events, returns the summed kernel time
+ * (ms), bytes and launch count since the last read, and clears them. */
+int nqs_profile_gemm(int enable);
+int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches);
 
 /* Model handle: validates the descriptor and uploads the immutable constants (Gs, W, knots).
  * Replaces the flax module construction in src/nqs/psiformer.py:100-116. */
