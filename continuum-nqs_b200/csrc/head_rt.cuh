@@ -253,8 +253,9 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
     int* piv = reinterpret_cast<int*>(hbuf + (TAN ? NP * LD : 2 * NP));  // pivot row per column
     bool used = false;
     int step = l;  // the column this lane's row pivots (padding rows keep their own index)
-    double logabs = 0.0;
-    cplx sgn = mk(1.0, 0.0);
+    // product of the pivots, kept as prod * 2^pexp with max(|re|, |im|) of prod in [0.5, 1)
+    cplx prod = mk(1.0, 0.0);
+    int pexp = 0;
     int sing = 0;
 #pragma unroll 1
     for (int c = 0; c < N; ++c) {
@@ -274,14 +275,17 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
       const int src = (lane & 16) | p;
       const cplx pv = mk(__shfl_sync(0xffffffffu, mr[0].re, src),
                          __shfl_sync(0xffffffffu, mr[0].im, src));
-      const double apv = hypot(pv.re, pv.im);
-      if (apv == 0.0) {
+      const bool zero = (pv.re == 0.0 && pv.im == 0.0);
+      if (zero) {
         sing = 1;
       } else {
-        logabs += log(apv);
-        sgn = cmul(sgn, mk(pv.re / apv, pv.im / apv));
+        prod = cmul(prod, pv);
+        int e;
+        frexp(fmax(fabs(prod.re), fabs(prod.im)), &e);
+        prod = mk(ldexp(prod.re, -e), ldexp(prod.im, -e));
+        pexp += e;
       }
-      const cplx ipv = (apv == 0.0) ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
+      const cplx ipv = zero ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
       const bool me = (l == p);
       if (me) {
         used = true;
@@ -339,8 +343,10 @@ __global__ void __launch_bounds__(64) k_head_rt(JobBatch jb, ModelConst mc,
         if (piv[c2] < l) ++inv_cnt;
 #pragma unroll
     for (int o = 8; o > 0; o >>= 1) inv_cnt += __shfl_xor_sync(0xffffffffu, inv_cnt, o);
-    if (inv_cnt & 1) sgn = mk(-sgn.re, -sgn.im);
-    const cplx logdet = sing ? mk(-INFINITY, 0.0) : mk(logabs, atan2(sgn.im, sgn.re));
+    if (inv_cnt & 1) prod = mk(-prod.re, -prod.im);
+    const cplx logdet = sing ? mk(-INFINITY, 0.0)
+                             : mk(log(hypot(prod.re, prod.im)) + pexp * 0.6931471805599453,
+                                  atan2(prod.im, prod.re));
     __syncwarp();
     // ---- tangents (also for singular matrices, whose results phase 3 discards) ----
     cplx lapk = mk(0, 0), sq = mk(0, 0);

@@ -188,9 +188,11 @@ __global__ void __launch_bounds__(256) k_dsyrk_lower(DTile a) {
       if (gj >= a.M || gj > gi) continue;
       if (a.nsplit > 1) {
         a.Cpart[((size_t)blockIdx.z * a.M + gi) * a.M + gj] = acc[i][j];
+      } else if (a.beta == 0.0) {  // C is not read
+        a.C[(size_t)gi * a.ldc + gj] = a.alpha * acc[i][j];
       } else {
         double* c = a.C + (size_t)gi * a.ldc + gj;
-        *c = a.alpha * acc[i][j] + (a.beta == 0.0 ? 0.0 : a.beta * (*c));
+        *c = a.alpha * acc[i][j] + a.beta * (*c);
       }
     }
   }
@@ -415,7 +417,53 @@ __global__ void k_store_diag(double* __restrict__ A, int64_t lda, int k0, int n,
   }
 }
 
-// Right-looking blocked Cholesky A = L L^T (lower triangle, in place), 64-column panels.
+// Look-ahead update of the next 64-column block: C[r][c] -= sum_j P[r][j] P[c][j] for r in
+// [0, rest), c in [0, min(64, rest)), c <= r, with P the 64-wide panel (rows 0.. of P are the
+// "column" rows). One CTA per 64 rows, 4 x 4 outputs per thread.
+__global__ void __launch_bounds__(256) k_panel_update(const double* __restrict__ P, int64_t ldp,
+                                                      int rest, double* __restrict__ C,
+                                                      int64_t ldc) {
+  extern __shared__ double pu_sm[];
+  double(*Pr)[CB + 1] = reinterpret_cast<double(*)[CB + 1]>(pu_sm);
+  double(*Pc)[CB + 1] = Pr + CB;
+  const int r0 = blockIdx.x * CB, nr = min(CB, rest - r0), nc = min(CB, rest);
+  for (int idx = threadIdx.x; idx < CB * CB; idx += blockDim.x) {
+    const int i = idx / CB, j = idx - i * CB;
+    Pr[i][j] = i < nr ? P[(size_t)(r0 + i) * ldp + j] : 0.0;
+    Pc[i][j] = i < nc ? P[(size_t)i * ldp + j] : 0.0;
+  }
+  __syncthreads();
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  double acc[4][4] = {};
+#pragma unroll 8
+  for (int k = 0; k < CB; ++k) {
+    double a4[4], b4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a4[u] = Pr[ty + 16 * u][k];
+      b4[u] = Pc[tx + 16 * u][k];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(a4[u], b4[v], acc[u][v]);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int r = r0 + ty + 16 * u;
+    if (r >= rest) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = tx + 16 * v;
+      if (c < nc && c <= r) C[(size_t)r * ldc + c] -= acc[u][v];
+    }
+  }
+}
+
+// Right-looking blocked Cholesky A = L L^T (lower triangle, in place), 64-column panels, with
+// one step of look-ahead: after step k's panel, the next 64 columns are updated first and the
+// next diagonal factor + panel solve run on a side stream while the rest of step k's trailing
+// update runs on the caller's stream (they touch disjoint columns).
 // part: scratch of at least 64 x 64 doubles for the diagonal factor.
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
@@ -423,23 +471,64 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
     set_error("cholesky_lower: scratch of %zu doubles < %d", part_elems, CB * CB);
     return NQS_ERR_WORKSPACE;
   }
-  int prev = -1;
-  for (int k0 = 0; k0 < n; k0 += CB) {
+  // side stream and two fork / join events per device, created once
+  static cudaStream_t side[64] = {};
+  static cudaEvent_t ev_fork[64] = {}, ev_join[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return NQS_ERR_UNSUPPORTED;
+  if (!side[dev]) {
+    // highest priority: the look-ahead CTAs are scheduled as soon as trailing-update CTAs retire
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&side[dev], cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork[dev], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join[dev], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("cholesky_lower: side stream / events");
+      return NQS_ERR_CUDA;
+    }
+  }
+  cudaStream_t s2 = side[dev];
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_panel_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double) * 2 * CB * (CB + 1)));
+    attr = true;
+  }
+  auto potrf = [&](int k0, int prev, cudaStream_t s) -> int {
     const int b = std::min(CB, n - k0);
     const int rest = n - k0 - b;
-    // panel rows per CTA: about two CTAs per SM, at least four rows per warp
     const int rpc = rest > 0 ? std::max(32, (rest + 2 * nsm - 1) / (2 * nsm)) : 1;
     const int grid = rest > 0 ? (rest + rpc - 1) / rpc : 1;
-    k_potrf_trsm<<<grid, 256, 0, st>>>(A, lda, k0, n, floor_p, bad, rpc, part, prev);
+    k_potrf_trsm<<<grid, 256, 0, s>>>(A, lda, k0, n, floor_p, bad, rpc, part, prev);
     NQS_CHECK_LAUNCH("k_potrf_trsm");
-    prev = k0;
-    if (rest <= 0) break;
-    // trailing: A[k0+b:, k0+b:] -= P P^T, P = A[k0+b:, k0:k0+b]
-    double* P = A + (size_t)(k0 + b) * lda + k0;
-    double* C = A + (size_t)(k0 + b) * lda + k0 + b;
-    NQS_TRY(dsyrk_lower(P, lda, rest, b, -1.0, 1.0, C, lda, nullptr, 0, nsm, st));
+    return NQS_OK;
+  };
+  NQS_TRY(potrf(0, -1, st));
+  int last = 0;
+  for (int k0 = 0; k0 + CB < n; k0 += CB) {
+    const int rest = n - k0 - CB;  // rows / columns after this panel
+    const double* P = A + (size_t)(k0 + CB) * lda + k0;
+    double* C = A + (size_t)(k0 + CB) * lda + k0 + CB;
+    // (a) next 64 columns of the trailing matrix
+    k_panel_update<<<(rest + CB - 1) / CB, 256, sizeof(double) * 2 * CB * (CB + 1), st>>>(
+        P, lda, rest, C, lda);
+    NQS_CHECK_LAUNCH("k_panel_update");
+    // next diagonal factor + panel solve on the side stream
+    cudaEventRecord(ev_fork[dev], st);
+    cudaStreamWaitEvent(s2, ev_fork[dev], 0);
+    NQS_TRY(potrf(k0 + CB, k0, s2));
+    cudaEventRecord(ev_join[dev], s2);
+    last = k0 + CB;
+    // (b) the rest of this step's trailing update
+    if (rest > CB) {
+      const double* P2 = A + (size_t)(k0 + 2 * CB) * lda + k0;
+      double* C2 = A + (size_t)(k0 + 2 * CB) * lda + k0 + 2 * CB;
+      NQS_TRY(dsyrk_lower(P2, lda, rest - CB, CB, -1.0, 1.0, C2, lda, nullptr, 0, nsm, st));
+    }
+    cudaStreamWaitEvent(st, ev_join[dev], 0);
   }
-  k_store_diag<<<1, 256, 0, st>>>(A, lda, prev, n, part);
+  k_store_diag<<<1, 256, 0, st>>>(A, lda, last, n, part);
   NQS_CHECK_LAUNCH("k_store_diag");
   return NQS_OK;
 }

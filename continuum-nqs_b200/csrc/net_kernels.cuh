@@ -562,15 +562,23 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
   const int ld = 3 * d;
   const T sc = T(1) / sqrt(T(HD));
   // rows >= N are never copied: zero them once (zero probabilities times zero values)
-  for (int idx = lane; idx < 8 * NT * HD; idx += 32) Kv[idx] = T(0);
-  __syncwarp();
+  if (N < NT) {
+    for (int idx = lane; idx < 8 * (NT - N) * HD; idx += 32) {
+      const int tile = idx / ((NT - N) * HD), r = idx - tile * (NT - N) * HD;
+      Kv[tile * NT * HD + N * HD + r] = T(0);
+    }
+    __syncwarp();
+  }
+  // channel c -> buffer b (Q, K, V tiles); the value channel's K and V go straight to their
+  // resident slots
   auto issue = [&](int c, int b) {
     if (c < C) {
       T* dst = buf + b * 3 * NT * HD;
       for (int q = lane; q < 3 * N * CH; q += 32) {
         const int t = q / (N * CH), r = q - t * (N * CH), tok = r / CH, ch = r - tok * CH;
         const T* src = QKV + (((size_t)job * N + tok) * C + c) * ld + t * d + h * HD + ch * V;
-        cp_async16(dst + (t * NT + tok) * HD + ch * V, src);
+        T* tile = (c == 0 && t > 0) ? (t == 1 ? Kv : Vv) : dst + t * NT * HD;
+        cp_async16(tile + tok * HD + ch * V, src);
       }
     }
     cp_async_commit();
@@ -585,8 +593,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
   T q[HD], a[8], ao[8];
   {
     const T* Q0 = buf;
-    const T* K0 = buf + NT * HD;
-    const T* V0 = buf + 2 * NT * HD;
+    const T* K0 = Kv;
+    const T* V0 = Vv;
     lds_row<T, HD>(Q0 + i * HD, q);
     T s[8];
     T mx = T(-INFINITY);
@@ -626,11 +634,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
       for (int e = 0; e < HE; ++e) o[e] = fma(a[m], v0[e], fma(ao[m], v1[e], o[e]));
     }
     if (live) stg_row<T, HE>(out_row(0), o);
-    // keep the value channel's K, V resident
-    for (int idx = lane; idx < N * HD; idx += 32) {
-      Kv[idx] = K0[idx];
-      Vv[idx] = V0[idx];
-    }
   }
   __syncwarp();
   issue(2, 0);
