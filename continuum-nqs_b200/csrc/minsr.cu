@@ -178,22 +178,131 @@ __global__ void __launch_bounds__(256) k_dsyrk_lower(DTile a) {
       buf ^= 1;
     }
   }
+  // epilogue, one output row at a time: that row's C values are all loaded before any of them is
+  // stored (loads may not move above stores to the same array, so element-wise read-modify-write
+  // would serialise 64 memory round trips per thread)
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int gi = i0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
     if (gi >= a.M) continue;
+    double cv[8];
+    if (a.nsplit == 1 && a.beta != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int gj = j0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+        cv[j] = (gj < a.M && gj <= gi) ? a.C[(size_t)gi * a.ldc + gj] : 0.0;
+      }
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int gj = j0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
       if (gj >= a.M || gj > gi) continue;
-      if (a.nsplit > 1) {
+      if (a.nsplit > 1)
         a.Cpart[((size_t)blockIdx.z * a.M + gi) * a.M + gj] = acc[i][j];
-      } else if (a.beta == 0.0) {  // C is not read
+      else if (a.beta == 0.0)  // C is not read
         a.C[(size_t)gi * a.ldc + gj] = a.alpha * acc[i][j];
-      } else {
-        double* c = a.C + (size_t)gi * a.ldc + gj;
-        *c = a.alpha * acc[i][j] + a.beta * (*c);
+      else
+        a.C[(size_t)gi * a.ldc + gj] = a.alpha * acc[i][j] + a.beta * cv[j];
+    }
+  }
+}
+
+// ---- same contraction with a 3-stage cp.async pipeline (operand rows 16-byte aligned) ----
+// 128 x 128 tile, K in chunks of 16 doubles; thread (ty, tx) owns rows ty + 16 i and columns
+// tx + 16 j (i, j < 8): a warp's A reads are broadcasts, its B reads at most 2-way bank conflicts.
+// The shared row stride (18 doubles = 144 bytes) keeps every cp.async destination 16-byte aligned.
+constexpr int DK = 16, DSTAGES = 3, DLD = DK + 2;
+static_assert((DLD * sizeof(double)) % 16 == 0, "cp.async rows must start on 16 bytes");
+// copies n_src (0, 8 or 16) bytes and zero-fills the rest of the 16
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, int n_src) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = n_src;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(n)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(256) k_dsyrk_cp(DTile a) {
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;                                  // [DSTAGES][128][DLD]
+  double* Bs = dsm + DSTAGES * 128 * DLD;            // [DSTAGES][128][DLD]
+  int ti, tj;
+  tile_of(blockIdx.x, &ti, &tj);
+  const int i0 = ti * 128, j0 = tj * 128;
+  const int64_t kb = (int64_t)blockIdx.z * a.kchunk;
+  const int64_t ke = min(a.K, kb + a.kchunk);
+  const int nk = (int)((ke - kb + DK - 1) / DK);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // stage loader: 128 rows x 8 chunks of 2 doubles for A and for B = 2048 copies, 8 per thread
+  auto load_stage = [&](int st, int kc) {
+    const int64_t k0 = kb + (int64_t)kc * DK;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = tid + 256 * q, r = idx >> 3, c = (idx & 7) * 2;
+      const int64_t k = k0 + c;
+      const int gi = i0 + r, gj = j0 + r;
+      const int nb = k < ke ? (int)min((int64_t)16, (ke - k) * 8) : 0;
+      const bool va = gi < a.M && nb > 0, vb = gj < a.M && nb > 0;
+      cp_async16_zfill(As + ((size_t)st * 128 + r) * DLD + c,
+                       va ? a.A + (size_t)gi * a.lda + k : a.A, va ? nb : 0);
+      cp_async16_zfill(Bs + ((size_t)st * 128 + r) * DLD + c,
+                       vb ? a.B + (size_t)gj * a.ldb + k : a.B, vb ? nb : 0);
+    }
+  };
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+#pragma unroll
+  for (int s = 0; s < DSTAGES - 1; ++s) {
+    if (s < nk) load_stage(s, s);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int kc = 0; kc < nk; ++kc) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(DSTAGES - 2) : "memory");
+    __syncthreads();
+    const int nxt = kc + DSTAGES - 1;
+    if (nxt < nk) load_stage(nxt % DSTAGES, nxt);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const double* as = As + (size_t)(kc % DSTAGES) * 128 * DLD;
+    const double* bs = Bs + (size_t)(kc % DSTAGES) * 128 * DLD;
+#pragma unroll
+    for (int kk = 0; kk < DK; ++kk) {
+      double av[8], bv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) av[i] = as[(ty + 16 * i) * DLD + kk];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) bv[j] = bs[(tx + 16 * j) * DLD + kk];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  // epilogue, one output row at a time (its C values loaded before any is stored)
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gi = i0 + ty + 16 * i;
+    if (gi >= a.M) continue;
+    double cv[8];
+    if (a.nsplit == 1 && a.beta != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int gj = j0 + tx + 16 * j;
+        cv[j] = (gj < a.M && gj <= gi) ? a.C[(size_t)gi * a.ldc + gj] : 0.0;
       }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int gj = j0 + tx + 16 * j;
+      if (gj >= a.M || gj > gi) continue;
+      if (a.nsplit > 1)
+        a.Cpart[((size_t)blockIdx.z * a.M + gi) * a.M + gj] = acc[i][j];
+      else if (a.beta == 0.0)
+        a.C[(size_t)gi * a.ldc + gj] = a.alpha * acc[i][j];
+      else
+        a.C[(size_t)gi * a.ldc + gj] = a.alpha * acc[i][j] + a.beta * cv[j];
     }
   }
 }
@@ -222,9 +331,22 @@ int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, do
     while (nsplit > 1 && (size_t)nsplit * M * M > part_elems) --nsplit;
   }
   DTile a{A, lda, A, lda, C, ldc, M, K, alpha, beta, nsplit, 0, part};
-  a.kchunk = ((K + nsplit - 1) / nsplit + 7) / 8 * 8;
-  k_dsyrk_lower<<<dim3(tiles, 1, nsplit), 256, 0, st>>>(a);
-  NQS_CHECK_LAUNCH("k_dsyrk_lower");
+  const bool cp = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda % 2) == 0;
+  if (cp) {
+    a.kchunk = ((K + nsplit - 1) / nsplit + DK - 1) / DK * DK;
+    const size_t sm = sizeof(double) * 2 * DSTAGES * 128 * DLD;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_dsyrk_cp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      attr = true;
+    }
+    k_dsyrk_cp<<<dim3(tiles, 1, nsplit), 256, sm, st>>>(a);
+    NQS_CHECK_LAUNCH("k_dsyrk_cp");
+  } else {
+    a.kchunk = ((K + nsplit - 1) / nsplit + 7) / 8 * 8;
+    k_dsyrk_lower<<<dim3(tiles, 1, nsplit), 256, 0, st>>>(a);
+    NQS_CHECK_LAUNCH("k_dsyrk_lower");
+  }
   if (nsplit > 1) {
     const int64_t n = (int64_t)M * M;
     k_splitk_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, nsplit, M, C, ldc, alpha,
@@ -869,6 +991,7 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
     m1[c] = (mu && in) ? mu[K + k0 + c] : 0.0;
   }
   DD acc[4];
+#pragma unroll 4
   for (int m = m_lo; m < m_hi; ++m) {
     const TO* row = O + (size_t)m * K + k0;
     double o[4];
@@ -958,6 +1081,8 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
   bool hi_half[RB];
 #pragma unroll
   for (int i = 0; i < RB; ++i) hi_half[i] = m0 + i >= Mh;
+  // which column-mean halves this CTA's rows use (uniform per CTA)
+  const bool need0 = mu && m0 < Mh, need1 = mu && m0 + nr - 1 >= Mh;
   const int64_t step = (int64_t)blockDim.x * 4;
   for (int64_t k = (int64_t)threadIdx.x * 4; k < K; k += step) {
     double vv[4], vl[4], u0[4], u1[4];
@@ -966,8 +1091,8 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
       const bool in = VEC || k + c < K;
       vv[c] = in ? v[k + c] : 0.0;
       vl[c] = in ? v_lo[k + c] : 0.0;
-      u0[c] = (mu && in) ? mu[k + c] : 0.0;
-      u1[c] = (mu && in) ? mu[K + k + c] : 0.0;
+      u0[c] = (need0 && in) ? mu[k + c] : 0.0;
+      u1[c] = (need1 && in) ? mu[K + k + c] : 0.0;
     }
 #pragma unroll
     for (int i = 0; i < RB; ++i) {
@@ -991,7 +1116,7 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
       for (int c = 0; c < 4; ++c) {
         const double oc = o[c] - (hi_half[i] ? u1[c] : u0[c]);
         acc[i].add_prod(oc, vv[c]);
-        acc[i].add_prod(oc, vl[c]);
+        acc[i].c = fma(oc, vl[c], acc[i].c);  // the low word's product, into the compensation
       }
     }
   }
@@ -1032,7 +1157,7 @@ template <typename TO>
 static int gemv_n_resid(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* v,
                         const double* v_lo, const double* b, double lam0, const double* lam_extra,
                         const double* x, double* r, cudaStream_t st) {
-  constexpr int RB = 4;
+  constexpr int RB = 8;
   const unsigned g = (unsigned)((M + RB - 1) / RB);
   if (K % 4 == 0)
     k_gemv_n_resid_rows<TO, RB, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, v_lo, b, lam0,
