@@ -4,8 +4,9 @@
  *
  * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an int status
  * (NQS_OK == 0). All array arguments are CALLER-OWNED DEVICE memory unless a name ends in _host.
- * The library allocates nothing per call: scratch memory is a caller-provided workspace whose size
- * the matching *_workspace_size function reports. Work is enqueued on the given cudaStream_t
+ * The library allocates no device memory per call: scratch memory is a caller-provided workspace
+ * whose size the matching *_workspace_size function reports. (The first Cholesky on a device creates
+ * one high-priority side stream and two events, kept for the process, for its look-ahead.) Work is enqueued on the given cudaStream_t
  * (passed as void*) and is asynchronous; no entry point synchronises the device except
  * nqs_model_create / nqs_ewald_create (one-time uploads of constants).
  *
