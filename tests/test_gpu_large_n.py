@@ -1,0 +1,64 @@
+"""Shapes past 16 electrons (the sizes of the reference's configurations 4 and 5): the head and
+attention kernels take their general paths there. log psi, the local energy (forward Laplacian and
+spin-orbit flips) and the per-sample Jacobian against the FP64 oracle (reference
+src/nqs/psiformer.py:118-189, src/nqs/local_energy.py:40-117, src/nqs/minsr.py:56-65)."""
+import numpy as np
+import pytest
+
+from helpers import build, configs, perturb
+from oracle import nqs_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _close_mod_2pi(a, b, tol):
+    d = complex(a) - complex(b)
+    return abs(d.real) < tol and abs((d.imag + np.pi) % (2 * np.pi) - np.pi) < tol
+
+
+@pytest.mark.parametrize("kw", [
+    # configuration-4-like: width 64, 3 blocks, 2 determinants, N between 16 and 26
+    dict(N=20, L=9.0, embed=64, depth=3, heads=4, n_freq=8, n_dets=2),
+    # configuration-5 shape: N = 48, width 128, 8 heads, 8 determinants, RBF Jastrow
+    dict(N=48, L=14.0, embed=128, depth=2, heads=8, n_freq=8, n_dets=8, use_jastrow=True,
+         n_knots=16),
+])
+def test_logpsi_large_n_matches_oracle(kw):
+    from nqs.psiformer import make_logpsi
+    g, model = build(**kw)
+    p = perturb(model.init(0), 0.02, 41)
+    R, S = configs(model.n_elec, model.L, 3, 42)
+    lp = make_logpsi(model, p)(R, S).cpu()
+    for w in range(R.shape[0]):
+        ref = O.logpsi(model, p, R[w], S[w])
+        assert _close_mod_2pi(lp[w], ref, 1e-10), (w, complex(lp[w]), complex(ref))
+    # antisymmetry: swapping electrons 0 and 1 (positions and spins) flips the sign
+    perm = list(range(model.n_elec))
+    perm[0], perm[1] = 1, 0
+    l1 = make_logpsi(model, p)(R[:, perm], S[:, perm]).cpu()
+    ratio = np.exp(complex(l1[0] - lp[0]))
+    assert abs(ratio + 1) < 1e-9
+
+
+def test_local_energy_n18_matches_oracle():
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import make_logpsi
+    g, model = build(N=18, L=8.5, n_dets=2, use_jastrow=True, n_knots=4)
+    p = perturb(model.init(0), 0.05, 43)
+    R, S = configs(model.n_elec, model.L, 2, 44)
+    e = make_local_energy(make_logpsi(model, p), 1.0, 1.0, 0.5)(R, S).cpu()
+    for w in range(2):
+        ref = O.local_energy(lambda r, s: O.logpsi(model, p, r, s), R[w], S[w], 1.0, 1.0, 0.5)
+        assert abs(complex(e[w]) - complex(ref)) < 1e-9 * max(1.0, abs(complex(ref)))
+
+
+def test_per_sample_O_n18_matches_oracle():
+    from nqs.minsr import per_sample_O, real_ravel
+    g, model = build(N=18, L=8.5, n_dets=2, use_jastrow=True, n_knots=4)
+    p = perturb(model.init(0), 0.05, 45)
+    theta, unravel = real_ravel(p)
+    R, S = configs(model.n_elec, model.L, 2, 46)
+    Og = per_sample_O(model, theta.cuda(), unravel, R, S).cpu()
+    ot, ou = O.real_ravel(p["params"])
+    Oo = O.per_sample_O(model, ot, ou, R, S)
+    assert (Og - Oo).abs().max() < 1e-10 * max(1.0, float(Oo.abs().max()))
