@@ -52,6 +52,10 @@ inline HeadRtPlan head_rt_plan(int N, int nG, int K, int n_tan, bool tan, bool l
   // per half-warp: pivot-row broadcast (and, with tangents, the D_t / B_t matrix), pivot order
   p.hw_bytes = round128(16 * (size_t)(tan ? kHeadTok * kHeadLd : 2 * kHeadTok) + 4 * kHeadTok);
   p.bytes = p.jpc * p.job_bytes + 4 * p.hw_bytes;
+  while (p.jpc > 1 && p.bytes > 200 * 1024) {  // large envelopes (many plane waves): fewer jobs
+    --p.jpc;
+    p.bytes = p.jpc * p.job_bytes + 4 * p.hw_bytes;
+  }
   return p;
 }
 

@@ -174,16 +174,20 @@ __global__ void k_eloc_assemble(int W, int N, const cplx* __restrict__ L0,
                                 const cplx* __restrict__ g, const cplx* __restrict__ lap,
                                 const cplx* __restrict__ Lf, const cplx* __restrict__ gf,
                                 const int32_t* __restrict__ S, const double* __restrict__ coul,
-                                double m_star, double lambda_r, double h_z,
-                                cplx* __restrict__ out) {
+                                const double* __restrict__ field, double m_star, double lambda_r,
+                                double h_z, cplx* __restrict__ out) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
   cplx g2 = mk(0, 0);
   for (int t = 0; t < 2 * N; ++t) cfma(g2, g[(size_t)w * 2 * N + t], g[(size_t)w * 2 * N + t]);
   const cplx kin = cscale(cadd(lap[w], g2), -1.0 / (2.0 * m_star));
-  double sg = 0.0;
-  for (int i = 0; i < N; ++i) sg += 1.0 - 2.0 * (double)S[(size_t)w * N + i];
-  const double ez = -0.5 * h_z * sg;
+  double sg = 0.0, fz = 0.0;
+  for (int i = 0; i < N; ++i) {
+    const double sz = 1.0 - 2.0 * (double)S[(size_t)w * N + i];
+    sg += sz;
+    if (field) fz += field[((size_t)w * N + i) * 3 + 2] * sz;  // sum_i f_z(r_i) (sigma_z)_ss
+  }
+  const double ez = -0.5 * h_z * sg - fz;
   cplx soc = mk(0, 0);
   if (Lf) {
     const cplx l0 = L0[w];
@@ -198,6 +202,10 @@ __global__ void k_eloc_assemble(int W, int N, const cplx* __restrict__ L0,
       const double sgy = S[j] == 0 ? -1.0 : 1.0;
       const cplx e = cadd(cmul(mk(0, -1), ay), cscale(ax, sgy));
       soc = cadd(soc, cscale(e, lambda_r));
+      if (field) {  // -(f_x sigma_x + f_y sigma_y)_{s s'} Psi(s')/Psi(s): sigma_y = i sgy
+        const double* f = field + j * 3;
+        soc = csub(soc, cmul(mk(f[0], f[1] * sgy), ratio));
+      }
     }
   }
   cplx e = cadd(cadd(kin, mk(ez, 0.0)), soc);
@@ -504,9 +512,9 @@ int nqs_logpsi(NqsModel* m, const double* theta, const double* R, const int32_t*
 
 static int local_energy_impl(NqsModel* m, const double* theta, const double* R, const int32_t* S,
                              int W, double m_star, double lambda_r, double h_z,
-                             const NqsEwald* ewald, double* out_eloc, double* out_logpsi,
-                             double* out_grad, double* out_lap, int prec, void* wsp, size_t wsb,
-                             cudaStream_t st, bool energy) {
+                             const NqsEwald* ewald, const double* field, double* out_eloc,
+                             double* out_logpsi, double* out_grad, double* out_lap, int prec,
+                             void* wsp, size_t wsb, cudaStream_t st, bool energy) {
   if (W < 0 || (W > 0 && (!R || !S))) return NQS_ERR_INVALID_ARG;
   if (W == 0) return NQS_OK;
   if (!m->fl_ok) {
@@ -534,15 +542,15 @@ static int local_energy_impl(NqsModel* m, const double* theta, const double* R, 
     NQS_CHECK_LAUNCH("copy outputs");
     return NQS_OK;
   }
-  const bool soc = lambda_r != 0.0;
+  const bool soc = lambda_r != 0.0 || field;  // the field's sigma_x, sigma_y need the flips too
   if (soc) {
     JobBatch sb{JOB_SOC, W * N, N, 3, 2, 0, 0, R, S, nullptr};
     NQS_TRY(run_net(m, c, prec, sb, HeadOut{Lf, gf, nullptr}, st));
   }
   if (ewald) NQS_TRY(nqs_ewald_energy(ewald, R, W, N, coul, st));
   k_eloc_assemble<<<(W + 127) / 128, 128, 0, st>>>(W, N, L0, g, lap, soc ? Lf : nullptr, gf, S,
-                                                    ewald ? coul : nullptr, m_star, lambda_r, h_z,
-                                                    (cplx*)out_eloc);
+                                                    ewald ? coul : nullptr, field, m_star,
+                                                    lambda_r, h_z, (cplx*)out_eloc);
   NQS_CHECK_LAUNCH("k_eloc_assemble");
   if (out_logpsi) cudaMemcpyAsync(out_logpsi, L0, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st);
   return NQS_OK;
@@ -553,15 +561,27 @@ int nqs_local_energy(NqsModel* m, const double* theta, const double* R, const in
                      double* out_eloc, double* out_logpsi, int prec, void* wsp, size_t wsb,
                      void* stream) {
   if (!out_eloc && W > 0) return NQS_ERR_INVALID_ARG;
-  return local_energy_impl(m, theta, R, S, W, m_star, lambda_r, h_z, ewald, out_eloc, out_logpsi,
-                           nullptr, nullptr, prec, wsp, wsb, (cudaStream_t)stream, true);
+  return local_energy_impl(m, theta, R, S, W, m_star, lambda_r, h_z, ewald, nullptr, out_eloc,
+                           out_logpsi, nullptr, nullptr, prec, wsp, wsb, (cudaStream_t)stream,
+                           true);
+}
+
+int nqs_local_energy_field(NqsModel* m, const double* theta, const double* R, const int32_t* S,
+                           int W, double m_star, double lambda_r, double h_z,
+                           const NqsEwald* ewald, const double* field, double* out_eloc,
+                           double* out_logpsi, int prec, void* wsp, size_t wsb, void* stream) {
+  if ((!out_eloc || !field) && W > 0) return NQS_ERR_INVALID_ARG;
+  return local_energy_impl(m, theta, R, S, W, m_star, lambda_r, h_z, ewald, field, out_eloc,
+                           out_logpsi, nullptr, nullptr, prec, wsp, wsb, (cudaStream_t)stream,
+                           true);
 }
 
 int nqs_grad_laplacian(NqsModel* m, const double* theta, const double* R, const int32_t* S,
                        int W, double* out_logpsi, double* out_grad, double* out_lap, int prec,
                        void* wsp, size_t wsb, void* stream) {
-  return local_energy_impl(m, theta, R, S, W, 1.0, 0.0, 0.0, nullptr, nullptr, out_logpsi,
-                           out_grad, out_lap, prec, wsp, wsb, (cudaStream_t)stream, false);
+  return local_energy_impl(m, theta, R, S, W, 1.0, 0.0, 0.0, nullptr, nullptr, nullptr,
+                           out_logpsi, out_grad, out_lap, prec, wsp, wsb, (cudaStream_t)stream,
+                           false);
 }
 
 int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, double* logpsi_io,

@@ -232,7 +232,7 @@ class VMCIteration:
 
     def __init__(self, model, theta, R, S, *, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
                  lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, clip_k=5.0, n_spin_flips=2,
-                 seed=0, counter=0, precision="fp64", gram=None, n_refine=None):
+                 seed=0, counter=0, precision="fp64", gram=None, n_refine=None, ext_field=None):
         from . import _lib
         from .psiformer import _prec, as_batch
         _lib.require_cuda()
@@ -265,6 +265,10 @@ class VMCIteration:
         self.acc_spin = torch.zeros(self.W, dtype=F64, device=dev)
         self.status = torch.zeros(3, dtype=torch.int32, device=dev)
         self.damping = torch.zeros(1, dtype=F64, device=dev)  # extra damping of a TC Gram
+        # external spin field (vectorised ext_field: positions (..., 2) -> (..., 3))
+        self.ext_field = ext_field
+        self.field = (torch.empty(self.W, self.N, 3, dtype=F64, device=dev)
+                      if ext_field is not None else None)
         h = model.native().handle
         self.h = h
         sizes = [_lib.workspace_for(h, op, self.W, self.prec)[1]
@@ -286,11 +290,19 @@ class VMCIteration:
 
     def energies(self):
         from . import _lib
-        _lib.check(_lib.lib().nqs_local_energy(
-            self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W, self.m_star,
-            self.lambda_r, self.h_z, self.ewald.handle if self.ewald else None, _lib.ptr(self.e),
-            None, self.prec, _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
-            "nqs_local_energy")
+        ew = self.ewald.handle if self.ewald else None
+        if self.ext_field is None:
+            _lib.check(_lib.lib().nqs_local_energy(
+                self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W,
+                self.m_star, self.lambda_r, self.h_z, ew, _lib.ptr(self.e), None, self.prec,
+                _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()), "nqs_local_energy")
+        else:
+            self.field.copy_(torch.as_tensor(self.ext_field(self.R), dtype=F64))
+            _lib.check(_lib.lib().nqs_local_energy_field(
+                self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W,
+                self.m_star, self.lambda_r, self.h_z, ew, _lib.ptr(self.field), _lib.ptr(self.e),
+                None, self.prec, _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
+                "nqs_local_energy_field")
 
     def jacobian(self):
         from . import _lib
@@ -328,8 +340,6 @@ def train_minsr(model, params, L, n_elec, key, *, m_star=1.0, lambda_r=1.0, h_z=
     uniform walkers and `burn` sweeps; a warm ensemble (R0, S0) skips the burn stage."""
     from .random import as_key, key_to_seed, split
     from .sampler import init_walkers_uniform
-    if ext_field is not None:
-        raise NotImplementedError("ext_field is not implemented by the CUDA kernels")
     theta, unravel = real_ravel(params)
     kk, ks = split(as_key(key), 2)
     if R0 is None:
@@ -338,7 +348,8 @@ def train_minsr(model, params, L, n_elec, key, *, m_star=1.0, lambda_r=1.0, h_z=
         R, S = torch.as_tensor(R0), torch.as_tensor(S0)
     it = VMCIteration(model, theta, R, S, m_star=m_star, lambda_r=lambda_r, h_z=h_z,
                       coulomb=coulomb, lr=lr, lam=lam, n_sweeps=n_sweeps, step_size=step_size,
-                      clip_k=clip_k, seed=key_to_seed(ks), precision=precision, gram=gram)
+                      clip_k=clip_k, seed=key_to_seed(ks), precision=precision, gram=gram,
+                      ext_field=ext_field)
     if R0 is None and burn > 0:
         it.sample(burn)
     hist = history if history is not None else {"E": [], "Eerr": []}

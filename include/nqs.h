@@ -137,6 +137,15 @@ int nqs_local_energy(NqsModel* model, const double* theta, const double* R, cons
                      int n_walkers, double m_star, double lambda_r, double h_z,
                      const NqsEwald* ewald, double* out_eloc, double* out_logpsi,
                      int precision, void* workspace, size_t workspace_bytes, void* stream);
+/* nqs_local_energy with an external spin field (the ext_field of make_local_energy,
+ * src/nqs/local_energy.py:41-42,86-88,109-111): field = f(r_i) evaluated by the caller at the
+ * walkers' positions, float64[W][N][3] (f_x, f_y, f_z), adding
+ *   - sum_i f_z(r_i) (sigma_z)_{s_i s_i}  -  sum_i [f_x sigma_x + f_y sigma_y]_{s_i s'} Psi(s')/Psi. */
+int nqs_local_energy_field(NqsModel* model, const double* theta, const double* R,
+                           const int32_t* S, int n_walkers, double m_star, double lambda_r,
+                           double h_z, const NqsEwald* ewald, const double* field,
+                           double* out_eloc, double* out_logpsi, int precision, void* workspace,
+                           size_t workspace_bytes, void* stream);
 
 /* Gradient and Laplacian of log psi (forward Laplacian): out_grad complex[W][2N],
  * out_lap complex[W], out_logpsi complex[W] (each nullable). */

@@ -182,9 +182,11 @@ def slater_logpsi(Gs, W, R, S):
 # ----------------------------------------------------------------------------------------------
 # local energy  (reference: src/nqs/local_energy.py:40-117, dense-Hessian default path)
 # ----------------------------------------------------------------------------------------------
-def local_energy(lp: Callable, R, S, m_star=1.0, lambda_r=1.0, h_z=0.0):
+def local_energy(lp: Callable, R, S, m_star=1.0, lambda_r=1.0, h_z=0.0, ext_field=None):
     """E_loc(R,S) for a single configuration with a dense Hessian kinetic term
-    (local_energy.py:63-115). lp(R,S) -> complex."""
+    (local_energy.py:63-115). lp(R,S) -> complex. ext_field(r) -> (3,) real (one position) adds
+    -sum_i f_z (sigma_z)_{s_i s_i} - sum_i [f_x sigma_x + f_y sigma_y]_{s_i s'} ratio_i
+    (local_energy.py:86-88,109-111)."""
     N = R.shape[0]
     rf = R.reshape(-1)
 
@@ -200,6 +202,10 @@ def local_energy(lp: Callable, R, S, m_star=1.0, lambda_r=1.0, h_z=0.0):
     E_kin = -1.0 / (2.0 * m_star) * (lap + torch.sum(g * g))
     sgn = 1.0 - 2.0 * S.to(F64)
     E_Z = -0.5 * h_z * torch.sum(sgn)
+    fields = None
+    if ext_field is not None:
+        fields = [torch.as_tensor(ext_field(R[i]), dtype=F64) for i in range(N)]
+        E_Z = E_Z - sum(float(fields[i][2]) * float(sgn[i]) for i in range(N))
     E_soc = torch.zeros((), dtype=C128)
     for i in range(N):
         s_i = int(S[i])
@@ -209,9 +215,12 @@ def local_energy(lp: Callable, R, S, m_star=1.0, lambda_r=1.0, h_z=0.0):
         Lf = lp(R, Sf)
         if not torch.isfinite(Lf.real):
             # exactly singular flipped determinant: Psi(s') = 0, the reference's guarded
-            # ratio * gradient is 0 (local_energy.py:99-105)
+            # ratio * gradient is 0 (local_energy.py:99-105); so is the field term
             continue
         ratio = torch.exp(Lf - L0)
+        if fields is not None:
+            sy_f = -1j if s_i == 0 else 1j
+            E_soc = E_soc - (float(fields[i][0]) + float(fields[i][1]) * sy_f) * ratio
         gf = grad(Lr)(rf, Sf) + 1j * grad(Li)(rf, Sf)
         ampgx = ratio * gf[2 * i]
         ampgy = ratio * gf[2 * i + 1]

@@ -146,3 +146,21 @@ def test_oracle_real_ravel_layout():
             assert torch.equal(theta[off + n:off + 2 * n], leaf.imag.reshape(-1))
         else:
             assert torch.equal(theta[off:off + n], leaf.reshape(-1).to(torch.float64))
+
+
+def test_spiral_zero_variance_oracle():
+    """The reference's non-collinear gate (tests/test_nqs_spiral.py:45-57, test_nqs_folx.py:59-70):
+    the exact spin-spiral determinant has E_loc = E_gs with the spiral ext_field, here for the
+    oracle and the restated spiral_gs (src/nqs/spiral_reference.py:24-75)."""
+    from nqs.spiral import spiral_field, spiral_gs
+    res = spiral_gs(N=7, L=8.0, Q_int=(1, 0), B=0.3, lambda_r=1.0, h_z=0.0, n_cut=10,
+                    twist=(0.1, 0.17))
+    assert res["cutoff_ok"] and res["gap"] > 1e-6
+    f = spiral_field(res["B"], res["Q"])
+    lp = lambda R, S: O.slater_logpsi(res["Gs"], res["W"], R, S)  # noqa: E731
+    rng = np.random.default_rng(0)
+    for _ in range(3):
+        R = torch.as_tensor(rng.uniform(0, res["L"], (7, 2)))
+        S = torch.as_tensor(rng.integers(0, 2, 7))
+        e = complex(O.local_energy(lp, R, S, 1.0, res["lambda_r"], 0.0, ext_field=f))
+        assert abs(e.real - res["E_gs"]) < 1e-10 and abs(e.imag) < 1e-10
