@@ -164,3 +164,22 @@ def test_spiral_zero_variance_oracle():
         S = torch.as_tensor(rng.integers(0, 2, 7))
         e = complex(O.local_energy(lp, R, S, 1.0, res["lambda_r"], 0.0, ext_field=f))
         assert abs(e.real - res["E_gs"]) < 1e-10 and abs(e.imag) < 1e-10
+
+
+def test_ed2_noninteracting_limit_and_convergence():
+    """The two-electron plane-wave ED (oracle/ed2.py): without Coulomb it reproduces the
+    non-interacting Rashba ground state of the reference's rashba module (src/nqs/
+    rashba_reference.py:83-108) for two twists; with Coulomb it converges in the cutoff towards
+    the committed golden value (tests/golden/ed2_config1.json, made by make_ed2.py)."""
+    import json
+    from oracle import ed2
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ed2_config1.json")))
+    L = g["L"]
+    A = np.diag([L, L])
+    for tw in ((0.0, 0.0), TWIST):
+        ref = rashba.noninteracting_gs(N=2, L=L, m_star=1.0, lambda_r=0.5, h_z=0.1, n_cut=10,
+                                       twist=tw)["E_gs"]
+        assert abs(ed2.ground_energy(A, 5, 1.0, 0.5, 0.1, alpha=0.0, twist=tw) - ref) < 1e-10
+    e10 = ed2.ground_energy(A, 10, 1.0, 0.5, 0.1, alpha=1.0, ewald_alpha=5.0 / L)
+    assert e10 > g["E_ed_ncut16"] > g["E_ed_ncut24"]  # variational in the cutoff
+    assert e10 - g["E_ed_ncut24"] < 3e-5
