@@ -213,6 +213,22 @@ __global__ void k_eloc_assemble(int W, int N, const cplx* __restrict__ L0,
   out[w] = e;
 }
 
+// single-particle spin estimators from the flip ratios (observables.py:31-45):
+// ratio_i = exp(L(flip i) - L) (non-finite -> 0), sx = ratio, sy = -i sz ratio, sz = 1 - 2 s_i
+__global__ void k_spin_estimators(int W, int N, const cplx* __restrict__ L0,
+                                  const cplx* __restrict__ Lf, const int32_t* __restrict__ S,
+                                  cplx* __restrict__ sx, cplx* __restrict__ sy,
+                                  double* __restrict__ sz) {
+  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (size_t)W * N) return;
+  cplx r = cexp_(csub(Lf[j], L0[j / N]));
+  if (!cfinite(r)) r = mk(0, 0);
+  const double z = 1.0 - 2.0 * (double)S[j];
+  sx[j] = r;
+  sy[j] = mk(z * r.im, -z * r.re);  // -i z r
+  sz[j] = z;
+}
+
 }  // namespace nqs
 
 using namespace nqs;
@@ -508,6 +524,32 @@ int nqs_logpsi(NqsModel* m, const double* theta, const double* R, const int32_t*
   NQS_TRY(begin(m, theta, prec, wsp, wsb, st, &c));
   JobBatch jb{JOB_VALUE, W, m->hm.mc.N, 1, 0, 0, 0, R, S, nullptr};
   return run_net(m, c, prec, jb, HeadOut{(cplx*)out_logpsi, nullptr, nullptr}, st);
+}
+
+int nqs_spin_estimators(NqsModel* m, const double* theta, const double* R, const int32_t* S,
+                        int W, double* out_sx, double* out_sy, double* out_sz, int prec,
+                        void* wsp, size_t wsb, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (W < 0 || (W > 0 && (!R || !S || !out_sx || !out_sy || !out_sz)))
+    return NQS_ERR_INVALID_ARG;
+  if (W == 0) return NQS_OK;
+  NQS_TRY(check_ws(m, NQS_OP_LOCAL_E, W, prec, wsb));
+  Ctx c;
+  NQS_TRY(begin(m, theta, prec, wsp, wsb, st, &c));
+  const int N = m->hm.mc.N;
+  cplx* L0 = c.ws.take<cplx>(W);
+  cplx* Lf = c.ws.take<cplx>((size_t)W * N);
+  if (!Lf) return NQS_ERR_WORKSPACE;
+  JobBatch jb{JOB_VALUE, W, N, 1, 0, 0, 0, R, S, nullptr};
+  NQS_TRY(run_net(m, c, prec, jb, HeadOut{L0, nullptr, nullptr}, st));
+  // the N single-spin flips of every walker, values only
+  JobBatch fb{JOB_SOC, W * N, N, 1, 0, 0, 0, R, S, nullptr};
+  NQS_TRY(run_net(m, c, prec, fb, HeadOut{Lf, nullptr, nullptr}, st));
+  const size_t n = (size_t)W * N;
+  k_spin_estimators<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+      W, N, L0, Lf, S, (cplx*)out_sx, (cplx*)out_sy, out_sz);
+  NQS_CHECK_LAUNCH("k_spin_estimators");
+  return NQS_OK;
 }
 
 static int local_energy_impl(NqsModel* m, const double* theta, const double* R, const int32_t* S,

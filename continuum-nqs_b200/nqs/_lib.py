@@ -71,6 +71,8 @@ _SIGS = {
     "nqs_local_energy": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double, c_double,
                           c_double, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_size_t,
                           c_void_p], c_int),
+    "nqs_spin_estimators": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                             c_void_p, c_int, c_void_p, c_size_t, c_void_p], c_int),
     "nqs_local_energy_field": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double,
                                 c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                                 c_void_p, c_size_t, c_void_p], c_int),

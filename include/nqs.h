@@ -147,6 +147,14 @@ int nqs_local_energy_field(NqsModel* model, const double* theta, const double* R
                            double* out_eloc, double* out_logpsi, int precision, void* workspace,
                            size_t workspace_bytes, void* stream);
 
+/* Single-particle spin estimators of W configurations from the N spin-flip ratios
+ * ratio_i = Psi(s_i -> 1 - s_i) / Psi (src/nqs/observables.py:31-45): out_sx = ratio (complex
+ * [W][N]), out_sy = -i sz ratio (complex [W][N]), out_sz = 1 - 2 s_i (float64 [W][N]); a
+ * non-finite ratio (exactly singular flipped determinant) gives 0. Workspace: NQS_OP_LOCAL_E. */
+int nqs_spin_estimators(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                        int n_walkers, double* out_sx, double* out_sy, double* out_sz,
+                        int precision, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Gradient and Laplacian of log psi (forward Laplacian): out_grad complex[W][2N],
  * out_lap complex[W], out_logpsi complex[W] (each nullable). */
 int nqs_grad_laplacian(NqsModel* model, const double* theta, const double* R, const int32_t* S,
