@@ -176,6 +176,57 @@ __global__ void k_center_cvt(const TO* __restrict__ O, int W, int64_t P, int64_t
     D[(size_t)r * ldd + p] = (TD)v;
 }
 
+// vectorised form: 8 consecutive columns x CVT_ROWS rows per thread (the column means are read
+// once per thread); VEC: P % 4 == 0 so the 8 source columns are two 16-byte loads (float)
+constexpr int CVT_ROWS = 16;
+template <typename TO, typename TD, bool VEC>
+__global__ void __launch_bounds__(256) k_center_cvt8(const TO* __restrict__ O, int W, int M,
+                                                     int64_t P, int64_t ldd,
+                                                     const double* __restrict__ mu,
+                                                     TD* __restrict__ D) {
+  const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  if (p0 >= ldd) return;
+  const int r0 = blockIdx.y * CVT_ROWS, r1 = min(M, r0 + CVT_ROWS);
+  double m0[8], m1[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const bool in = p0 + c < P;
+    m0[c] = (in && r0 < W) ? mu[p0 + c] : 0.0;
+    m1[c] = (in && r1 > W) ? mu[P + p0 + c] : 0.0;
+  }
+  for (int r = r0; r < r1; ++r) {
+    const TO* src = O + (size_t)r * P + p0;
+    double v[8];
+    if (VEC && sizeof(TO) == 4 && p0 + 8 <= P) {
+      const float4 a = reinterpret_cast<const float4*>(src)[0];
+      const float4 b = reinterpret_cast<const float4*>(src)[1];
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[c] = p0 + c < P ? (double)src[c] : 0.0;
+    }
+    const bool hi = r >= W;
+    TD out[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double x = p0 + c < P ? v[c] - (hi ? m1[c] : m0[c]) : 0.0;
+      if constexpr (sizeof(TD) == 2)
+        out[c] = __double2bfloat16(x);
+      else
+        out[c] = (TD)x;
+    }
+    TD* dst = D + (size_t)r * ldd + p0;
+    if (p0 + 8 <= ldd) {
+#pragma unroll
+      for (int c = 0; c < 8 * (int)sizeof(TD) / 16; ++c)
+        reinterpret_cast<int4*>(dst)[c] = reinterpret_cast<const int4*>(out)[c];
+    } else {  // row end (ldd a multiple of 4, not 8): element stores inside the row only
+      for (int c = 0; c < 8 && p0 + c < ldd; ++c) dst[c] = out[c];
+    }
+  }
+}
+
 }  // namespace tc
 
 static int64_t tc_ld(int64_t P, int prec) {
@@ -186,6 +237,23 @@ static int64_t tc_ld(int64_t P, int prec) {
 size_t gram_tc_workspace(int W, int64_t P, int prec) {
   const size_t es = prec == 1 ? 2 : 4;
   return (size_t)2 * W * tc_ld(P, prec) * es + 1024;
+}
+
+// centred copy of O in the Gram operand type (ldd: multiple of 8 elements, 16-byte rows)
+template <typename TD>
+static int center_cvt(const void* O, int o_dtype, int W, int M, int64_t P, int64_t ldd,
+                      const double* mu, TD* d, cudaStream_t st) {
+  const dim3 g((unsigned)(((ldd + 7) / 8 + 255) / 256),
+               (unsigned)((M + tc::CVT_ROWS - 1) / tc::CVT_ROWS));
+  const bool vec = (P % 4) == 0 && (reinterpret_cast<uintptr_t>(O) & 15) == 0;
+  if (o_dtype == 0)
+    tc::k_center_cvt8<double, TD, false><<<g, 256, 0, st>>>((const double*)O, W, M, P, ldd, mu, d);
+  else if (vec)
+    tc::k_center_cvt8<float, TD, true><<<g, 256, 0, st>>>((const float*)O, W, M, P, ldd, mu, d);
+  else
+    tc::k_center_cvt8<float, TD, false><<<g, 256, 0, st>>>((const float*)O, W, M, P, ldd, mu, d);
+  NQS_CHECK_LAUNCH("k_center_cvt8");
+  return NQS_OK;
 }
 
 // Encode the tensor map and launch the Gram on an operand already in D (rows M, ld ldd).
@@ -239,26 +307,18 @@ int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int 
   (void)nsm;
   const int64_t ldd = tc_ld(P, prec);
   const int M = 2 * W;
-  const dim3 g((unsigned)((ldd + 255) / 256), (unsigned)M);
   void* D;
   if (prec == 1) {
     __nv_bfloat16* d = ws.take<__nv_bfloat16>((size_t)M * ldd);
     if (!d) return NQS_ERR_WORKSPACE;
-    if (o_dtype == 0)
-      tc::k_center_cvt<double, __nv_bfloat16><<<g, 256, 0, st>>>((const double*)O, W, P, ldd, mu, d);
-    else
-      tc::k_center_cvt<float, __nv_bfloat16><<<g, 256, 0, st>>>((const float*)O, W, P, ldd, mu, d);
+    NQS_TRY(center_cvt(O, o_dtype, W, M, P, ldd, mu, d, st));
     D = d;
   } else {
     float* d = ws.take<float>((size_t)M * ldd);
     if (!d) return NQS_ERR_WORKSPACE;
-    if (o_dtype == 0)
-      tc::k_center_cvt<double, float><<<g, 256, 0, st>>>((const double*)O, W, P, ldd, mu, d);
-    else
-      tc::k_center_cvt<float, float><<<g, 256, 0, st>>>((const float*)O, W, P, ldd, mu, d);
+    NQS_TRY(center_cvt(O, o_dtype, W, M, P, ldd, mu, d, st));
     D = d;
   }
-  NQS_CHECK_LAUNCH("k_center_cvt");
   return gram_tc_launch(D, prec, M, P, ldd, T, M, err, st);
 }
 

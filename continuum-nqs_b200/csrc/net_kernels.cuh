@@ -1112,7 +1112,45 @@ __device__ __noinline__ static void det_factor(cplx* Wk, cplx* inv, int N, int* 
 // Pair Jastrow u(r), u'(r), u''(r) (psiformer.py:168-186).
 __device__ __forceinline__ void jastrow_u(const ModelConst& mc, const HeadParams& hp, double r,
                                           bool same, double* u, double* u1, double* u2) {
-  if (mc.jastrow_kind == 0) {
+  if (mc.jastrow_kind == 0 && mc.knots_uniform) {
+    // centres mu_k = k w, width w: with t = r / w, g_k = exp(-(t - k)^2) satisfies
+    //   g_{k+1} = g_k exp(2 (t - k) - 1),   g_{k-1} = g_k exp(-2 (t - k) - 1),
+    // and each factor changes by exp(-2) per step; started at the knot nearest t (g = O(1)),
+    // so tails underflow harmlessly. 3 exponentials per pair instead of n_knots.
+    const double* c = same ? hp.jas_same : hp.jas_opp;
+    const double iw = 1.0 / mc.wdt;
+    const double t = r * iw;
+    const int nk = mc.n_knots;
+    const int k0 = min(max((int)rint(t), 0), nk - 1);
+    const double e2 = 0.1353352832366127;  // exp(-2)
+    double a0 = 0, a1 = 0, a2 = 0;
+    auto acc = [&](int k, double g) {
+      const double z = t - (double)k;
+      const double ce = c[k] * g;
+      a0 += ce;
+      a1 += ce * (-2.0 * z * iw);
+      a2 += ce * (4.0 * z * z - 2.0) * iw * iw;
+    };
+    const double z0 = t - (double)k0;
+    const double g0 = exp(-(z0 * z0));
+    acc(k0, g0);
+    double g = g0, q = exp(2.0 * z0 - 1.0);  // upward factor
+    for (int k = k0 + 1; k < nk; ++k) {
+      g *= q;
+      q *= e2;
+      acc(k, g);
+    }
+    g = g0;
+    q = exp(-2.0 * z0 - 1.0);  // downward factor
+    for (int k = k0 - 1; k >= 0; --k) {
+      g *= q;
+      q *= e2;
+      acc(k, g);
+    }
+    *u = a0;
+    *u1 = a1;
+    *u2 = a2;
+  } else if (mc.jastrow_kind == 0) {
     const double* c = same ? hp.jas_same : hp.jas_opp;
     double a0 = 0, a1 = 0, a2 = 0;
     const double iw = 1.0 / mc.wdt;

@@ -146,6 +146,7 @@ __device__ __forceinline__ int job_spin(const JobBatch& jb, const JobInfo& ji, i
 struct ModelConst {
   int N, d, depth, H, ff, nf, K, nG;
   int learnable_env, use_jastrow, jastrow_kind, n_knots;
+  int knots_uniform;  // rbf centres k * wdt (k = 0..n_knots-1): the Gaussians follow a recurrence
   double cusp;
   double A[4], Ainv[4];
   double rcut, wdt;

@@ -374,6 +374,9 @@ int nqs_model_create(const NqsModelDesc* d, NqsModel** out) {
   std::vector<double> kn(nk, 0.0);
   if (nk > 1 || (d->use_jastrow && d->jastrow_kind == 0 && d->knots_host))
     for (size_t i = 0; i < nk; ++i) kn[i] = d->knots_host[i];
+  mc.knots_uniform = nk > 1;
+  for (size_t i = 0; i < nk && mc.knots_uniform; ++i)
+    if (std::fabs(kn[i] - (double)i * mc.wdt) > 1e-12 * mc.rcut) mc.knots_uniform = 0;
   ce = cudaMemcpy(hm.d_knots, kn.data(), nk * sizeof(double), cudaMemcpyHostToDevice);
   if (ce != cudaSuccess) {
     nqs_model_destroy(m);
