@@ -222,6 +222,8 @@ int g_gemm_n = 0;
 double g_gemm_bytes = 0.0;
 }  // namespace
 
+bool profiling_enabled() { return g_gemm_prof; }
+
 bool rowgemm_tc_ok(int K, int ldx, int Nout) {
   return K % tc::RG_KB == 0 && K <= 128 && ldx % 4 == 0 && Nout >= 1 && Nout <= 256;
 }

@@ -104,6 +104,13 @@ bool rowgemm_tc_ok(int K, int ldx, int Nout);
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
                cudaStream_t st, int act = 0);  // act 1: tanh-GELU on the output (C == 1 only)
+// one whole transformer block of single-channel rows in one launch (block_tc.cu); *done is false
+// when the shape or the operand alignment is not covered and the caller runs the unfused block
+bool block_value_tc_ok(int N, int d, int H, int ff);
+int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, int b,
+                   const BlockW<float>& bw, cudaStream_t st, bool* done);
+extern bool g_block_fusion;
+bool profiling_enabled();  // nqs_profile_gemm(1) is in force
 size_t tc_weights_bytes(const NqsModelDesc& d);
 int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,
                      cudaStream_t st);

@@ -73,10 +73,33 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
     }
     const int rows = (int)(cb.n_jobs * rpj);
     const int ntok = cb.n_jobs * N;
-    k_embed<T><<<(ntok + 7) / 8, 256, 0, st>>>(cb, mc, w.emb_w, w.emb_b, X);
-    NQS_CHECK_LAUNCH("k_embed");
+    if constexpr (sizeof(T) == 4) {
+      if (C == 1 && (mc.nf == 4 || mc.nf == 8) && d % 4 == 0) {
+        const size_t smem = sizeof(float) * ((size_t)(4 * mc.nf + 3) * d);
+        if (mc.nf == 8)
+          k_embed_value<8><<<(ntok + 127) / 128, 128, smem, st>>>(cb, mc, w.emb_w, w.emb_b, X);
+        else
+          k_embed_value<4><<<(ntok + 127) / 128, 128, smem, st>>>(cb, mc, w.emb_w, w.emb_b, X);
+        NQS_CHECK_LAUNCH("k_embed_value");
+      } else {
+        k_embed<T><<<(ntok + 7) / 8, 256, 0, st>>>(cb, mc, w.emb_w, w.emb_b, X);
+        NQS_CHECK_LAUNCH("k_embed");
+      }
+    } else {
+      k_embed<T><<<(ntok + 7) / 8, 256, 0, st>>>(cb, mc, w.emb_w, w.emb_b, X);
+      NQS_CHECK_LAUNCH("k_embed");
+    }
+    // single-channel rows of the float32 path: each block is one fused launch (block_tc.cu)
+    const bool fused = tcn && C == 1 && g_block_fusion && block_value_tc_ok(N, d, mc.H, mc.ff);
     for (int b = 0; b < mc.depth; ++b) {
       const BlockW<T>& bw = w.blk[b];
+      if constexpr (sizeof(T) == 4) {
+        if (fused) {
+          bool done = false;
+          NQS_TRY(block_value_tc((float*)X, cb.n_jobs, N, d, mc.H, w.tc, b, bw, st, &done));
+          if (done) continue;
+        }
+      }
       NQS_TRY(launch_layernorm<T>(ntok, C, cb.n_tan, cb.has_lap, d, X, bw.ln0_s, bw.ln0_b, Hb,
                                   st));
       GemmArgs<T> g{};

@@ -96,6 +96,62 @@ __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
   }
 }
 
+// Value-only batches of the float32 path: one thread per token row. The embedding matrix and
+// bias are staged in shared memory (every thread of a warp reads the same entry: broadcast), the
+// 4 NF features live in registers, and each row leaves as float4 stores. Features and sums are
+// the same operations in the same order as the value branch of k_embed (angle reduced to
+// [-pi, pi] in float64, sincosf, float sums over k, then the spin row and the bias).
+template <int NF>
+__global__ void __launch_bounds__(128) k_embed_value(JobBatch jb, ModelConst mc,
+                                                     const float* __restrict__ Wemb,
+                                                     const float* __restrict__ bemb,
+                                                     float* __restrict__ X) {
+  constexpr int F = 4 * NF;
+  extern __shared__ __align__(16) float sW[];  // (F + 2) rows of d, then the d biases
+  const int d = mc.d;
+  for (int i = threadIdx.x; i < (F + 2) * d; i += blockDim.x) sW[i] = Wemb[i];
+  for (int i = threadIdx.x; i < d; i += blockDim.x) sW[(F + 2) * d + i] = bemb[i];
+  __syncthreads();
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= jb.n_jobs * jb.N) return;
+  const int j = gt / jb.N, tok = gt - j * jb.N;
+  const JobInfo ji = job_info(jb, j);
+  const double* r = jb.R + ((size_t)ji.walker * jb.N + tok) * 2;
+  const double r0 = r[0], r1 = r[1];
+  const int s = job_spin(jb, ji, tok);
+  float sv[F];
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    const double sa = r0 * mc.Ainv[al * 2 + 0] + r1 * mc.Ainv[al * 2 + 1];
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      const double ang = ((2.0 * kPi) * sa) * (double)m;
+      const double red = ang - (2.0 * kPi) * rint(ang * (0.5 / kPi));
+      sincosf((float)red, &sv[al * 2 * NF + m - 1], &sv[al * 2 * NF + NF + m - 1]);
+    }
+  }
+  float* xrow = X + ((size_t)j * jb.N + tok) * d;
+  const float4* W4 = reinterpret_cast<const float4*>(sW);
+  const int d4 = d / 4;
+  for (int n4 = 0; n4 < d4; ++n4) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < F; ++k) {
+      const float4 w = W4[k * d4 + n4];
+      acc.x = fmaf(sv[k], w.x, acc.x);
+      acc.y = fmaf(sv[k], w.y, acc.y);
+      acc.z = fmaf(sv[k], w.z, acc.z);
+      acc.w = fmaf(sv[k], w.w, acc.w);
+    }
+    const float4 ws = W4[(F + s) * d4 + n4], b = W4[(F + 2) * d4 + n4];
+    acc.x = (acc.x + ws.x) + b.x;
+    acc.y = (acc.y + ws.y) + b.y;
+    acc.z = (acc.z + ws.z) + b.z;
+    acc.w = (acc.w + ws.w) + b.w;
+    reinterpret_cast<float4*>(xrow)[n4] = acc;
+  }
+}
+
 // ============================================================================================
 // LayerNorm with tangent and Laplacian channels (flax LayerNorm: eps 1e-6, scale, bias)
 //   u = x - mean(x), v = mean(u^2), rho = (v+eps)^-1/2, y = u rho g + b
@@ -539,16 +595,17 @@ __device__ __forceinline__ void stg_row(T* __restrict__ p, const T* r) {
 
 constexpr int kAttnTok = 16;  // token slots of k_attention_rt
 
-template <typename T, int HD>
+template <typename T, int HD, bool VAL = false>
 __host__ __device__ constexpr size_t attention_rt_warp_bytes() {
-  return sizeof(T) * 8 * kAttnTok * HD;  // resident K, V + two buffers of Q, K, V
+  // resident K, V + two buffers of Q, K, V; value-only batches: K, V, Q
+  return sizeof(T) * (VAL ? 3 : 8) * kAttnTok * HD;
 }
 
-template <typename T, int HD, bool LAP>
+template <typename T, int HD, bool LAP, bool VAL = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(int n_jobs, int N, int C, int n_tan,
                                                          int d, int H, const T* __restrict__ QKV,
                                                          T* __restrict__ OUT) {
-  constexpr bool has_lap = LAP;
+  constexpr bool has_lap = LAP;  // VAL: single-channel batch (C == 1)
   constexpr int NT = kAttnTok, HE = HD / 2, V = 16 / sizeof(T), CH = HD / V;  // 16-B chunks/row
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int pair = blockIdx.x * nwarp + wib;
@@ -556,14 +613,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
   const int job = pair / H, h = pair - job * H;
   const int i = lane >> 1, hh = lane & 1;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* Kv = reinterpret_cast<T*>(smraw + (size_t)wib * attention_rt_warp_bytes<T, HD>());
+  T* Kv = reinterpret_cast<T*>(smraw + (size_t)wib * attention_rt_warp_bytes<T, HD, VAL>());
   T* Vv = Kv + NT * HD;
   T* buf = Vv + NT * HD;  // buf + b * 3 * NT * HD: Q, K, V tiles of one channel
   const int ld = 3 * d;
   const T sc = T(1) / sqrt(T(HD));
   // rows >= N are never copied: zero them once (zero probabilities times zero values)
   if (N < NT) {
-    for (int idx = lane; idx < 8 * (NT - N) * HD; idx += 32) {
+    for (int idx = lane; idx < (VAL ? 3 : 8) * (NT - N) * HD; idx += 32) {
       const int tile = idx / ((NT - N) * HD), r = idx - tile * (NT - N) * HD;
       Kv[tile * NT * HD + N * HD + r] = T(0);
     }
@@ -587,8 +644,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
   const bool live = i < N;
   // ---- value channel ----
   issue(0, 0);
-  issue(1, 1);
-  cp_async_wait<1>();
+  if (VAL) {
+    cp_async_wait<0>();
+  } else {
+    issue(1, 1);
+    cp_async_wait<1>();
+  }
   __syncwarp();
   T q[HD], a[8], ao[8];
   {
@@ -635,6 +696,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_attention_rt(in
     }
     if (live) stg_row<T, HE>(out_row(0), o);
   }
+  if (VAL) return;
   __syncwarp();
   issue(2, 0);
   T Pqk[8], Psq[8], Pav[HE];
@@ -789,18 +851,27 @@ inline size_t attention_smem(int N, int hd) {
 template <typename T, int HD>
 inline int launch_attention_rt(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
                                const T* QKV, T* OUT, cudaStream_t st) {
-  const size_t wb = attention_rt_warp_bytes<T, HD>();
-  int wpc = 8;
-  while (wpc > 1 && wpc * wb > 96 * 1024) wpc /= 2;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_attention_rt<T, HD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          96 * 1024);
     cudaFuncSetAttribute(k_attention_rt<T, HD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          96 * 1024);
+    cudaFuncSetAttribute(k_attention_rt<T, HD, false, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     attr = true;
   }
   const long long pairs = (long long)n_jobs * H;
+  if (C == 1) {  // value-only batch: three tiles per warp, eight warps per CTA
+    const size_t wbv = attention_rt_warp_bytes<T, HD, true>();
+    k_attention_rt<T, HD, false, true><<<(unsigned)((pairs + 7) / 8), 256, 8 * wbv, st>>>(
+        n_jobs, N, C, n_tan, d, H, QKV, OUT);
+    NQS_CHECK_LAUNCH("k_attention_rt");
+    return NQS_OK;
+  }
+  const size_t wb = attention_rt_warp_bytes<T, HD>();
+  int wpc = 8;
+  while (wpc > 1 && wpc * wb > 96 * 1024) wpc /= 2;
   const unsigned grid = (unsigned)((pairs + wpc - 1) / wpc);
   if (has_lap)
     k_attention_rt<T, HD, true><<<grid, 32 * wpc, wpc * wb, st>>>(n_jobs, N, C, n_tan, d, H, QKV,

@@ -184,6 +184,8 @@ _SIGS.update({
                          c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),
     "nqs_profile_gemm": ([c_int], c_int),
+    "nqs_set_block_fusion": ([c_int], c_int),
+    "nqs_profile_block_read": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "nqs_profile_gemm_read": ([c_void_p, c_void_p, c_void_p], c_int),
     "nqs_profile_events": ([c_void_p, c_void_p], c_int),
     "nqs_gram": ([c_void_p, c_int, c_int, c_int64, c_int64, c_void_p, c_int64, c_void_p, c_void_p],

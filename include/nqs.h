@@ -108,6 +108,17 @@ int nqs_profile_events(void* start_event, void* stop_event);
  * (ms), bytes and launch count since the last read, and clears them. */
 int nqs_profile_gemm(int enable);
 int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches);
+/* Implementation selection (no reference counterpart; process-wide, default on): with fusion on,
+ * each transformer block of a single-channel (value) pass of the float32 path runs as one fused
+ * tensor-core launch when N <= 16, embed_dim is 32 or 64 and ff_mult is 2; off, the same block
+ * runs as separate LayerNorm / GEMM / attention / GEMM launches. Both compute the same function
+ * with the same TF32 products; the switch exists so that the two can be compared. */
+int nqs_set_block_fusion(int enable);
+/* Per-launch timing of the fused value-pass blocks (profiling aid, no reference counterpart),
+ * recorded while nqs_profile_gemm(1) is in force: summed kernel time (ms), algorithmic HBM bytes
+ * (rows in and out, weights once), tensor-core and attention flops, and the launch count since
+ * the last read, which clears them. */
+int nqs_profile_block_read(double* ms, double* bytes, double* flops, long long* launches);
 
 /* Model handle: validates the descriptor and uploads the immutable constants (Gs, W, knots).
  * Replaces the flax module construction in src/nqs/psiformer.py:100-116. */
