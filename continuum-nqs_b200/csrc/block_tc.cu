@@ -102,12 +102,27 @@ __device__ __forceinline__ bool group_bar_or(int g, bool pred) {
   return res != 0;
 }
 // read-only parameter loads kept inside the tile loop (not hoisted into registers across tiles)
+// and kept in L1 (evict_last), where they stay hot for every tile of the CTA
 __device__ __forceinline__ float4 ldp4(const float* p) {
   float4 v;
-  asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+  asm volatile("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                : "l"(p));
   return v;
+}
+// activation rows are read once: no L1 allocation, so they do not evict the parameters
+__device__ __forceinline__ float4 ld_stream4(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
+// K / V staging rows: 16-byte chunk c of row r sits at chunk c ^ kv_sw(r), so that the 8 rows
+// of one store phase hit 8 different bank groups
+template <int HD>
+__device__ __forceinline__ int kv_sw(int r) {
+  return HD == 16 ? ((r >> 1) & 3) : ((r >> 2) & 1);
 }
 // tanh-GELU as x sigmoid(2w) = x / (1 + e^{-2w}), w = sqrt(2/pi) (x + 0.044715 x^3): the same
 // function as x (1 + tanh w) / 2 (jax.nn.gelu, approximate=True), with one exponential and one
@@ -269,7 +284,7 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
       for (int it = 0; it < D / 4; ++it) {
         const int f = it * 32 + lane, rr = f / (D / 4), c = f - rr * (D / 4);
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (rr < nw) v = src[f];
+        if (rr < nw) v = ld_stream4(src + f);
         *st_chunk<D>(wstl, rr, c) = v;
       }
       __syncwarp();
@@ -315,9 +330,10 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
       }
 #pragma unroll
       for (int c = 0; c < HD / 4; ++c) {
-        reinterpret_cast<float4*>(sKl + r * HD)[c] =
+        const int cs = c ^ kv_sw<HD>(r);
+        reinterpret_cast<float4*>(sKl + r * HD)[cs] =
             make_float4(k[4 * c], k[4 * c + 1], k[4 * c + 2], k[4 * c + 3]);
-        reinterpret_cast<float4*>(sVl + r * HD)[c] =
+        reinterpret_cast<float4*>(sVl + r * HD)[cs] =
             make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
       }
       group_bar(g);
@@ -332,10 +348,11 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
           s[j] = -INFINITY;
           if (j < a.N) {
             const float4* kr = reinterpret_cast<const float4*>(sKl + (wb + j) * HD);
+            const int sj = kv_sw<HD>(wb + j);
             float acc = 0.f;
 #pragma unroll
             for (int c = 0; c < HD / 4; ++c) {
-              const float4 kk = kr[c];
+              const float4 kk = kr[c ^ sj];
               acc = fmaf(q[4 * c], kk.x, acc);
               acc = fmaf(q[4 * c + 1], kk.y, acc);
               acc = fmaf(q[4 * c + 2], kk.z, acc);
@@ -357,9 +374,10 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
           if (j < a.N) {
             const float p = s[j] * inv;
             const float4* vr = reinterpret_cast<const float4*>(sVl + (wb + j) * HD);
+            const int sj = kv_sw<HD>(wb + j);
 #pragma unroll
             for (int c = 0; c < HD / 4; ++c) {
-              const float4 vv = vr[c];
+              const float4 vv = vr[c ^ sj];
               o[4 * c] = fmaf(p, vv.x, o[4 * c]);
               o[4 * c + 1] = fmaf(p, vv.y, o[4 * c + 1]);
               o[4 * c + 2] = fmaf(p, vv.z, o[4 * c + 2]);

@@ -973,8 +973,11 @@ __global__ void k_gemv_t(const TO* __restrict__ O, int M, int Mh, int64_t K,
 }
 
 // Split form of k_gemv_t for the large solves: each thread owns 4 consecutive columns and one
-// slice of rows (blockIdx.y), writes the double-double partial (s, c) of its slice to
-// part[y][k][2]; k_gemv_t_reduce adds the slices. VEC: K % 4 == 0 (16-byte row starts).
+// slice of rows (blockIdx.y) and writes its slice's partial sum to part[y][k]; k_gemv_t_reduce
+// adds the slices in slice order. Float64 accumulation (the products of float32 O entries and
+// float64 weights, summed over at most 512 rows per slice, then over the slices): residuals to
+// float64 working accuracy, which is what the refinement against the exact operator needs to
+// reproduce a float64 solve. VEC: K % 4 == 0 (16-byte row starts).
 template <typename TO, bool VEC>
 __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, int M, int Mh,
                                                       int64_t K, const double* __restrict__ mu,
@@ -990,7 +993,7 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
     m0[c] = (mu && in) ? mu[k0 + c] : 0.0;
     m1[c] = (mu && in) ? mu[K + k0 + c] : 0.0;
   }
-  DD acc[4];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
   for (int m = m_lo; m < m_hi; ++m) {
     const TO* row = O + (size_t)m * K + k0;
@@ -1011,15 +1014,11 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
     const double xm = x[m];
     const bool lo_half = m < Mh;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[c].add_prod(o[c] - (lo_half ? m0[c] : m1[c]), xm);
+    for (int c = 0; c < 4; ++c) acc[c] = fma(o[c] - (lo_half ? m0[c] : m1[c]), xm, acc[c]);
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c)
-    if (k0 + c < K) {
-      double* pp = part + ((size_t)blockIdx.y * K + k0 + c) * 2;
-      pp[0] = acc[c].s;
-      pp[1] = acc[c].c;
-    }
+    if (k0 + c < K) part[(size_t)blockIdx.y * K + k0 + c] = acc[c];
 }
 
 template <typename TO>
@@ -1028,16 +1027,11 @@ __global__ void k_gemv_t_reduce(const double* __restrict__ part, int nsplit, int
                                 double* __restrict__ theta, double lr) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
-  DD acc;
-  for (int z = 0; z < nsplit; ++z) {
-    const double* pp = part + ((size_t)z * K + k) * 2;
-    acc.add(pp[0]);
-    acc.c += pp[1];
-  }
-  const double hi = acc.s + acc.c;
-  if (out) out[k] = hi;
-  if (out_lo) out_lo[k] = acc.c - (hi - acc.s);
-  if (theta) theta[k] -= lr * hi;
+  double acc = 0.0;
+  for (int z = 0; z < nsplit; ++z) acc += part[(size_t)z * K + k];
+  if (out) out[k] = acc;
+  if (out_lo) out_lo[k] = 0.0;
+  if (theta) theta[k] -= lr * acc;
 }
 
 // out = (O - mu)^T x through the split kernel when the scratch holds the slices, else k_gemv_t
@@ -1046,7 +1040,7 @@ static int gemv_t(const TO* O, int M, int Mh, int64_t K, const double* mu, const
                   double* out, double* out_lo, double* theta, double lr, double* part,
                   size_t part_elems, cudaStream_t st) {
   int nsplit = std::max(1, std::min(16, M / 512));
-  while (nsplit > 1 && (size_t)nsplit * K * 2 > part_elems) --nsplit;
+  while (nsplit > 1 && (size_t)nsplit * K > part_elems) --nsplit;
   if (nsplit <= 1 || !part) {
     k_gemv_t<TO><<<(unsigned)((K + 255) / 256), 256, 0, st>>>(O, M, Mh, K, mu, x, out, out_lo,
                                                                theta, lr);
@@ -1066,31 +1060,32 @@ static int gemv_t(const TO* O, int M, int Mh, int64_t K, const double* mu, const
   return NQS_OK;
 }
 
-// Residual r = b - lam x - (O - mu)(v + v_lo) for RB rows per CTA (v, v_lo and mu read once per
-// CTA for all its rows), double-double accumulation; 4 consecutive columns per thread when VEC.
+// Residual r = b - lam x - (O - mu) v for RB rows per CTA (v and mu read once per CTA for all
+// its rows), float64 accumulation; 4 consecutive columns per thread when VEC.
 template <typename TO, int RB, bool VEC>
 __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
     const TO* __restrict__ O, int M, int Mh, int64_t K, const double* __restrict__ mu,
-    const double* __restrict__ v, const double* __restrict__ v_lo, const double* __restrict__ b,
-    double lam0, const double* __restrict__ lam_extra, const double* __restrict__ x,
-    double* __restrict__ r) {
+    const double* __restrict__ v, const double* __restrict__ b, double lam0,
+    const double* __restrict__ lam_extra, const double* __restrict__ x, double* __restrict__ r) {
   const double lam = lam0 + (lam_extra ? *lam_extra : 0.0);
   const int m0 = blockIdx.x * RB;
   const int nr = min(RB, M - m0);
-  DD acc[RB];
+  double acc[RB];
   bool hi_half[RB];
 #pragma unroll
-  for (int i = 0; i < RB; ++i) hi_half[i] = m0 + i >= Mh;
+  for (int i = 0; i < RB; ++i) {
+    acc[i] = 0.0;
+    hi_half[i] = m0 + i >= Mh;
+  }
   // which column-mean halves this CTA's rows use (uniform per CTA)
   const bool need0 = mu && m0 < Mh, need1 = mu && m0 + nr - 1 >= Mh;
   const int64_t step = (int64_t)blockDim.x * 4;
   for (int64_t k = (int64_t)threadIdx.x * 4; k < K; k += step) {
-    double vv[4], vl[4], u0[4], u1[4];
+    double vv[4], u0[4], u1[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const bool in = VEC || k + c < K;
       vv[c] = in ? v[k + c] : 0.0;
-      vl[c] = in ? v_lo[k + c] : 0.0;
       u0[c] = (need0 && in) ? mu[k + c] : 0.0;
       u1[c] = (need1 && in) ? mu[K + k + c] : 0.0;
     }
@@ -1113,57 +1108,38 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
         for (int c = 0; c < 4; ++c) o[c] = k + c < K ? (double)row[c] : 0.0;
       }
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const double oc = o[c] - (hi_half[i] ? u1[c] : u0[c]);
-        acc[i].add_prod(oc, vv[c]);
-        acc[i].c = fma(oc, vl[c], acc[i].c);  // the low word's product, into the compensation
-      }
+      for (int c = 0; c < 4; ++c) acc[i] = fma(o[c] - (hi_half[i] ? u1[c] : u0[c]), vv[c], acc[i]);
     }
   }
-  __shared__ double red_s[RB][8], red_c[RB][8];
+  __shared__ double red[RB][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int i = 0; i < RB; ++i) {
+    double a = acc[i];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double os = __shfl_xor_sync(0xffffffffu, acc[i].s, off);
-      const double oc = __shfl_xor_sync(0xffffffffu, acc[i].c, off);
-      acc[i].add(os);
-      acc[i].c += oc;
-    }
-    if (lane == 0) {
-      red_s[i][w] = acc[i].s;
-      red_c[i][w] = acc[i].c;
-    }
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if (lane == 0) red[i][w] = a;
   }
   __syncthreads();
   if (threadIdx.x < nr) {
     const int i = threadIdx.x, m = m0 + i;
-    DD t;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
-      t.add(red_s[i][q]);
-      t.c += red_c[i][q];
-    }
-    DD qd;  // b - lam x - t
-    qd.add(b[m]);
-    qd.add_prod(-lam, x[m]);
-    qd.add(-t.s);
-    qd.c -= t.c;
-    r[m] = qd.s + qd.c;
+    double t = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[i][q];
+    r[m] = (b[m] - lam * x[m]) - t;
   }
 }
 
 template <typename TO>
 static int gemv_n_resid(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* v,
-                        const double* v_lo, const double* b, double lam0, const double* lam_extra,
-                        const double* x, double* r, cudaStream_t st) {
-  constexpr int RB = 8;
+                        const double* b, double lam0, const double* lam_extra, const double* x,
+                        double* r, cudaStream_t st) {
+  constexpr int RB = 16;
   const unsigned g = (unsigned)((M + RB - 1) / RB);
   if (K % 4 == 0)
-    k_gemv_n_resid_rows<TO, RB, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, v_lo, b, lam0,
-                                                         lam_extra, x, r);
+    k_gemv_n_resid_rows<TO, RB, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, b, lam0, lam_extra,
+                                                         x, r);
   else
-    k_gemv_n_resid_rows<TO, RB, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, v_lo, b, lam0,
+    k_gemv_n_resid_rows<TO, RB, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, b, lam0,
                                                           lam_extra, x, r);
   NQS_CHECK_LAUNCH("k_gemv_n_resid_rows");
   return NQS_OK;
@@ -1196,7 +1172,7 @@ __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__
 
 // Solve (A A^T + lam I) y = b given the Cholesky factor L of (A A^T + lam I), with n_refine
 // steps of iterative refinement against the exact operator y -> A (A^T y) + lam y, where
-// A = O - mu (centred on the fly). On return tmpK holds A^T y.
+// A = O - mu (centred on the fly). On return tmpK holds A^T y (tmpK_lo is spare scratch).
 template <typename TO>
 static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
                          const double* mu, double lam, const double* lam_extra, const double* b,
@@ -1209,8 +1185,8 @@ static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
   NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 0, st));
   NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 1, st));
   for (int it = 0; it < n_refine; ++it) {
-    NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, tmpK, tmpK_lo, nullptr, 0.0, part, part_elems, st));
-    NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, tmpK_lo, b, lam, lam_extra, y, r, st));
+    NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, tmpK, nullptr, nullptr, 0.0, part, part_elems, st));
+    NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, b, lam, lam_extra, y, r, st));
     NQS_TRY(trsv_grid(L, M, M, dinv, r, xb, 0, st));
     NQS_TRY(trsv_grid(L, M, M, dinv, r, xb, 1, st));
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
