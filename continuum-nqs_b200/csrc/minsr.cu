@@ -833,6 +833,130 @@ __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L,
   }
 }
 
+// Triangular solves as a wavefront over 64-row blocks (one CTA per block row, all CTAs resident
+// through a cooperative launch), without grid barriers:
+//   forward    CTA s:  x_s = D_s (v_s - sum_{t<s} L_st x_t)        (t ascending)
+//   transposed CTA s:  x_s = D_s^T (v_s - sum_{t>s} L_ts^T x_t)    (t descending)
+// CTA s applies each x_t as soon as CTA t has published it (flag[t], release / acquire at GPU
+// scope), with its operand panel L_st already in registers, so the chain costs one flag hop and
+// two 64 x 64 mat-vecs per block. Every wait is bounded: a CTA that gives up records the timeout
+// in flag[kTrsvErrSlot], publishes NaN for its block (its dependants then finish at once) and
+// returns. v is overwritten with x. Sums run in a fixed order (deterministic).
+constexpr int kTrsvErrSlot = 255;  // flags[0..254]: blocks; flags[255]: timeout record
+constexpr uint32_t kTrsvWaitLimit = 1u << 21;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L, int64_t ldl,
+                                                    int n, const double* __restrict__ dinv,
+                                                    double* v, int* flags, int transposed) {
+  const int nblk = (n + CB - 1) / CB;
+  const int s = blockIdx.x;
+  const int k0 = s * CB, bs = min(CB, n - k0);
+  const int tid = threadIdx.x;
+  __shared__ double red[4][CB];
+  __shared__ double rhs[CB];
+  // the wait's verdict, double-buffered by iteration parity: thread 0 writes iteration it+1's
+  // slot only after every thread has passed iteration it+1's barrier, i.e. has read slot it
+  __shared__ int give_up_buf[2];
+  bool give_up = false;
+  // forward: output row r = tid / 4, columns q*16 .. q*16+15 (q = tid % 4) of each 64-block;
+  // transposed: output m = tid % 64 (a column of L), rows q*16 .. q*16+15 (q = tid / 64)
+  const int r = transposed ? (tid & 63) : (tid >> 2);
+  const int q = transposed ? (tid >> 6) : (tid & 3);
+  double dreg[16];
+  {
+    const double* D = dinv + (size_t)s * CB * CB;
+#pragma unroll
+    for (int c = 0; c < 16; ++c)
+      dreg[c] = transposed ? D[(q * 16 + c) * CB + r] : D[r * CB + q * 16 + c];
+  }
+  double acc = 0.0;
+  const int nt = transposed ? nblk - 1 - s : s;  // blocks this row depends on
+  __syncthreads();
+  for (int it = 0; it < nt; ++it) {
+    const int t = transposed ? nblk - 1 - it : it;
+    const int kt = t * CB, bt = min(CB, n - kt);
+    double lreg[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int jj = q * 16 + c;
+      lreg[c] = 0.0;
+      if (!transposed && r < bs && jj < bt) lreg[c] = L[(size_t)(k0 + r) * ldl + kt + jj];
+      if (transposed && r < bs && jj < bt) lreg[c] = L[(size_t)(kt + jj) * ldl + k0 + r];
+    }
+    if (tid == 0) {
+      int gu = 0;
+      uint32_t w = 0;
+      while (ld_acquire_gpu(flags + t) == 0) {
+        if (++w >= kTrsvWaitLimit || ld_acquire_gpu(flags + kTrsvErrSlot) != 0) {
+          gu = 1;
+          break;
+        }
+        if (w > 64) __nanosleep(64);
+      }
+      give_up_buf[it & 1] = gu;
+    }
+    __syncthreads();
+    give_up = give_up_buf[it & 1] != 0;
+    if (give_up) break;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int jj = q * 16 + c;
+      const double xj = jj < bt ? __ldcg(v + kt + jj) : 0.0;
+      acc = fma(lreg[c], xj, acc);
+    }
+  }
+  if (give_up) {
+    if (tid == 0) atomicExch(flags + kTrsvErrSlot, 1);
+    if (tid < bs) v[k0 + tid] = __longlong_as_double(0x7ff8000000000000ll);
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release_gpu(flags + s, 1);
+    }
+    return;
+  }
+  // rhs = v_s - (sum over the four column quarters)
+  if (!transposed) {
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (q == 0 && r < CB) rhs[r] = r < bs ? v[k0 + r] - acc : 0.0;
+  } else {
+    red[q][r] = acc;
+    __syncthreads();
+    if (tid < CB)
+      rhs[tid] = tid < bs ? v[k0 + tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]))
+                          : 0.0;
+  }
+  __syncthreads();
+  // x_s = D rhs (forward) or D^T rhs (transposed)
+  double xs = 0.0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) xs = fma(dreg[c], rhs[q * 16 + c], xs);
+  if (!transposed) {
+    xs += __shfl_xor_sync(0xffffffffu, xs, 1);
+    xs += __shfl_xor_sync(0xffffffffu, xs, 2);
+    if (q == 0 && r < bs) v[k0 + r] = xs;
+  } else {
+    red[q][r] = xs;
+    __syncthreads();
+    if (tid < bs) v[k0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    st_release_gpu(flags + s, 1);
+  }
+}
+
 static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, double* v,
                      double* xb, int transposed, cudaStream_t st) {
   static int grid = 0;
@@ -842,6 +966,29 @@ static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, do
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trsv_grid, 256, 0);
     grid = per >= 1 ? nsm : 1;  // one CTA per SM keeps the grid barrier cheap
+  }
+  // the wavefront form while its flags fit the 2 x 64 exchange buffer and every block row's CTA
+  // can be resident at once; the grid-barrier form otherwise
+  static int max_resident = 0;
+  if (!max_resident) {
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trsv_flags, 256, 0);
+    max_resident = std::max(1, nsm * per);
+  }
+  const int nblk = (n + CB - 1) / CB;
+  static_assert(sizeof(int) * (kTrsvErrSlot + 1) <= sizeof(double) * 2 * CB, "flag slots");
+  if (nblk <= kTrsvErrSlot && nblk <= max_resident) {
+    int* flags = reinterpret_cast<int*>(xb);
+    cudaMemsetAsync(flags, 0, sizeof(int) * (kTrsvErrSlot + 1), st);
+    void* fargs[] = {(void*)&L, (void*)&ldl, (void*)&n, (void*)&dinv,
+                     (void*)&v, (void*)&flags, (void*)&transposed};
+    const cudaError_t e =
+        cudaLaunchCooperativeKernel((const void*)k_trsv_flags, nblk, 256, fargs, 0, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_trsv_flags");
+    NQS_CHECK_LAUNCH("k_trsv_flags");
+    return NQS_OK;
   }
   void* args[] = {(void*)&L,  (void*)&ldl, (void*)&n, (void*)&dinv,
                   (void*)&v, (void*)&xb,  (void*)&transposed};
@@ -994,7 +1141,7 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
     m1[c] = (mu && in) ? mu[K + k0 + c] : 0.0;
   }
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
+#pragma unroll 8
   for (int m = m_lo; m < m_hi; ++m) {
     const TO* row = O + (size_t)m * K + k0;
     double o[4];
@@ -1063,7 +1210,7 @@ static int gemv_t(const TO* O, int M, int Mh, int64_t K, const double* mu, const
 // Residual r = b - lam x - (O - mu) v for RB rows per CTA (v and mu read once per CTA for all
 // its rows), float64 accumulation; 4 consecutive columns per thread when VEC.
 template <typename TO, int RB, bool VEC>
-__global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
+__global__ void __launch_bounds__(256, sizeof(TO) == 4 ? 2 : 1) k_gemv_n_resid_rows(
     const TO* __restrict__ O, int M, int Mh, int64_t K, const double* __restrict__ mu,
     const double* __restrict__ v, const double* __restrict__ b, double lam0,
     const double* __restrict__ lam_extra, const double* __restrict__ x, double* __restrict__ r) {
@@ -1089,27 +1236,31 @@ __global__ void __launch_bounds__(256) k_gemv_n_resid_rows(
       u0[c] = (need0 && in) ? mu[k + c] : 0.0;
       u1[c] = (need1 && in) ? mu[K + k + c] : 0.0;
     }
+    // all RB rows' loads are issued before any of them is used (rows past the end read row
+    // m0 again and are never reduced)
+    TO o[RB][4];
 #pragma unroll
     for (int i = 0; i < RB; ++i) {
-      if (i >= nr) break;
-      const TO* row = O + (size_t)(m0 + i) * K + k;
-      double o[4];
+      const TO* row = O + (size_t)(m0 + (i < nr ? i : 0)) * K + k;
       if (VEC) {
         if (sizeof(TO) == 4) {
           const float4 f = *reinterpret_cast<const float4*>(row);
-          o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+          o[i][0] = f.x; o[i][1] = f.y; o[i][2] = f.z; o[i][3] = f.w;
         } else {
           const double2 a = reinterpret_cast<const double2*>(row)[0];
           const double2 bb = reinterpret_cast<const double2*>(row)[1];
-          o[0] = a.x; o[1] = a.y; o[2] = bb.x; o[3] = bb.y;
+          o[i][0] = a.x; o[i][1] = a.y; o[i][2] = bb.x; o[i][3] = bb.y;
         }
       } else {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) o[c] = k + c < K ? (double)row[c] : 0.0;
+        for (int c = 0; c < 4; ++c) o[i][c] = k + c < K ? row[c] : TO(0);
       }
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[i] = fma(o[c] - (hi_half[i] ? u1[c] : u0[c]), vv[c], acc[i]);
     }
+#pragma unroll
+    for (int i = 0; i < RB; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        acc[i] = fma((double)o[i][c] - (hi_half[i] ? u1[c] : u0[c]), vv[c], acc[i]);
   }
   __shared__ double red[RB][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
