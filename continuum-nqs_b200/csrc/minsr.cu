@@ -266,17 +266,22 @@ __global__ void __launch_bounds__(256) k_dsyrk_cp(DTile a) {
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     const double* as = As + (size_t)(kc % DSTAGES) * 128 * DLD;
     const double* bs = Bs + (size_t)(kc % DSTAGES) * 128 * DLD;
+    // two k per step: one 16-byte shared load per row gives (k, k + 1) (rows start on 16 bytes:
+    // DLD * 8 = 144)
 #pragma unroll
-    for (int kk = 0; kk < DK; ++kk) {
-      double av[8], bv[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) av[i] = as[(ty + 16 * i) * DLD + kk];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) bv[j] = bs[(tx + 16 * j) * DLD + kk];
+    for (int kk = 0; kk < DK; kk += 2) {
+      double2 av[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
+        av[i] = *reinterpret_cast<const double2*>(as + (ty + 16 * i) * DLD + kk);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+      for (int j = 0; j < 8; ++j) {
+        const double2 bv = *reinterpret_cast<const double2*>(bs + (tx + 16 * j) * DLD + kk);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][j] = fma(av[i].x, bv.x, acc[i][j]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][j] = fma(av[i].y, bv.y, acc[i][j]);
+      }
     }
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -880,6 +885,8 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
   }
   double acc = 0.0;
   const int nt = transposed ? nblk - 1 - s : s;  // blocks this row depends on
+  // this block's right-hand side: written by no other CTA, read before the wait chain
+  const double vs = (tid < bs) ? v[k0 + tid] : 0.0;
   __syncthreads();
   for (int it = 0; it < nt; ++it) {
     const int t = transposed ? nblk - 1 - it : it;
@@ -928,13 +935,16 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
   if (!transposed) {
     acc += __shfl_xor_sync(0xffffffffu, acc, 1);
     acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-    if (q == 0 && r < CB) rhs[r] = r < bs ? v[k0 + r] - acc : 0.0;
+    if (q == 0) red[0][r] = acc;  // the row sums, handed to thread r below
+  }
+  __syncthreads();
+  if (!transposed) {
+    if (tid < CB) rhs[tid] = tid < bs ? vs - red[0][tid] : 0.0;
   } else {
     red[q][r] = acc;
     __syncthreads();
     if (tid < CB)
-      rhs[tid] = tid < bs ? v[k0 + tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]))
-                          : 0.0;
+      rhs[tid] = tid < bs ? vs - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
   }
   __syncthreads();
   // x_s = D rhs (forward) or D^T rhs (transposed)
