@@ -544,41 +544,53 @@ __global__ void k_store_diag(double* __restrict__ A, int64_t lda, int k0, int n,
   }
 }
 
-// Look-ahead update of the next 64-column block: C[r][c] -= sum_j P[r][j] P[c][j] for r in
-// [0, rest), c in [0, min(64, rest)), c <= r, with P the 64-wide panel (rows 0.. of P are the
-// "column" rows). One CTA per 64 rows, 4 x 4 outputs per thread.
+// Update of ncb consecutive 64-column blocks by a kw-wide panel (kw a multiple of 64):
+//   block y (columns c0 + 64 y of the caller's frame): C_y[r][c] -= sum_j P_y[r][j] P_y[c][j]
+//   for r in [0, rest - 64 y), c in [0, min(64, rest - 64 y)), c <= r,
+// with P_y = P + 64 y ldp (rows 0.. of P_y are the rows matching block y's columns) and
+// C_y = C + 64 y (ldc + 1). One CTA per (64 rows, block), 4 x 4 outputs per thread; the sum runs
+// over the panel's 64-column chunks in order.
 __global__ void __launch_bounds__(256) k_panel_update(const double* __restrict__ P, int64_t ldp,
                                                       int rest, double* __restrict__ C,
-                                                      int64_t ldc) {
+                                                      int64_t ldc, int kw) {
   extern __shared__ double pu_sm[];
   double(*Pr)[CB + 1] = reinterpret_cast<double(*)[CB + 1]>(pu_sm);
   double(*Pc)[CB + 1] = Pr + CB;
-  const int r0 = blockIdx.x * CB, nr = min(CB, rest - r0), nc = min(CB, rest);
-  for (int idx = threadIdx.x; idx < CB * CB; idx += blockDim.x) {
-    const int i = idx / CB, j = idx - i * CB;
-    Pr[i][j] = i < nr ? P[(size_t)(r0 + i) * ldp + j] : 0.0;
-    Pc[i][j] = i < nc ? P[(size_t)i * ldp + j] : 0.0;
-  }
-  __syncthreads();
+  const int y = blockIdx.y;
+  const int rest_y = rest - CB * y;
+  const int r0 = blockIdx.x * CB;
+  if (r0 >= rest_y) return;  // whole CTA
+  P += (size_t)CB * y * ldp;
+  C += (size_t)CB * y * (ldc + 1);
+  const int nr = min(CB, rest_y - r0), nc = min(CB, rest_y);
   const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
   double acc[4][4] = {};
-#pragma unroll 8
-  for (int k = 0; k < CB; ++k) {
-    double a4[4], b4[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      a4[u] = Pr[ty + 16 * u][k];
-      b4[u] = Pc[tx + 16 * u][k];
+  for (int kc = 0; kc < kw; kc += CB) {
+    if (kc) __syncthreads();  // the previous chunk is no longer read
+    for (int idx = threadIdx.x; idx < CB * CB; idx += blockDim.x) {
+      const int i = idx / CB, j = idx - i * CB;
+      Pr[i][j] = i < nr ? P[(size_t)(r0 + i) * ldp + kc + j] : 0.0;
+      Pc[i][j] = i < nc ? P[(size_t)i * ldp + kc + j] : 0.0;
     }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < CB; ++k) {
+      double a4[4], b4[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 4; ++u) {
+        a4[u] = Pr[ty + 16 * u][k];
+        b4[u] = Pc[tx + 16 * u][k];
+      }
 #pragma unroll
-      for (int v = 0; v < 4; ++v) acc[u][v] = fma(a4[u], b4[v], acc[u][v]);
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a4[u], b4[v], acc[u][v]);
+    }
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const int r = r0 + ty + 16 * u;
-    if (r >= rest) continue;
+    if (r >= rest_y) continue;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int c = tx + 16 * v;
@@ -587,10 +599,14 @@ __global__ void __launch_bounds__(256) k_panel_update(const double* __restrict__
   }
 }
 
-// Right-looking blocked Cholesky A = L L^T (lower triangle, in place), 64-column panels, with
-// one step of look-ahead: after step k's panel, the next 64 columns are updated first and the
-// next diagonal factor + panel solve run on a side stream while the rest of step k's trailing
-// update runs on the caller's stream (they touch disjoint columns).
+// Right-looking blocked Cholesky A = L L^T (lower triangle, in place), two-level: 64-column
+// panels inside 256-column outer blocks. A panel updates only the columns of its own outer block
+// (k_panel_update); the trailing matrix beyond an outer block is updated once, by all of its
+// panels together (dsyrk with K = 256), so the trailing matrix is read and written once per
+// outer block instead of once per panel. One step of look-ahead: after a panel, the next 64
+// columns are updated first (at an outer-block end, by the whole outer block) and the next
+// diagonal factor + panel solve run on a side stream while the rest of the step's updates run on
+// the caller's stream (they touch disjoint columns).
 // part: scratch of at least 64 x 64 doubles for the diagonal factor.
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
@@ -631,27 +647,42 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
     NQS_CHECK_LAUNCH("k_potrf_trsm");
     return NQS_OK;
   };
+  constexpr int NB = 4 * CB;  // outer block
+  // columns [c0, c0 + 64 ncb) updated by the panel of columns [p0, p0 + kw)
+  auto pupd = [&](int p0, int kw, int c0, int ncb) {
+    const int rest = n - c0;
+    k_panel_update<<<dim3((rest + CB - 1) / CB, ncb), 256, sizeof(double) * 2 * CB * (CB + 1),
+                     st>>>(A + (size_t)c0 * lda + p0, lda, rest, A + (size_t)c0 * lda + c0, lda,
+                           kw);
+    NQS_CHECK_LAUNCH("k_panel_update");
+  };
   NQS_TRY(potrf(0, -1, st));
   int last = 0;
   for (int k0 = 0; k0 + CB < n; k0 += CB) {
-    const int rest = n - k0 - CB;  // rows / columns after this panel
-    const double* P = A + (size_t)(k0 + CB) * lda + k0;
-    double* C = A + (size_t)(k0 + CB) * lda + k0 + CB;
-    // (a) next 64 columns of the trailing matrix
-    k_panel_update<<<(rest + CB - 1) / CB, 256, sizeof(double) * 2 * CB * (CB + 1), st>>>(
-        P, lda, rest, C, lda);
-    NQS_CHECK_LAUNCH("k_panel_update");
+    const int ob = (k0 / NB) * NB, oe = std::min(n, ob + NB);  // this panel's outer block
+    const int cs = k0 + CB;  // the next panel's first column
+    const bool boundary = cs == oe;
+    // (a) the next 64 columns: by this panel, or at an outer-block end by the whole outer block
+    //     (whose updates of later columns were deferred)
+    if (boundary)
+      pupd(ob, oe - ob, cs, 1);
+    else
+      pupd(k0, CB, cs, 1);
     // next diagonal factor + panel solve on the side stream
     cudaEventRecord(ev_fork[dev], st);
     cudaStreamWaitEvent(s2, ev_fork[dev], 0);
-    NQS_TRY(potrf(k0 + CB, k0, s2));
+    NQS_TRY(potrf(cs, k0, s2));
     cudaEventRecord(ev_join[dev], s2);
-    last = k0 + CB;
-    // (b) the rest of this step's trailing update
-    if (rest > CB) {
-      const double* P2 = A + (size_t)(k0 + 2 * CB) * lda + k0;
-      double* C2 = A + (size_t)(k0 + 2 * CB) * lda + k0 + 2 * CB;
-      NQS_TRY(dsyrk_lower(P2, lda, rest - CB, CB, -1.0, 1.0, C2, lda, nullptr, 0, nsm, st));
+    last = cs;
+    if (!boundary) {
+      // (b) the rest of this outer block's columns, by this panel
+      const int nb = (oe - cs - CB + CB - 1) / CB;
+      if (nb > 0) pupd(k0, CB, cs + CB, nb);
+    } else if (cs + CB < n) {
+      // (c) the deferred trailing update beyond the next panel, by the whole outer block
+      const int m0 = cs + CB;
+      NQS_TRY(dsyrk_lower(A + (size_t)m0 * lda + ob, lda, n - m0, oe - ob, -1.0, 1.0,
+                          A + (size_t)m0 * lda + m0, lda, nullptr, 0, nsm, st));
     }
     cudaStreamWaitEvent(st, ev_join[dev], 0);
   }
