@@ -398,22 +398,20 @@ __global__ void k_add_diag_noise(double* A, int64_t lda, int n, double lam, doub
 }
 
 // Diagonal-block Cholesky + panel solve of one right-looking step, fused. Every CTA factors the
-// b x b diagonal block [k0, k0+b) redundantly: each thread owns a fixed set of lower-triangle
-// elements in registers (element e of the row-major lower triangle -> thread e % 256); in step j
-// the owners of column j publish it (double-buffered) and every owner of (i, k), k > j, applies
-// a_ik -= a_ij a_kj / d_j with the unscaled column, so one barrier per column suffices. The CTA
-// then solves its share of the panel rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L^-T,
-// four rows per warp side by side. The factor is written to Ld rather than into A (other CTAs may
-// still be reading the block); the next step's CTA 0 (or k_store_diag after the last step) copies
-// it into A. Pivots d_j below *floor_p are raised to it (counted in bad[2]); a non-positive pivot
-// sets bad[0] (CTA 0 records both).
-constexpr int kCholElems = (CB * (CB + 1) / 2 + 255) / 256;  // lower-triangle elements per thread
+// b x b diagonal block [k0, k0+b) redundantly in shared memory, in 8-column sub-panels: warp 0
+// factors a sub-panel with its rows in registers (shuffles carry the pivot row's entries), the
+// whole CTA then applies the sub-panel's rank-8 update a_ik -= sum_c a_ic a_kc / d_c to the
+// trailing block (unscaled columns, square roots deferred to the end). The CTA then solves its
+// share of the panel rows r in [k0+b, n): A[r][k0:k0+b] <- A[r][k0:k0+b] L^-T, four rows per warp
+// side by side. The factor is written to Ld rather than into A (other CTAs may still be reading
+// the block); the next step's CTA 0 (or k_store_diag after the last step) copies it into A.
+// Pivots d_j below *floor_p are raised to it (counted in bad[2]); a non-positive pivot sets
+// bad[0] (CTA 0 records both).
 
 __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int64_t lda, int k0,
                                                     int n, const double* __restrict__ floor_p,
                                                     int* __restrict__ bad, int rpc,
                                                     double* __restrict__ Ld, int prev_k0) {
-  __shared__ double col[2][CB];
   __shared__ double L[CB][CB + 1];
   __shared__ double rdiag[CB];
   const int b = min(CB, n - k0);
@@ -428,65 +426,92 @@ __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int6
   }
   const double fl = floor_p ? *floor_p : 0.0;
   __shared__ double dval[CB], dinv[CB];
-  // pivot d_j (raised to the floor when below it) and its reciprocal, set by the owner of (j, j)
-  auto set_pivot = [&](int j, double d) {
-    const bool floored = floor_p && !(d > fl);
-    if (floored) d = fl;
-    const bool pos = d > 0.0;
-    if (blockIdx.x == 0) {
-      if (floored) atomicAdd(bad + 2, 1);
-      if (!pos) bad[0] = 1;
-    }
-    dval[j] = d;
-    dinv[j] = pos ? 1.0 / d : NAN;
-  };
-  // owned elements: e = tid + 256 q of the row-major lower triangle of the b x b block
-  double v[kCholElems];
-  int ei[kCholElems], ek[kCholElems];
-  const int ne = b * (b + 1) / 2;
-#pragma unroll
-  for (int q = 0; q < kCholElems; ++q) {
-    const int e = tid + 256 * q;
-    int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-    while ((i + 1) * (i + 2) / 2 <= e) ++i;
-    while (i * (i + 1) / 2 > e) --i;
-    const int k = e - i * (i + 1) / 2;
-    const bool own = e < ne;
-    ei[q] = own ? i : 0;
-    ek[q] = own ? k : -1;  // not owned: never updated, never published
-    v[q] = own ? A[(size_t)(k0 + i) * lda + k0 + k] : 0.0;
-    if (own && k == 0) col[0][i] = v[q];
-    if (own && e == 0) set_pivot(0, v[q]);
+  // working copy of the diagonal block (lower triangle) in L; it becomes the factor in place
+  for (int idx = tid; idx < CB * CB; idx += blockDim.x) {
+    const int i = idx / CB, k = idx - i * CB;
+    L[i][k] = (i < b && k <= i) ? A[(size_t)(k0 + i) * lda + k0 + k] : 0.0;
   }
   __syncthreads();
-  // elimination with the unscaled columns (a_ik -= a_ij a_kj / d_j); square roots deferred
-  for (int j = 0; j < b; ++j) {
-    const double* cj = col[j & 1];
-    double* cn = col[(j + 1) & 1];
-    const double inv = dinv[j];
+  // eight 8-column sub-panels: warp 0 factors sub-panel [j0, j0 + jw) of rows [j0, b) with the
+  // rows in registers (lane l: rows j0 + l and j0 + l + 32), unscaled columns a_ik -= a_ic a_kc / d_c
+  // and pivots d_c (raised to the floor when below it); then every thread applies the sub-panel's
+  // rank-jw update to the trailing block, four threads per row.
+  const int lane = tid & 31;
+  for (int j0 = 0; j0 < b; j0 += 8) {
+    const int jw = min(8, b - j0);
+    if (tid < 32) {
+      const int ra = j0 + lane, rb = j0 + lane + 32;
+      double pa[8], pb[8];
 #pragma unroll
-    for (int q = 0; q < kCholElems; ++q) {
-      const int i = ei[q], k = ek[q];
-      const double u = cj[i] * cj[k > 0 ? k : 0] * inv;
-      if (k > j) v[q] -= u;
-      if (k == j + 1) {
-        cn[i] = v[q];
-        if (i == k) set_pivot(k, v[q]);
+      for (int c = 0; c < 8; ++c) {
+        pa[c] = (ra < b && c < jw) ? L[ra][j0 + c] : 0.0;
+        pb[c] = (rb < b && c < jw) ? L[rb][j0 + c] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < jw) {
+          double d = __shfl_sync(0xffffffffu, pa[c], c);  // row j0 + c, column c
+          const bool floored = floor_p && !(d > fl);
+          if (floored) d = fl;
+          const bool pos = d > 0.0;
+          if (lane == 0) {
+            if (blockIdx.x == 0) {
+              if (floored) atomicAdd(bad + 2, 1);
+              if (!pos) bad[0] = 1;
+            }
+            dval[j0 + c] = d;
+          }
+          const double inv = pos ? 1.0 / d : NAN;
+          if (lane == 0) dinv[j0 + c] = inv;
+          if (lane == c) pa[c] = d;  // the (floored) pivot is the stored diagonal
+#pragma unroll
+          for (int k = c + 1; k < 8; ++k) {
+            const double akc = __shfl_sync(0xffffffffu, pa[c], k) * inv;  // row j0 + k, column c
+            if (k < jw) {
+              pa[k] -= pa[c] * akc;
+              pb[k] -= pb[c] * akc;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < jw && ra < b && ra >= j0 + c) L[ra][j0 + c] = pa[c];
+        if (c < jw && rb < b) L[rb][j0 + c] = pb[c];
+      }
+    }
+    __syncthreads();
+    // trailing update: rows i, columns k in [j0 + jw, i]
+    const int t0 = j0 + jw, m = b - t0;
+    if (m > 0) {
+      const int i = t0 + (tid >> 2), q = tid & 3;
+      if (tid >> 2 < m) {
+        double pi[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) pi[c] = c < jw ? L[i][j0 + c] * dinv[j0 + c] : 0.0;
+        for (int k = t0 + q; k <= i; k += 4) {
+          double acc = 0.0;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) acc = fma(pi[c], L[k][j0 + c], acc);
+          L[i][k] -= acc;
+        }
       }
     }
     __syncthreads();
   }
   // L[i][k] = a_ik / sqrt(d_k) (i > k), L[k][k] = sqrt(d_k)
-#pragma unroll
-  for (int q = 0; q < kCholElems; ++q) {
-    const int i = ei[q], k = ek[q];
-    if (k >= 0) {
+  for (int idx = tid; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, k = idx - i * b;
+    if (k <= i) {
       const double d = dval[k];
       const bool pos = d > 0.0;
       const double sd = pos ? sqrt(d) : NAN;
-      L[i][k] = (i == k) ? sd : v[q] / sd;
-      if (i == k) rdiag[k] = pos ? 1.0 / sd : NAN;
+      L[i][k] = (i == k) ? sd : L[i][k] / sd;
     }
+  }
+  if (tid < b) {
+    const double d = dval[tid];
+    rdiag[tid] = d > 0.0 ? 1.0 / sqrt(d) : NAN;
   }
   __syncthreads();
   if (blockIdx.x == 0)
@@ -496,7 +521,7 @@ __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int6
     }
   // panel rows of this CTA, four per warp at once: x L^T = a ->
   //   x_j = (a_j - sum_{m<j} x_m L[j][m]) / L[j][j]
-  const int lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  const int w = tid >> 5, nw = blockDim.x >> 5;
   const int r_lo = k0 + b + blockIdx.x * rpc, r_hi = min(n, r_lo + rpc);
   for (int r0 = r_lo + 4 * w; r0 < r_hi; r0 += 4 * nw) {
     double x0[4], x1[4];
