@@ -1207,27 +1207,38 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
     m1[c] = (mu && in) ? mu[K + k0 + c] : 0.0;
   }
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
-  for (int m = m_lo; m < m_hi; ++m) {
-    const TO* row = O + (size_t)m * K + k0;
-    double o[4];
-    if (VEC) {
-      if (sizeof(TO) == 4) {
-        const float4 f = *reinterpret_cast<const float4*>(row);
-        o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+  // eight rows per step, all eight rows' loads issued before the first is used (rows past the
+  // slice re-read row m_lo with weight 0)
+  constexpr int RU = 8;
+  for (int mb = m_lo; mb < m_hi; mb += RU) {
+    TO o[RU][4];
+    double xm[RU];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const bool in = mb + u < m_hi;
+      const TO* row = O + (size_t)(in ? mb + u : m_lo) * K + k0;
+      xm[u] = in ? x[mb + u] : 0.0;
+      if (VEC) {
+        if (sizeof(TO) == 4) {
+          const float4 f = *reinterpret_cast<const float4*>(row);
+          o[u][0] = f.x; o[u][1] = f.y; o[u][2] = f.z; o[u][3] = f.w;
+        } else {
+          const double2 a = reinterpret_cast<const double2*>(row)[0];
+          const double2 b = reinterpret_cast<const double2*>(row)[1];
+          o[u][0] = a.x; o[u][1] = a.y; o[u][2] = b.x; o[u][3] = b.y;
+        }
       } else {
-        const double2 a = reinterpret_cast<const double2*>(row)[0];
-        const double2 b = reinterpret_cast<const double2*>(row)[1];
-        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) o[u][c] = k0 + c < K ? row[c] : TO(0);
       }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) o[c] = k0 + c < K ? (double)row[c] : 0.0;
     }
-    const double xm = x[m];
-    const bool lo_half = m < Mh;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[c] = fma(o[c] - (lo_half ? m0[c] : m1[c]), xm, acc[c]);
+    for (int u = 0; u < RU; ++u) {
+      const bool lo_half = mb + u < Mh;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        acc[c] = fma((double)o[u][c] - (lo_half ? m0[c] : m1[c]), xm[u], acc[c]);
+    }
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c)
