@@ -201,55 +201,40 @@ __global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, 
 #pragma unroll
   for (int q = 0; q < Q; ++q) acc[q] = 0;
   const T rho3 = rho * rho * rho;
-  // tangent rows four at a time: the four rows' loads are in flight before the first reduction
-  constexpr int TP = 4;
-  for (int t0 = 0; t0 < n_tan; t0 += TP) {
-    T dus[TP][Q];
+  for (int t = 0; t < n_tan; ++t) {
+    const T* xt = x + (size_t)(1 + t) * d;
+    T du[Q];
+    s = 0;
 #pragma unroll
-    for (int tt = 0; tt < TP; ++tt) {
-      const T* xt = x + (size_t)(1 + t0 + tt) * d;
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      du[q] = f < d ? xt[f] : T(0);
+      s += du[q];
+    }
+    const T mt = warp_sum(s) * inv_d;
+    T s2 = 0, s3 = 0;
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const int f = lane + 32 * q;
-        dus[tt][q] = (t0 + tt < n_tan && f < d) ? xt[f] : T(0);
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      if (f < d) {
+        du[q] -= mt;
+        s2 += u[q] * du[q];
+        s3 += du[q] * du[q];
       }
     }
+    const T dv = T(2) * warp_sum(s2) * inv_d;
+    const T drho = T(-0.5) * rho3 * dv;
+    T* yt = y + (size_t)(1 + t) * d;
 #pragma unroll
-    for (int tt = 0; tt < TP; ++tt) {
-      const int t = t0 + tt;
-      if (t >= n_tan) break;  // warp-uniform
-      T du[Q];
-      s = 0;
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        du[q] = dus[tt][q];
-        s += du[q];
+    for (int q = 0; q < Q; ++q) {
+      const int f = lane + 32 * q;
+      if (f < d) {
+        yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
+        acc[q] += du[q] * drho;
       }
-      const T mt = warp_sum(s) * inv_d;
-      T s2 = 0, s3 = 0;
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const int f = lane + 32 * q;
-        if (f < d) {
-          du[q] -= mt;
-          s2 += u[q] * du[q];
-          s3 += du[q] * du[q];
-        }
-      }
-      const T dv = T(2) * warp_sum(s2) * inv_d;
-      const T drho = T(-0.5) * rho3 * dv;
-      T* yt = y + (size_t)(1 + t) * d;
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const int f = lane + 32 * q;
-        if (f < d) {
-          yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
-          acc[q] += du[q] * drho;
-        }
-      }
-      S1 += dv * dv;
-      S2 += warp_sum(s3) * inv_d;
     }
+    S1 += dv * dv;
+    S2 += warp_sum(s3) * inv_d;
   }
   if (has_lap) {
     const T* xl = x + (size_t)(C - 1) * d;
