@@ -159,12 +159,11 @@ __global__ void __launch_bounds__(128) k_embed_value(JobBatch jb, ModelConst mc,
 //   Lap y = g (Lap u rho + 2 sum_t d_t u d_t rho + u Lap rho),
 //   Lap rho = 3/4 rho^5 sum_t (d_t v)^2 - 1/2 rho^3 Lap v,  Lap v = 2 mean(u Lap u) + 2 sum_t mean((d_t u)^2)
 // ============================================================================================
-template <typename T>
+template <typename T, int Q = NQS_MAX_EMBED / 32>  // Q >= d / 32 features per lane
 __global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, int has_lap, int d,
                                                    const T* __restrict__ X,
                                                    const T* __restrict__ g,
                                                    const T* __restrict__ b, T* __restrict__ Y) {
-  constexpr int Q = NQS_MAX_EMBED / 32;
   const int lane = threadIdx.x & 31;
   const int tok = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (tok >= n_tok) return;
@@ -201,40 +200,56 @@ __global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, 
 #pragma unroll
   for (int q = 0; q < Q; ++q) acc[q] = 0;
   const T rho3 = rho * rho * rho;
-  for (int t = 0; t < n_tan; ++t) {
-    const T* xt = x + (size_t)(1 + t) * d;
-    T du[Q];
-    s = 0;
+  // tangent rows TP at a time: their loads are in flight before the first reduction (the narrow
+  // instantiations, Q <= 2, keep the registers for this without losing occupancy)
+  constexpr int TP = Q <= 2 ? 4 : 1;
+  for (int t0 = 0; t0 < n_tan; t0 += TP) {
+    T dus[TP][Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      du[q] = f < d ? xt[f] : T(0);
-      s += du[q];
-    }
-    const T mt = warp_sum(s) * inv_d;
-    T s2 = 0, s3 = 0;
+    for (int tt = 0; tt < TP; ++tt) {
+      const T* xt = x + (size_t)(1 + t0 + tt) * d;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) {
-        du[q] -= mt;
-        s2 += u[q] * du[q];
-        s3 += du[q] * du[q];
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        dus[tt][q] = (t0 + tt < n_tan && f < d) ? xt[f] : T(0);
       }
     }
-    const T dv = T(2) * warp_sum(s2) * inv_d;
-    const T drho = T(-0.5) * rho3 * dv;
-    T* yt = y + (size_t)(1 + t) * d;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int f = lane + 32 * q;
-      if (f < d) {
-        yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
-        acc[q] += du[q] * drho;
+    for (int tt = 0; tt < TP; ++tt) {
+      const int t = t0 + tt;
+      if (t >= n_tan) break;  // warp-uniform
+      T du[Q];
+      s = 0;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        du[q] = dus[tt][q];
+        s += du[q];
       }
+      const T mt = warp_sum(s) * inv_d;
+      T s2 = 0, s3 = 0;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        if (f < d) {
+          du[q] -= mt;
+          s2 += u[q] * du[q];
+          s3 += du[q] * du[q];
+        }
+      }
+      const T dv = T(2) * warp_sum(s2) * inv_d;
+      const T drho = T(-0.5) * rho3 * dv;
+      T* yt = y + (size_t)(1 + t) * d;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int f = lane + 32 * q;
+        if (f < d) {
+          yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
+          acc[q] += du[q] * drho;
+        }
+      }
+      S1 += dv * dv;
+      S2 += warp_sum(s3) * inv_d;
     }
-    S1 += dv * dv;
-    S2 += warp_sum(s3) * inv_d;
   }
   if (has_lap) {
     const T* xl = x + (size_t)(C - 1) * d;
@@ -963,7 +978,13 @@ inline int launch_layernorm(int n_tok, int C, int n_tan, int has_lap, int d, con
     k_layernorm1<T, R><<<(nw + 7) / 8, 256, 0, st>>>(n_tok, d, X, g, b, Y);
     NQS_CHECK_LAUNCH("k_layernorm1");
   } else {
-    k_layernorm<T><<<(n_tok + 7) / 8, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
+    const unsigned grid = (unsigned)((n_tok + 7) / 8);
+    if (d <= 32)
+      k_layernorm<T, 1><<<grid, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
+    else if (d <= 64)
+      k_layernorm<T, 2><<<grid, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
+    else
+      k_layernorm<T><<<grid, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
     NQS_CHECK_LAUNCH("k_layernorm");
   }
   return NQS_OK;
