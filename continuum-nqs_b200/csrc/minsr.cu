@@ -1522,7 +1522,7 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * n);              // etil
   add(sizeof(double) * n);              // y
   add(sizeof(double) * n);              // refinement residual
-  add(sizeof(double) * 2 * P);          // Otil^T y (double-double)
+  add(sizeof(double) * 2 * P);          // Otil^T y and a spare P-vector
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
   add(sizeof(double) * trsv_elems(n));  // triangular-solve exchange + diagonal-block inverses
