@@ -924,7 +924,7 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
   const int tid = threadIdx.x;
   __shared__ double red[4][CB];
   __shared__ double rhs[CB];
-  // the wait's verdict, double-buffered by iteration parity: thread 0 writes iteration it+1's
+  // the wait's outcome, double-buffered by iteration parity: thread 0 writes iteration it+1's
   // slot only after every thread has passed iteration it+1's barrier, i.e. has read slot it
   __shared__ int give_up_buf[2];
   bool give_up = false;
