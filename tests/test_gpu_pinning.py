@@ -68,3 +68,46 @@ def test_observables_on_spin_independent_state():
     assert abs(mG[0, 0] - 1.0) < 1e-9 and abs(mG[1, 0]) < 1e-9
     cl = classify_state(lp, R, S, A, ngrid=8, nshell=3)
     assert cl["label"] == "in-plane / Rashba-FM", cl["label"]
+
+
+def test_skyrmion_envelope_is_an_eigenstate_under_its_texture():
+    """Zero-backflow Psiformer on the skyrmion-background envelope (nqs.rashba.cell_skx_envelope:
+    the occupied orbitals of h0 - lambda_tex n(r).sigma on a hexagonal supercell, 421 plane
+    waves) with ext_field = lambda_tex n(r): the local energy is the band energy E_band at every
+    configuration (to the basis truncation, ~1e-6 here), and matches the oracle."""
+    import importlib.util
+    import os
+    from nqs import rashba
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import ContinuumSpinorPsiformer, make_logpsi
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(os.path.dirname(__file__), "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    q1, q2, A, keys, vals = mg.skx_case()
+    lam_tex, N = 0.5, 7
+    skx = rashba.cell_skx_envelope(A, N, keys, vals, q1, q2, lam_tex, 1.0, 0.3, 0.05, 12,
+                                   (0.1, 0.17), gtol=1e-16)
+    G = np.array([a * q1 + b * q2 for a, b in keys])
+
+    def field(R):  # lambda_tex Re sum_Q S_Q e^{i Q.r}
+        R = torch.as_tensor(R)
+        g = torch.as_tensor(G, dtype=R.dtype, device=R.device)
+        ph = R @ g.T
+        Sr = torch.as_tensor(vals.real, dtype=R.dtype, device=R.device)
+        Si = torch.as_tensor(vals.imag, dtype=R.dtype, device=R.device)
+        return lam_tex * (torch.cos(ph) @ Sr - torch.sin(ph) @ Si)
+
+    model = ContinuumSpinorPsiformer(n_elec=N, Gs=skx["Gs"], W=skx["W"], L=A, embed_dim=16,
+                                     depth=1, n_heads=4, n_freq=4)
+    p = model.init(0)
+    rng = np.random.default_rng(91)
+    R = torch.as_tensor(rng.uniform(0, 1, (24, N, 2)) @ np.asarray(A).T)
+    S = torch.as_tensor(rng.integers(0, 2, (24, N)))
+    E = make_local_energy(make_logpsi(model, p), 1.0, 0.3, 0.05, ext_field=field)(R, S).cpu()
+    assert (E.real - skx["E_band"]).abs().max() < 2e-5, float((E.real - skx["E_band"]).abs().max())
+    assert E.imag.abs().max() < 2e-5
+    for w in range(2):
+        ref = O.local_energy(lambda r, s: O.logpsi(model, p, r, s), R[w], S[w], 1.0, 0.3, 0.05,
+                             ext_field=field)
+        assert abs(complex(E[w]) - complex(ref)) < 1e-9 * max(1.0, abs(complex(ref)))
