@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import build, configs, perturb
+from helpers import TWIST, build, configs, perturb
 from oracle import nqs_oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -92,3 +92,31 @@ def test_tensor_core_network_matches_simt_and_fp64():
     assert abs(float(E["mixed"].real.mean() - E["fp64"].real.mean())) < 2e-2
     v64 = float(E["fp64"].real.var())
     assert abs(float(E["mixed"].real.var()) - v64) < 0.05 * v64
+
+
+def test_slater_trial_callables():
+    """nqs.slater (reference src/nqs/slater_reference.py): log psi of the multi-G spinor
+    determinant against the oracle's direct slogdet, and the exact Rashba ground state through
+    make_logpsi_slater is zero-variance in the device local energy (reference
+    tests/test_nqs_folx.py:22-30) and samples on its cell."""
+    from nqs import rashba
+    from nqs.local_energy import make_local_energy
+    from nqs.sampler import run_chain
+    from nqs.slater import make_logpsi_general, make_logpsi_slater
+    rng = np.random.default_rng(12)
+    N, nG, L = 5, 9, 6.0
+    Gs = rng.normal(size=(nG, 2))
+    W = rng.normal(size=(N, nG, 2)) + 1j * rng.normal(size=(N, nG, 2))
+    R = torch.as_tensor(rng.uniform(0, L, (4, N, 2)))
+    S = torch.as_tensor(rng.integers(0, 2, (4, N)))
+    lp = make_logpsi_general(Gs, W, cell=L)(R, S).cpu()
+    for w in range(4):
+        assert _close_mod_2pi(lp[w], O.slater_logpsi(Gs, W, R[w], S[w]), 1e-11)
+    g = rashba.noninteracting_gs(N=7, L=8.0, m_star=1.0, lambda_r=1.0, h_z=0.5, n_cut=10,
+                                 twist=TWIST)
+    f = make_logpsi_slater(*rashba.occupied_orbital_matrix(g), cell=8.0)
+    R, S = configs(7, 8.0, 16, 13)
+    E = make_local_energy(f, 1.0, 1.0, 0.5)(R, S).cpu()
+    assert E.real.std() < 1e-10 and abs(float(E.real.mean()) - g["E_gs"]) < 1e-10
+    Rc, Sc, acc_p, acc_s = run_chain(f, 8.0, 7, 3, n_walkers=32, n_sweeps=4, burn=2, step=0.5)[:4]
+    assert Rc.shape == (32, 7, 2) and torch.isfinite(Rc).all()

@@ -246,3 +246,21 @@ def test_ed2_noninteracting_limit_and_convergence():
     e10 = ed2.ground_energy(A, 10, 1.0, 0.5, 0.1, alpha=1.0, ewald_alpha=5.0 / L)
     assert e10 > g["E_ed_ncut16"] > g["E_ed_ncut24"]  # variational in the cutoff
     assert e10 - g["E_ed_ncut24"] < 3e-5
+
+
+def test_slater_model_is_the_slater_determinant():
+    """The network behind nqs.slater (zero backflow, no Jastrow, one determinant) reproduces the
+    spinor Slater determinant of the reference (slater_reference.py:21-37) on the oracle."""
+    from nqs.slater import slater_model
+    rng = np.random.default_rng(11)
+    N, nG, L = 5, 9, 6.0
+    Gs = rng.normal(size=(nG, 2))
+    W = rng.normal(size=(N, nG, 2)) + 1j * rng.normal(size=(N, nG, 2))
+    model, params = slater_model(Gs, W, cell=L)
+    for w in range(3):
+        R = torch.as_tensor(rng.uniform(0, L, (N, 2)))
+        S = torch.as_tensor(rng.integers(0, 2, N))
+        a = complex(O.logpsi(model, params, R, S))
+        b = complex(O.slater_logpsi(Gs, W, R, S))
+        assert abs(a.real - b.real) < 1e-12
+        assert abs((a.imag - b.imag + np.pi) % (2 * np.pi) - np.pi) < 1e-12
