@@ -258,6 +258,21 @@ def as_batch(R, S):
     return R, S, single
 
 
+def periodic_features(R, cell, n_freq):
+    """The network's input features (reference psiformer.py:84-97), as a host / device torch
+    function: fractional coordinates s = R A^-T (no wrap: the features are lattice-periodic) and,
+    per electron, [sin(2 pi m s_x), cos(2 pi m s_x), sin(2 pi m s_y), cos(2 pi m s_y)] blocks for
+    m = 1..n_freq, i.e. (..., N, 2) -> (..., N, 4 n_freq) in the order [x: sin, cos; y: sin, cos].
+    The kernels compute the same features in-kernel; this is for inspection and tests."""
+    from .cell import cell_matrix
+    R = torch.as_tensor(R)
+    A = torch.as_tensor(cell_matrix(cell), dtype=R.dtype, device=R.device)
+    s = R @ torch.linalg.inv(A).T
+    m = torch.arange(1, n_freq + 1, dtype=R.dtype, device=R.device)
+    ang = (2.0 * np.pi) * s[..., :, None] * m
+    return torch.cat([torch.sin(ang), torch.cos(ang)], dim=-1).reshape(*R.shape[:-1], 4 * n_freq)
+
+
 class LogPsi:
     """logpsi(R, S) bound to a model and parameters (make_logpsi, psiformer.py:192-196)."""
 

@@ -264,3 +264,30 @@ def test_slater_model_is_the_slater_determinant():
         b = complex(O.slater_logpsi(Gs, W, R, S))
         assert abs(a.real - b.real) < 1e-12
         assert abs((a.imag - b.imag + np.pi) % (2 * np.pi) - np.pi) < 1e-12
+
+
+def test_periodic_features_match_oracle():
+    from nqs.psiformer import periodic_features
+    rng = np.random.default_rng(14)
+    A = np.array([[6.0, 2.0], [0.0, 5.0]])
+    R = torch.as_tensor(rng.uniform(-3, 9, (5, 2)))
+    f = periodic_features(R, A, 3)
+    assert f.shape == (5, 12)
+    assert torch.allclose(f, O.periodic_features(R, A, 3), atol=1e-14, rtol=0)
+    # batched input and lattice periodicity
+    Rb = torch.stack([R, R + torch.as_tensor(A[:, 0])])
+    fb = periodic_features(Rb, A, 3)
+    assert fb.shape == (2, 5, 12) and torch.allclose(fb[0], fb[1], atol=1e-12, rtol=0)
+
+
+def test_spiral_texture_is_the_slater_spin_density():
+    from nqs.observables import slater_spin_density
+    from nqs.spiral import spin_texture, spiral_gs
+    res = spiral_gs(N=5, L=7.0, Q_int=(1, 0), B=0.3, lambda_r=1.0, h_z=0.0, n_cut=4,
+                    twist=(0.1, 0.17))
+    t = spin_texture(res, ngrid=6)
+    assert t.shape == (6, 6, 3)
+    r = np.array([0.5, 0.5]) * 7.0 / 6  # first mesh point
+    from oracle import observables_oracle as OO
+    assert np.abs(t[0, 0] - OO.slater_spin_density_at(r, res["Gs"], res["W"])).max() < 1e-11
+    assert np.abs(t - slater_spin_density(res["Gs"], res["W"], 7.0 * np.eye(2), 6)).max() == 0
