@@ -129,3 +129,14 @@ def test_slater_spin_density_matches_oracle():
     Wu[..., 1] = 0
     mu = slater_spin_density(Gs, Wu, A, ngrid=4)
     assert np.abs(mu[..., :2]).max() < 1e-12 and (mu[..., 2] > 0).all()
+
+
+def test_pins_have_magnitude_h_pin():
+    """Skyrmion (m0 = 0.3, the default), FM and cycloidal-spiral fields are h_pin times a unit
+    vector at any position (reference tests/test_nqs_production.py:47-60)."""
+    from nqs.pinning import berg_luscher_realspace, make_fm_pin, make_skx_pin, make_spiral_pin
+    pts = torch.as_tensor(np.vstack([[1.3, -0.7], _points(20, 9)]))
+    for pin in (make_skx_pin(Q1, Q2, 0.7), make_fm_pin(0.7), make_spiral_pin(Q1, 0.7)):
+        n = np.linalg.norm(pin(pts).numpy(), axis=-1)
+        assert np.abs(n - 0.7).max() < 1e-9
+    assert abs(berg_luscher_realspace(make_skx_pin(Q1, Q2, 1.0, m0=0.3), CELL, ngrid=36)) > 0.5
