@@ -6,6 +6,7 @@ paramsr_direction run in libnqs kernels.
 """
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 F64 = torch.float64
@@ -328,6 +329,39 @@ class VMCIteration:
         self.energies()
         self.jacobian()
         self.update()
+
+    def state_dict(self):
+        """What a resume needs beyond the constructor arguments: theta, the walkers and the
+        position of the Metropolis random stream (seed, sweep counter), as host copies."""
+        return {"theta": self.theta.cpu(), "R": self.R.cpu(), "S": self.S.cpu(),
+                "seed": self.seed, "counter": self.counter}
+
+    def load_state_dict(self, st):
+        """Restore a state_dict (shapes must match this iteration's model and walker count); the
+        next sweeps continue the same random stream."""
+        theta = torch.as_tensor(st["theta"], dtype=F64)
+        R = torch.as_tensor(st["R"], dtype=F64)
+        S = torch.as_tensor(st["S"])
+        if theta.shape != self.theta.shape or R.shape != self.R.shape or S.shape != self.S.shape:
+            raise ValueError("checkpoint shapes do not match this VMC iteration")
+        self.theta.copy_(theta)
+        self.R.copy_(R)
+        self.S.copy_(S.to(self.S.dtype))
+        self.seed, self.counter = int(st["seed"]), int(st["counter"])
+
+
+def save_checkpoint(path, it):
+    """Write a VMC iteration's state_dict (theta, walkers, random-stream position) to an .npz."""
+    st = it.state_dict()
+    np.savez(path, theta=st["theta"].numpy(), R=st["R"].numpy(), S=st["S"].numpy(),
+             seed=np.int64(st["seed"]), counter=np.int64(st["counter"]))
+
+
+def load_checkpoint(path):
+    """The state_dict saved by save_checkpoint (torch tensors on the host, ints)."""
+    z = np.load(path)
+    return {"theta": torch.as_tensor(z["theta"]), "R": torch.as_tensor(z["R"]),
+            "S": torch.as_tensor(z["S"]), "seed": int(z["seed"]), "counter": int(z["counter"])}
 
 
 def train_minsr(model, params, L, n_elec, key, *, m_star=1.0, lambda_r=1.0, h_z=0.0,

@@ -56,3 +56,4 @@ def test_reference_arm_rank_above_zero_exits_quietly(monkeypatch, capsys):
     monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--gpus", "2"])
     bench.run_reference(bench.parse())
     assert capsys.readouterr().out == ""
+

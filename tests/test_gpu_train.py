@@ -46,3 +46,27 @@ def test_adam_training_descends_to_Egs():
     assert E_final < E_init - 1e-3
     assert (E_final - g["E_gs"]) / excess < 0.05, (E_init, E_final, g["E_gs"])
     assert E_final > g["E_gs"] - 0.02
+
+
+def test_checkpoint_resume_is_bit_identical(tmp_path):
+    """Two VMC steps straight through equal one step, a checkpoint written to disk, a fresh
+    iteration restored from it, and one more step (same theta, walkers and random stream)."""
+    import torch
+    from nqs.minsr import VMCIteration, load_checkpoint, save_checkpoint, real_ravel
+    from nqs.sampler import init_walkers_uniform
+    g, model = build(N=5, L=7.0, hz=0.5, embed=16, heads=4)
+    theta, _ = real_ravel(perturb(model.init(0), 0.05, 8, only="backflow"))
+    R0, S0 = init_walkers_uniform(5, 64, 5, 7.0)
+    kw = dict(m_star=1.0, lambda_r=1.0, h_z=0.5, lr=0.05, lam=1e-3, n_sweeps=4, step_size=0.5,
+              seed=11)
+    a = VMCIteration(model, theta, R0, S0, **kw)
+    a.step()
+    save_checkpoint(tmp_path / "ck.npz", a)
+    a.step()
+    b = VMCIteration(model, theta, R0, S0, **kw)  # different state until restored
+    b.load_state_dict(load_checkpoint(tmp_path / "ck.npz"))
+    b.step()
+    torch.cuda.synchronize()
+    assert torch.equal(a.theta, b.theta)
+    assert torch.equal(a.R, b.R) and torch.equal(a.S, b.S)
+    assert a.counter == b.counter
