@@ -20,6 +20,10 @@ NQS_OK = 0
 NQS_ERR_INVALID_ARG = 1
 NQS_ERR_UNSUPPORTED = 2
 NQS_ERR_WORKSPACE = 3
+NQS_ERR_CUDA = 4
+NQS_ERR_NONFINITE = 5
+NQS_ERR_TIMEOUT = 6
+NQS_ERR_NOT_SPD = 7
 
 PREC_FP64 = 0
 PREC_MIXED = 1

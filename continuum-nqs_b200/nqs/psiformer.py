@@ -166,6 +166,18 @@ class ContinuumSpinorPsiformer:
             return h
         torch.cuda.init()
         L = _lib.lib()
+        desc, keep = self.descriptor()
+        handle = ctypes.c_void_p()
+        _lib.check(L.nqs_model_create(ctypes.byref(desc), ctypes.byref(handle)),
+                   "nqs_model_create")
+        del keep  # the constants were copied to the device by nqs_model_create
+        h = _NativeModel(handle)
+        self._native[dev.index] = h
+        return h
+
+    def descriptor(self):
+        """(NqsModelDesc, host arrays it points to) for nqs_model_create; keep the arrays alive
+        until the call returns."""
         desc = _lib.NqsModelDesc()
         desc.n_elec, desc.embed_dim, desc.depth = self.n_elec, self.embed_dim, self.depth
         desc.n_heads, desc.ff_mult, desc.n_freq = self.n_heads, self.ff_mult, self.n_freq
@@ -204,12 +216,7 @@ class ContinuumSpinorPsiformer:
         for b in range(self.depth):
             for q, sub in enumerate(_lib.BLOCK_PARAMS):
                 desc.off_block[b][q] = g(f"TransformerBlock_{b}", *sub)
-        handle = ctypes.c_void_p()
-        _lib.check(L.nqs_model_create(ctypes.byref(desc), ctypes.byref(handle)),
-                   "nqs_model_create")
-        h = _NativeModel(handle)
-        self._native[dev.index] = h
-        return h
+        return desc, (Gs, Wri, knots)
 
     # ---------------------------------------------------------------- forward
     def apply(self, params, R, S, precision: str = "fp64"):
