@@ -265,6 +265,21 @@ def as_batch(R, S):
     return R, S, single
 
 
+def split_heads(x, n_heads):
+    """(..., N, d) -> (..., n_heads, N, d / n_heads): head h holds features [h hd, (h + 1) hd)
+    (reference psiformer.py:38-41; the attention kernels use this feature-to-head map)."""
+    x = torch.as_tensor(x)
+    *lead, N, d = x.shape
+    return x.reshape(*lead, N, n_heads, d // n_heads).movedim(-2, -3)
+
+
+def merge_heads(x):
+    """Inverse of split_heads: (..., n_heads, N, hd) -> (..., N, n_heads hd)."""
+    x = torch.as_tensor(x).movedim(-3, -2)
+    *lead, N, nh, hd = x.shape
+    return x.reshape(*lead, N, nh * hd)
+
+
 def periodic_features(R, cell, n_freq):
     """The network's input features (reference psiformer.py:84-97), as a host / device torch
     function: fractional coordinates s = R A^-T (no wrap: the features are lattice-periodic) and,
