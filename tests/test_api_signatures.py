@@ -59,3 +59,19 @@ def test_split_merge_heads_roundtrip():
     assert h.shape == (2, 4, 5, 3)
     assert torch.equal(h[1, 2, 3], x[1, 3, 6:9])  # head 2 = features [6, 9)
     assert torch.equal(merge_heads(h), x)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference not mounted")
+def test_wavefunction_fields_match_reference():
+    """ContinuumSpinorPsiformer's constructor fields and defaults equal the flax module's
+    (psiformer.py:100-116)."""
+    from nqs.psiformer import ContinuumSpinorPsiformer
+    tree = ast.parse(open(os.path.join(REF, "psiformer.py")).read())
+    cls = next(n for n in tree.body
+               if isinstance(n, ast.ClassDef) and n.name == "ContinuumSpinorPsiformer")
+    fields = [(s.target.id, s.value) for s in cls.body if isinstance(s, ast.AnnAssign)]
+    sig = inspect.signature(ContinuumSpinorPsiformer)
+    assert list(sig.parameters)[:len(fields)] == [n for n, _ in fields]
+    for n, v in fields:
+        if v is not None:
+            assert sig.parameters[n].default == ast.literal_eval(v), n
