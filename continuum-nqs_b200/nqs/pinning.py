@@ -1,8 +1,7 @@
 """Pinning fields: external spin fields that seed a competing order (host-side setup).
 
 Restates the reference module src/nqs/pinning.py (make_skx_pin :22-42, make_fm_pin :45-51,
-make_spiral_pin :54-67, make_overhauser_pin :70-78, load_hf_texture :81-92, make_hf_skx_pin
-:95-109, make_pin :112-129, berg_luscher_realspace :132-151), which imports JAX. A pinning field
+make_spiral_pin :54-67, make_overhauser_pin :70-78, make_pin :112-129), which imports JAX. A pinning field
 adds H_pin = -sum_i B(r_i) . sigma_i to the Hamiltonian; the constructors return the ext_field
 B(r) that nqs.local_energy.make_local_energy(..., ext_field=...) takes (and evaluates on the
 device at the walkers' positions): a callable vectorised over positions, torch (..., 2) ->
@@ -92,38 +91,6 @@ def make_overhauser_pin(Q, h_pin):
     return ext_field
 
 
-def load_hf_texture(path):
-    """A converged Hartree-Fock texture file (.npz with q1, q2, s_keys, s_vals, BL, E_var, q_star,
-    e_per_cell, and optionally the charge harmonics n_keys, n_vals) as a dict."""
-    d = np.load(path)
-    out = dict(q1=d["q1"], q2=d["q2"], s_keys=d["s_keys"], s_vals=d["s_vals"], BL=float(d["BL"]),
-               E_var=float(d["E_var"]), q_star=float(d["q_star"]),
-               e_per_cell=float(d["e_per_cell"]))
-    if "n_keys" in d.files:
-        out["n_keys"] = d["n_keys"]
-        out["n_vals"] = d["n_vals"]
-    return out
-
-
-def make_hf_skx_pin(s_keys, s_vals, q1, q2, h_pin):
-    """h_pin times the unit texture m(r) = Re sum_G S_G e^{i G.r}, G = m q1 + n q2 for the integer
-    pairs (m, n) of s_keys (nG, 2), S_G the complex spin components s_vals (nG, 3)."""
-    q1, q2 = _vec(q1), _vec(q2)
-    keys = np.asarray(s_keys).reshape(-1, 2)
-    G = keys[:, :1] * q1[None, :] + keys[:, 1:2] * q2[None, :]  # (nG, 2)
-    S = np.asarray(s_vals, dtype=complex).reshape(-1, 3)
-
-    def ext_field(R):
-        R = torch.as_tensor(R)
-        g = torch.as_tensor(G, dtype=R.dtype, device=R.device)
-        ph = R @ g.T                                           # (..., nG)
-        Sr = torch.as_tensor(S.real, dtype=R.dtype, device=R.device)
-        Si = torch.as_tensor(S.imag, dtype=R.dtype, device=R.device)
-        m = torch.cos(ph) @ Sr - torch.sin(ph) @ Si           # Re(e^{i ph} S)
-        return _unit(m, h_pin)
-    return ext_field
-
-
 def make_pin(kind, q1, q2, h_pin, **kw):
     """Field by competitor name ("fluid" gives None: no field)."""
     if kind == "fluid":
@@ -141,16 +108,3 @@ def make_pin(kind, q1, q2, h_pin, **kw):
     if kind == "skx_bloch":
         return make_skx_pin(q1, q2, h_pin, neel=False, **kw)
     raise ValueError(kind)
-
-
-def berg_luscher_realspace(field_fn, A, ngrid=24):
-    """Lattice skyrmion number of the unit texture field/|field| over the cell A (columns are the
-    lattice vectors), sampled at the ngrid x ngrid cell-centred fractional points; see
-    nqs.observables.berg_luscher for the lattice formula."""
-    from .observables import berg_luscher
-    A = np.asarray(A, dtype=float)
-    f = (np.arange(ngrid) + 0.5) / ngrid
-    fu, fv = np.meshgrid(f, f, indexing="ij")
-    R = np.stack([fu, fv], axis=-1) @ A.T                     # (ngrid, ngrid, 2)
-    m = np.asarray(field_fn(torch.as_tensor(R)))
-    return berg_luscher(m)

@@ -4,8 +4,8 @@ The warm-start envelope of the wavefunction (plane-wave momenta Gs and spinor co
 the analytic energy E_gs used by the zero-variance certificates come from here. It restates the
 reference module src/nqs/rashba_reference.py (h0_k :36-39, bands_k :42-46, bands_analytic :49-54,
 allowed_k :57-65, single_particle_levels :68-80, noninteracting_gs :83-108,
-occupied_orbital_matrix :111-119, planewave_envelope :122-133, cell_rashba_envelope :136-160,
-cell_skx_envelope :163-219, ring_minimum :222-231) with the same conventions:
+occupied_orbital_matrix :111-119, planewave_envelope :122-133, cell_rashba_envelope :136-160)
+with the same conventions:
 
     h0(k) = k^2/(2 m*) I + lambda_R (sigma_x k_y + sigma_y k_x) - (h_z/2) sigma_z
 
@@ -67,76 +67,6 @@ def single_particle_levels(L, m_star=1.0, lambda_r=1.0, h_z=0.0, n_cut=8, twist=
             out.append(dict(E=Eu, kx=kx, ky=ky, band=1, n=(int(nx), int(ny)), chi=cu))
     out.sort(key=lambda d: d["E"])
     return out
-
-
-def ring_minimum(m_star=1.0, lambda_r=1.0, h_z=0.0):
-    """(k, E) at the minimum of the continuum lower band E(k) = k^2/(2 m*) - sqrt(lambda_R^2 k^2 +
-    h_z^2/4): for lambda_R^2 m* > |h_z| / 2 the ring k^2 = lambda_R^2 m*^2 - h_z^2 / (4 lambda_R^2),
-    otherwise k = 0 (solved in closed form; the reference scans a fine k grid for h_z != 0)."""
-    lr2 = lambda_r * lambda_r
-    if lr2 * m_star > 0.5 * abs(h_z) and lambda_r != 0.0:
-        k = float(np.sqrt(lr2 * m_star * m_star - 0.25 * h_z * h_z / lr2))
-    else:
-        k = 0.0
-    return k, float(k * k / (2.0 * m_star) - np.sqrt(lr2 * k * k + 0.25 * h_z * h_z))
-
-
-def cell_skx_envelope(A, N, s_keys, s_vals, q1, q2, lambda_tex=1.0, m_star=1.0, lambda_r=1.0,
-                      h_z=0.0, n_cut=8, twist=(0.0, 0.0), gtol=1e-3, n_keys=None, n_vals=None,
-                      lambda_chg=0.0):
-    """Occupied orbitals of h0(k) + V on the cell A (columns = lattice vectors), V the static
-    texture potential -lambda_tex n(r).sigma with n(r) = Re sum_Q S_Q e^{i Q.r}, Q = m q1 + n q2
-    over s_keys / s_vals (plus, with n_keys / n_vals and lambda_chg != 0, the spin-independent
-    Hartree term lambda_chg (2 pi / |Q|) n_Q at each Q != 0). V couples plane wave k to k + Q when
-    k + Q is on the cell's momentum grid, with 2x2 spin block -lambda_tex sum_a S_Q,a sigma_a.
-    Plane waves whose total occupied weight is below gtol x the largest are dropped.
-    Returns dict(Gs (n_G, 2), W (N, n_G, 2), E_band, gap, w (all eigenvalues), npw, n_G,
-    lambda_tex)."""
-    A = np.array([[float(A), 0.0], [0.0, float(A)]]) if np.ndim(A) == 0 else np.asarray(A, float)
-    Ainv = np.linalg.inv(A)
-    B = 2.0 * np.pi * Ainv.T
-    kt = Ainv.T @ np.asarray(twist, float)
-    ns = np.arange(-n_cut, n_cut + 1)
-    nn = np.array([(a, b) for a in ns for b in ns], dtype=float)   # grid index of each plane wave
-    Ks = nn @ B.T + kt
-    npw = len(Ks)
-    side = 2 * n_cut + 1
-    q1, q2 = np.asarray(q1, float), np.asarray(q2, float)
-    sig = (_SX, _SY, _SZ)
-
-    def couple(H, Q, M):
-        # k + Q on the grid <=> Q has integer coordinates in the basis B (A^T Q / 2 pi)
-        c = A.T @ Q / (2.0 * np.pi)
-        ci = np.rint(c)
-        if np.abs(c - ci).max() > 1e-6:
-            return
-        tgt = nn + ci
-        ok = (np.abs(tgt) <= n_cut).all(axis=1)
-        src = np.nonzero(ok)[0]
-        dst = ((tgt[ok, 0] + n_cut) * side + (tgt[ok, 1] + n_cut)).astype(int)
-        for i, j in zip(src, dst):
-            H[2 * j:2 * j + 2, 2 * i:2 * i + 2] += M
-
-    H = np.zeros((2 * npw, 2 * npw), dtype=complex)
-    for i in range(npw):
-        H[2 * i:2 * i + 2, 2 * i:2 * i + 2] = h0_k(Ks[i, 0], Ks[i, 1], m_star, lambda_r, h_z)
-    Sv = np.asarray(s_vals, dtype=complex).reshape(-1, 3)
-    for (a, b), S in zip(np.asarray(s_keys).reshape(-1, 2), Sv):
-        couple(H, a * q1 + b * q2, -lambda_tex * (S[0] * sig[0] + S[1] * sig[1] + S[2] * sig[2]))
-    if n_keys is not None and lambda_chg != 0.0:
-        for (a, b), nq in zip(np.asarray(n_keys).reshape(-1, 2), np.asarray(n_vals, complex)):
-            Q = a * q1 + b * q2
-            qm = float(np.hypot(Q[0], Q[1]))
-            if qm >= 1e-9:
-                couple(H, Q, lambda_chg * (2.0 * np.pi / qm) * nq * np.eye(2))
-    H = 0.5 * (H + H.conj().T)
-    w, v = np.linalg.eigh(H)
-    W = np.transpose(v[:, :N].reshape(npw, 2, N), (2, 0, 1))     # W[a, g, s]
-    wt = np.sum(np.abs(W) ** 2, axis=(0, 2))
-    keep = wt > gtol * wt.max()
-    return dict(Gs=Ks[keep].copy(), W=W[:, keep, :].copy(), E_band=float(np.sum(w[:N])),
-                gap=float(w[N] - w[N - 1]), w=w, npw=npw, n_G=int(keep.sum()),
-                lambda_tex=lambda_tex)
 
 
 def _levels(kpts, m_star, lambda_r, h_z):

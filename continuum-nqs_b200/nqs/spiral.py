@@ -1,7 +1,7 @@
 """Exact non-interacting spin-spiral ground state and its field (host-side setup).
 
 Restates the reference module src/nqs/spiral_reference.py (spiral_gs :24-65, spiral_field
-:68-75, spin_texture :78-95), which imports JAX and cannot run here. Single-particle Hamiltonian:
+:68-75), which imports JAX and cannot run here. Single-particle Hamiltonian:
 
     h = h0(k) - B (sigma_x cos Q.r + sigma_y sin Q.r),     Q = (2 pi / L) Q_int
 
@@ -59,11 +59,3 @@ def spiral_field(B, Q):
         ph = Qx * R[..., 0] + Qy * R[..., 1]
         return torch.stack([B * torch.cos(ph), B * torch.sin(ph), torch.zeros_like(ph)], dim=-1)
     return f
-
-
-def spin_texture(res, ngrid=12):
-    """<sigma(r)> of the occupied spiral determinant on the cell-centred ngrid x ngrid mesh of the
-    L x L box: (ngrid, ngrid, 3), for checking that the texture is non-collinear."""
-    from .observables import slater_spin_density
-    L = float(res["L"])
-    return slater_spin_density(res["Gs"], res["W"], np.array([[L, 0.0], [0.0, L]]), ngrid)

@@ -1,7 +1,8 @@
 """Generate tests/golden/rashba_gs.npz from the REFERENCE's own pure-numpy module
 src/nqs/rashba_reference.py (it imports without JAX). Run in a container where the reference is
 mounted:  python tests/golden/make_golden.py /path/to/continuum-nqs
-The fixture pins the host-side restatement nqs.rashba (and through it every E_gs certificate)."""
+(or with the environment variable NQS_REFERENCE_ROOT naming that checkout). The fixture pins the
+host-side restatement nqs.rashba (and through it every E_gs certificate)."""
 import os
 import sys
 
@@ -33,35 +34,16 @@ def main(ref_root):
         out[f"c{c}_Chi"] = Chi
         out[f"c{c}_env_Gs"] = env["Gs"]
         out[f"c{c}_env_W"] = env["W"]
-    # skyrmion-background envelope on a commensurate supercell (texture harmonics from a fixed
-    # seed), band energies at a few momenta, and the ring minimum at h_z = 0
-    from src.nqs.rashba_reference import (bands_analytic, bands_k, cell_skx_envelope,
-                                          ring_minimum)
-    q1, q2, A, keys, vals = skx_case()
-    skx = cell_skx_envelope(A, 7, keys, vals, q1, q2, 0.5, 1.0, 0.3, 0.05, 4, (0.1, 0.17))
-    out["skx_E_band"] = np.array(skx["E_band"])
-    out["skx_gap"] = np.array(skx["gap"])
-    out["skx_w"] = skx["w"]
-    out["skx_Gs"] = skx["Gs"]
-    out["skx_W"] = skx["W"]
+    # band energies at a few momenta
+    from src.nqs.rashba_reference import bands_analytic, bands_k
     ks = np.array([[0.0, 0.0], [0.3, -0.7], [1.1, 0.4]])
     out["bands_k"] = np.array([bands_k(kx, ky, 1.0, 0.7, 0.3)[:2] for kx, ky in ks])
     out["bands_analytic"] = np.array([bands_analytic(kx, ky, 1.0, 0.7, 0.3) for kx, ky in ks])
-    out["ring_hz0"] = np.array(ring_minimum(1.0, 0.3, 0.0))
     np.savez(os.path.join(os.path.dirname(os.path.abspath(__file__)), "rashba_gs.npz"), **out)
 
 
-def skx_case():
-    """Triple-Q texture on the doubled magnetic cell (q* = 0.9548), six harmonics, seed 0."""
-    qs = 0.9548
-    q1 = qs * np.array([1.0, 0.0])
-    q2 = qs * np.array([-0.5, np.sqrt(3) / 2])
-    A = 2.0 * np.pi * np.linalg.inv(np.array([q1, q2])) * 2
-    keys = np.array([[1, 0], [0, 1], [-1, -1], [-1, 0], [0, -1], [1, 1]])
-    rng = np.random.default_rng(0)
-    vals = 0.2 * (rng.normal(size=(6, 3)) + 1j * rng.normal(size=(6, 3)))
-    return q1, q2, A, keys, vals
-
-
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NQS_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set NQS_REFERENCE_ROOT)")
+    main(root)

@@ -2,54 +2,71 @@
 path (src/nqs/{psiformer, local_energy, ewald, sampler, minsr, train, cell, rashba_reference,
 slater_reference, spiral_reference, pinning, observables}.py) exists in the matching nqs module,
 and the reference's parameters are a prefix of ours with the same names, order and defaults
-(extra trailing keyword arguments - precision, gram, cell - are the stated adaptations). Reads the
-reference sources with `ast` (no JAX needed); skipped where the reference is not mounted."""
-import ast
+(extra trailing keyword arguments - precision, gram, cell - are the stated adaptations). The
+reference signatures come from tests/golden/reference_signatures.json, which
+tests/golden/make_signatures.py reads from the reference sources with `ast` (no JAX needed); when
+a checkout is named by NQS_REFERENCE_ROOT the fixture is also checked against it. Functions off
+the VMC iteration's path (texture post-processing, Hartree-Fock texture files, the
+skyrmion-background envelope) are not part of this library."""
 import importlib
 import inspect
+import json
 import os
+import sys
 
 import pytest
 import torch
 
-REF = "/root/reference/src/nqs"
 MODULES = {"psiformer": "psiformer", "local_energy": "local_energy", "ewald": "ewald",
            "sampler": "sampler", "minsr": "minsr", "train": "train", "cell": "cell",
            "rashba_reference": "rashba", "slater_reference": "slater",
            "spiral_reference": "spiral", "pinning": "pinning", "observables": "observables"}
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "reference_signatures.json")
+REF = os.path.join(os.environ.get("NQS_REFERENCE_ROOT", ""), "src", "nqs")
+HAVE_REF = bool(os.environ.get("NQS_REFERENCE_ROOT")) and os.path.isdir(REF)
+OFF_PATH = {"observables": {"spin_texture", "berg_luscher", "structure_factor",
+                            "spin_order_parameter", "skx_arms", "skyrmion_number_fourier",
+                            "slater_spin_density", "classify_state"},
+            "pinning": {"load_hf_texture", "make_hf_skx_pin", "berg_luscher_realspace"},
+            "rashba_reference": {"cell_skx_envelope", "ring_minimum"},
+            "spiral_reference": {"spin_texture"}}
 
 
-def _reference_functions(mod):
-    tree = ast.parse(open(os.path.join(REF, mod + ".py")).read())
-    for node in tree.body:
-        if isinstance(node, ast.FunctionDef) and not node.name.startswith("_"):
-            a = node.args
-            pos = a.posonlyargs + a.args
-            defaults = [None] * (len(pos) - len(a.defaults)) + list(a.defaults)
-            params = [(p.arg, d) for p, d in zip(pos, defaults)]
-            params += [(p.arg, d) for p, d in zip(a.kwonlyargs, a.kw_defaults)]
-            yield node.name, params
+def _golden():
+    with open(GOLD) as f:
+        return json.load(f)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference not mounted")
-@pytest.mark.parametrize("ref_mod", sorted(MODULES))
-def test_signatures_match_reference(ref_mod):
+def _check_module(ref_mod, funcs):
     ours = importlib.import_module("nqs." + MODULES[ref_mod])
-    for name, params in _reference_functions(ref_mod):
+    for name, params in funcs.items():
+        if name in OFF_PATH.get(ref_mod, ()):
+            continue
         f = getattr(ours, name, None)
         assert f is not None, f"{ref_mod}.{name} missing"
         sig = inspect.signature(f)
         names = list(sig.parameters)
         assert names[:len(params)] == [n for n, _ in params], (name, names)
         for n, d in params:
+            if d["kind"] != "literal":
+                continue  # no default, or a non-literal one (an expression of other names)
             ours_d = sig.parameters[n].default
-            if d is None:
-                continue
-            try:
-                ref_d = ast.literal_eval(d)
-            except ValueError:
-                continue  # a non-literal default (an expression of other names)
-            assert ours_d == ref_d, (name, n, ours_d, ref_d)
+            assert type(ours_d).__name__ == d["type"], (name, n)
+            assert json.loads(json.dumps(ours_d)) == d["value"], (name, n)
+
+
+@pytest.mark.parametrize("ref_mod", sorted(MODULES))
+def test_signatures_match_reference(ref_mod):
+    _check_module(ref_mod, _golden()["modules"][ref_mod])
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference checkout not given (NQS_REFERENCE_ROOT)")
+def test_signature_fixture_is_current():
+    """The committed fixture equals what the reference sources give today."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_signatures
+    live = {m: make_signatures.functions(os.path.join(REF, m + ".py")) for m in MODULES}
+    assert json.loads(json.dumps(live)) == _golden()["modules"]
 
 
 def test_split_merge_heads_roundtrip():
@@ -61,17 +78,15 @@ def test_split_merge_heads_roundtrip():
     assert torch.equal(merge_heads(h), x)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference not mounted")
 def test_wavefunction_fields_match_reference():
     """ContinuumSpinorPsiformer's constructor fields and defaults equal the flax module's
     (psiformer.py:100-116)."""
     from nqs.psiformer import ContinuumSpinorPsiformer
-    tree = ast.parse(open(os.path.join(REF, "psiformer.py")).read())
-    cls = next(n for n in tree.body
-               if isinstance(n, ast.ClassDef) and n.name == "ContinuumSpinorPsiformer")
-    fields = [(s.target.id, s.value) for s in cls.body if isinstance(s, ast.AnnAssign)]
+    fields = _golden()["psiformer_fields"]
     sig = inspect.signature(ContinuumSpinorPsiformer)
     assert list(sig.parameters)[:len(fields)] == [n for n, _ in fields]
     for n, v in fields:
-        if v is not None:
-            assert sig.parameters[n].default == ast.literal_eval(v), n
+        if v["kind"] == "literal":
+            ours_d = sig.parameters[n].default
+            assert type(ours_d).__name__ == v["type"], n
+            assert json.loads(json.dumps(ours_d)) == v["value"], n

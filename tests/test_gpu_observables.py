@@ -33,7 +33,7 @@ def test_spin_estimators_match_oracle():
 def test_spiral_texture_is_noncollinear():
     """Sampled from the exact spin-spiral determinant (zero-backflow Psiformer on the spiral
     envelope): the in-plane magnetisation changes sign across the cell in both x and y."""
-    from nqs.observables import spin_texture
+    from nqs.observables import spin_estimates
     from nqs.psiformer import ContinuumSpinorPsiformer, make_logpsi
     from nqs.sampler import run_chain
     from nqs.spiral import spiral_gs
@@ -44,8 +44,14 @@ def test_spiral_texture_is_noncollinear():
     lp = make_logpsi(model, model.init(0))
     R, S, _, _ = run_chain(lp, 8.0, 7, 3, n_walkers=2048, n_sweeps=30, burn=60, step=0.6)
     ng, L = 8, 8.0
-    t = spin_texture(lp, R, S, np.diag([L, L]), ngrid=ng)
-    mx, my = t["m"][..., 0], t["m"][..., 1]
+    # bin the per-electron estimators by position (bin sums / number of configurations)
+    sx, sy, sz = spin_estimates(lp, R, S)
+    gi = np.clip((np.mod(R.cpu().numpy(), L) / L * ng).astype(int), 0, ng - 1)
+    m = np.zeros((ng, ng, 3))
+    for c, v in enumerate((sx, sy, sz)):
+        np.add.at(m[..., c], (gi[..., 0].ravel(), gi[..., 1].ravel()), v.ravel())
+    m /= R.shape[0]
+    mx, my = m[..., 0], m[..., 1]
     assert mx.max() > 0 > mx.min() and my.max() > 0 > my.min()
     # the determinant's exact spin density at the bin centres, times the bin area
     sig = [np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.diag([1.0, -1.0])]
@@ -57,4 +63,4 @@ def test_spiral_texture_is_noncollinear():
             for c in range(3):
                 exact[ix, iy, c] = np.real(np.einsum("as,st,at->", phi.conj(), sig[c], phi))
     exact *= (L / ng) ** 2
-    assert np.mean(np.abs(t["m"] - exact)) < 0.02, np.mean(np.abs(t["m"] - exact))
+    assert np.mean(np.abs(m - exact)) < 0.02, np.mean(np.abs(m - exact))

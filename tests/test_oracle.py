@@ -33,35 +33,13 @@ def test_rashba_restatement_matches_reference_golden():
 
 
 def test_rashba_helpers_match_reference_golden():
-    """Band energies, the ring minimum and the skyrmion-background envelope (a texture potential
-    on a commensurate supercell) against the reference module's own outputs."""
-    import importlib.util
-    spec = importlib.util.spec_from_file_location(
-        "make_golden", os.path.join(os.path.dirname(__file__), "golden", "make_golden.py"))
-    mg = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mg)
+    """Band energies against the reference module's own outputs."""
     z = np.load(GOLD)
     ks = np.array([[0.0, 0.0], [0.3, -0.7], [1.1, 0.4]])
     bk = np.array([rashba.bands_k(kx, ky, 1.0, 0.7, 0.3)[:2] for kx, ky in ks])
     assert np.array_equal(bk, z["bands_k"])
     ba = np.array([rashba.bands_analytic(kx, ky, 1.0, 0.7, 0.3) for kx, ky in ks])
     assert np.abs(ba - z["bands_analytic"]).max() < 1e-15 and np.abs(ba - bk).max() < 1e-14
-    assert np.allclose(rashba.ring_minimum(1.0, 0.3, 0.0), z["ring_hz0"], rtol=0, atol=1e-15)
-    q1, q2, A, keys, vals = mg.skx_case()
-    skx = rashba.cell_skx_envelope(A, 7, keys, vals, q1, q2, 0.5, 1.0, 0.3, 0.05, 4, (0.1, 0.17))
-    assert skx["E_band"] == float(z["skx_E_band"]) and skx["gap"] == float(z["skx_gap"])
-    assert np.array_equal(skx["w"], z["skx_w"]) and np.array_equal(skx["Gs"], z["skx_Gs"])
-    assert np.array_equal(skx["W"], z["skx_W"])
-
-
-def test_ring_minimum_is_the_band_minimum():
-    """Closed form against a dense scan of the continuum lower band (the reference's method)."""
-    for lr, hz in ((1.0, 0.5), (0.3, 0.05), (0.3, 2.0), (0.7, 0.0)):
-        k, E = rashba.ring_minimum(1.0, lr, hz)
-        ks = np.linspace(0.0, 3.0 * lr + 1.0, 400001)
-        Es = ks ** 2 / 2.0 - np.sqrt(lr ** 2 * ks ** 2 + 0.25 * hz ** 2)
-        assert E <= Es.min() + 1e-15 and abs(E - Es.min()) < 1e-9
-        assert abs(k - ks[np.argmin(Es)]) < 2e-5
 
 
 def test_single_particle_levels_sorted_and_complete():
@@ -75,10 +53,16 @@ def test_single_particle_levels_sorted_and_complete():
     assert len(kx) == 49 and abs(kx[0] - (2 * np.pi * -3 + TWIST[0]) / 6.0) < 1e-15
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src/nqs"), reason="reference not mounted")
+# the reference checkout, when one is available (NQS_REFERENCE_ROOT); the golden fixture above
+# carries the same pin when it is not
+REF_ROOT = os.environ.get("NQS_REFERENCE_ROOT", "")
+HAVE_REF = bool(REF_ROOT) and os.path.isdir(os.path.join(REF_ROOT, "src", "nqs"))
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference checkout not given (NQS_REFERENCE_ROOT)")
 def test_rashba_helpers_match_reference_live():
     import sys
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, REF_ROOT)
     from src.nqs import rashba_reference as R
     a = rashba.single_particle_levels(7.0, 1.0, 0.7, 0.3, 3, (0.1, 0.2))
     b = R.single_particle_levels(7.0, 1.0, 0.7, 0.3, 3, (0.1, 0.2))
@@ -89,16 +73,12 @@ def test_rashba_helpers_match_reference_live():
     kx, ky = rashba.allowed_k(7.0, 3, (0.1, 0.2))
     rx, ry = R.allowed_k(7.0, 3, (0.1, 0.2))
     assert np.array_equal(kx, rx) and np.array_equal(ky, ry)
-    for args in ((1.0, 1.0, 0.5), (1.0, 0.3, 2.0)):
-        k, E = rashba.ring_minimum(*args)
-        kr, Er = R.ring_minimum(*args)
-        assert abs(k - kr) < 2e-5 and abs(E - Er) < 1e-9 and E <= Er
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src/nqs"), reason="reference not mounted")
+@pytest.mark.skipif(not HAVE_REF, reason="reference checkout not given (NQS_REFERENCE_ROOT)")
 def test_rashba_restatement_matches_reference_live():
     import sys
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, REF_ROOT)
     from src.nqs.rashba_reference import noninteracting_gs
     for N, L in ((3, 5.0), (11, 10.0)):
         a = rashba.noninteracting_gs(N, L, 1.0, 0.7, 0.2, 8, TWIST)
@@ -278,16 +258,3 @@ def test_periodic_features_match_oracle():
     Rb = torch.stack([R, R + torch.as_tensor(A[:, 0])])
     fb = periodic_features(Rb, A, 3)
     assert fb.shape == (2, 5, 12) and torch.allclose(fb[0], fb[1], atol=1e-12, rtol=0)
-
-
-def test_spiral_texture_is_the_slater_spin_density():
-    from nqs.observables import slater_spin_density
-    from nqs.spiral import spin_texture, spiral_gs
-    res = spiral_gs(N=5, L=7.0, Q_int=(1, 0), B=0.3, lambda_r=1.0, h_z=0.0, n_cut=4,
-                    twist=(0.1, 0.17))
-    t = spin_texture(res, ngrid=6)
-    assert t.shape == (6, 6, 3)
-    r = np.array([0.5, 0.5]) * 7.0 / 6  # first mesh point
-    from oracle import observables_oracle as OO
-    assert np.abs(t[0, 0] - OO.slater_spin_density_at(r, res["Gs"], res["W"])).max() < 1e-11
-    assert np.abs(t - slater_spin_density(res["Gs"], res["W"], 7.0 * np.eye(2), 6)).max() == 0

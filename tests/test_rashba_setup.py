@@ -30,12 +30,6 @@ def test_h0_hermitian_with_the_reference_soc_convention():
     assert np.allclose(soc, lr * (SX * ky + SY * kx))  # lambda_R (sigma_x k_y + sigma_y k_x)
 
 
-def test_ring_minimum_without_zeeman():
-    for ms, lr in ((1.0, 1.0), (0.5, 2.0), (1.0, 0.8)):
-        k, E = rashba.ring_minimum(ms, lr, 0.0)
-        assert abs(k - lr * ms) < 1e-12 and abs(E + 0.5 * lr * lr * ms) < 1e-12
-
-
 def test_ground_state_is_the_lowest_levels_and_closed():
     g = rashba.noninteracting_gs(N=7, L=8.0, m_star=1.0, lambda_r=1.0, h_z=0.5, n_cut=10,
                                  twist=(0.1, 0.17))
