@@ -1393,6 +1393,35 @@ __global__ void k_adam(double* __restrict__ th, const double* __restrict__ g, do
   th[i] -= lr * (mi / c1) / (sqrt(vi / c2) + eps);
 }
 
+// The same step with optax's treatment of complex leaves (the reference's train.py applies
+// optax.adam to jax.grad of a real loss). For a complex leaf element c = a + i b JAX's gradient is
+// the complex number G = dL/da - i dL/db, optax keeps one complex first moment m_c of G and one
+// real second moment v of |G|^2, and c <- c - lr (m_c/c1) / (sqrt(v/c2) + eps). On the real ravel
+// (re block, im block) that is: the re component's first moment tracks dL/da, the im component's
+// tracks -dL/db, both share v (|G|^2 = (dL/da)^2 + (dL/db)^2). partner[k] is the index of the
+// other component of k's complex element, or -1 for a real parameter; g is the real-ravel
+// gradient (dL/da, dL/db). Both components compute the same v.
+__global__ void k_adam_complex(double* __restrict__ th, const double* __restrict__ g,
+                               double* __restrict__ m, double* __restrict__ v,
+                               const int64_t* __restrict__ partner, int64_t n, double lr,
+                               double b1, double b2, double eps, double c1, double c2) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double gk = g[k];
+  const int64_t q = partner[k];
+  double gm = gk, sq = gk * gk;
+  if (q >= 0) {
+    const double gq = g[q];
+    if (q < k) gm = -gk;  // the imaginary component: G = dL/da - i dL/db
+    sq = q < k ? gq * gq + gk * gk : gk * gk + gq * gq;  // same rounding on both components
+  }
+  const double mk_ = b1 * m[k] + (1.0 - b1) * gm;
+  const double vk = b2 * v[k] + (1.0 - b2) * sq;
+  m[k] = mk_;
+  v[k] = vk;
+  th[k] -= lr * (mk_ / c1) / (sqrt(vk / c2) + eps);
+}
+
 __global__ void k_axpy(int n, const double* __restrict__ a, double* __restrict__ y) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += a[i];
@@ -1704,9 +1733,14 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
 int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int W, int64_t P,
                         double* out_grad, void* wsp, size_t wsb, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
-  if (!O || !e || !out_grad || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || !wsp ||
-      wsb < sizeof(double) * 2 * (size_t)W + 256)
+  if (!O || !e || !out_grad || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || !wsp) {
+    set_error("nqs_energy_gradient: invalid argument");
     return NQS_ERR_INVALID_ARG;
+  }
+  if (wsb < sizeof(double) * 2 * (size_t)W + 256) {
+    set_error("nqs_energy_gradient: workspace %zu < %zu", wsb, sizeof(double) * 2 * (size_t)W + 256);
+    return NQS_ERR_WORKSPACE;
+  }
   double* x = (double*)wsp;
   k_center_eps<<<1, 1024, 0, st>>>((const cplx*)e, W, x);
   NQS_CHECK_LAUNCH("k_center_eps");
@@ -1737,7 +1771,8 @@ double* g_eg_scratch_ptr[kScratchDevices];  // address of g_eg_scratch per devic
 }  // namespace
 
 // Resolves the scratch address of the current device once (cudaGetSymbolAddress with that
-// device current) and caches it per ordinal.
+// device current) and caches it per ordinal for the life of the process (a device reset while
+// the library is loaded would leave the cached address stale; that is documented as unsupported).
 static int eg_scratch(double** out) {
   int dev = -1;
   cudaError_t rc = cudaGetDevice(&dev);
@@ -1801,6 +1836,20 @@ int nqs_adam_update(double* theta, const double* grad, double* m, double* v, int
   k_adam<<<(unsigned)((P + 255) / 256), 256, 0, (cudaStream_t)stream>>>(theta, grad, m, v, P, lr,
                                                                          b1, b2, eps, c1, c2);
   NQS_CHECK_LAUNCH("k_adam");
+  return NQS_OK;
+}
+
+int nqs_adam_update_complex(double* theta, const double* grad, double* m, double* v,
+                            const int64_t* partner, int64_t P, double lr, double b1, double b2,
+                            double eps, int t, void* stream) {
+  if (!theta || !grad || !m || !v || !partner || P < 1 || t < 1) {
+    set_error("nqs_adam_update_complex: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  const double c1 = 1.0 - pow(b1, (double)t), c2 = 1.0 - pow(b2, (double)t);
+  k_adam_complex<<<(unsigned)((P + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      theta, grad, m, v, partner, P, lr, b1, b2, eps, c1, c2);
+  NQS_CHECK_LAUNCH("k_adam_complex");
   return NQS_OK;
 }
 

@@ -91,13 +91,21 @@ HeadParams make_head_params(const NqsModelDesc& d, const double* theta64);
 // theta float64 -> float32 copy
 int theta_to_f32(const double* theta, float* out, int64_t n, cudaStream_t st);
 
-// Reverse mode: per-sample Jacobian rows (Re in [0,W), Im in [W,2W)) of a [2W][P] matrix.
+// Reverse mode: per-sample Jacobian rows (Re in [0,W), Im in [W,2W)) of a [2W][P] matrix, or
+// the vector-Jacobian product grad[k] = sum_w Re(ct_w O[w][k]) without O. ckpt: keep only each
+// transformer block's input and recompute the block's activations before its reverse step.
+template <typename T>
+size_t backward_scratch(const ModelConst& mc, int W, bool ckpt);
 template <typename T>
 size_t per_sample_O_scratch(const ModelConst& mc, int W);
 template <typename T, typename TO>
 int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
-                     const double* R, const int32_t* S, int W, TO* O, Arena& ws,
+                     const double* R, const int32_t* S, int W, TO* O, bool ckpt, Arena& ws,
                      cudaStream_t st);
+template <typename T>
+int logpsi_vjp_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                   const double* R, const int32_t* S, int W, const cplx* ct, double* grad,
+                   bool ckpt, Arena& ws, cudaStream_t st);
 
 // tensor-core row GEMM (gemm_tc.cu)
 bool rowgemm_tc_ok(int K, int ldx, int Nout);

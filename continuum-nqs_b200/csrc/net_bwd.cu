@@ -5,8 +5,17 @@
 // log psi is complex and holomorphic in the complex parameters, the backbone is real, so every
 // real activation carries a complex adjoint stored as two channels (re, im) and pushed through the
 // real layers independently. For a complex leaf c = a + i b, dL/da = dL/dc and dL/db = i dL/dc.
-// The forward pass is recomputed per chunk of walkers with every block's activations kept
-// (attention probabilities are recomputed from q, k inside the attention backward).
+// The forward pass is recomputed per chunk of walkers. By default every block's activations are
+// kept; with per-block checkpointing only each block's input is kept and the block's forward is
+// recomputed from it just before its reverse step (same kernels, same inputs: the recomputed
+// activations are bit-identical, so is O). Attention probabilities are always recomputed from
+// q, k inside the attention backward.
+//
+// The adjoints reach the parameters through a writer: ORows stores each walker's two Jacobian
+// rows; VjpAcc contracts them with a per-walker complex cotangent c_w on the fly,
+//   grad_k += Re(c_w O[w][k]),
+// so a vector-Jacobian product never materialises O (src/nqs/train.py:53-59 differentiates the
+// surrogate 2 mean Re[conj(e - mean e) log psi] this way).
 #include <cstdio>
 #include <algorithm>
 
@@ -19,6 +28,7 @@ namespace nqs {
 // --------------------------------------------------------------------------------------------
 template <typename TO>
 struct ORows {
+  static constexpr bool kVjp = false;
   TO* O;
   int64_t P;
   int W;  // total walkers (Im rows start at W)
@@ -31,6 +41,23 @@ struct ORows {
                                         double gim) const {
     put(w, off + e, gre, gim);        // d/d Re c = g
     put(w, off + n + e, -gim, gre);   // d/d Im c = i g
+  }
+};
+
+// contraction writer of the vector-Jacobian product: grad[col] += Re(c_w (re + i im)), double
+// atomics (grad zeroed by the caller)
+struct VjpAcc {
+  static constexpr bool kVjp = true;
+  double* grad;
+  const cplx* ct;  // cotangent per walker (global walker index)
+  __device__ __forceinline__ void put(int w, int64_t col, double re, double im) const {
+    const cplx c = ct[w];
+    atomicAdd(grad + col, c.re * re - c.im * im);
+  }
+  __device__ __forceinline__ void put_c(int w, int64_t off, int64_t n, int64_t e, double gre,
+                                        double gim) const {
+    put(w, off + e, gre, gim);
+    put(w, off + n + e, -gim, gre);
   }
 };
 
@@ -139,14 +166,130 @@ static int launch_wgrad(int nw, int N, int d_in, int d_out, const T* X, int ldx,
 }
 
 // --------------------------------------------------------------------------------------------
+// weight gradient of a Dense layer contracted with the cotangent and summed over walkers:
+//   H[i][o] = sum_rows X[row][i] (c_w(row) Ybar[row][o])   (complex; i == d_in is the bias, X = 1)
+// grid (ceil((d_in + 1) / 32), ceil(d_out / 64), row slices); each CTA reduces its rows in
+// registers (4 inputs x 4 outputs x 2 parts per thread, operands staged 32 rows at a time) and
+// adds to grad with double atomics: real leaf += Re H, complex leaf Re part += Re H, Im part
+// -= Im H (d/d Im c = i d/dc).
+// --------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) k_wgrad_vjp(int rows, int N, int d_in, int d_out,
+                                                   const T* __restrict__ X, int ldx,
+                                                   const T* __restrict__ Yb, int ldy,
+                                                   const cplx* __restrict__ ct, int w0,
+                                                   double* __restrict__ grad, int64_t off_k,
+                                                   int64_t off_b, int is_complex,
+                                                   int rows_per_cta) {
+  constexpr int TI = 32, TO = 64, RB = 32;
+  __shared__ T xs[RB][TI];
+  __shared__ T ysr[RB][TO], ysi[RB][TO];
+  const int i0 = blockIdx.x * TI, o0 = blockIdx.y * TO;
+  const int r0 = blockIdx.z * rows_per_cta, r1 = min(rows, r0 + rows_per_cta);
+  const int tid = threadIdx.x, ti = tid >> 4, to = tid & 15;  // inputs 4 ti + v, outputs to + 16 u
+  T ar[4][4], ai[4][4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ar[v][u] = ai[v][u] = T(0);
+  for (int rb = r0; rb < r1; rb += RB) {
+    for (int idx = tid; idx < RB * TI; idx += blockDim.x) {
+      const int r = idx / TI, i = idx - r * TI, row = rb + r, ii = i0 + i;
+      T v = T(0);
+      if (row < r1) v = ii < d_in ? X[(size_t)row * ldx + ii] : (ii == d_in ? T(1) : T(0));
+      xs[r][i] = v;
+    }
+    for (int idx = tid; idx < RB * TO; idx += blockDim.x) {
+      const int r = idx / TO, o = idx - r * TO, row = rb + r, oo = o0 + o;
+      T vr = T(0), vi = T(0);
+      if (row < r1 && oo < d_out) {
+        const cplx c = ct[w0 + row / N];
+        const T a = Yb[((size_t)row * 2) * ldy + oo], b = Yb[((size_t)row * 2 + 1) * ldy + oo];
+        vr = (T)c.re * a - (T)c.im * b;
+        vi = (T)c.re * b + (T)c.im * a;
+      }
+      ysr[r][o] = vr;
+      ysi[r][o] = vi;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < RB; ++r) {
+      T xv[4], yr[4], yi[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) xv[v] = xs[r][4 * ti + v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        yr[u] = ysr[r][to + 16 * u];
+        yi[u] = ysi[r][to + 16 * u];
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          ar[v][u] = fma(xv[v], yr[u], ar[v][u]);
+          ai[v][u] = fma(xv[v], yi[u], ai[v][u]);
+        }
+    }
+    __syncthreads();
+  }
+  if (r0 >= r1) return;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const int i = i0 + 4 * ti + v;
+    if (i > d_in) continue;
+    const int64_t base = i < d_in ? off_k : off_b;
+    if (base < 0) continue;
+    const int64_t n = i < d_in ? (int64_t)d_in * d_out : (int64_t)d_out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int o = o0 + to + 16 * u;
+      if (o >= d_out) continue;
+      const int64_t e = i < d_in ? (int64_t)i * d_out + o : (int64_t)o;
+      atomicAdd(grad + base + e, (double)ar[v][u]);
+      if (is_complex) atomicAdd(grad + base + n + e, -(double)ai[v][u]);
+    }
+  }
+}
+
+template <typename T>
+static int launch_wgrad_vjp(int nw, int N, int d_in, int d_out, const T* X, int ldx,
+                            const T* Yb, int ldy, const VjpAcc& o, int w0, int64_t off_k,
+                            int64_t off_b, int is_c, cudaStream_t st) {
+  const int rows = nw * N;
+  const int gi = (d_in + 1 + 31) / 32, go = (d_out + 63) / 64;
+  // about four CTAs per SM in total, at least 64 rows per slice
+  int slices = std::max(1, std::min((rows + 63) / 64, 592 / std::max(1, gi * go)));
+  const int per = (rows + slices - 1) / slices;
+  slices = (rows + per - 1) / per;
+  k_wgrad_vjp<T><<<dim3(gi, go, slices), 128, 0, st>>>(rows, N, d_in, d_out, X, ldx, Yb, ldy, o.ct,
+                                                       w0, o.grad, off_k, off_b, is_c, per);
+  NQS_CHECK_LAUNCH("k_wgrad_vjp");
+  return NQS_OK;
+}
+
+// the weight-gradient step of either writer
+template <typename T, typename TO>
+static int wgrad(const ORows<TO>& o, int nw, int N, int d_in, int d_out, const T* X, int ldx,
+                 const T* Yb, int ldy, int w0, int64_t off_k, int64_t off_b, int is_c,
+                 cudaStream_t st) {
+  return launch_wgrad<T, TO>(nw, N, d_in, d_out, X, ldx, Yb, ldy, o, w0, off_k, off_b, is_c, st);
+}
+template <typename T>
+static int wgrad(const VjpAcc& o, int nw, int N, int d_in, int d_out, const T* X, int ldx,
+                 const T* Yb, int ldy, int w0, int64_t off_k, int64_t off_b, int is_c,
+                 cudaStream_t st) {
+  return launch_wgrad_vjp<T>(nw, N, d_in, d_out, X, ldx, Yb, ldy, o, w0, off_k, off_b, is_c, st);
+}
+
+// --------------------------------------------------------------------------------------------
 // LayerNorm backward (one CTA per walker): x rows [tok][d], Ybar [tok][2][d]
 //   z = (x - mu) rho, zbar = ybar g, xbar = rho (zbar - mean(zbar) - z mean(zbar z))
 //   dL/dscale = sum_tok ybar z, dL/dbias = sum_tok ybar
 // --------------------------------------------------------------------------------------------
-template <typename T, typename TO>
+template <typename T, class Wr>
 __global__ void __launch_bounds__(256) k_ln_bwd(int N, int d, const T* __restrict__ X,
                                                 const T* __restrict__ Yb, const T* __restrict__ g,
-                                                T* __restrict__ Xb, int accumulate, ORows<TO> o,
+                                                T* __restrict__ Xb, int accumulate, Wr o,
                                                 int w0, int64_t off_scale, int64_t off_bias) {
   constexpr int Q = NQS_MAX_EMBED / 32;
   const int wl = blockIdx.x, w = w0 + wl;
@@ -367,11 +510,11 @@ inline size_t head_bwd_smem(int N, int nG, int K, bool env_grad) {
   return nc * 16 + 2 * N * sizeof(double) + (N + 2) * sizeof(int);
 }
 
-template <typename TIN, typename T, typename TO>
+template <typename TIN, typename T, class Wr>
 __global__ void __launch_bounds__(256) k_head_bwd(JobBatch jb, ModelConst mc,
                                                   const TIN* __restrict__ BF, int ldbf,
                                                   HeadParams hp, T* __restrict__ X1,
-                                                  T* __restrict__ X2, ORows<TO> o,
+                                                  T* __restrict__ X2, Wr o,
                                                   HeadOffsets off) {
   const int wl = blockIdx.x;
   const int N = jb.N, nG = mc.nG, K = mc.K, KN = K * N;
@@ -543,46 +686,110 @@ __global__ void __launch_bounds__(256) k_head_bwd(JobBatch jb, ModelConst mc,
 // --------------------------------------------------------------------------------------------
 template <typename T>
 struct SaveBufs {
+  // per block: the block input; with all activations kept, also every intermediate (with
+  // checkpointing the intermediates live in slot 0 and are recomputed per block)
   T *xin[NQS_MAX_DEPTH], *h0[NQS_MAX_DEPTH], *qkv[NQS_MAX_DEPTH], *ao[NQS_MAX_DEPTH];
   T *xmid[NQS_MAX_DEPTH], *h1[NQS_MAX_DEPTH], *a0[NQS_MAX_DEPTH], *g0[NQS_MAX_DEPTH];
   T *xL, *hf, *bf, *feat;
   T *xb, *hb, *big, *X1, *X2;
 };
 
-template <typename T>
-size_t bwd_row_elems(const ModelConst& mc) {
-  const size_t d = mc.d, D = (size_t)mc.ff * d, KN = (size_t)mc.K * mc.N;
-  const size_t per_block = 6 * d + 3 * d + 2 * D - d;  // xin h0 qkv(3d) ao xmid h1 a0 g0
-  const size_t big = std::max({6 * d, 2 * D, 2 * KN});
-  return (size_t)mc.depth * per_block + 2 * d + 2 * KN + (4 * mc.nf + 2) + 2 * d + 2 * d + big +
-         4 * KN;
+// elements per activation row of one block's intermediates (h0 qkv(3d) ao xmid h1 a0 g0)
+static size_t block_inter_elems(const ModelConst& mc) {
+  const size_t d = mc.d, D = (size_t)mc.ff * d;
+  return 7 * d + 2 * D;
 }
 
-size_t bwd_chunk_walkers(const ModelConst& mc, int W) {
-  const size_t rows = (size_t)1 << 17;
+template <typename T>
+size_t bwd_row_elems(const ModelConst& mc, bool ckpt) {
+  const size_t d = mc.d, D = (size_t)mc.ff * d, KN = (size_t)mc.K * mc.N;
+  const size_t inter = block_inter_elems(mc);
+  const size_t blocks = (size_t)mc.depth * d + (ckpt ? (mc.depth ? inter : 0) : mc.depth * inter);
+  const size_t big = std::max({6 * d, 2 * D, 2 * KN});
+  return blocks + d /* xL */ + d /* hf */ + 2 * KN /* bf */ + (4 * mc.nf + 2) + 2 * d + 2 * d +
+         big + 4 * KN;
+}
+
+// walkers per chunk: 2^17 activation rows with every block kept; with checkpointing the rows
+// that fit in the same bytes, at most 2^18 (the two-channel adjoint GEMMs then see at most 2^19
+// rows, the forward network's chunk limit)
+template <typename T>
+size_t bwd_chunk_walkers(const ModelConst& mc, int W, bool ckpt) {
+  size_t rows = (size_t)1 << 17;
+  if (ckpt)
+    rows = std::min<size_t>((size_t)1 << 18,
+                            rows * bwd_row_elems<T>(mc, false) / bwd_row_elems<T>(mc, true));
   return std::max<size_t>(1, std::min<size_t>((size_t)W, rows / mc.N));
 }
 
 template <typename T>
-size_t per_sample_O_scratch(const ModelConst& mc, int W) {
-  const size_t nw = bwd_chunk_walkers(mc, W);
-  return nw * mc.N * bwd_row_elems<T>(mc) * sizeof(T) + 64 * 256;
+size_t backward_scratch(const ModelConst& mc, int W, bool ckpt) {
+  const size_t nw = bwd_chunk_walkers<T>(mc, W, ckpt);
+  return nw * mc.N * bwd_row_elems<T>(mc, ckpt) * sizeof(T) + 64 * 256;
 }
 
-template <typename T, typename TO>
-int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
-                     const double* R, const int32_t* S, int W, TO* O, Arena& ws,
-                     cudaStream_t st) {
+template <typename T>
+size_t per_sample_O_scratch(const ModelConst& mc, int W) {
+  return backward_scratch<T>(mc, W, false);
+}
+
+// forward of block l from x = b.xin[l] into the block's intermediates (slot s), and, when y is
+// given, its output y = xmid + W1 GELU(W0 LN1 xmid) + b1
+template <typename T>
+static int block_forward(const ModelConst& mc, const BlockW<T>& bw, SaveBufs<T>& b, int l, int s,
+                         int nw, T* y, cudaStream_t st) {
+  const int N = mc.N, d = mc.d, D = mc.ff * d, H = mc.H, nt = nw * N;
+  const T* x = b.xin[l];
+  NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[s], st));
+  GemmArgs<T> g{};
+  g.X = b.h0[s]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+  g.Y = b.qkv[s]; g.ldy = 3 * d; g.nseg = 3;
+  g.seg[0] = GemmSeg<T>{bw.wq, bw.bq, d, d, 0, 0};
+  g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
+  g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
+  NQS_TRY(launch_gemm<T>(g, st));
+  NQS_TRY(launch_attention<T>(nw, N, 1, 0, 0, d, H, b.qkv[s], b.ao[s], st));
+  g = GemmArgs<T>{};
+  g.X = b.ao[s]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+  g.Y = b.xmid[s]; g.ldy = d; g.Res = x; g.ldr = d; g.nseg = 1;
+  g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
+  NQS_TRY(launch_gemm<T>(g, st));
+  NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xmid[s], bw.ln1_s, bw.ln1_b, b.h1[s], st));
+  g = GemmArgs<T>{};
+  g.X = b.h1[s]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
+  g.Y = b.a0[s]; g.ldy = D; g.nseg = 1;
+  g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
+  NQS_TRY(launch_gemm<T>(g, st));
+  cudaMemcpyAsync(b.g0[s], b.a0[s], sizeof(T) * (size_t)nt * D, cudaMemcpyDeviceToDevice, st);
+  const size_t nel = (size_t)nt * D;
+  k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, 1, 0, 0, D, b.g0[s]);
+  NQS_CHECK_LAUNCH("k_gelu");
+  if (y) {
+    g = GemmArgs<T>{};
+    g.X = b.g0[s]; g.ldx = D; g.rows = nt; g.K = D; g.C = 1;
+    g.Y = y; g.ldy = d; g.Res = b.xmid[s]; g.ldr = d;
+    g.nseg = 1;
+    g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
+    NQS_TRY(launch_gemm<T>(g, st));
+  }
+  return NQS_OK;
+}
+
+template <typename T, class Wr>
+static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                        const double* R, const int32_t* S, int W, const Wr& wr, bool ckpt,
+                        Arena& ws, cudaStream_t st) {
   const ModelConst& mc = hm.mc;
   const NqsModelDesc& dsc = hm.desc;
   const int N = mc.N, d = mc.d, D = mc.ff * d, KN = mc.K * N, H = mc.H;
   const int Fp = 4 * mc.nf + 2;
-  const int nwc = (int)bwd_chunk_walkers(mc, W);
+  const int nwc = (int)bwd_chunk_walkers<T>(mc, W, ckpt);
   const size_t rows = (size_t)nwc * N;
   const size_t save = ws.used;
   SaveBufs<T> b{};
   for (int l = 0; l < mc.depth; ++l) {
     b.xin[l] = ws.take<T>(rows * d);
+    if (ckpt && l > 0) continue;
     b.h0[l] = ws.take<T>(rows * d);
     b.qkv[l] = ws.take<T>(rows * 3 * d);
     b.ao[l] = ws.take<T>(rows * d);
@@ -601,18 +808,17 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
   b.X1 = ws.take<T>(rows * 2 * KN);
   b.X2 = ws.take<T>(rows * 2 * KN);
   if (!b.X2) {
-    set_error("workspace too small for the per-sample Jacobian");
+    set_error("workspace too small for the reverse pass");
     return NQS_ERR_WORKSPACE;
   }
-  ORows<TO> orows{O, dsc.n_params, W};
   const size_t hsm = head_bwd_smem(N, mc.nG, mc.K, mc.learnable_env);
   const size_t absm = sizeof(T) * (size_t)(5 * N * (d / H) + 2 * N * N + N);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_head_bwd<T, T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_head_bwd<T, T, Wr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          220 * 1024);
     cudaFuncSetAttribute(k_attn_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ln_bwd<T, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ln_bwd<T, Wr>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
   const HeadOffsets hoff{dsc.off_det_logw, dsc.off_jas_c_same, dsc.off_jas_c_opp,
@@ -621,44 +827,12 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
     const int nw = std::min(nwc, W - w0);
     const int nt = nw * N;
     JobBatch jb{JOB_VALUE, nw, N, 1, 0, 0, w0, R, S, nullptr};
-    // ---------------- forward with saved activations ----------------
-    T* x = b.xin[0] ? b.xin[0] : b.xL;
+    // ---------------- forward, keeping what the reverse pass needs ----------------
     k_embed<T><<<(nt + 7) / 8, 256, 0, st>>>(jb, mc, w.emb_w, w.emb_b, mc.depth ? b.xin[0] : b.xL);
     NQS_CHECK_LAUNCH("k_embed");
-    for (int l = 0; l < mc.depth; ++l) {
-      const BlockW<T>& bw = w.blk[l];
-      x = b.xin[l];
-      NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[l], st));
-      GemmArgs<T> g{};
-      g.X = b.h0[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
-      g.Y = b.qkv[l]; g.ldy = 3 * d; g.nseg = 3;
-      g.seg[0] = GemmSeg<T>{bw.wq, bw.bq, d, d, 0, 0};
-      g.seg[1] = GemmSeg<T>{bw.wk, bw.bk, d, d, d, 0};
-      g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
-      NQS_TRY(launch_attention<T>(nw, N, 1, 0, 0, d, H, b.qkv[l], b.ao[l], st));
-      g = GemmArgs<T>{};
-      g.X = b.ao[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
-      g.Y = b.xmid[l]; g.ldy = d; g.Res = x; g.ldr = d; g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.wo, bw.bo, d, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
-      NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xmid[l], bw.ln1_s, bw.ln1_b, b.h1[l], st));
-      g = GemmArgs<T>{};
-      g.X = b.h1[l]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
-      g.Y = b.a0[l]; g.ldy = D; g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.w0, bw.b0, D, D, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
-      cudaMemcpyAsync(b.g0[l], b.a0[l], sizeof(T) * (size_t)nt * D, cudaMemcpyDeviceToDevice, st);
-      const size_t nel = (size_t)nt * D;
-      k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, 1, 0, 0, D, b.g0[l]);
-      NQS_CHECK_LAUNCH("k_gelu");
-      g = GemmArgs<T>{};
-      g.X = b.g0[l]; g.ldx = D; g.rows = nt; g.K = D; g.C = 1;
-      g.Y = (l + 1 < mc.depth) ? b.xin[l + 1] : b.xL; g.ldy = d; g.Res = b.xmid[l]; g.ldr = d;
-      g.nseg = 1;
-      g.seg[0] = GemmSeg<T>{bw.w1, bw.b1, d, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
-    }
+    for (int l = 0; l < mc.depth; ++l)
+      NQS_TRY(block_forward<T>(mc, w.blk[l], b, l, ckpt ? 0 : l, nw,
+                               (l + 1 < mc.depth) ? b.xin[l + 1] : b.xL, st));
     NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xL, w.lnf_s, w.lnf_b, b.hf, st));
     {
       GemmArgs<T> g{};
@@ -669,9 +843,9 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       NQS_TRY(launch_gemm<T>(g, st));
     }
     // ---------------- reverse ----------------
-    k_head_bwd<T, T, TO><<<nw, 256, hsm, st>>>(jb, mc, b.bf, 2 * KN, hp, b.X1, b.X2, orows, hoff);
+    k_head_bwd<T, T, Wr><<<nw, 256, hsm, st>>>(jb, mc, b.bf, 2 * KN, hp, b.X1, b.X2, wr, hoff);
     NQS_CHECK_LAUNCH("k_head_bwd");
-    // backflow: hbar = X1 Wr^T + X2 Wi^T ; O of the complex kernel / bias
+    // backflow: hbar = X1 Wr^T + X2 Wi^T ; the complex kernel / bias
     {
       GemmArgs<T> g{};
       g.X = b.X1; g.ldx = KN; g.rows = 2 * nt; g.K = KN; g.C = 2; g.trans_w = 1;
@@ -682,36 +856,38 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       g.seg[0] = GemmSeg<T>{w.bf_w_im, nullptr, KN, d, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));
     }
-    NQS_TRY(launch_wgrad<T, TO>(nw, N, d, KN, b.hf, d, b.X1, KN, orows, w0,
-                                dsc.off_backflow_kernel, dsc.off_backflow_bias, 1, st));
+    NQS_TRY(wgrad<T>(wr, nw, N, d, KN, b.hf, d, b.X1, KN, w0, dsc.off_backflow_kernel,
+                     dsc.off_backflow_bias, 1, st));
     // final LayerNorm
-    k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
-        N, d, b.xL, b.hb, w.lnf_s, b.xb, 0, orows, w0, dsc.off_final_ln_scale,
+    k_ln_bwd<T, Wr><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+        N, d, b.xL, b.hb, w.lnf_s, b.xb, 0, wr, w0, dsc.off_final_ln_scale,
         dsc.off_final_ln_bias);
     NQS_CHECK_LAUNCH("k_ln_bwd");
     for (int l = mc.depth - 1; l >= 0; --l) {
       const BlockW<T>& bw = w.blk[l];
       const int64_t* of = dsc.off_block[l];
+      const int s = ckpt ? 0 : l;
+      if (ckpt) NQS_TRY(block_forward<T>(mc, bw, b, l, 0, nw, nullptr, st));  // recompute
       // MLP: x_out = xmid + g0 W1 + b1
       GemmArgs<T> g{};
       g.X = b.xb; g.ldx = d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
       g.Y = b.big; g.ldy = D; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.w1, nullptr, d, D, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));  // gbar0 = xbar W1^T
-      NQS_TRY(launch_wgrad<T, TO>(nw, N, D, d, b.g0[l], D, b.xb, d, orows, w0,
-                                  of[NQS_B_DENSE1_KERNEL], of[NQS_B_DENSE1_BIAS], 0, st));
+      NQS_TRY(wgrad<T>(wr, nw, N, D, d, b.g0[s], D, b.xb, d, w0, of[NQS_B_DENSE1_KERNEL],
+                       of[NQS_B_DENSE1_BIAS], 0, st));
       const size_t nel = (size_t)nt * D;
-      k_gelu_bwd<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, D, b.a0[l], b.big);
+      k_gelu_bwd<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, D, b.a0[s], b.big);
       NQS_CHECK_LAUNCH("k_gelu_bwd");
       g = GemmArgs<T>{};
       g.X = b.big; g.ldx = D; g.rows = 2 * nt; g.K = D; g.C = 2; g.trans_w = 1;
       g.Y = b.hb; g.ldy = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.w0, nullptr, D, d, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));  // hbar1 = abar0 W0^T
-      NQS_TRY(launch_wgrad<T, TO>(nw, N, d, D, b.h1[l], d, b.big, D, orows, w0,
-                                  of[NQS_B_DENSE0_KERNEL], of[NQS_B_DENSE0_BIAS], 0, st));
-      k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
-          N, d, b.xmid[l], b.hb, bw.ln1_s, b.xb, 1, orows, w0, of[NQS_B_LN1_SCALE],
+      NQS_TRY(wgrad<T>(wr, nw, N, d, D, b.h1[s], d, b.big, D, w0, of[NQS_B_DENSE0_KERNEL],
+                       of[NQS_B_DENSE0_BIAS], 0, st));
+      k_ln_bwd<T, Wr><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+          N, d, b.xmid[s], b.hb, bw.ln1_s, b.xb, 1, wr, w0, of[NQS_B_LN1_SCALE],
           of[NQS_B_LN1_BIAS]);
       NQS_CHECK_LAUNCH("k_ln_bwd");
       // attention: xmid = xin + ao Wo + bo
@@ -720,52 +896,78 @@ int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp
       g.Y = b.hb; g.ldy = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.wo, nullptr, d, d, 0, 0};
       NQS_TRY(launch_gemm<T>(g, st));  // aobar
-      NQS_TRY(launch_wgrad<T, TO>(nw, N, d, d, b.ao[l], d, b.xb, d, orows, w0,
-                                  of[NQS_B_O_KERNEL], of[NQS_B_O_BIAS], 0, st));
-      k_attn_bwd<T><<<nw * H, 128, absm, st>>>(N, d, H, b.qkv[l], b.hb, b.big);
+      NQS_TRY(wgrad<T>(wr, nw, N, d, d, b.ao[s], d, b.xb, d, w0, of[NQS_B_O_KERNEL],
+                       of[NQS_B_O_BIAS], 0, st));
+      k_attn_bwd<T><<<nw * H, 128, absm, st>>>(N, d, H, b.qkv[s], b.hb, b.big);
       NQS_CHECK_LAUNCH("k_attn_bwd");
       // h0bar = qbar Wq^T + kbar Wk^T + vbar Wv^T
       const T* wts[3] = {bw.wq, bw.wk, bw.wv};
-      for (int s = 0; s < 3; ++s) {
+      for (int q = 0; q < 3; ++q) {
         g = GemmArgs<T>{};
-        g.X = b.big + s * d; g.ldx = 3 * d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
-        g.Y = b.hb; g.ldy = d; g.Res = s ? b.hb : nullptr; g.ldr = d; g.nseg = 1;
-        g.seg[0] = GemmSeg<T>{wts[s], nullptr, d, d, 0, 0};
+        g.X = b.big + q * d; g.ldx = 3 * d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
+        g.Y = b.hb; g.ldy = d; g.Res = q ? b.hb : nullptr; g.ldr = d; g.nseg = 1;
+        g.seg[0] = GemmSeg<T>{wts[q], nullptr, d, d, 0, 0};
         NQS_TRY(launch_gemm<T>(g, st));
       }
       const int kk[3] = {NQS_B_Q_KERNEL, NQS_B_K_KERNEL, NQS_B_V_KERNEL};
       const int kb[3] = {NQS_B_Q_BIAS, NQS_B_K_BIAS, NQS_B_V_BIAS};
-      for (int s = 0; s < 3; ++s)
-        NQS_TRY(launch_wgrad<T, TO>(nw, N, d, d, b.h0[l], d, b.big + s * d, 3 * d, orows, w0,
-                                    of[kk[s]], of[kb[s]], 0, st));
-      k_ln_bwd<T, TO><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
-          N, d, b.xin[l], b.hb, bw.ln0_s, b.xb, 1, orows, w0, of[NQS_B_LN0_SCALE],
+      for (int q = 0; q < 3; ++q)
+        NQS_TRY(wgrad<T>(wr, nw, N, d, d, b.h0[s], d, b.big + q * d, 3 * d, w0, of[kk[q]],
+                         of[kb[q]], 0, st));
+      k_ln_bwd<T, Wr><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
+          N, d, b.xin[l], b.hb, bw.ln0_s, b.xb, 1, wr, w0, of[NQS_B_LN0_SCALE],
           of[NQS_B_LN0_BIAS]);
       NQS_CHECK_LAUNCH("k_ln_bwd");
     }
     // embedding
     k_features<T><<<(nt * Fp + 255) / 256, 256, 0, st>>>(jb, mc, b.feat);
     NQS_CHECK_LAUNCH("k_features");
-    NQS_TRY(launch_wgrad<T, TO>(nw, N, Fp, d, b.feat, Fp, b.xb, d, orows, w0,
-                                dsc.off_embed_kernel, dsc.off_embed_bias, 0, st));
+    NQS_TRY(wgrad<T>(wr, nw, N, Fp, d, b.feat, Fp, b.xb, d, w0, dsc.off_embed_kernel,
+                     dsc.off_embed_bias, 0, st));
   }
   ws.used = save;
   return NQS_OK;
 }
 
+template <typename T, typename TO>
+int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                     const double* R, const int32_t* S, int W, TO* O, bool ckpt, Arena& ws,
+                     cudaStream_t st) {
+  const ORows<TO> orows{O, hm.desc.n_params, W};
+  return backward_run<T, ORows<TO>>(hm, w, hp, R, S, W, orows, ckpt, ws, st);
+}
+
+template <typename T>
+int logpsi_vjp_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
+                   const double* R, const int32_t* S, int W, const cplx* ct, double* grad,
+                   bool ckpt, Arena& ws, cudaStream_t st) {
+  const cudaError_t e = cudaMemsetAsync(grad, 0, sizeof(double) * hm.desc.n_params, st);
+  if (e != cudaSuccess) return cuda_status(e, "nqs_logpsi_vjp: clear");
+  const VjpAcc acc{grad, ct};
+  return backward_run<T, VjpAcc>(hm, w, hp, R, S, W, acc, ckpt, ws, st);
+}
+
+template size_t backward_scratch<double>(const ModelConst&, int, bool);
+template size_t backward_scratch<float>(const ModelConst&, int, bool);
 template size_t per_sample_O_scratch<double>(const ModelConst&, int);
 template size_t per_sample_O_scratch<float>(const ModelConst&, int);
 template int per_sample_O_run<double, double>(const HostModel&, const NetW<double>&,
                                               const HeadParams&, const double*, const int32_t*,
-                                              int, double*, Arena&, cudaStream_t);
+                                              int, double*, bool, Arena&, cudaStream_t);
 template int per_sample_O_run<float, float>(const HostModel&, const NetW<float>&,
                                             const HeadParams&, const double*, const int32_t*, int,
-                                            float*, Arena&, cudaStream_t);
+                                            float*, bool, Arena&, cudaStream_t);
 template int per_sample_O_run<float, double>(const HostModel&, const NetW<float>&,
                                              const HeadParams&, const double*, const int32_t*,
-                                             int, double*, Arena&, cudaStream_t);
+                                             int, double*, bool, Arena&, cudaStream_t);
 template int per_sample_O_run<double, float>(const HostModel&, const NetW<double>&,
                                              const HeadParams&, const double*, const int32_t*,
-                                             int, float*, Arena&, cudaStream_t);
+                                             int, float*, bool, Arena&, cudaStream_t);
+template int logpsi_vjp_run<double>(const HostModel&, const NetW<double>&, const HeadParams&,
+                                    const double*, const int32_t*, int, const cplx*, double*,
+                                    bool, Arena&, cudaStream_t);
+template int logpsi_vjp_run<float>(const HostModel&, const NetW<float>&, const HeadParams&,
+                                   const double*, const int32_t*, int, const cplx*, double*,
+                                   bool, Arena&, cudaStream_t);
 
 }  // namespace nqs

@@ -444,9 +444,14 @@ size_t plan_bytes(const NqsModel* m, int op, int W, int prec) {
       p.add(net_bytes(mc, prec, chunk_rows(JOB_VALUE, W, N, 1, kMaxRows)));
       break;
     case NQS_OP_PER_SAMPLE_O:
-      p.add(prec == NQS_PREC_FP64 ? per_sample_O_scratch<double>(mc, W)
-                                  : per_sample_O_scratch<float>(mc, W));
+    case NQS_OP_PER_SAMPLE_O_CKPT:
+    case NQS_OP_LOGPSI_VJP:
+    case NQS_OP_LOGPSI_VJP_CKPT: {
+      const bool ckpt = op == NQS_OP_PER_SAMPLE_O_CKPT || op == NQS_OP_LOGPSI_VJP_CKPT;
+      p.add(prec == NQS_PREC_FP64 ? backward_scratch<double>(mc, W, ckpt)
+                                  : backward_scratch<float>(mc, W, ckpt));
       break;
+    }
     default:
       return 0;
   }
@@ -706,25 +711,68 @@ int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, dou
 
 }  // extern "C"
 
-extern "C" int nqs_per_sample_O(NqsModel* m, const double* theta, const double* R,
-                                const int32_t* S, int W, void* out_O, int out_dtype, int prec,
-                                void* wsp, size_t wsb, void* stream) {
-  cudaStream_t st = (cudaStream_t)stream;
-  if (W < 0 || (W > 0 && (!R || !S || !out_O)) || (out_dtype != 0 && out_dtype != 1))
+static int per_sample_O_impl(NqsModel* m, const double* theta, const double* R,
+                             const int32_t* S, int W, void* out_O, int out_dtype, int prec,
+                             bool ckpt, void* wsp, size_t wsb, cudaStream_t st) {
+  if (W < 0 || (W > 0 && (!R || !S || !out_O)) || (out_dtype != 0 && out_dtype != 1)) {
+    set_error("nqs_per_sample_O: invalid argument");
     return NQS_ERR_INVALID_ARG;
+  }
   if (W == 0) return NQS_OK;
-  NQS_TRY(check_ws(m, NQS_OP_PER_SAMPLE_O, W, prec, wsb));
+  NQS_TRY(check_ws(m, ckpt ? NQS_OP_PER_SAMPLE_O_CKPT : NQS_OP_PER_SAMPLE_O, W, prec, wsb));
   Ctx c;
   NQS_TRY(begin(m, theta, prec, wsp, wsb, st, &c));
   const HeadParams hp = make_head_params(m->hm.desc, c.theta64);
   if (prec == NQS_PREC_FP64) {
     const NetW<double> w = make_netw<double>(m->hm.desc, c.theta64, c.theta64);
     if (out_dtype == 0)
-      return per_sample_O_run<double, double>(m->hm, w, hp, R, S, W, (double*)out_O, c.ws, st);
-    return per_sample_O_run<double, float>(m->hm, w, hp, R, S, W, (float*)out_O, c.ws, st);
+      return per_sample_O_run<double, double>(m->hm, w, hp, R, S, W, (double*)out_O, ckpt, c.ws,
+                                              st);
+    return per_sample_O_run<double, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
   }
   const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
   if (out_dtype == 0)
-    return per_sample_O_run<float, double>(m->hm, w, hp, R, S, W, (double*)out_O, c.ws, st);
-  return per_sample_O_run<float, float>(m->hm, w, hp, R, S, W, (float*)out_O, c.ws, st);
+    return per_sample_O_run<float, double>(m->hm, w, hp, R, S, W, (double*)out_O, ckpt, c.ws, st);
+  return per_sample_O_run<float, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
+}
+
+extern "C" int nqs_per_sample_O(NqsModel* m, const double* theta, const double* R,
+                                const int32_t* S, int W, void* out_O, int out_dtype, int prec,
+                                void* wsp, size_t wsb, void* stream) {
+  return per_sample_O_impl(m, theta, R, S, W, out_O, out_dtype, prec, false, wsp, wsb,
+                           (cudaStream_t)stream);
+}
+
+extern "C" int nqs_per_sample_O_ex(NqsModel* m, const double* theta, const double* R,
+                                   const int32_t* S, int W, void* out_O, int out_dtype, int prec,
+                                   int checkpoint_blocks, void* wsp, size_t wsb, void* stream) {
+  return per_sample_O_impl(m, theta, R, S, W, out_O, out_dtype, prec, checkpoint_blocks != 0,
+                           wsp, wsb, (cudaStream_t)stream);
+}
+
+extern "C" int nqs_logpsi_vjp(NqsModel* m, const double* theta, const double* R,
+                              const int32_t* S, int W, const double* cotangent, double* out_grad,
+                              int prec, int checkpoint_blocks, void* wsp, size_t wsb,
+                              void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!m || W < 0 || !out_grad || (W > 0 && (!R || !S || !cotangent))) {
+    set_error("nqs_logpsi_vjp: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  if (W == 0) {
+    const cudaError_t e = cudaMemsetAsync(out_grad, 0, sizeof(double) * m->hm.desc.n_params, st);
+    return e == cudaSuccess ? NQS_OK : cuda_status(e, "nqs_logpsi_vjp: clear");
+  }
+  const bool ckpt = checkpoint_blocks != 0;
+  NQS_TRY(check_ws(m, ckpt ? NQS_OP_LOGPSI_VJP_CKPT : NQS_OP_LOGPSI_VJP, W, prec, wsb));
+  Ctx c;
+  NQS_TRY(begin(m, theta, prec, wsp, wsb, st, &c));
+  const HeadParams hp = make_head_params(m->hm.desc, c.theta64);
+  const cplx* ct = (const cplx*)cotangent;
+  if (prec == NQS_PREC_FP64) {
+    const NetW<double> w = make_netw<double>(m->hm.desc, c.theta64, c.theta64);
+    return logpsi_vjp_run<double>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
+  }
+  const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  return logpsi_vjp_run<float>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
 }

@@ -30,6 +30,7 @@ PREC_MIXED = 1
 PREC_MIXED_SIMT = 2
 
 OP_LOGPSI, OP_LOCAL_E, OP_MCMC, OP_PER_SAMPLE_O = 0, 1, 2, 3
+OP_PER_SAMPLE_O_CKPT, OP_LOGPSI_VJP, OP_LOGPSI_VJP_CKPT = 4, 5, 6
 
 MAX_DEPTH = 16
 B_NPARAM = 16
@@ -87,6 +88,10 @@ _SIGS = {
                          c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_size_t, c_void_p], c_int),
     "nqs_per_sample_O": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
                           c_void_p, c_size_t, c_void_p], c_int),
+    "nqs_per_sample_O_ex": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                             c_int, c_int, c_void_p, c_size_t, c_void_p], c_int),
+    "nqs_logpsi_vjp": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                        c_int, c_void_p, c_size_t, c_void_p], c_int),
     "nqs_ewald_create": ([POINTER(c_double), c_double, c_double, c_int, c_int, POINTER(c_void_p)],
                          c_int),
     "nqs_ewald_destroy": ([c_void_p], c_int),
@@ -186,6 +191,8 @@ _SIGS.update({
                                      c_void_p], c_int),
     "nqs_adam_update": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_double,
                          c_double, c_double, c_int, c_void_p], c_int),
+    "nqs_adam_update_complex": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                 c_double, c_double, c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),
     "nqs_profile_gemm": ([c_int], c_int),
     "nqs_set_block_fusion": ([c_int], c_int),

@@ -182,7 +182,7 @@ def clip_energies(e, clip_k):
     """median-MAD clip of Re e (minsr.py:145-148) and the energy statistics, on the device.
     Returns (e_clip complex (W,), stats f64[5] = mean, err, var, median, mad)."""
     from . import _lib
-    e = torch.as_tensor(e).to(torch.complex128).contiguous()
+    e = torch.as_tensor(e).to(torch.complex128).resolve_conj().contiguous()
     out = torch.empty_like(e)
     stats = torch.empty(5, dtype=F64, device=e.device)
     _lib.check(_lib.lib().nqs_clip_energies(_lib.ptr(e), e.shape[0], float(clip_k), _lib.ptr(out),
@@ -258,7 +258,7 @@ class VMCIteration:
         self.n_refine = int(n_refine if n_refine is not None else (1 if self.gram == "fp64" else 2))
         dev = self.R.device
         self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
-        self.O = torch.empty(2 * self.W, self.P, dtype=self.o_dtype, device=dev)
+        self._O = None  # the [2W][P] Jacobian, allocated on first use
         self.e = torch.empty(self.W, dtype=torch.complex128, device=dev)
         self.e_clip = torch.empty_like(self.e)
         self.stats = torch.zeros(5, dtype=F64, device=dev)
@@ -278,13 +278,34 @@ class VMCIteration:
                                  _GRAM[self.gram]))
         self.ws = _lib.workspace.get(max(sizes))
 
-    def sample(self, n_sweeps=None):
+    @property
+    def O(self):
+        if self._O is None:
+            self._O = torch.empty(2 * self.W, self.P, dtype=self.o_dtype, device=self.R.device)
+        return self._O
+
+    def sample(self, n_sweeps=None, inject=None):
+        """n_sweeps Metropolis sweeps (default: the iteration's). inject: optional pre-drawn
+        randomness (normals [n][W][N][2], position uniforms [n][W], flip indices and flip
+        uniforms [n][n_spin_flips][W]) used verbatim instead of the counter-based stream (the
+        counter still advances)."""
         from . import _lib
         L = _lib.lib()
         n = self.n_sweeps if n_sweeps is None else n_sweeps
+        inj = [None] * 4
+        if inject is not None:
+            dev = self.R.device
+            inj = [torch.as_tensor(inject[0], dtype=F64).to(dev).contiguous(),
+                   torch.as_tensor(inject[1], dtype=F64).to(dev).contiguous(),
+                   torch.as_tensor(inject[2]).to(dev, torch.int32).contiguous(),
+                   torch.as_tensor(inject[3], dtype=F64).to(dev).contiguous()]
+            if (tuple(inj[0].shape) != (n, self.W, self.N, 2) or tuple(inj[1].shape) != (n, self.W)
+                    or tuple(inj[2].shape) != (n, self.n_flips, self.W)
+                    or tuple(inj[3].shape) != (n, self.n_flips, self.W)):
+                raise ValueError("injected randomness has the wrong shape")
         _lib.check(L.nqs_mcmc_sweeps(
             self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), None, self.W, n,
-            self.n_flips, self.step_size, self.seed, self.counter, None, None, None, None,
+            self.n_flips, self.step_size, self.seed, self.counter, *[_lib.ptr(x) for x in inj],
             _lib.ptr(self.acc_pos), _lib.ptr(self.acc_spin), None, self.prec, _lib.ptr(self.ws),
             self.ws.numel(), _lib.stream_ptr()), "nqs_mcmc_sweeps")
         self.counter += n
@@ -324,8 +345,9 @@ class VMCIteration:
             self.lr, _lib.ptr(self.status), _lib.ptr(self.damping), _lib.ptr(self.ws),
             self.ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
 
-    def step(self):
-        self.sample()
+    def step(self, inject=None):
+        """One iteration; inject as in sample() replaces the sweeps' random draws."""
+        self.sample(inject=inject)
         self.energies()
         self.jacobian()
         self.update()

@@ -295,30 +295,87 @@ def periodic_features(R, cell, n_freq):
     return torch.cat([torch.sin(ang), torch.cos(ang)], dim=-1).reshape(*R.shape[:-1], 4 * n_freq)
 
 
-class LogPsi:
-    """logpsi(R, S) bound to a model and parameters (make_logpsi, psiformer.py:192-196)."""
+def _logpsi_values(model, theta, R, S, prec):
+    W = R.shape[0]
+    out = torch.empty(W, dtype=C128, device=R.device)
+    h = model.native().handle
+    ws, _ = _lib.workspace_for(h, _lib.OP_LOGPSI, W, prec)
+    _lib.check(_lib.lib().nqs_logpsi(h, _lib.ptr(theta), _lib.ptr(R), _lib.ptr(S), W,
+                                     _lib.ptr(out), prec, _lib.ptr(ws), ws.numel(),
+                                     _lib.stream_ptr()), "nqs_logpsi")
+    return out
 
-    def __init__(self, model: ContinuumSpinorPsiformer, theta: torch.Tensor, precision="fp64"):
+
+def logpsi_vjp(model, theta, R, S, cotangent, precision="fp64", checkpoint_blocks=False):
+    """sum_w Re(cotangent_w d log psi(R_w, S_w) / d theta) as float64[P] (nqs_logpsi_vjp): the
+    derivative the Adam driver takes of its surrogate loss (train.py:53-59) without forming the
+    per-sample Jacobian."""
+    prec = _prec(precision)
+    R, S, _ = as_batch(R, S)
+    W = R.shape[0]
+    theta = theta.detach().to(R.device, F64).contiguous()
+    # resolve_conj: a lazily conjugated view (torch.conj) keeps the unconjugated numbers in memory
+    ct = torch.as_tensor(cotangent).to(R.device, C128).reshape(W).resolve_conj().contiguous()
+    out = torch.empty(model.n_params(), dtype=F64, device=R.device)
+    h = model.native().handle
+    op = _lib.OP_LOGPSI_VJP_CKPT if checkpoint_blocks else _lib.OP_LOGPSI_VJP
+    ws, _ = _lib.workspace_for(h, op, W, prec)
+    _lib.check(_lib.lib().nqs_logpsi_vjp(h, _lib.ptr(theta), _lib.ptr(R), _lib.ptr(S), W,
+                                         _lib.ptr(ct), _lib.ptr(out), prec,
+                                         int(bool(checkpoint_blocks)), _lib.ptr(ws), ws.numel(),
+                                         _lib.stream_ptr()), "nqs_logpsi_vjp")
+    return out
+
+
+class _LogPsiFn(torch.autograd.Function):
+    """log psi as a differentiable function of theta: forward nqs_logpsi, backward nqs_logpsi_vjp.
+    PyTorch hands a complex output the gradient g = dL/dRe + i dL/dIm, so dL/dtheta =
+    sum_w Re(conj(g_w) d log psi_w / d theta): the VJP with cotangent conj(g)."""
+
+    @staticmethod
+    def forward(ctx, theta, R, S, model, prec, checkpoint_blocks):
+        ctx.model, ctx.prec, ctx.ckpt = model, prec, checkpoint_blocks
+        ctx.save_for_backward(theta, R, S)
+        return _logpsi_values(model, theta.detach().contiguous(), R, S, prec)
+
+    @staticmethod
+    def backward(ctx, g):
+        theta, R, S = ctx.saved_tensors
+        gt = None
+        if ctx.needs_input_grad[0]:
+            gt = logpsi_vjp(ctx.model, theta, R, S, torch.conj(g), ctx.prec, ctx.ckpt)
+        return gt, None, None, None, None, None
+
+
+class LogPsi:
+    """logpsi(R, S) bound to a model and parameters (make_logpsi, psiformer.py:192-196). When
+    theta requires grad (and grad mode is on) the output is differentiable with respect to theta
+    through the hand-written reverse mode (nqs_logpsi_vjp)."""
+
+    def __init__(self, model: ContinuumSpinorPsiformer, theta: torch.Tensor, precision="fp64",
+                 checkpoint_blocks=False):
         self.model = model
         self.theta = theta
         self.precision = _prec(precision)
+        self.checkpoint_blocks = bool(checkpoint_blocks)
 
     def __call__(self, R, S):
         R, S, single = as_batch(R, S)
-        W = R.shape[0]
-        out = torch.empty(W, dtype=C128, device=R.device)
-        h = self.model.native().handle
-        ws, nb = _lib.workspace_for(h, _lib.OP_LOGPSI, W, self.precision)
-        _lib.check(_lib.lib().nqs_logpsi(h, _lib.ptr(self.theta), _lib.ptr(R), _lib.ptr(S), W,
-                                         _lib.ptr(out), self.precision, _lib.ptr(ws), ws.numel(),
-                                         _lib.stream_ptr()), "nqs_logpsi")
+        if torch.is_grad_enabled() and self.theta.requires_grad:
+            out = _LogPsiFn.apply(self.theta, R, S, self.model, self.precision,
+                                  self.checkpoint_blocks)
+        else:
+            out = _logpsi_values(self.model, self.theta.detach(), R, S, self.precision)
         return out[0] if single else out
 
 
 def make_logpsi(model, params, precision="fp64"):
-    """Bind params -> logpsi(R, S) -> complex (psiformer.py:192-196)."""
+    """Bind params -> logpsi(R, S) -> complex (psiformer.py:192-196). params is the flax-style
+    tree or the real ravel theta; a float64 CUDA theta that requires grad is kept as is, so the
+    log psi values are differentiable with respect to it."""
     if isinstance(params, torch.Tensor):
-        theta = params.to(_lib.device(), F64).contiguous()
+        theta = params if (params.is_cuda and params.dtype == F64 and params.is_contiguous()) \
+            else params.to(_lib.device(), F64).contiguous()
     else:
         theta = model.theta(params)
     return LogPsi(model, theta, precision)

@@ -1,11 +1,12 @@
 """VMC training with Adam (drop-in for src/nqs/train.py:28-96).
 
-One step: n_sweeps Metropolis sweeps -> local energies -> the surrogate-loss gradient
-g = 2 mean_w Re[conj(e_w - mean e) d log psi_w / d theta] -> an Adam update, all on the device.
-The gradient is the per-sample Jacobian contracted with the centred energies (nqs_energy_gradient),
-so it is exactly the derivative of the reference's surrogate with respect to the REAL ravel theta.
-(For complex leaves JAX's grad returns d/dRe - i d/dIm and optax's Adam then keeps one second
-moment per complex element; here every real component has its own moment — stated difference.)
+One step: n_sweeps Metropolis sweeps -> local energies -> the gradient of the reference's
+surrogate loss 2 mean_w Re[conj(e_w - mean e) log psi_w] (train.py:53-59), taken by torch autograd
+through the differentiable log psi of nqs.psiformer (forward nqs_logpsi, backward the hand-written
+vector-Jacobian product nqs_logpsi_vjp, which never forms the per-sample Jacobian) -> the Adam
+step of optax.adam as train.py applies it to jax.grad's tree: a complex leaf element moves as one
+complex number with JAX's gradient dL/dRe - i dL/dIm, one complex first moment and one shared
+second moment |G|^2 (nqs_adam_update_complex). Everything runs on the device.
 """
 from __future__ import annotations
 
@@ -15,36 +16,80 @@ from . import _lib
 from .minsr import real_ravel
 
 
-class Adam:
-    """optax.adam-like: init(theta) -> state; update(grad, state, theta) applies the step."""
+def complex_partners(model):
+    """int64[P]: for each component of a complex leaf element the theta index of the other
+    component (re block k <-> im block k + n), -1 for a real parameter."""
+    P = model.n_params()
+    partner = torch.full((P,), -1, dtype=torch.int64)
+    for _, shape, is_c, off in model.leaves():
+        if is_c:
+            n = 1
+            for x in shape:
+                n *= int(x)
+            k = torch.arange(off, off + n, dtype=torch.int64)
+            partner[k] = k + n
+            partner[k + n] = k
+    return partner
 
-    def __init__(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+
+class Adam:
+    """optax.adam on the real ravel: init(theta) -> state; update(grad, state, theta) applies the
+    step in place. grad is the real-ravel gradient (dL/dRe, dL/dIm for complex leaves). With a
+    model (partner table from complex_partners) complex leaf elements take optax's complex step;
+    without one every component is a real parameter."""
+
+    def __init__(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, model=None):
         self.lr, self.b1, self.b2, self.eps = float(lr), float(b1), float(b2), float(eps)
+        self.model = model
 
     def init(self, theta):
-        return {"m": torch.zeros_like(theta), "v": torch.zeros_like(theta), "t": 0}
+        st = {"m": torch.zeros_like(theta), "v": torch.zeros_like(theta), "t": 0}
+        if self.model is not None:
+            st["partner"] = complex_partners(self.model).to(theta.device)
+        return st
 
     def update(self, grad, state, theta):
         state["t"] += 1
-        _lib.check(_lib.lib().nqs_adam_update(
-            _lib.ptr(theta), _lib.ptr(grad), _lib.ptr(state["m"]), _lib.ptr(state["v"]),
-            theta.numel(), self.lr, self.b1, self.b2, self.eps, state["t"], _lib.stream_ptr()),
-            "nqs_adam_update")
+        if "partner" in state:
+            _lib.check(_lib.lib().nqs_adam_update_complex(
+                _lib.ptr(theta), _lib.ptr(grad), _lib.ptr(state["m"]), _lib.ptr(state["v"]),
+                _lib.ptr(state["partner"]), theta.numel(), self.lr, self.b1, self.b2, self.eps,
+                state["t"], _lib.stream_ptr()), "nqs_adam_update_complex")
+        else:
+            _lib.check(_lib.lib().nqs_adam_update(
+                _lib.ptr(theta), _lib.ptr(grad), _lib.ptr(state["m"]), _lib.ptr(state["v"]),
+                theta.numel(), self.lr, self.b1, self.b2, self.eps, state["t"],
+                _lib.stream_ptr()), "nqs_adam_update")
         return state
 
 
-def adam(lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
-    return Adam(lr, b1, b2, eps)
+def adam(lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, model=None):
+    return Adam(lr, b1, b2, eps, model)
+
+
+def surrogate_gradient(model, theta, R, S, e, precision="fp64"):
+    """d/dtheta of the reference's surrogate 2 mean_w Re[conj(e_w - mean e) log psi_theta(R_w,
+    S_w)] (train.py:53-59) by torch autograd through the differentiable log psi (backward =
+    nqs_logpsi_vjp). Returns the real-ravel gradient float64[P]."""
+    from .psiformer import LogPsi
+    th = theta.detach().requires_grad_(True)
+    with torch.enable_grad():
+        lp = LogPsi(model, th, precision)(R, S)
+        ec = torch.conj(e - e.mean()).detach()
+        loss = 2.0 * torch.real(ec * lp).mean()
+        (g,) = torch.autograd.grad(loss, th)
+    return g
 
 
 def make_train_step(model, L, n_elec, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
                     optimizer=None, n_sweeps=10, step_size=0.4, n_spin_flips=2):
     """Return (optimizer, step(theta, opt_state, R, S, key)) (train.py:28-65). theta is the real
     ravel on the device and is updated in place; returns
-    (theta, opt_state, R, S, E, Eerr, acc_pos, acc_spin)."""
+    (theta, opt_state, R, S, E, Eerr, acc_pos, acc_spin). The default optimizer is optax.adam(1e-3)
+    with the complex-leaf treatment of the reference."""
     from .minsr import VMCIteration
     from .random import as_key, key_to_seed
-    optimizer = optimizer or adam(1e-3)
+    optimizer = optimizer or adam(1e-3, model=model)
     cache = {}
 
     def step(theta, opt_state, R, S, key):
@@ -55,19 +100,13 @@ def make_train_step(model, L, n_elec, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb
                               coulomb=coulomb, n_sweeps=n_sweeps, step_size=step_size,
                               n_spin_flips=n_spin_flips, precision="fp64")
             cache["it"] = it
-            cache["g"] = torch.empty_like(it.theta)
         it.theta = theta
         it.R.copy_(torch.as_tensor(R))
         it.S.copy_(torch.as_tensor(S))
         it.seed, it.counter = key_to_seed((s, 0)), c
         it.sample()
         it.energies()
-        it.jacobian()
-        g = cache["g"]
-        ws = _lib.workspace.get(16 * it.W + 4096)
-        _lib.check(_lib.lib().nqs_energy_gradient(
-            _lib.ptr(it.O), 0, _lib.ptr(it.e), it.W, it.P, _lib.ptr(g), _lib.ptr(ws), ws.numel(),
-            _lib.stream_ptr()), "nqs_energy_gradient")
+        g = surrogate_gradient(model, theta, it.R, it.S, it.e)
         opt_state = optimizer.update(g, opt_state, theta)
         er = it.e.real
         return (theta, opt_state, it.R, it.S, er.mean(), er.std(unbiased=False) / it.W ** 0.5,
@@ -87,7 +126,7 @@ def train(model, params, L, n_elec, key, *, m_star=1.0, lambda_r=1.0, h_z=0.0, c
     """Run VMC training with Adam; return (params, history) (train.py:75-96)."""
     from .random import as_key, fold_in, split
     optimizer, step = make_train_step(model, L, n_elec, m_star, lambda_r, h_z, coulomb,
-                                      optimizer or adam(lr), n_sweeps, step_size)
+                                      optimizer or adam(lr, model=model), n_sweeps, step_size)
     theta, unravel = real_ravel(params)
     theta = theta.to(_lib.device()).contiguous()
     opt_state = optimizer.init(theta)

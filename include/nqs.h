@@ -23,6 +23,7 @@
  *   nqs_mcmc_sweeps     <- make_mcmc sweep scanned over sweeps, vmapped      src/nqs/sampler.py:25-91,
  *                                                                            src/nqs/minsr.py:107-118
  *   nqs_per_sample_O    <- per_sample_O                                      src/nqs/minsr.py:56-65
+ *   nqs_logpsi_vjp      <- jax.grad of the surrogate loss in make_train_step src/nqs/train.py:53-59
  *   nqs_minsr_direction <- _otil_etil + minsr_direction                      src/nqs/minsr.py:68-81
  *   nqs_clip_energies   <- the median-MAD clip inside train_minsr            src/nqs/minsr.py:142-150
  */
@@ -131,6 +132,9 @@ int64_t nqs_model_n_params(const NqsModel* model);
 #define NQS_OP_LOCAL_E     1
 #define NQS_OP_MCMC        2
 #define NQS_OP_PER_SAMPLE_O 3
+#define NQS_OP_PER_SAMPLE_O_CKPT 4   /* nqs_per_sample_O_ex with checkpoint_blocks != 0       */
+#define NQS_OP_LOGPSI_VJP  5         /* nqs_logpsi_vjp, every block's activations kept        */
+#define NQS_OP_LOGPSI_VJP_CKPT 6     /* nqs_logpsi_vjp with checkpoint_blocks != 0            */
 int nqs_workspace_size(const NqsModel* model, int op, int n_walkers, int precision,
                        size_t* bytes);
 
@@ -195,6 +199,29 @@ int nqs_mcmc_sweeps(NqsModel* model, const double* theta, double* R_io, int32_t*
 int nqs_per_sample_O(NqsModel* model, const double* theta, const double* R, const int32_t* S,
                      int n_walkers, void* out_O, int out_dtype, int precision,
                      void* workspace, size_t workspace_bytes, void* stream);
+/* nqs_per_sample_O with activation checkpointing (the same per_sample_O, src/nqs/minsr.py:56-65):
+ * checkpoint_blocks != 0 keeps only each transformer block's input during the forward and
+ * recomputes the block's activations (LayerNorms, q/k/v, attention output, MLP) just before its
+ * reverse step. O is bit-identical to the stored-activation pass; the activation memory per
+ * walker drops from depth x (block intermediates) to one block's, so a workspace of the same size
+ * holds more walkers per chunk. Workspace: NQS_OP_PER_SAMPLE_O_CKPT (NQS_OP_PER_SAMPLE_O when
+ * checkpoint_blocks == 0). */
+int nqs_per_sample_O_ex(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                        int n_walkers, void* out_O, int out_dtype, int precision,
+                        int checkpoint_blocks, void* workspace, size_t workspace_bytes,
+                        void* stream);
+/* Vector-Jacobian product of log psi over W configurations without forming O:
+ *   out_grad[k] = sum_w Re(cotangent_w * d log psi(R_w, S_w) / d theta_k)     (float64[P])
+ * cotangent: complex[W]. This is jax.vjp of the vmapped log psi (JAX's convention for a complex
+ * output of real parameters), the derivative train.py takes of its surrogate loss
+ * 2 mean_w Re[conj(e_w - mean e) log psi_w] (src/nqs/train.py:53-59) with
+ * cotangent_w = (2/W) conj(e_w - mean e). Hand-written reverse mode; the weight gradients are
+ * reduced over walkers on the device (float64 atomics, so the last bits depend on the order).
+ * checkpoint_blocks as in nqs_per_sample_O_ex. Workspace: NQS_OP_LOGPSI_VJP or
+ * NQS_OP_LOGPSI_VJP_CKPT. */
+int nqs_logpsi_vjp(NqsModel* model, const double* theta, const double* R, const int32_t* S,
+                   int n_walkers, const double* cotangent, double* out_grad, int precision,
+                   int checkpoint_blocks, void* workspace, size_t workspace_bytes, void* stream);
 
 /* MinSR direction (src/nqs/minsr.py:68-81): O is the [2W][P] output of nqs_per_sample_O
  * (o_dtype 0 = f64, 1 = f32), eps complex[W] the (clipped) local energies.
@@ -246,7 +273,9 @@ int nqs_energy_gradient(const void* O, int o_dtype, const double* e, int n_walke
  * NQS_ERR_UNSUPPORTED with the reason in nqs_last_error). The first call on each device resolves
  * that array's address with the device current; make it before any stream capture. All calls on
  * a device share the array: calls that overlap in time (other streams, other host threads) race
- * and must be serialised by the caller. */
+ * and must be serialised by the caller. The resolved address is cached per device ordinal for the
+ * life of the process: resetting a device (cudaDeviceReset, or tearing down its primary context)
+ * while libnqs is loaded is not supported for this entry point. */
 #define NQS_NOALLOC_MAX_WALKERS 32768
 int nqs_energy_gradient_noalloc(const void* O, int o_dtype, const double* e, int n_walkers,
                                 int64_t n_params, double* out_grad, void* stream);
@@ -254,6 +283,15 @@ int nqs_energy_gradient_noalloc(const void* O, int o_dtype, const double* e, int
  * the step count used for bias correction. m, v: float64[P] moment buffers (start at 0). */
 int nqs_adam_update(double* theta, const double* grad, double* m, double* v, int64_t n_params,
                     double lr, double b1, double b2, double eps, int t, void* stream);
+/* The Adam step of optax.adam applied to the tree gradient that jax.grad gives train.py
+ * (src/nqs/train.py:53-61): a complex leaf element c = a + i b is updated as one complex number
+ * with JAX's gradient G = dL/da - i dL/db, one complex first moment and the real second moment of
+ * |G|^2. grad is the real-ravel gradient (dL/da, dL/db) that nqs_logpsi_vjp returns; partner
+ * (int64[P], device) gives for each component of a complex element the index of the other one
+ * (re block k <-> im block k + n) and -1 for a real parameter. */
+int nqs_adam_update_complex(double* theta, const double* grad, double* m, double* v,
+                            const int64_t* partner, int64_t n_params, double lr, double b1,
+                            double b2, double eps, int t, void* stream);
 
 /* Median-MAD clip of Re e (src/nqs/minsr.py:145-148): med = median(Re e),
  * mad = median(|Re e - med|) + 1e-12, Re e clipped to med +- clip_k mad, Im kept.

@@ -450,19 +450,25 @@ def clip_energies(e, clip_k):
 # ----------------------------------------------------------------------------------------------
 def vmc_iteration(spec, theta, unravel, R, S, *, A, step, n_sweeps, n_spin_flips, rng,
                   m_star, lambda_r, h_z, ewald: Ewald | None, lam, lr, clip_k,
-                  n_walkers_elocal=None):
+                  n_walkers_elocal=None, draws=None):
     """Sample (n_sweeps Metropolis sweeps), E_loc (dense Hessian), O (reverse mode), clip,
-    MinSR direction, update. `rng` is a numpy Generator supplying the proposals. When
+    MinSR direction, update. `rng` is a numpy Generator supplying the proposals, or `draws` the
+    pre-drawn randomness in the device's injected layout (normals [n_sweeps][W][N][2], position
+    uniforms [n_sweeps][W], flip indices and flip uniforms [n_sweeps][n_spin_flips][W]). When
     `n_walkers_elocal` is given only that many walkers enter E_loc / O / MinSR (a bounded
     sample for timing)."""
     params = unravel(theta)
     lp = lambda r, s: logpsi(spec, params, r, s)  # noqa: E731
     Wn, N = S.shape
-    for _ in range(n_sweeps):
+    for sw in range(n_sweeps):
         for w in range(Wn):
-            R[w], S[w], *_ = mcmc_sweep(
-                lp, A, R[w], S[w], step, torch.as_tensor(rng.standard_normal((N, 2))),
-                rng.uniform(), rng.integers(0, N, n_spin_flips), rng.uniform(size=n_spin_flips))
+            if draws is None:
+                nrm, up = torch.as_tensor(rng.standard_normal((N, 2))), rng.uniform()
+                fi, uf = rng.integers(0, N, n_spin_flips), rng.uniform(size=n_spin_flips)
+            else:
+                nrm, up = torch.as_tensor(draws[0][sw, w]), float(draws[1][sw, w])
+                fi, uf = draws[2][sw, :, w], draws[3][sw, :, w]
+            R[w], S[w], *_ = mcmc_sweep(lp, A, R[w], S[w], step, nrm, up, fi, uf)
     Wm = Wn if n_walkers_elocal is None else n_walkers_elocal
     e = torch.stack([local_energy(lp, R[w], S[w], m_star, lambda_r, h_z) for w in range(Wm)])
     if ewald is not None:
@@ -470,3 +476,59 @@ def vmc_iteration(spec, theta, unravel, R, S, *, A, step, n_sweeps, n_spin_flips
     O = per_sample_O(spec, theta, unravel, R[:Wm], S[:Wm])
     d = minsr_direction(O, clip_energies(e, clip_k), lam)
     return theta - lr * d, R, S, e
+
+
+# ----------------------------------------------------------------------------------------------
+# the Adam driver's gradient and step  (reference: src/nqs/train.py:53-61 with optax.adam)
+# ----------------------------------------------------------------------------------------------
+def surrogate_grad(spec, theta, unravel, R, S, e):
+    """train.py:53-59 — the real-ravel gradient of 2 mean_w Re[conj(e_w - mean e) log psi(R_w,
+    S_w)] (reverse mode through the oracle log psi), (dL/dRe, dL/dIm) for complex leaves."""
+    ec = torch.conj(e - e.mean())
+
+    def loss(t):
+        p = unravel(t)
+        lp = torch.stack([logpsi(spec, p, R[w], S[w]) for w in range(R.shape[0])])
+        return 2.0 * torch.real(ec * lp).mean()
+
+    return grad(loss)(theta)
+
+
+def jax_grad_tree(unravel, g):
+    """The tree jax.grad returns for a real loss, from the real-ravel gradient g: a real leaf
+    takes its components, a complex leaf c = a + i b the complex number dL/da - i dL/db (JAX's
+    transpose convention for complex inputs)."""
+    tree = unravel(g)
+
+    def conj_tree(node):
+        return {k: conj_tree(v) if isinstance(v, dict) else (torch.conj(v) if v.is_complex() else v)
+                for k, v in node.items()}
+
+    return conj_tree(tree)
+
+
+def optax_adam(params, grads, state, lr, b1=0.9, b2=0.999, eps=1e-8):
+    """optax.adam(lr) = scale_by_adam(b1, b2, eps) then scale_by_learning_rate, applied with
+    optax.apply_updates, on trees of torch tensors (complex leaves included):
+    mu <- b1 mu + (1 - b1) g;  nu <- b2 nu + (1 - b2) |g|^2;  t <- t + 1;
+    p <- p - lr (mu / (1 - b1^t)) / (sqrt(nu / (1 - b2^t)) + eps).
+    state: None (zeros) or the (t, mu, nu) this function returned. Returns (params, state)."""
+    flat_p = flatten_sorted(params)
+    flat_g = dict(flatten_sorted(grads))
+    if state is None:
+        state = (0, {k: torch.zeros_like(v) for k, v in flat_p},
+                 {k: torch.zeros(v.shape, dtype=F64) for k, v in flat_p})
+    t, mu, nu = state
+    t += 1
+    out, mu2, nu2 = {}, {}, {}
+    for k, p in flat_p:
+        gk = flat_g[k]
+        mu2[k] = b1 * mu[k] + (1.0 - b1) * gk
+        sq = (gk.real ** 2 + gk.imag ** 2) if gk.is_complex() else gk ** 2
+        nu2[k] = b2 * nu[k] + (1.0 - b2) * sq
+        upd = (mu2[k] / (1.0 - b1 ** t)) / (torch.sqrt(nu2[k] / (1.0 - b2 ** t)) + eps)
+        node = out
+        for q in k[:-1]:
+            node = node.setdefault(q, {})
+        node[k[-1]] = p - lr * upd
+    return out, (t, mu2, nu2)

@@ -1,0 +1,171 @@
+"""The vector-Jacobian product of log psi (nqs_logpsi_vjp), its torch.autograd wrapper, the
+per-block activation checkpointing of the reverse pass, and the Adam driver's gradient and step,
+against the oracle (reference src/nqs/train.py:53-61, src/nqs/minsr.py:56-65)."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import build, configs, perturb
+from oracle import nqs_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+KW = [dict(n_dets=3, use_jastrow=True, n_knots=5),
+      dict(use_jastrow=True, jastrow_kind="cusp", learnable_env=True, n_dets=2)]
+
+
+def _cotangent(W, seed):
+    rng = np.random.default_rng(seed)
+    return torch.complex(torch.as_tensor(rng.standard_normal(W)),
+                         torch.as_tensor(rng.standard_normal(W)))
+
+
+@pytest.mark.parametrize("kw", KW)
+def test_vjp_matches_oracle_jacobian(kw):
+    """sum_w Re(c_w O[w]) against the oracle's reverse-mode per-sample Jacobian (1e-10), and
+    the same with the per-block checkpointed reverse pass."""
+    from nqs.minsr import real_ravel
+    from nqs.psiformer import logpsi_vjp
+    g, model = build(**kw)
+    p = perturb(model.init(0), 0.05, 41)
+    theta, _ = real_ravel(p)
+    R, S = configs(model.n_elec, model.L, 5, 42)
+    c = _cotangent(5, 43)
+    ot, ou = O.real_ravel(p["params"])
+    Oo = O.per_sample_O(model, ot, ou, R, S)
+    ref = (c[:, None] * Oo).real.sum(0)
+    scale = max(1.0, float(ref.abs().max()))
+    for ckpt in (False, True):
+        v = logpsi_vjp(model, theta.cuda(), R, S, c, checkpoint_blocks=ckpt).cpu()
+        assert float((v - ref).abs().max()) < 1e-10 * scale, (ckpt, float((v - ref).abs().max()))
+
+
+def test_vjp_equals_contracted_jacobian_config2_model():
+    """At the configuration-2 model (N=16, width 64, 4 blocks, K=4, 16-knot Jastrow), float64:
+    the VJP equals the device per-sample Jacobian contracted with the cotangent."""
+    from nqs import rashba
+    from nqs.minsr import per_sample_O_rows
+    from nqs.psiformer import ContinuumSpinorPsiformer, logpsi_vjp
+    L = float(np.sqrt(np.pi * 16) * 5.0)
+    env = rashba.cell_rashba_envelope(L, 16, 1.0, 0.3, 0.05, 10, (0.1, 0.17))
+    model = ContinuumSpinorPsiformer(16, env["Gs"], env["W"], L, embed_dim=64, depth=4, n_heads=4,
+                                     n_freq=8, n_dets=4, use_jastrow=True, n_knots=16)
+    p = model.init_normal(0, std=0.02, backflow_std=1e-3, jastrow_std=0.02, logw_std=0.1)
+    theta = model.theta(p)
+    R, S = configs(16, L, 64, 5)
+    c = _cotangent(64, 6).cuda()
+    rows = per_sample_O_rows(model, theta, R, S)
+    ref = rows[:64].T @ c.real - rows[64:].T @ c.imag
+    v = logpsi_vjp(model, theta, R, S, c)
+    assert float((v - ref).abs().max() / ref.abs().max()) < 1e-12
+
+
+@pytest.mark.parametrize("precision,dtype", [("fp64", torch.float64), ("mixed", torch.float32)])
+def test_checkpointed_jacobian_is_bit_identical(precision, dtype):
+    """Recomputing each block's activations from its input reproduces the stored-activation
+    Jacobian bit for bit (same kernels, same inputs)."""
+    from nqs import _lib
+    from nqs.psiformer import _prec
+    g, model = build(N=5, embed=32, depth=3, heads=4, n_dets=2, use_jastrow=True, n_knots=5)
+    theta = model.theta(perturb(model.init(0), 0.05, 51))
+    R, S = configs(model.n_elec, model.L, 96, 52)
+    R, S = R.cuda(), S.cuda().to(torch.int32)
+    P, W = model.n_params(), 96
+    h = model.native().handle
+    prec = _prec(precision)
+    outs = []
+    for ckpt in (0, 1):
+        out = torch.full((2 * W, P), float("nan"), dtype=dtype, device="cuda")
+        ws, _ = _lib.workspace_for(h, _lib.OP_PER_SAMPLE_O_CKPT if ckpt else _lib.OP_PER_SAMPLE_O,
+                                   W, prec)
+        _lib.check(_lib.lib().nqs_per_sample_O_ex(
+            h, _lib.ptr(theta), _lib.ptr(R), _lib.ptr(S), W, _lib.ptr(out),
+            0 if dtype == torch.float64 else 1, prec, ckpt, _lib.ptr(ws), ws.numel(),
+            _lib.stream_ptr()), "nqs_per_sample_O_ex")
+        outs.append(out)
+    assert torch.isfinite(outs[0]).all()
+    assert torch.equal(outs[0], outs[1])
+
+
+def test_checkpointing_shrinks_the_workspace():
+    """Per-block checkpointing keeps one block's intermediates instead of all of them."""
+    import ctypes
+    from nqs import _lib
+    g, model = build(N=5, embed=32, depth=4, heads=4)
+    h = model.native().handle
+    sz = []
+    for op in (_lib.OP_PER_SAMPLE_O, _lib.OP_PER_SAMPLE_O_CKPT):
+        n = ctypes.c_size_t(0)
+        _lib.check(_lib.lib().nqs_workspace_size(h, op, 64, _lib.PREC_FP64, ctypes.byref(n)),
+                   "nqs_workspace_size")
+        sz.append(n.value)
+    assert sz[1] < 0.6 * sz[0], sz
+
+
+def test_autograd_surrogate_gradient_matches_oracle():
+    """torch autograd through the differentiable log psi (backward = nqs_logpsi_vjp) of the
+    reference's surrogate 2 mean Re[conj(e - mean e) log psi] equals the oracle's reverse-mode
+    gradient of the same loss (1e-10), and so does the per-sample-Jacobian route
+    (nqs_energy_gradient)."""
+    from nqs import _lib
+    from nqs.minsr import per_sample_O_rows, real_ravel
+    from nqs.train import surrogate_gradient
+    g, model = build(n_dets=2, use_jastrow=True, n_knots=4)
+    p = perturb(model.init(0), 0.05, 61)
+    theta, _ = real_ravel(p)
+    R, S = configs(model.n_elec, model.L, 6, 62)
+    e = _cotangent(6, 63) + 3.0
+    gd = surrogate_gradient(model, theta.cuda(), R, S, e.cuda()).cpu()
+    ot, ou = O.real_ravel(p["params"])
+    go = O.surrogate_grad(model, ot, ou, R, S.long(), e)
+    tol = 1e-10 * max(1.0, float(go.abs().max()))
+    assert float((gd - go).abs().max()) < tol
+    rows = per_sample_O_rows(model, theta.cuda(), R, S)
+    ge = torch.empty(rows.shape[1], dtype=torch.float64, device="cuda")
+    ws = _lib.workspace.get(16 * 6 + 4096)
+    ec = e.cuda().contiguous()
+    _lib.check(_lib.lib().nqs_energy_gradient(_lib.ptr(rows), 0, _lib.ptr(ec), 6, rows.shape[1],
+                                              _lib.ptr(ge), _lib.ptr(ws), ws.numel(),
+                                              _lib.stream_ptr()), "nqs_energy_gradient")
+    assert float((ge.cpu() - go).abs().max()) < tol
+
+
+def test_energy_gradient_against_float64_expression():
+    """nqs_energy_gradient against the plain float64 expression
+    (2/W) (O_re^T Re(e - mean e) + O_im^T Im(e - mean e)) on a random [2W][P] matrix."""
+    from nqs import _lib
+    rng = np.random.default_rng(71)
+    W, P = 300, 1000
+    Orows = torch.as_tensor(rng.standard_normal((2 * W, P))).cuda()
+    e = torch.complex(torch.as_tensor(rng.standard_normal(W)),
+                      torch.as_tensor(rng.standard_normal(W))).cuda()
+    ec = e - e.mean()
+    ref = (2.0 / W) * (Orows[:W].T @ ec.real + Orows[W:].T @ ec.imag)
+    out = torch.empty(P, dtype=torch.float64, device="cuda")
+    ws = _lib.workspace.get(16 * W + 4096)
+    _lib.check(_lib.lib().nqs_energy_gradient(_lib.ptr(Orows), 0, _lib.ptr(e), W, P,
+                                              _lib.ptr(out), _lib.ptr(ws), ws.numel(),
+                                              _lib.stream_ptr()), "nqs_energy_gradient")
+    assert float((out - ref).abs().max()) < 1e-12 * float(ref.abs().max())
+
+
+def test_adam_complex_step_matches_optax_restatement():
+    """Three Adam steps on the real ravel with the complex-leaf partner table equal optax.adam
+    applied to the trees jax.grad would give (oracle restatement), to 1e-14."""
+    from nqs.minsr import real_ravel
+    from nqs.train import Adam
+    g, model = build(n_dets=2, learnable_env=True)
+    p = perturb(model.init(0), 0.05, 81)
+    theta, _ = real_ravel(p)
+    opt = Adam(lr=1e-2, model=model)
+    th = theta.cuda().clone()
+    st = opt.init(th)
+    tree, ost = p["params"], None
+    rng = np.random.default_rng(82)
+    ot, ou = O.real_ravel(p["params"])
+    for _ in range(3):
+        gv = torch.as_tensor(rng.standard_normal(theta.shape[0]))
+        st = opt.update(gv.cuda(), st, th)
+        tree, ost = O.optax_adam(tree, O.jax_grad_tree(ou, gv), ost, 1e-2)
+    ref, _ = O.real_ravel(tree)
+    assert float((th.cpu() - ref).abs().max()) < 1e-14
