@@ -773,7 +773,9 @@ static int trtri_diag(const double* L, int64_t ldl, int n, double* dinv, cudaStr
 __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L, int64_t ldl,
                                                    int n, const double* __restrict__ dinv,
                                                    double* __restrict__ v,
-                                                   double* __restrict__ xb, int transposed) {
+                                                   double* __restrict__ xb, int transposed,
+                                                   const int* __restrict__ skip) {
+  if (skip && *skip) return;  // uniform over the grid: written by an earlier launch
   cg::grid_group grid = cg::this_grid();
   const int nblk = (n + CB - 1) / CB;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -917,7 +919,11 @@ __device__ __forceinline__ void st_release_gpu(int* p, int v) {
 
 __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L, int64_t ldl,
                                                     int n, const double* __restrict__ dinv,
-                                                    double* v, int* flags, int transposed) {
+                                                    double* v, int* flags, int transposed,
+                                                    const int* __restrict__ skip,
+                                                    uint32_t wait_limit, int dead_block) {
+  // skip: uniform over the grid (written by an earlier launch), so no CTA is left waiting
+  if (skip && *skip) return;
   const int nblk = (n + CB - 1) / CB;
   const int s = blockIdx.x;
   const int k0 = s * CB, bs = min(CB, n - k0);
@@ -959,7 +965,7 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
       int gu = 0;
       uint32_t w = 0;
       while (ld_acquire_gpu(flags + t) == 0) {
-        if (++w >= kTrsvWaitLimit || ld_acquire_gpu(flags + kTrsvErrSlot) != 0) {
+        if (++w >= wait_limit || ld_acquire_gpu(flags + kTrsvErrSlot) != 0) {
           gu = 1;
           break;
         }
@@ -1017,14 +1023,17 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
     if (tid < bs) v[k0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
   }
   __syncthreads();
-  if (tid == 0) {
+  // dead_block (self-test of the bounded waits only; -1 otherwise): that block never publishes,
+  // so its dependants run into their wait limit
+  if (tid == 0 && s != dead_block) {
     __threadfence();
     st_release_gpu(flags + s, 1);
   }
 }
 
 static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, double* v,
-                     double* xb, int transposed, cudaStream_t st) {
+                     double* xb, int transposed, cudaStream_t st, const int* skip = nullptr,
+                     uint32_t wait_limit = kTrsvWaitLimit, int dead_block = -1) {
   static int grid = 0;
   if (!grid) {
     int dev = 0, nsm = 0, per = 0;
@@ -1048,16 +1057,18 @@ static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, do
   if (nblk <= kTrsvErrSlot && nblk <= max_resident) {
     int* flags = reinterpret_cast<int*>(xb);
     cudaMemsetAsync(flags, 0, sizeof(int) * (kTrsvErrSlot + 1), st);
-    void* fargs[] = {(void*)&L, (void*)&ldl, (void*)&n, (void*)&dinv,
-                     (void*)&v, (void*)&flags, (void*)&transposed};
+    void* fargs[] = {(void*)&L,         (void*)&ldl,   (void*)&n,
+                     (void*)&dinv,      (void*)&v,     (void*)&flags,
+                     (void*)&transposed, (void*)&skip, (void*)&wait_limit,
+                     (void*)&dead_block};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((const void*)k_trsv_flags, nblk, 256, fargs, 0, st);
     if (e != cudaSuccess) return cuda_status(e, "k_trsv_flags");
     NQS_CHECK_LAUNCH("k_trsv_flags");
     return NQS_OK;
   }
-  void* args[] = {(void*)&L,  (void*)&ldl, (void*)&n, (void*)&dinv,
-                  (void*)&v, (void*)&xb,  (void*)&transposed};
+  void* args[] = {(void*)&L,  (void*)&ldl, (void*)&n,          (void*)&dinv,
+                  (void*)&v, (void*)&xb,  (void*)&transposed, (void*)&skip};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_trsv_grid, grid, 256, args, 0, st);
   if (e != cudaSuccess) return cuda_status(e, "k_trsv_grid");
   NQS_CHECK_LAUNCH("k_trsv_grid");
@@ -1170,7 +1181,9 @@ template <typename TO>
 __global__ void k_gemv_t(const TO* __restrict__ O, int M, int Mh, int64_t K,
                          const double* __restrict__ mu, const double* __restrict__ x,
                          double* __restrict__ out, double* __restrict__ out_lo,
-                         double* __restrict__ theta, double lr) {
+                         double* __restrict__ theta, double lr,
+                         const int* __restrict__ skip = nullptr) {
+  if (skip && *skip) return;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
   const double m0 = mu ? mu[k] : 0.0, m1 = mu ? mu[K + k] : 0.0;
@@ -1195,7 +1208,9 @@ template <typename TO, bool VEC>
 __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, int M, int Mh,
                                                       int64_t K, const double* __restrict__ mu,
                                                       const double* __restrict__ x, int mchunk,
-                                                      double* __restrict__ part) {
+                                                      double* __restrict__ part,
+                                                      const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int64_t k0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
   if (k0 >= K) return;
   const int m_lo = blockIdx.y * mchunk, m_hi = min(M, m_lo + mchunk);
@@ -1248,7 +1263,9 @@ __global__ void __launch_bounds__(256) k_gemv_t_split(const TO* __restrict__ O, 
 template <typename TO>
 __global__ void k_gemv_t_reduce(const double* __restrict__ part, int nsplit, int64_t K,
                                 double* __restrict__ out, double* __restrict__ out_lo,
-                                double* __restrict__ theta, double lr) {
+                                double* __restrict__ theta, double lr,
+                                const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
   double acc = 0.0;
@@ -1262,24 +1279,24 @@ __global__ void k_gemv_t_reduce(const double* __restrict__ part, int nsplit, int
 template <typename TO>
 static int gemv_t(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* x,
                   double* out, double* out_lo, double* theta, double lr, double* part,
-                  size_t part_elems, cudaStream_t st) {
+                  size_t part_elems, cudaStream_t st, const int* skip = nullptr) {
   int nsplit = std::max(1, std::min(16, M / 512));
   while (nsplit > 1 && (size_t)nsplit * K > part_elems) --nsplit;
   if (nsplit <= 1 || !part) {
     k_gemv_t<TO><<<(unsigned)((K + 255) / 256), 256, 0, st>>>(O, M, Mh, K, mu, x, out, out_lo,
-                                                               theta, lr);
+                                                               theta, lr, skip);
     NQS_CHECK_LAUNCH("k_gemv_t");
     return NQS_OK;
   }
   const int mchunk = (M + nsplit - 1) / nsplit;
   const dim3 g((unsigned)((K + 1023) / 1024), (unsigned)nsplit);
   if (K % 4 == 0)
-    k_gemv_t_split<TO, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part);
+    k_gemv_t_split<TO, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part, skip);
   else
-    k_gemv_t_split<TO, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part);
+    k_gemv_t_split<TO, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, x, mchunk, part, skip);
   NQS_CHECK_LAUNCH("k_gemv_t_split");
   k_gemv_t_reduce<TO><<<(unsigned)((K + 255) / 256), 256, 0, st>>>(part, nsplit, K, out, out_lo,
-                                                                   theta, lr);
+                                                                   theta, lr, skip);
   NQS_CHECK_LAUNCH("k_gemv_t_reduce");
   return NQS_OK;
 }
@@ -1290,7 +1307,9 @@ template <typename TO, int RB, bool VEC>
 __global__ void __launch_bounds__(256, sizeof(TO) == 4 ? 2 : 1) k_gemv_n_resid_rows(
     const TO* __restrict__ O, int M, int Mh, int64_t K, const double* __restrict__ mu,
     const double* __restrict__ v, const double* __restrict__ b, double lam0,
-    const double* __restrict__ lam_extra, const double* __restrict__ x, double* __restrict__ r) {
+    const double* __restrict__ lam_extra, const double* __restrict__ x, double* __restrict__ r,
+    const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const double lam = lam0 + (lam_extra ? *lam_extra : 0.0);
   const int m0 = blockIdx.x * RB;
   const int nr = min(RB, M - m0);
@@ -1353,22 +1372,22 @@ __global__ void __launch_bounds__(256, sizeof(TO) == 4 ? 2 : 1) k_gemv_n_resid_r
     const int i = threadIdx.x, m = m0 + i;
     double t = 0.0;
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[i][q];
-    r[m] = (b[m] - lam * x[m]) - t;
+    r[m] = ((b ? b[m] : 0.0) - lam * x[m]) - t;
   }
 }
 
 template <typename TO>
 static int gemv_n_resid(const TO* O, int M, int Mh, int64_t K, const double* mu, const double* v,
                         const double* b, double lam0, const double* lam_extra, const double* x,
-                        double* r, cudaStream_t st) {
+                        double* r, cudaStream_t st, const int* skip = nullptr) {
   constexpr int RB = 16;
   const unsigned g = (unsigned)((M + RB - 1) / RB);
   if (K % 4 == 0)
     k_gemv_n_resid_rows<TO, RB, true><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, b, lam0, lam_extra,
-                                                         x, r);
+                                                         x, r, skip);
   else
     k_gemv_n_resid_rows<TO, RB, false><<<g, 256, 0, st>>>(O, M, Mh, K, mu, v, b, lam0,
-                                                          lam_extra, x, r);
+                                                          lam_extra, x, r, skip);
   NQS_CHECK_LAUNCH("k_gemv_n_resid_rows");
   return NQS_OK;
 }
@@ -1448,6 +1467,140 @@ static int solve_refined(const double* L, int M, int Mh, int64_t K, const TO* O,
     NQS_TRY(trsv_grid(L, M, M, dinv, r, xb, 1, st));
     k_axpy<<<(M + 255) / 256, 256, 0, st>>>(M, r, y);
     NQS_CHECK_LAUNCH("k_axpy");
+  }
+  return NQS_OK;
+}
+
+// --------------------------------------------------------------------------------------------
+// Preconditioned conjugate gradients for (A A^T + lam I) y = b at the caller's lam, A = O - mu
+// applied from O itself (float64 accumulation, two passes over O per iteration), preconditioned
+// by M = L L^T, the float64 Cholesky factor of a tensor-core Gram + (lam + delta) I. Scalars stay
+// on the device (no host synchronisation). pcg[0] = r.z, pcg[1] = r0.z0; it_info[0] = stop flag
+// (1 converged, 2 breakdown), it_info[1] = iterations done. Once the flag is set every later
+// kernel of the loop returns at once.
+// --------------------------------------------------------------------------------------------
+constexpr int kPcgThreads = 1024;
+
+__device__ double block_sum_1024(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    red[32] = t;
+  }
+  __syncthreads();
+  t = red[32];
+  __syncthreads();
+  return t;
+}
+
+// p = z, pcg[0] = pcg[1] = r.z, flags cleared
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n, const double* __restrict__ r,
+                                                          const double* __restrict__ z,
+                                                          double* __restrict__ p,
+                                                          double* __restrict__ pcg,
+                                                          int* __restrict__ it_info) {
+  __shared__ double red[33];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    p[i] = z[i];
+    a = fma(r[i], z[i], a);
+  }
+  const double rz = block_sum_1024(a, red);
+  if (threadIdx.x == 0) {
+    pcg[0] = rz;
+    pcg[1] = rz;
+    it_info[0] = (rz > 0.0 && isfinite(rz)) ? 0 : 1;  // b = 0 (or M r = 0): nothing to do
+    it_info[1] = 0;
+  }
+}
+
+// qn = -A p: alpha = r.z / (p.A p); y += alpha p; r -= alpha A p (= r + alpha qn)
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_alpha(int n, const double* __restrict__ p,
+                                                           const double* __restrict__ qn,
+                                                           double* __restrict__ y,
+                                                           double* __restrict__ r,
+                                                           const double* __restrict__ pcg,
+                                                           int* __restrict__ it_info) {
+  if (it_info[0]) return;
+  __shared__ double red[33];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a = fma(p[i], -qn[i], a);
+  const double pAp = block_sum_1024(a, red);
+  if (!(pAp > 0.0) || !isfinite(pAp)) {  // loss of positivity: keep the current iterate
+    if (threadIdx.x == 0) it_info[0] = 2;
+    return;
+  }
+  const double alpha = pcg[0] / pAp;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    y[i] = fma(alpha, p[i], y[i]);
+    r[i] = fma(alpha, qn[i], r[i]);
+  }
+}
+
+// z <- r (the triangular solves then overwrite z with M^-1 r)
+__global__ void k_pcg_copy(int n, const double* __restrict__ r, double* __restrict__ z,
+                           const int* __restrict__ it_info) {
+  if (it_info[0]) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = r[i];
+}
+
+// beta = r.z / previous r.z; p = z + beta p; stop when sqrt(r.z / r0.z0) <= tol
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_beta(int n, const double* __restrict__ r,
+                                                          const double* __restrict__ z,
+                                                          double* __restrict__ p,
+                                                          double* __restrict__ pcg,
+                                                          int* __restrict__ it_info, double tol) {
+  if (it_info[0]) return;
+  __shared__ double red[33];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a = fma(r[i], z[i], a);
+  const double rz = block_sum_1024(a, red);
+  const double beta = rz / pcg[0];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = fma(beta, p[i], z[i]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    pcg[0] = rz;
+    it_info[1] += 1;
+    if (!(rz > tol * tol * pcg[1])) it_info[0] = 1;
+  }
+}
+
+template <typename TO>
+static int solve_pcg(const double* L, int M, int Mh, int64_t K, const TO* O, const double* mu,
+                     double lam, const double* b, double* y, double* r, double* z, double* p,
+                     double* q, double* pcg, int* it_info, double* tmpK, double* xb, int max_it,
+                     double tol, double* part, size_t part_elems, cudaStream_t st) {
+  double* dinv = xb + 2 * CB;
+  NQS_TRY(trtri_diag(L, M, M, dinv, st));
+  // y0 = M^-1 b, r0 = b - A y0, z0 = M^-1 r0
+  cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
+  NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 0, st));
+  NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 1, st));
+  NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, tmpK, nullptr, nullptr, 0.0, part, part_elems, st));
+  NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, b, lam, nullptr, y, r, st));
+  cudaMemcpyAsync(z, r, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
+  NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 0, st));
+  NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 1, st));
+  k_pcg_init<<<1, kPcgThreads, 0, st>>>(M, r, z, p, pcg, it_info);
+  NQS_CHECK_LAUNCH("k_pcg_init");
+  for (int it = 0; it < max_it; ++it) {
+    // q = -(A A^T + lam I) p
+    NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, p, tmpK, nullptr, nullptr, 0.0, part, part_elems, st,
+                       it_info));
+    NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, nullptr, lam, nullptr, p, q, st, it_info));
+    k_pcg_alpha<<<1, kPcgThreads, 0, st>>>(M, p, q, y, r, pcg, it_info);
+    NQS_CHECK_LAUNCH("k_pcg_alpha");
+    k_pcg_copy<<<(M + 255) / 256, 256, 0, st>>>(M, r, z, it_info);
+    NQS_CHECK_LAUNCH("k_pcg_copy");
+    NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 0, st, it_info));
+    NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 1, st, it_info));
+    k_pcg_beta<<<1, kPcgThreads, 0, st>>>(M, r, z, p, pcg, it_info, tol);
+    NQS_CHECK_LAUNCH("k_pcg_beta");
   }
   return NQS_OK;
 }
@@ -1538,6 +1691,18 @@ __global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W
 // ============================================================================================
 // host driver
 // ============================================================================================
+// relative reduction of the preconditioned residual sqrt(r.z / r0.z0) at which the conjugate
+// gradients stop by default
+constexpr double kPcgDefaultTol = 1e-3;
+
+// caller-facing status from the internal slots: [0] non-positive pivot, [1] Gram timeout,
+// [2] floored pivots, [3] PCG iterations, [4] PCG stop reason (0 iteration limit, 1 converged,
+// 2 breakdown); n_info of them are written
+__global__ void k_pack_info(const int* __restrict__ bad, int* __restrict__ info, int n_info) {
+  if (threadIdx.x != 0) return;
+  const int v[5] = {bad[0], bad[1], bad[2], bad[5], bad[4]};
+  for (int i = 0; i < n_info && i < 5; ++i) info[i] = v[i];
+}
 size_t minsr_part_elems(int W) {
   const size_t n = 2 * (size_t)W;
   return std::max<size_t>(std::min<size_t>(16 * n * n, (size_t)8 << 20), (size_t)CB * CB);
@@ -1550,12 +1715,14 @@ size_t minsr_workspace(int W, int64_t P, int odtype, int gram) {
   add(sizeof(double) * 2 * P);          // column means
   add(sizeof(double) * n);              // etil
   add(sizeof(double) * n);              // y
-  add(sizeof(double) * n);              // refinement residual
+  add(sizeof(double) * n);              // refinement / PCG residual
+  add(sizeof(double) * 3 * n);          // PCG z, p, q
+  add(sizeof(double) * 4);              // PCG scalars
   add(sizeof(double) * 2 * P);          // Otil^T y and a spare P-vector
   add(sizeof(double) * n * n);          // T -> L
   add(sizeof(double) * (2 * n + 5));    // Gram row sums, block sums, mean diagonal
   add(sizeof(double) * trsv_elems(n));  // triangular-solve exchange + diagonal-block inverses
-  add(sizeof(int) * 4);                 // status
+  add(sizeof(int) * 8);                 // status, PCG stop flag and iteration count
   add(sizeof(double) * 2);              // pivot floor, extra damping
   add(sizeof(double) * minsr_part_elems(W));  // split-K partials
   if (gram == 0 && odtype == 1) add(sizeof(double) * n * P);  // float64 Otil from float32 O
@@ -1575,13 +1742,14 @@ int nqs_minsr_workspace_size(int W, int64_t P, int o_dtype, int gram_prec, size_
   return NQS_OK;
 }
 
-int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t P, double lam,
-                        int gram_prec, int n_refine, double* out_dtheta, double* theta_io,
-                        double lr, int* status_dev, double* damping_out, void* wsp, size_t wsb,
-                        void* stream) {
-  cudaStream_t st = (cudaStream_t)stream;
+static int minsr_direction_impl(void* O, int o_dtype, const double* eps, int W, int64_t P,
+                                double lam, int gram_prec, int max_it, double tol,
+                                double* out_dtheta, double* theta_io, double lr, int* info_dev,
+                                int n_info, double* damping_out, void* wsp, size_t wsb,
+                                cudaStream_t st) {
   if (!O || !eps || W < 1 || P < 1 || (o_dtype != 0 && o_dtype != 1) || gram_prec < 0 ||
-      gram_prec > 2 || n_refine < 0 || n_refine > 8 || (!out_dtheta && !theta_io)) {
+      gram_prec > 2 || max_it < 0 || max_it > 64 || !(tol >= 0.0) ||
+      (!out_dtheta && !theta_io)) {
     set_error("nqs_minsr_direction: invalid argument");
     return NQS_ERR_INVALID_ARG;
   }
@@ -1596,19 +1764,21 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   double* et = ws.take<double>(n);
   double* y = ws.take<double>(n);
   double* r = ws.take<double>(n);
+  double* zpq = ws.take<double>(3 * (size_t)n);
+  double* pcg = ws.take<double>(4);
   double* tmpK = ws.take<double>(P);
   double* tmpK_lo = ws.take<double>(P);
   double* xb = ws.take<double>(trsv_elems(n));
   double* rsum = ws.take<double>(2 * (size_t)n + 5);
   double* T = ws.take<double>((size_t)n * n);
-  int* bad = ws.take<int>(4);
+  int* bad = ws.take<int>(8);  // [0..2] status, [4] PCG stop reason, [5] PCG iterations
   const size_t part_elems = minsr_part_elems(W);
   double* part = ws.take<double>(part_elems);
   if (!part) return NQS_ERR_WORKSPACE;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaMemsetAsync(bad, 0, sizeof(int) * 4, st);
+  cudaMemsetAsync(bad, 0, sizeof(int) * 8, st);
   const dim3 cg((unsigned)((P + 255) / 256), 2);
   if (o_dtype == 0)
     k_colmean<double><<<cg, 256, 0, st>>>((const double*)O, W, P, mu);
@@ -1649,12 +1819,12 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
     k_gram_center<<<dim3((n + 255) / 256, n), 256, 0, st>>>(T, n, W, rsum, rsum + 2 * n);
     NQS_CHECK_LAUNCH("k_gram_center");
   }
-  // A tensor-core Gram accumulated in float32 carries absolute errors ~ u T_ii (u = 2^-8 BF16
-  // operands, 2^-11 TF32), far above a small lam along the Jacobian's near-null directions. Its
-  // solve therefore uses the damping lam + delta, delta = u mean(T_ii) (written to damping_out),
-  // and the refinement below solves that system exactly against the true operator.
+  // A tensor-core Gram differs from Otil Otil^T by its operand rounding (a PSD perturbation of
+  // the small eigenvalues) and by the float32 accumulation (a slightly indefinite one, of order
+  // 1e-4 mean(T_ii) on the Jacobians of the wavefunction). Its Cholesky factor with the shift
+  // lam + delta, delta = 1e-4 mean(T_ii), preconditions conjugate gradients on the exact system
+  // (Otil Otil^T + lam I) y = etil, applied from O itself: the solve is at the caller's lam.
   const double* floor_p = nullptr;
-  const double* lam_x = nullptr;
   if (gram_prec == 0) {
     k_add_diag<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam);
     NQS_CHECK_LAUNCH("k_add_diag");
@@ -1662,31 +1832,62 @@ int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t 
   } else {
     double* fl = ws.take<double>(2);
     if (!fl) return NQS_ERR_WORKSPACE;
-    k_add_diag_noise<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam,
-                                                       gram_prec == 1 ? 0x1p-8 : 0x1p-11,
-                                                       rsum + 2 * n + 4, fl + 1);
+    k_add_diag_noise<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam, 1e-4, rsum + 2 * n + 4,
+                                                       fl + 1);
     NQS_CHECK_LAUNCH("k_add_diag_noise");
     k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-16 : 0x1p-20, fl);
     NQS_CHECK_LAUNCH("k_pivot_floor");
     floor_p = fl;
-    lam_x = fl + 1;
     if (damping_out) cudaMemcpyAsync(damping_out, fl + 1, sizeof(double), cudaMemcpyDeviceToDevice, st);
   }
   NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
-  if (op_dtype == 0)
-    NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
-                                  tmpK_lo, xb, n_refine, part, part_elems, st));
-  else
-    NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, lam_x, et, y, r, tmpK,
-                                 tmpK_lo, xb, n_refine, part, part_elems, st));
+  double* z = zpq;
+  double* pp = zpq + n;
+  double* q = zpq + 2 * (size_t)n;
+  if (gram_prec == 0) {
+    if (op_dtype == 0)
+      NQS_TRY(solve_refined<double>(T, n, W, P, (const double*)Oop, mu_op, lam, nullptr, et, y, r,
+                                    tmpK, tmpK_lo, xb, max_it, part, part_elems, st));
+    else
+      NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, nullptr, et, y, r,
+                                   tmpK, tmpK_lo, xb, max_it, part, part_elems, st));
+  } else {
+    if (op_dtype == 0)
+      NQS_TRY(solve_pcg<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, z, pp, q,
+                                pcg, bad + 4, tmpK, xb, max_it, tol, part, part_elems, st));
+    else
+      NQS_TRY(solve_pcg<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, z, pp, q, pcg,
+                               bad + 4, tmpK, xb, max_it, tol, part, part_elems, st));
+  }
   if (op_dtype == 0)
     NQS_TRY(gemv_t<double>((const double*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io,
                            lr, part, part_elems, st));
   else
     NQS_TRY(gemv_t<float>((const float*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io, lr,
                           part, part_elems, st));
-  if (status_dev) cudaMemcpyAsync(status_dev, bad, 3 * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (info_dev) {
+    k_pack_info<<<1, 32, 0, st>>>(bad, info_dev, n_info);
+    NQS_CHECK_LAUNCH("k_pack_info");
+  }
   return NQS_OK;
+}
+
+int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int W, int64_t P, double lam,
+                        int gram_prec, int n_refine, double* out_dtheta, double* theta_io,
+                        double lr, int* status_dev, double* damping_out, void* wsp, size_t wsb,
+                        void* stream) {
+  return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, n_refine, kPcgDefaultTol,
+                              out_dtheta, theta_io, lr, status_dev, 3, damping_out, wsp, wsb,
+                              (cudaStream_t)stream);
+}
+
+int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int W, int64_t P,
+                           double lam, int gram_prec, int max_iters, double tol,
+                           double* out_dtheta, double* theta_io, double lr, int* info_dev,
+                           double* damping_out, void* wsp, size_t wsb, void* stream) {
+  return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, max_iters, tol, out_dtheta,
+                              theta_io, lr, info_dev, 5, damping_out, wsp, wsb,
+                              (cudaStream_t)stream);
 }
 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {

@@ -184,6 +184,9 @@ _SIGS.update({
     "nqs_minsr_direction": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_double, c_int, c_int,
                              c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_size_t,
                              c_void_p], c_int),
+    "nqs_minsr_direction_ex": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_double, c_int, c_int,
+                                c_double, c_void_p, c_void_p, c_double, c_void_p, c_void_p,
+                                c_void_p, c_size_t, c_void_p], c_int),
     "nqs_clip_energies": ([c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p], c_int),
     "nqs_energy_gradient": ([c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_size_t,
                              c_void_p], c_int),

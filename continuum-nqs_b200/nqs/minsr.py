@@ -103,27 +103,36 @@ def _as_rows(O):
 _GRAM = {"fp64": 0, "bf16": 1, "tf32": 2}
 
 
+PCG_MAX_ITERS = 24  # conjugate-gradient iterations allowed to a tensor-core Gram's solve
+PCG_TOL = 1e-3      # ... and the preconditioned-residual reduction at which it stops
+
+
 def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True,
-               n_refine=1, damping_out=None):
-    """Sample-space natural gradient on the device. O_rows is [2W][P] (f64 or f32; a float64
-    O_rows is centred in place by the float64 Gram). Returns dtheta (P,) and updates theta in
-    place by -lr dtheta when given."""
+               n_refine=None, damping_out=None, info=None, tol=PCG_TOL):
+    """Sample-space natural gradient on the device, at damping lam. O_rows is [2W][P] (f64 or
+    f32; a float64 O_rows is centred in place by the float64 Gram). gram "fp64": float64 Gram,
+    Cholesky and n_refine (default 1) refinement steps; "bf16" / "tf32": tensor-core Gram whose
+    factor preconditions conjugate gradients on the exact system (n_refine = iteration limit,
+    default PCG_MAX_ITERS, stopping at tol). info (optional int32[5] on the device) receives
+    the status and the CG iteration count (nqs_minsr_direction_ex). Returns dtheta (P,) and
+    updates theta in place by -lr dtheta when given."""
     from . import _lib
     _lib.require_cuda()
     dev = O_rows.device
     n, P = O_rows.shape
     W = n // 2
-    eps = torch.as_tensor(eps).to(dev, torch.complex128).contiguous()
+    eps = torch.as_tensor(eps).to(dev, torch.complex128).resolve_conj().contiguous()
     od = 0 if O_rows.dtype == torch.float64 else 1
     g = _GRAM[gram]
+    if n_refine is None:
+        n_refine = 1 if g == 0 else PCG_MAX_ITERS
     nb = ctypes_size(W, P, od, g)
     ws = _lib.workspace.get(nb)
     d = torch.empty(P, dtype=F64, device=dev) if want_direction else None
-    _lib.check(_lib.lib().nqs_minsr_direction(
-        _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, int(n_refine), _lib.ptr(d),
-        _lib.ptr(theta),
-        float(lr), None, _lib.ptr(damping_out), _lib.ptr(ws), ws.numel(), _lib.stream_ptr()),
-        "nqs_minsr_direction")
+    _lib.check(_lib.lib().nqs_minsr_direction_ex(
+        _lib.ptr(O_rows), od, _lib.ptr(eps), W, P, float(lam), g, int(n_refine), float(tol),
+        _lib.ptr(d), _lib.ptr(theta), float(lr), _lib.ptr(info), _lib.ptr(damping_out),
+        _lib.ptr(ws), ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction_ex")
     return d
 
 
@@ -136,7 +145,7 @@ def ctypes_size(W, P, od, g):
     return n.value
 
 
-def minsr_direction(O, eps, lam, gram="fp64", n_refine=2):
+def minsr_direction(O, eps, lam, gram="fp64", n_refine=None):
     """Natural-gradient direction via the SAMPLE-space (2W x 2W) solve (minsr.py:76-81).
     O: complex (W, P) or real [2W][P]; the input is not modified."""
     rows = _as_rows(O)
@@ -255,7 +264,8 @@ class VMCIteration:
         self.prec_name = precision
         self.prec = _prec(precision)
         self.gram = gram or ("fp64" if self.prec == _lib.PREC_FP64 else "bf16")
-        self.n_refine = int(n_refine if n_refine is not None else (1 if self.gram == "fp64" else 2))
+        self.n_refine = int(n_refine if n_refine is not None
+                            else (1 if self.gram == "fp64" else PCG_MAX_ITERS))
         dev = self.R.device
         self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
         self._O = None  # the [2W][P] Jacobian, allocated on first use
@@ -264,8 +274,10 @@ class VMCIteration:
         self.stats = torch.zeros(5, dtype=F64, device=dev)
         self.acc_pos = torch.zeros(self.W, dtype=F64, device=dev)
         self.acc_spin = torch.zeros(self.W, dtype=F64, device=dev)
-        self.status = torch.zeros(3, dtype=torch.int32, device=dev)
-        self.damping = torch.zeros(1, dtype=F64, device=dev)  # extra damping of a TC Gram
+        # [0] non-positive pivot, [1] Gram timeout, [2] floored pivots, [3] CG iterations,
+        # [4] CG stop reason (nqs_minsr_direction_ex)
+        self.status = torch.zeros(5, dtype=torch.int32, device=dev)
+        self.damping = torch.zeros(1, dtype=F64, device=dev)  # preconditioner shift of a TC Gram
         # external spin field (vectorised ext_field: positions (..., 2) -> (..., 3))
         self.ext_field = ext_field
         self.field = (torch.empty(self.W, self.N, 3, dtype=F64, device=dev)
@@ -339,11 +351,11 @@ class VMCIteration:
         _lib.check(L.nqs_clip_energies(_lib.ptr(self.e), self.W, self.clip_k,
                                        _lib.ptr(self.e_clip), _lib.ptr(self.stats),
                                        _lib.stream_ptr()), "nqs_clip_energies")
-        _lib.check(L.nqs_minsr_direction(
+        _lib.check(L.nqs_minsr_direction_ex(
             _lib.ptr(self.O), 0 if self.o_dtype == torch.float64 else 1, _lib.ptr(self.e_clip),
-            self.W, self.P, self.lam, _GRAM[self.gram], self.n_refine, None, _lib.ptr(self.theta),
-            self.lr, _lib.ptr(self.status), _lib.ptr(self.damping), _lib.ptr(self.ws),
-            self.ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction")
+            self.W, self.P, self.lam, _GRAM[self.gram], self.n_refine, PCG_TOL, None,
+            _lib.ptr(self.theta), self.lr, _lib.ptr(self.status), _lib.ptr(self.damping),
+            _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()), "nqs_minsr_direction_ex")
 
     def step(self, inject=None):
         """One iteration; inject as in sample() replaces the sweeps' random draws."""

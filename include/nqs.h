@@ -226,21 +226,31 @@ int nqs_logpsi_vjp(NqsModel* model, const double* theta, const double* R, const 
 /* MinSR direction (src/nqs/minsr.py:68-81): O is the [2W][P] output of nqs_per_sample_O
  * (o_dtype 0 = f64, 1 = f32), eps complex[W] the (clipped) local energies.
  *   Otil = O - column mean (per half), etil = [Re; Im](eps - mean eps),
- *   T = Otil Otil^T, (T + lam I) = L L^T (float64 Cholesky), y = (T + lam I)^-1 etil,
- *   dtheta = Otil^T y;  out_dtheta (nullable) receives dtheta, theta_io (nullable) is updated
- *   theta -= lr dtheta in the same pass.
- * gram_prec: 0 = float64 SIMT Gram (a float64 O is centred IN PLACE), 1 = BF16 tcgen05 Gram,
- * 2 = TF32 tcgen05 Gram (both float32 accumulation). A tensor-core Gram solves with the damping
- * lam + delta, delta = u mean(diag T) (u = 2^-8 BF16, 2^-11 TF32: its absolute rounding level);
- * damping_out (nullable, device double) receives delta (0 for the float64 Gram). n_refine (0..8)
- * steps of iterative refinement of y against the exact operator Otil Otil^T + (lam + delta) I
- * (applied with O itself, never the rounded Gram). status_dev (nullable, device int) is set
- * non-zero when a Cholesky pivot was not positive; status_dev[1] when a tensor-core Gram CTA hit
- * its bounded-wait limit; status_dev[2] counts pivots raised to the floor u * max T_ii
- * (u = 2^-16 BF16, 2^-20 TF32) in the factor of a tensor-core Gram, which only preconditions the
- * refinement against the exact operator (3 ints). */
+ *   y = (Otil Otil^T + lam I)^-1 etil,  dtheta = Otil^T y;  out_dtheta (nullable) receives
+ *   dtheta, theta_io (nullable) is updated theta -= lr dtheta in the same pass.
+ * gram_prec 0: float64 SIMT Gram T = Otil Otil^T (a float64 O is centred IN PLACE), float64
+ *   Cholesky of T + lam I, then max_iters (0..64) steps of iterative refinement against the
+ *   exact operator.
+ * gram_prec 1 (BF16) / 2 (TF32): the Gram runs on the tcgen05 tensor cores (float32
+ *   accumulation); the float64 Cholesky factor of T + (lam + delta) I, delta = 1e-4 mean(T_ii),
+ *   preconditions conjugate gradients on the EXACT system (Otil Otil^T + lam I) y = etil, whose
+ *   operator is applied from O itself with float64 accumulation: the solve is at the caller's
+ *   lam. CG stops after max_iters iterations or when the preconditioned residual has fallen by
+ *   tol (sqrt(r.z / r0.z0) <= tol); the iterations left are skipped on the device.
+ * damping_out (nullable, device double) receives delta (0 for the float64 Gram).
+ * info_dev (nullable, device int[5]): [0] non-zero when a Cholesky pivot was not positive,
+ * [1] a tensor-core Gram CTA hit its bounded-wait limit, [2] pivots raised to the floor
+ * u max T_ii (u = 2^-16 BF16, 2^-20 TF32) in the preconditioner's factor, [3] CG iterations done,
+ * [4] why CG stopped (0 iteration limit, 1 converged, 2 loss of positivity). */
 int nqs_minsr_workspace_size(int n_walkers, int64_t n_params, int o_dtype, int gram_prec,
                              size_t* bytes);
+int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int n_walkers,
+                           int64_t n_params, double lam, int gram_prec, int max_iters, double tol,
+                           double* out_dtheta, double* theta_io, double lr, int* info_dev,
+                           double* damping_out, void* workspace, size_t workspace_bytes,
+                           void* stream);
+/* The same with tol = 1e-3, max_iters = n_refine and status_dev (nullable, device int[3]) =
+ * info_dev[0..2]. */
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
                         int64_t n_params, double lam, int gram_prec, int n_refine,
                         double* out_dtheta, double* theta_io, double lr, int* status_dev,
