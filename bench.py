@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sample work")
+    ap.add_argument("--trajectory", type=int, default=5,
+                    help="iterations of the mixed-vs-float64 trajectory comparison (0: skip)")
     return ap.parse_args()
 
 
@@ -254,27 +256,30 @@ def run_ours(a, rank, world):
     if not a.no_fp64 and a.fp64_steps > 0:
         from nqs.minsr import minsr_step
         it64 = VMCIteration(model, it.theta, it.R, it.S, precision="fp64", **common)
-        # accuracy of the mixed path against float64 on identical walkers and parameters
+        # accuracy of the mixed path against float64 on identical walkers and parameters, both
+        # solved at the configured damping lam
         it.energies()
         it64.energies()
         em, e64 = it.e.real.double(), it64.e.real.double()
         it.jacobian()
         it64.jacobian()
         delta = torch.zeros(1, dtype=torch.float64, device=dev)
+        info = torch.zeros(5, dtype=torch.int32, device=dev)
         d_mixed = minsr_step(it.O.clone(), it.e, su.lam, "bf16", n_refine=it.n_refine,
-                             damping_out=delta)
-        dl = float(delta.item())
+                             damping_out=delta, info=info)
         d_64 = minsr_step(it64.O.clone(), it64.e, su.lam, "fp64")
-        d_64d = minsr_step(it64.O.clone(), it64.e, su.lam + dl, "fp64")
-        n64, n64d = float(d_64.norm()), float(d_64d.norm())
+        n64 = float(d_64.norm())
+        inf = info.tolist()
         acc = {"dE_per_electron": float((em.mean() - e64.mean()).abs()) / su.N,
                "dE_target": 1e-4,
                "dvar_rel": float((em.var() - e64.var()).abs() / e64.var()),
                "dvar_target": 0.05,
-               "bf16_gram_extra_damping": dl,
-               "dtheta_rel_vs_fp64_same_damping": float((d_mixed - d_64d).norm()) / n64d,
+               "lam": su.lam,
                "dtheta_rel_vs_fp64_lam": float((d_mixed - d_64).norm()) / n64,
                "dtheta_cos_vs_fp64_lam": float((d_mixed * d_64).sum()) / (float(d_mixed.norm()) * n64),
+               "dtheta_target": 1e-2,
+               "bf16_preconditioner_shift": float(delta.item()),
+               "pcg_iterations": inf[3], "pcg_stop": ["limit", "converged", "breakdown"][inf[4]],
                "E_fp64": float(e64.mean()), "E_mixed": float(em.mean())}
         it64.step()
         torch.cuda.synchronize()
@@ -288,6 +293,9 @@ def run_ours(a, rank, world):
         fp64 = {"ms_per_step": ms64, "VMC_iter_per_s": 1000.0 / ms64,
                 "mixed_speedup": ms64 / ms, "E": float(it64.stats[0])}
         del it64
+    traj = None
+    if not a.no_fp64 and a.trajectory > 0:
+        traj = trajectories(model, it, common, a.trajectory, su)
     # ------------------------------------------------ roofline of the dominant kernel: the
     # tensor-core row GEMMs of the network (HBM-bound), timed per launch over the timed steps
     peaks, src = load_peaks()
@@ -339,7 +347,32 @@ def run_ours(a, rank, world):
                  "algorithmic_flops": gflop}
     return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof,
                 roofline_second=roof_other, roofline_gram=roof_gram, clocks=clk,
-                launches=launches, su=su, model=model, P=it.P, acc=acc)
+                launches=launches, su=su, model=model, P=it.P, acc=acc, traj=traj)
+
+
+def trajectories(model, it, common, n_iter, su):
+    """n_iter VMC iterations of the mixed path and of the all-float64 path from the same theta,
+    walkers and random stream (seed, counter): per iteration |dE|/N and the relative difference
+    of var(E_loc) between the two runs, and their maxima."""
+    from nqs.minsr import VMCIteration
+    st = it.state_dict()
+    runs = {}
+    for prec in ("mixed", "fp64"):
+        r = VMCIteration(model, st["theta"], st["R"], st["S"], precision=prec, **common)
+        r.load_state_dict(st)
+        E, V = [], []
+        for _ in range(n_iter):
+            r.step()
+            s = r.stats.cpu().tolist()
+            E.append(s[0])
+            V.append(s[2])
+        runs[prec] = (E, V)
+        del r
+    dE = [abs(a - b) / su.N for a, b in zip(runs["mixed"][0], runs["fp64"][0])]
+    dV = [abs(a - b) / b for a, b in zip(runs["mixed"][1], runs["fp64"][1])]
+    return {"iterations": n_iter, "dE_per_electron": dE, "dvar_rel": dV,
+            "max_dE_per_electron": max(dE), "max_dvar_rel": max(dV),
+            "E_mixed": runs["mixed"][0], "E_fp64": runs["fp64"][0]}
 
 
 def traffic_ratio():
@@ -356,88 +389,155 @@ def traffic_ratio():
 
 
 # ---------------------------------------------------------------------------------------------
-# CPU baseline: the float64 oracle on a bounded sample, extrapolated to the full iteration
+# CPU baseline: whole iterations of the float64 oracle port, measured at a few walker counts
 # ---------------------------------------------------------------------------------------------
-def cpu_sample(cfg, budget_s, walkers=None):
-    """Time the reference algorithm (oracle restatement: recomputed log psi per proposal, dense
-    Hessian kinetic term, reverse-mode per-sample gradients, explicit Gram + LU solve) on a
-    bounded sample and extrapolate to one full iteration. Returns (iter/s, description)."""
-    sys.path.insert(0, ROOT)
-    import numpy as np
-    from oracle import nqs_oracle as O
-    from nqs.configs import config
-    torch.set_num_threads(os.cpu_count() or 1)
-    model, params, su = config(cfg, walkers)
-    W, N = su.n_walkers, su.N
-    p = params
-    f = lambda r, s: O.logpsi(model, p, r, s)  # noqa: E731
-    rng = np.random.default_rng(0)
-    R = torch.as_tensor(rng.uniform(0, su.L, (N, 2)))
-    S = torch.as_tensor(rng.integers(0, 2, N))
-    def timed(fn, reps=1):
-        fn()  # warm: torch.func builds its transforms on the first call
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            fn()
-        return (time.perf_counter() - t0) / reps
+def workload_config(su, P):
+    """The `config` object both arms print (same workload, same keys)."""
+    return {"workload": f"{su.name}: N={su.N}, W={su.n_walkers}, P={P}; {su.n_sweeps} sweeps + "
+                        "local energies with Ewald + per-sample Jacobian + median-MAD clip + "
+                        "MinSR update",
+            "walkers": su.n_walkers, "electrons": su.N, "params": P}
 
-    # one walker, one sweep (1 joint move + 2 flips, log psi recomputed per proposal)
-    t_sweep = timed(lambda: O.mcmc_sweep(f, su.L, R, S, su.step,
-                                         torch.as_tensor(rng.standard_normal((N, 2))), 0.5,
-                                         rng.integers(0, N, 2), rng.uniform(size=2)), 2)
-    t_eloc = timed(lambda: O.local_energy(f, R, S, 1.0, su.lambda_r, su.h_z))
-    ew = O.Ewald(su.L, 1.0, su.ewald_eta, su.n_real, su.n_recip)
-    t_coul = timed(lambda: ew.energy(R.numpy()), 3)
-    theta, unravel = O.real_ravel(p["params"])
-    t_O = timed(lambda: O.per_sample_O(model, theta, unravel, R[None], S[None]))
-    P = theta.shape[0]
-    # explicit Gram of the 2W x P matrix (the reference forms the full Otil Otil^T) + LU solve,
-    # sampled at m rows and scaled by flops
-    m = min(2 * W, 512)
-    A = torch.randn(m, P, dtype=torch.float64)
-    t_g = timed(lambda: A @ A.T)
-    gemm_rate = 2.0 * m * m * P / t_g
-    n = min(2 * W, 2048)
-    Tm = torch.randn(n, n, dtype=torch.float64)
-    Tm = Tm @ Tm.T + n * torch.eye(n, dtype=torch.float64)
-    rhs = torch.randn(n, dtype=torch.float64)
-    t_lu = timed(lambda: torch.linalg.solve(Tm, rhs))
-    lu_rate = (2.0 / 3.0) * n ** 3 / t_lu
-    n2 = 2 * W
-    t_iter = (W * (su.n_sweeps * t_sweep + t_eloc + t_coul + t_O) + 2.0 * n2 * n2 * P / gemm_rate
-              + (2.0 / 3.0) * n2 ** 3 / lu_rate)
-    desc = (f"float64 oracle (torch CPU, {torch.get_num_threads()} threads) timed on 1 walker: "
-            f"sweep {t_sweep * 1e3:.1f} ms, E_loc (dense Hessian + SOC) {t_eloc * 1e3:.0f} ms, "
-            f"Ewald {t_coul * 1e3:.1f} ms, per-sample grad {t_O * 1e3:.0f} ms; Gram at "
-            f"{gemm_rate / 1e9:.0f} GFLOP/s ({m} rows sampled), LU at {lu_rate / 1e9:.0f} GFLOP/s "
-            f"(n={n}); extrapolated to W={W}: {t_iter:.0f} s per iteration")
-    return 1.0 / t_iter, desc, torch.get_num_threads()
+
+class CpuIteration:
+    """The reference algorithm on the host (oracle port: float64 torch on the CPU, all host
+    threads): whole VMC iterations (sweeps with log psi recomputed per proposal, dense-Hessian
+    local energies, Ewald, reverse-mode per-sample Jacobian, clip, explicit Gram + LU solve,
+    update) at a small walker count, and the explicit Gram / LU rates at the full size."""
+
+    def __init__(self, cfg, walkers=None):
+        sys.path.insert(0, ROOT)
+        import numpy as np
+        from oracle import nqs_oracle as O
+        from nqs.configs import config
+        torch.set_num_threads(os.cpu_count() or 1)
+        self.O, self.np = O, np
+        self.model, self.params, self.su = config(cfg, walkers)
+        self.theta, self.unravel = O.real_ravel(self.params["params"])
+        self.P = int(self.theta.shape[0])
+        self.ew = O.Ewald(self.su.L, 1.0, self.su.ewald_eta, self.su.n_real, self.su.n_recip)
+        self.rng = np.random.default_rng(0)
+
+    def iteration(self, W):
+        """Seconds of one whole oracle iteration over W walkers."""
+        su = self.su
+        R = torch.as_tensor(self.rng.uniform(0, su.L, (W, su.N, 2)))
+        S = torch.as_tensor(self.rng.integers(0, 2, (W, su.N)))
+        t0 = time.perf_counter()
+        self.O.vmc_iteration(self.model, self.theta, self.unravel, R, S, A=su.L, step=su.step,
+                             n_sweeps=su.n_sweeps, n_spin_flips=2, rng=self.rng, m_star=1.0,
+                             lambda_r=su.lambda_r, h_z=su.h_z, ewald=self.ew, lam=su.lam,
+                             lr=su.lr, clip_k=5.0)
+        return time.perf_counter() - t0
+
+    def rates(self):
+        """FLOP/s of the explicit Gram (2 n^2 P, sampled at 512 rows) and the LU solve
+        ((2/3) n^3, sampled at n = 2048), the two steps whose cost grows faster than W."""
+        n_full = 2 * self.su.n_walkers
+        m = min(n_full, 512)
+        A = torch.randn(m, self.P, dtype=torch.float64)
+        A @ A.T
+        t0 = time.perf_counter()
+        A @ A.T
+        gemm = 2.0 * m * m * self.P / (time.perf_counter() - t0)
+        n = min(n_full, 2048)
+        T = torch.randn(n, n, dtype=torch.float64)
+        T = T @ T.T + n * torch.eye(n, dtype=torch.float64)
+        rhs = torch.randn(n, dtype=torch.float64)
+        torch.linalg.solve(T, rhs)
+        t0 = time.perf_counter()
+        torch.linalg.solve(T, rhs)
+        lu = (2.0 / 3.0) * n ** 3 / (time.perf_counter() - t0)
+        return gemm, lu
+
+    def model_full(self, samples, gemm, lu):
+        """Seconds per full iteration: the mean measured time when the samples ran at the full
+        walker count; otherwise t(W) = a + b W fitted to the measured whole iterations (least
+        squares) plus the Gram and LU of the full 2W system at the measured rates."""
+        Ws = [w for w, _ in samples]
+        ts = [t for _, t in samples]
+        W = self.su.n_walkers
+        if set(Ws) == {W}:
+            t = sum(ts) / len(ts)
+            return t, 0.0, t / W
+        if len(set(Ws)) > 1:
+            n = len(Ws)
+            mw, mt = sum(Ws) / n, sum(ts) / n
+            b = sum((w - mw) * (t - mt) for w, t in samples) / sum((w - mw) ** 2 for w in Ws)
+            a = mt - b * mw
+        else:
+            a, b = 0.0, ts[0] / Ws[0]
+        n2 = 2 * W
+        t = a + b * W + 2.0 * n2 * n2 * self.P / gemm + (2.0 / 3.0) * n2 ** 3 / lu
+        return t, a, b
+
+    def describe(self, samples, a, b, gemm, lu, t_full):
+        Ws = sorted({w for w, _ in samples})
+        if Ws == [self.su.n_walkers]:
+            return (f"float64 oracle port (torch CPU, {torch.get_num_threads()} threads), whole "
+                    f"iterations at the configuration's W = {Ws[0]} measured end to end "
+                    f"({len(samples)} runs): {t_full:.1f} s per iteration")
+        return (f"float64 oracle port (torch CPU, {torch.get_num_threads()} threads), whole "
+                f"iterations measured at W = {Ws} ({len(samples)} runs, "
+                f"{1e3 * sum(t for _, t in samples) / len(samples):.0f} ms mean), fitted "
+                f"t = a + b W (a = {a:.3f} s, b = {b:.4f} s/walker); plus the explicit Gram "
+                f"2(2W)^2 P at {gemm / 1e9:.0f} GFLOP/s and the LU (2/3)(2W)^3 at {lu / 1e9:.0f} "
+                f"GFLOP/s measured here: {t_full:.0f} s per iteration at W = {self.su.n_walkers}")
+
+
+def sample_walkers(cpu, budget_s):
+    """Walker counts for the timed whole iterations: the configuration's own W when one whole
+    iteration fits in budget_s, else 1, 2, 4, ... while one iteration stays within about
+    budget_s / 4 (at least two distinct counts)."""
+    cpu.iteration(1)  # builds the torch.func transforms
+    t1 = cpu.iteration(1)
+    if cpu.su.n_walkers * t1 <= budget_s:
+        return [cpu.su.n_walkers]
+    Ws, w = [1], 2
+    while (len(Ws) < 2 or w * t1 <= budget_s / 4) and w <= cpu.su.n_walkers:
+        Ws.append(w)
+        w *= 2
+    return Ws
+
+
+def cpu_baseline(cfg, budget_s, walkers=None):
+    """(iter/s, description, threads) of the reference algorithm on the host cores."""
+    cpu = CpuIteration(cfg, walkers)
+    Ws = sample_walkers(cpu, budget_s)
+    samples = [(w, cpu.iteration(w)) for w in Ws]
+    gemm, lu = cpu.rates()
+    t_full, a, b = cpu.model_full(samples, gemm, lu)
+    return 1.0 / t_full, cpu.describe(samples, a, b, gemm, lu, t_full), torch.get_num_threads()
 
 
 def run_reference(a):
+    """The reference arm: the reference algorithm (the float64 oracle port: the reference's own
+    JAX code cannot be installed on this image) on the host cores. Each step is one whole
+    iteration at a small walker count (cycling through the sample counts), so ms_per_step is a
+    measured time; value is the full configuration's iterations/s from the fit."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    vals = []
-    desc = ""
-    cores = 1
+    cpu = CpuIteration(a.config, a.walkers)
+    Ws = sample_walkers(cpu, a.cpu_budget)
+    samples = []
     for i in range(a.warmup + a.steps):
-        v, desc, cores = cpu_sample(a.config, a.cpu_budget, a.walkers)
+        w = Ws[i % len(Ws)]
+        t = cpu.iteration(w)
         if i >= a.warmup:
-            vals.append(v)
-        if i == 0 and a.warmup + a.steps > 2:
-            pass
-    v = sum(vals) / max(len(vals), 1)
-    from nqs.configs import config
-    _, _, su = config(a.config, a.walkers)
+            samples.append((w, t))
+    gemm, lu = cpu.rates()
+    t_full, ca, cb = cpu.model_full(samples, gemm, lu)
+    v = 1.0 / t_full
+    ms = 1e3 * sum(t for _, t in samples) / max(len(samples), 1)
+    desc = cpu.describe(samples, ca, cb, gemm, lu, t_full)
     line = {"impl": "reference", "metric": "VMC iter/s", "value": v, "unit": "VMC iter/s",
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / v,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "ms_per_step_note": "measured whole oracle iterations at the sample walker counts",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"{su.name}: N={su.N}, W={su.n_walkers}, 10 sweeps + E_loc + "
-                                   "O + MinSR", "walkers": su.n_walkers, "electrons": su.N},
-            "cpu_baseline": {"value": v, "unit": "VMC iter/s", "cores": cores, "kind": "port",
-                             "sample": desc},
+            "data": "synthetic", "config": workload_config(cpu.su, cpu.P),
+            "cpu_baseline": {"value": v, "unit": "VMC iter/s", "cores": torch.get_num_threads(),
+                             "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": "VMC iter/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -459,7 +559,7 @@ def main():
     cpu = None
     if rank == 0 and not a.no_cpu:
         try:
-            v, desc, cores = cpu_sample(a.config, a.cpu_budget, a.walkers)
+            v, desc, cores = cpu_baseline(a.config, a.cpu_budget, a.walkers)
             cpu = {"value": v, "unit": "VMC iter/s", "cores": cores, "kind": "port", "sample": desc}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "VMC iter/s", "cores": None, "kind": "port",
@@ -477,17 +577,18 @@ def main():
         "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/bf16+f64",
         "data": "synthetic (seeded uniform walkers, N(0,0.02^2) weights)",
-        "config": {"workload": f"{su.name}: N={su.N}, W={W}, width 64, 4 blocks, K=4, Jastrow; "
-                               "10 sweeps + forward-Laplacian E_loc + Ewald + O + MinSR",
-                   "walkers": W, "electrons": su.N, "params": r["P"], "precision": "mixed",
-                   "gram": "bf16 tcgen05", "l2": "working set (O: 2W x P f32 = "
-                   f"{2 * W * r['P'] * 4 / 1e9:.1f} GB) exceeds L2 every step",
-                   "parallelism": f"{world} independent replicas"},
+        "config": workload_config(su, r["P"]),
+        "precision": {"network": "float32, Dense GEMMs tcgen05 TF32", "gram": "bf16 tcgen05",
+                      "determinants / Cholesky / energies": "float64"},
+        "l2": f"working set (O: 2W x P f32 = {2 * W * r['P'] * 4 / 1e9:.1f} GB) exceeds L2 "
+              "every step",
+        "parallelism": f"{world} independent replicas",
         "walker_steps_per_s": world * W * su.n_sweeps / (ph["sample_ms"] * 1e-3),
         "eloc_evals_per_s": world * W / (ph["local_energy_ms"] * 1e-3),
         "phases_ms": ph, "energy": {"mean": r["stats"][0], "err": r["stats"][1],
                                     "var": r["stats"][2]},
-        "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "roofline": r["roofline"],
+        "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "trajectory_vs_fp64": r["traj"],
+        "roofline": r["roofline"],
         "roofline_second": r["roofline_second"], "roofline_gram": r["roofline_gram"],
         "cpu_baseline": cpu,
         "e2e": r["e2e"], "clocks": r["clocks"], "gpu_launches": int(r["launches"]),
