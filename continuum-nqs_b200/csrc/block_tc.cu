@@ -52,6 +52,7 @@ struct BlkArgs {
   float* X;  // [rows][D], updated in place
   int rows, N, rpt, ntiles;
   int* err;
+  uint32_t wait_limit;
 };
 
 // TMEM -> registers, 32 lanes x NC columns (one column per register); completes with tmem_wait
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
   // wait for this group's last commit; every thread of the group leaves together and takes the
   // same decision (an abort anywhere in the CTA ends the group's tile loop)
   auto wait_mma = [&]() -> bool {
-    const bool ok = mbar_wait(bar, phase & 1, abort);
+    const bool ok = mbar_wait(bar, phase & 1, abort, a.wait_limit);
     ++phase;
     const bool bad = group_bar_or(g, !ok || *abort);
     fence_after();
@@ -599,6 +600,7 @@ int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, 
   a.rpt = (128 / N) * N;
   a.ntiles = (a.rows + a.rpt - 1) / a.rpt;
   a.err = tcn.err;
+  a.wait_limit = wait_limit_or(tc::WAIT_LIMIT);
   // every operand is read as float4: a layout whose parameter vectors do not start on 16 bytes
   // is left to the unfused launches (*done stays false)
   uintptr_t al = reinterpret_cast<uintptr_t>(X);

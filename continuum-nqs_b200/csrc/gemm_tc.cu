@@ -23,6 +23,7 @@ struct RowGemmArgs {
   int rows, K, Nout, Npad, C, res_inplace, stages, act;
   const float* bias;
   int* err;
+  uint32_t wait_limit;
 };
 
 // Persistent, warp-specialised: warp 0 streams 128-row A tiles through an S-stage TMA ring (the
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
       int issued = 0;
       for (int i = 0; i < my_tiles; ++i) {
         const int s = i % S;
-        if (i >= S && !mbar_wait(&aempty[s], ((i / S) - 1) & 1, abort)) break;
+        if (i >= S && !mbar_wait(&aempty[s], ((i / S) - 1) & 1, abort, g.wait_limit)) break;
         const int m0 = (blockIdx.x + i * gridDim.x) * RG_BM;
         mbar_expect_tx(&afull[s], (uint32_t)stage_bytes);
         for (int kb = 0; kb < nkb; ++kb)
@@ -108,18 +109,18 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
         issued = i + 1;
       }
       // drain: no bulk copy may still be writing shared memory when the CTA exits
-      mbar_wait(bfull, 0, abort);
+      mbar_wait(bfull, 0, abort, g.wait_limit);
       for (int i = max(0, issued - S); i < issued; ++i)
-        mbar_wait(&afull[i % S], (i / S) & 1, abort);
+        mbar_wait(&afull[i % S], (i / S) & 1, abort, g.wait_limit);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t id = make_idesc(1, RG_BM, g.Npad);
-      if (mbar_wait(bfull, 0, abort)) {
+      if (mbar_wait(bfull, 0, abort, g.wait_limit)) {
         for (int i = 0; i < my_tiles; ++i) {
           const int s = i % S, b = i & 1;
-          if (!mbar_wait(&afull[s], (i / S) & 1, abort)) break;
-          if (i >= 2 && !mbar_wait(&accempty[b], ((i >> 1) - 1) & 1, abort)) break;
+          if (!mbar_wait(&afull[s], (i / S) & 1, abort, g.wait_limit)) break;
+          if (i >= 2 && !mbar_wait(&accempty[b], ((i >> 1) - 1) & 1, abort, g.wait_limit)) break;
           fence_after();
           const uint32_t td = tmem + (uint32_t)b * ncols;
           const uint8_t* sa = sA + s * stage_bytes;
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
     int nst = 0;
     for (int i = 0; i < my_tiles; ++i) {
       const int b = i & 1;
-      const bool ok = mbar_wait(&accfull[b], (i >> 1) & 1, abort);
+      const bool ok = mbar_wait(&accfull[b], (i >> 1) & 1, abort, g.wait_limit);
       fence_after();
       if (!__all_sync(0xffffffffu, ok && !*abort)) break;
       const int r0 = (blockIdx.x + i * gridDim.x) * RG_BM + ew * 32;
@@ -312,7 +313,8 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     attr = true;
   }
-  tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, act, bias, err};
+  tc::RowGemmArgs a{rows, K, Nout, Npad, C, Res ? 1 : 0, S, act, bias, err,
+                    wait_limit_or(tc::WAIT_LIMIT)};
   const int ntiles = (rows + tc::RG_BM - 1) / tc::RG_BM;
   const bool prof = g_gemm_prof && g_gemm_n < kGemmProfCap;
   if (prof) {

@@ -49,7 +49,8 @@ __device__ __forceinline__ void tile_coords(int t, int* ti, int* tj) {
 template <int KIND>
 __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUtensorMap tmap,
                                                     int M, int64_t K, double* __restrict__ T,
-                                                    int64_t ldt, int* __restrict__ err) {
+                                                    int64_t ldt, int* __restrict__ err,
+                                                    uint32_t wait_limit) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~(uintptr_t)1023);
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
     int issued = 0;
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
-      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort)) break;
+      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort, wait_limit)) break;
       mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
       tma_load_2d(sA + s * A_BYTES, &tmap, kb * KE, i0, &full[s]);
       tma_load_2d(sB + s * B_BYTES, &tmap, kb * KE, j0, &full[s]);
@@ -102,13 +103,13 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
     }
     // drain: every issued stage's loads must have landed before the CTA may exit
     for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
-      mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort);
+      mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort, wait_limit);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
     constexpr uint32_t id = idesc<KIND>();
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
-      if (!mbar_wait(&full[s], (kb / STAGES) & 1, abort)) break;
+      if (!mbar_wait(&full[s], (kb / STAGES) & 1, abort, wait_limit)) break;
       fence_after();
       const uint8_t* a = sA + s * A_BYTES;
       const uint8_t* b = sB + s * B_BYTES;
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
   }
   // ---------------- epilogue (all 4 warps) ----------------
   __syncwarp();
-  const bool ok = mbar_wait(done, 0, abort);
+  const bool ok = mbar_wait(done, 0, abort, wait_limit);
   fence_after();
   const bool go = __all_sync(0xffffffffu, ok && !*abort);  // tcgen05.ld is warp-collective
   if (go) {
@@ -291,11 +292,13 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
   if (prec == 1) {
     cudaFuncSetAttribute(tc::k_gram_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
-    tc::k_gram_tc<0><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err);
+    tc::k_gram_tc<0><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err,
+                                                         wait_limit_or(tc::WAIT_LIMIT));
   } else {
     cudaFuncSetAttribute(tc::k_gram_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
-    tc::k_gram_tc<1><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err);
+    tc::k_gram_tc<1><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err,
+                                                         wait_limit_or(tc::WAIT_LIMIT));
   }
   NQS_CHECK_LAUNCH("k_gram_tc");
   if (g_prof_stop) cudaEventRecord(g_prof_stop, st);

@@ -1033,7 +1033,8 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
 
 static int trsv_grid(const double* L, int64_t ldl, int n, const double* dinv, double* v,
                      double* xb, int transposed, cudaStream_t st, const int* skip = nullptr,
-                     uint32_t wait_limit = kTrsvWaitLimit, int dead_block = -1) {
+                     uint32_t wait_limit = 0, int dead_block = -1) {
+  if (!wait_limit) wait_limit = wait_limit_or(kTrsvWaitLimit);
   static int grid = 0;
   if (!grid) {
     int dev = 0, nsm = 0, per = 0;
@@ -1888,6 +1889,28 @@ int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int W, int64
   return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, max_iters, tol, out_dtheta,
                               theta_io, lr, info_dev, 5, damping_out, wsp, wsb,
                               (cudaStream_t)stream);
+}
+
+int nqs_selftest_bounded_wait(const double* L, int n, int dead_block, unsigned wait_limit,
+                              double* v, void* wsp, size_t wsb, int* status_dev, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!L || !v || !wsp || !status_dev || n < 1 || n > CB * kTrsvErrSlot || wait_limit < 1 ||
+      dead_block < -1 || dead_block >= (n + CB - 1) / CB) {
+    set_error("nqs_selftest_bounded_wait: invalid argument");
+    return NQS_ERR_INVALID_ARG;
+  }
+  if (wsb < sizeof(double) * trsv_elems(n)) {
+    set_error("nqs_selftest_bounded_wait: workspace %zu < %zu", wsb,
+              sizeof(double) * trsv_elems(n));
+    return NQS_ERR_WORKSPACE;
+  }
+  double* xb = (double*)wsp;
+  double* dinv = xb + 2 * CB;
+  NQS_TRY(trtri_diag(L, n, n, dinv, st));
+  NQS_TRY(trsv_grid(L, n, n, dinv, v, xb, 0, st, nullptr, wait_limit, dead_block));
+  const cudaError_t e = cudaMemcpyAsync(status_dev, reinterpret_cast<int*>(xb) + kTrsvErrSlot,
+                                        sizeof(int), cudaMemcpyDeviceToDevice, st);
+  return e == cudaSuccess ? NQS_OK : cuda_status(e, "nqs_selftest_bounded_wait");
 }
 
 int nqs_gram_solve_workspace_size(int M, int64_t K, size_t* bytes) {

@@ -19,6 +19,12 @@ void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
 extern std::atomic<unsigned long long> g_launches;  // kernels launched by this library
 extern cudaEvent_t g_prof_start, g_prof_stop;      // optional events around the Gram kernel
+// bound of every device-side wait, in polls (0: each wait's built-in default); nqs_set_wait_limit
+extern std::atomic<unsigned> g_wait_limit;
+inline unsigned wait_limit_or(unsigned dflt) {
+  const unsigned v = g_wait_limit.load(std::memory_order_relaxed);
+  return v ? v : dflt;
+}
 }  // namespace nqs
 
 // every kernel launch is followed by exactly one NQS_CHECK_LAUNCH (it also counts the launch)

@@ -10,6 +10,7 @@
 namespace nqs {
 namespace tc {
 
+// default bound of an mbarrier wait (polls); nqs_set_wait_limit overrides it per process
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -34,9 +35,10 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait; returns false (and raises the CTA abort flag) when the limit runs out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
-  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+// bounded wait (limit polls); returns false (and raises the CTA abort flag) when it runs out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                          uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_try(bar, parity)) return true;
     if ((i & 255u) == 255u && *abort) return false;
   }

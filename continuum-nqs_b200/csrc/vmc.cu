@@ -19,6 +19,7 @@ namespace nqs {
 
 static thread_local char g_err[512] = "";
 std::atomic<unsigned long long> g_launches{0};
+std::atomic<unsigned> g_wait_limit{0};
 cudaEvent_t g_prof_start = nullptr, g_prof_stop = nullptr;
 
 void set_error(const char* fmt, ...) {
@@ -318,6 +319,11 @@ const char* nqs_last_error(void) { return g_err; }
 
 unsigned long long nqs_kernel_launches(void) { return g_launches.load(); }
 
+int nqs_set_wait_limit(unsigned polls) {
+  g_wait_limit.store(polls, std::memory_order_relaxed);
+  return NQS_OK;
+}
+
 int nqs_profile_events(void* start, void* stop) {
   g_prof_start = (cudaEvent_t)start;
   g_prof_stop = (cudaEvent_t)stop;
@@ -492,6 +498,24 @@ int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cud
   return NQS_OK;
 }
 
+// A bounded wait that ran out in a tensor-core row GEMM or fused block of this call (*err set)
+// leaves that pass's activations incomplete: every log psi, gradient and Laplacian the batch
+// produced becomes NaN, so the entry point's outputs (log psi, E_loc, O's forward inputs, the
+// Metropolis ratios, which then reject) carry the failure to the caller instead of wrong numbers.
+__global__ void k_poison_on_timeout(const int* __restrict__ err, cplx* __restrict__ L, size_t nL,
+                                    cplx* __restrict__ dL, size_t ndL, cplx* __restrict__ lap) {
+  if (!*err) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nL; i += stride) {
+    if (L) L[i] = cplx{nan, nan};
+    if (lap) lap[i] = cplx{nan, nan};
+  }
+  if (dL)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ndL; i += stride)
+      dL[i] = cplx{nan, nan};
+}
+
 int run_net(NqsModel* m, Ctx& c, int prec, const JobBatch& jb, HeadOut out, cudaStream_t st) {
   const HeadParams hp = make_head_params(m->hm.desc, c.theta64);
   if (prec == NQS_PREC_FP64) {
@@ -500,7 +524,13 @@ int run_net(NqsModel* m, Ctx& c, int prec, const JobBatch& jb, HeadOut out, cuda
   }
   NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
   w.tc = c.tc;
-  return net_forward<float>(m->hm, w, hp, jb, out, c.ws, kMaxRows, st);
+  NQS_TRY(net_forward<float>(m->hm, w, hp, jb, out, c.ws, kMaxRows, st));
+  if (c.tc.err) {
+    k_poison_on_timeout<<<64, 256, 0, st>>>(c.tc.err, out.L, (size_t)jb.n_jobs, out.dL,
+                                            (size_t)jb.n_jobs * jb.n_tan, out.lap);
+    NQS_CHECK_LAUNCH("k_poison_on_timeout");
+  }
+  return NQS_OK;
 }
 
 int check_ws(NqsModel* m, int op, int W, int prec, size_t wsb) {

@@ -197,6 +197,9 @@ _SIGS.update({
     "nqs_adam_update_complex": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                  c_double, c_double, c_double, c_double, c_int, c_void_p], c_int),
     "nqs_kernel_launches": ([], ctypes.c_ulonglong),
+    "nqs_set_wait_limit": ([ctypes.c_uint], c_int),
+    "nqs_selftest_bounded_wait": ([c_void_p, c_int, c_int, ctypes.c_uint, c_void_p, c_void_p,
+                                   c_size_t, c_void_p, c_void_p], c_int),
     "nqs_profile_gemm": ([c_int], c_int),
     "nqs_set_block_fusion": ([c_int], c_int),
     "nqs_profile_block_read": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),

@@ -102,6 +102,22 @@ unsigned long long nqs_kernel_launches(void);
 /* Optional cudaEvent_t pair (NULL to clear) recorded on the caller's stream immediately before and
  * after the Gram kernel inside nqs_minsr_direction, for timing it in isolation. */
 int nqs_profile_events(void* start_event, void* stop_event);
+/* Bound of every device-side wait of the library, in polls (no reference counterpart; failure
+ * detection, process-wide): the tensor-core kernels' mbarrier waits (default 2^22 polls) and the
+ * triangular solves' flag waits (default 2^21 polls, with back-off). 0 restores the defaults. A
+ * wait that runs out aborts its kernel without hanging: a tensor-core Gram reports it through
+ * nqs_minsr_direction's status; a network pass (nqs_logpsi, nqs_local_energy, nqs_mcmc_sweeps,
+ * ...) sets its log psi / gradient / Laplacian outputs to NaN; a triangular solve publishes NaN. */
+int nqs_set_wait_limit(unsigned polls);
+/* Self-test of the flag waits (no reference counterpart; used by the failure-detection test):
+ * solves L x = v in place (L: float64 [n][n] lower triangular, device; n <= 64 x 255) with the
+ * wavefront triangular solve whose 64-row block `dead_block` never publishes its result (-1: all
+ * publish), so the blocks after it wait at most wait_limit polls, give up and publish NaN.
+ * status_dev (device int) receives 1 when a wait ran out, else 0. Workspace: (2 x 64 + 64 x 64 x
+ * ceil(n / 64)) doubles. */
+int nqs_selftest_bounded_wait(const double* L, int n, int dead_block, unsigned wait_limit,
+                              double* v, void* workspace, size_t workspace_bytes, int* status_dev,
+                              void* stream);
 /* Per-launch timing of the tensor-core row GEMMs of the float32 network (profiling aid, no
  * reference counterpart): while enabled, every launch is bracketed by a pair of CUDA events (up to
  * 16384 launches are kept) and its algorithmic bytes (operand rows, weights, output, residual)
