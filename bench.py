@@ -311,8 +311,9 @@ def run_ours(a, rank, world):
             "traffic": per_launch_bytes * ratio if ratio else None,
             "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_ms,
             "launches_per_step": t_n / a.steps, "share_of_step": t_ms / a.steps / ms,
-            "traffic_source": "ncu dram bytes / algorithmic bytes of the same launches, "
-                              "profiles/k_rowgemm_tc_config2.md" if ratio else None}
+            "traffic_source": "ncu DRAM bytes / algorithmic bytes of all row-GEMM launches of one "
+                              "timed step at W = 1024 (profiles/rowgemm_traffic.json), times "
+                              "this run's algorithmic bytes per launch" if ratio else None}
     # the fused value-pass transformer blocks: bytes in/out + weights against HBM, with their
     # tensor-core + attention flops alongside
     b_ms, b_bytes, b_flops, b_n = block_prof
@@ -376,16 +377,13 @@ def trajectories(model, it, common, n_iter, su):
 
 
 def traffic_ratio():
-    """DRAM bytes per algorithmic byte of the row GEMM launches, from the committed ncu summary
-    (profiles/k_rowgemm_tc_config2.md, line 'dram_per_algorithmic: <x>'), or None."""
+    """DRAM bytes per algorithmic byte of the row-GEMM launches from an ncu capture of one timed
+    step (profiles/rowgemm_traffic.json, key dram_bytes_per_algorithmic_byte), or None."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_rowgemm_tc_config2.md")) as f:
-            for line in f:
-                if line.strip().startswith("dram_per_algorithmic:"):
-                    return float(line.split(":", 1)[1])
-    except (OSError, ValueError):
-        pass
-    return None
+        with open(os.path.join(ROOT, "profiles", "rowgemm_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_algorithmic_byte"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 # ---------------------------------------------------------------------------------------------

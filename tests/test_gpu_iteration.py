@@ -22,9 +22,14 @@ def _setup(n):
 
 
 def _walkers(su, W, seed):
+    """Uniform positions and spins; at configuration 1 the two occupied orbitals are the two
+    k = 0 spinors, so psi vanishes when both spins agree: those walkers get opposite spins (the
+    sampler never visits a node)."""
     rng = np.random.default_rng(seed)
     R = torch.as_tensor(rng.uniform(0, su.L, (W, su.N, 2)))
     S = torch.as_tensor(rng.integers(0, 2, (W, su.N)))
+    if su.N == 2:
+        S[:, 1] = 1 - S[:, 0]
     return R, S
 
 
