@@ -352,28 +352,38 @@ def run_ours(a, rank, world):
 
 
 def trajectories(model, it, common, n_iter, su):
-    """n_iter VMC iterations of the mixed path and of the all-float64 path from the same theta,
-    walkers and random stream (seed, counter): per iteration |dE|/N and the relative difference
-    of var(E_loc) between the two runs, and their maxima."""
+    """n_iter VMC iterations of the mixed path and of the all-float64 path, interleaved, from the
+    same theta, walkers and random stream (seed, counter). Per iteration: |dE|/N and its
+    statistical error sqrt(err_mixed^2 + err_fp64^2)/N, the relative difference of var(E_loc),
+    the relative difference of theta, and how many walkers' configurations differ between the
+    two runs (an accept decision that flips with the precision moves that walker onto its own
+    chain; beyond that point the two energies are no longer paired samples)."""
     from nqs.minsr import VMCIteration
     st = it.state_dict()
     runs = {}
     for prec in ("mixed", "fp64"):
         r = VMCIteration(model, st["theta"], st["R"], st["S"], precision=prec, **common)
         r.load_state_dict(st)
-        E, V = [], []
-        for _ in range(n_iter):
+        runs[prec] = r
+    out = {k: [] for k in ("dE_per_electron", "dE_err_per_electron", "dvar_rel", "dtheta_rel",
+                           "walkers_differing", "E_mixed", "E_fp64")}
+    for _ in range(n_iter):
+        for r in runs.values():
             r.step()
-            s = r.stats.cpu().tolist()
-            E.append(s[0])
-            V.append(s[2])
-        runs[prec] = (E, V)
-        del r
-    dE = [abs(a - b) / su.N for a, b in zip(runs["mixed"][0], runs["fp64"][0])]
-    dV = [abs(a - b) / b for a, b in zip(runs["mixed"][1], runs["fp64"][1])]
-    return {"iterations": n_iter, "dE_per_electron": dE, "dvar_rel": dV,
-            "max_dE_per_electron": max(dE), "max_dvar_rel": max(dV),
-            "E_mixed": runs["mixed"][0], "E_fp64": runs["fp64"][0]}
+        m, f = runs["mixed"], runs["fp64"]
+        sm, sf = m.stats.cpu().tolist(), f.stats.cpu().tolist()
+        out["E_mixed"].append(sm[0])
+        out["E_fp64"].append(sf[0])
+        out["dE_per_electron"].append(abs(sm[0] - sf[0]) / su.N)
+        out["dE_err_per_electron"].append(math.sqrt(sm[1] ** 2 + sf[1] ** 2) / su.N)
+        out["dvar_rel"].append(abs(sm[2] - sf[2]) / sf[2])
+        out["dtheta_rel"].append(float((m.theta - f.theta).norm() / f.theta.norm()))
+        diff = ((m.R - f.R).abs().amax(dim=(1, 2)) > 1e-9) | (m.S != f.S).any(dim=1)
+        out["walkers_differing"].append(int(diff.sum()))
+    del runs
+    out.update(iterations=n_iter, max_dE_per_electron=max(out["dE_per_electron"]),
+               max_dvar_rel=max(out["dvar_rel"]))
+    return out
 
 
 def traffic_ratio():
