@@ -155,7 +155,8 @@ def run_ours(a, rank, world):
     _, _, coul = make_ewald(su.L, alpha=1.0, ewald_alpha=su.ewald_eta, n_real=su.n_real,
                             n_recip=su.n_recip)
     common = dict(m_star=1.0, lambda_r=su.lambda_r, h_z=su.h_z, coulomb=coul, lr=su.lr,
-                  lam=su.lam, n_sweeps=su.n_sweeps, step_size=su.step, clip_k=5.0, seed=7 + rank)
+                  lam=su.lam, n_sweeps=su.n_sweeps, step_size=su.step, clip_k=5.0, seed=7 + rank,
+                  checkpoint_blocks=su.checkpoint_blocks)
     it = VMCIteration(model, theta, R0, S0, precision="mixed", gram="bf16", **common)
     it.sample(40)  # thermalise once before timing
     torch.cuda.synchronize()
@@ -255,19 +256,23 @@ def run_ours(a, rank, world):
     acc = None
     if not a.no_fp64 and a.fp64_steps > 0:
         from nqs.minsr import minsr_step
-        it64 = VMCIteration(model, it.theta, it.R, it.S, precision="fp64", **common)
         # accuracy of the mixed path against float64 on identical walkers and parameters, both
-        # solved at the configured damping lam
+        # solved at the configured damping lam; one Jacobian resident at a time (configuration
+        # 5's float64 Jacobian alone is 118 GB)
         it.energies()
-        it64.energies()
-        em, e64 = it.e.real.double(), it64.e.real.double()
+        em, e_mixed = it.e.real.double().clone(), it.e.clone()
         it.jacobian()
-        it64.jacobian()
         delta = torch.zeros(1, dtype=torch.float64, device=dev)
         info = torch.zeros(5, dtype=torch.int32, device=dev)
-        d_mixed = minsr_step(it.O.clone(), it.e, su.lam, "bf16", n_refine=it.n_refine,
+        d_mixed = minsr_step(it.O, e_mixed, su.lam, "bf16", n_refine=it.n_refine,
                              damping_out=delta, info=info)
-        d_64 = minsr_step(it64.O.clone(), it64.e, su.lam, "fp64")
+        it.release_jacobian()
+        torch.cuda.empty_cache()
+        it64 = VMCIteration(model, it.theta, it.R, it.S, precision="fp64", **common)
+        it64.energies()
+        e64 = it64.e.real.double()
+        it64.jacobian()
+        d_64 = minsr_step(it64.O, it64.e, su.lam, "fp64")
         n64 = float(d_64.norm())
         inf = info.tolist()
         acc = {"dE_per_electron": float((em.mean() - e64.mean()).abs()) / su.N,
@@ -293,9 +298,13 @@ def run_ours(a, rank, world):
         fp64 = {"ms_per_step": ms64, "VMC_iter_per_s": 1000.0 / ms64,
                 "mixed_speedup": ms64 / ms, "E": float(it64.stats[0])}
         del it64
+        torch.cuda.empty_cache()
     traj = None
     if not a.no_fp64 and a.trajectory > 0:
-        traj = trajectories(model, it, common, a.trajectory, su)
+        if 2 * su.n_walkers * it.P * 12 < 100e9:  # both runs' Jacobians resident at once
+            traj = trajectories(model, it, common, a.trajectory, su)
+        else:
+            traj = {"skipped": "the two runs' Jacobians (float32 + float64) do not fit together"}
     # ------------------------------------------------ roofline of the dominant kernel: the
     # tensor-core row GEMMs of the network (HBM-bound), timed per launch over the timed steps
     peaks, src = load_peaks()

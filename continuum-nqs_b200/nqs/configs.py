@@ -7,7 +7,13 @@ config2: N=16, r_s=5, Rashba 0.3, Zeeman 0.05; width 64, 4 blocks, 4 heads, 8 ha
          RBF pair Jastrow with 16 centres; Bloch envelopes of the non-interacting Rashba orbitals
          (twist (0.1, 0.17), where the closed shell has a gap); Dense kernels ~N(0, 0.02^2),
          backflow ~N(0, 1e-3^2), Jastrow ~N(0, 0.02^2); 4096 walkers; step 0.2 r_s; 10 sweeps.
-Both: Coulomb coupling 1 through the 2D Ewald sum with eta = 5/L, 7x7 real-space images
+config3: the configuration-2 model and walkers with MinSR damping 1e-4 and the per-block
+         checkpointed reverse pass for the per-sample Jacobian.
+config5: N=48, r_s=5, Rashba 0.3, Zeeman 0.05; width 128, 6 blocks, 8 heads, 8 harmonics, K=8,
+         RBF pair Jastrow with 16 centres; Bloch envelopes at zero twist (the closed shell's gap
+         there is 3.8e-4 Ha, against 5.1e-6 at twist (0.1, 0.17)); initialisation as
+         configuration 2; 8192 walkers, 20 sweeps; checkpointed reverse pass.
+All: Coulomb coupling 1 through the 2D Ewald sum with eta = 5/L, 7x7 real-space images
 (n_real = 3) and the |m| <= 8 reciprocal index box; 2 spin-flip proposals per sweep.
 """
 from __future__ import annotations
@@ -35,10 +41,11 @@ class VMCSetup:
     n_real: int = 3
     n_recip: int = 8
     E_gs: float = 0.0
+    checkpoint_blocks: bool = False
 
 
 def config(n: int, n_walkers: int | None = None):
-    """(model, params, setup) of configuration n (1 or 2)."""
+    """(model, params, setup) of configuration n (1, 2, 3 or 5)."""
     if n == 1:
         N, rs, lr_soc, hz = 2, 2.0, 0.5, 0.1
         L = math.sqrt(math.pi * N) * rs
@@ -47,7 +54,7 @@ def config(n: int, n_walkers: int | None = None):
                                          n_heads=4, n_freq=8, n_dets=1)
         params = model.init(0)
         W = 256
-    elif n == 2:
+    elif n in (2, 3):
         N, rs, lr_soc, hz = 16, 5.0, 0.3, 0.05
         L = math.sqrt(math.pi * N) * rs
         env = rashba.cell_rashba_envelope(L, N, 1.0, lr_soc, hz, 10, (0.1, 0.17))
@@ -56,8 +63,18 @@ def config(n: int, n_walkers: int | None = None):
                                          n_knots=16)
         params = model.init_normal(0, std=0.02, backflow_std=1e-3, jastrow_std=0.02)
         W = 4096
+    elif n == 5:
+        N, rs, lr_soc, hz = 48, 5.0, 0.3, 0.05
+        L = math.sqrt(math.pi * N) * rs
+        env = rashba.cell_rashba_envelope(L, N, 1.0, lr_soc, hz, 10, (0.0, 0.0))
+        model = ContinuumSpinorPsiformer(N, env["Gs"], env["W"], L, embed_dim=128, depth=6,
+                                         n_heads=8, n_freq=8, n_dets=8, use_jastrow=True,
+                                         n_knots=16)
+        params = model.init_normal(0, std=0.02, backflow_std=1e-3, jastrow_std=0.02)
+        W = 8192
     else:
         raise ValueError(f"unknown configuration {n}")
-    setup = VMCSetup(f"config{n}", N, L, lr_soc, hz, n_walkers or W, 10, 0.2 * rs, 1e-3, 0.05,
-                     5.0 / L, E_gs=env["E_gs"])
+    setup = VMCSetup(f"config{n}", N, L, lr_soc, hz, n_walkers or W, 20 if n == 5 else 10,
+                     0.2 * rs, 1e-4 if n == 3 else 1e-3, 0.05, 5.0 / L, E_gs=env["E_gs"],
+                     checkpoint_blocks=n in (3, 5))
     return model, params, setup

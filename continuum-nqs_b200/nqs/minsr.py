@@ -242,7 +242,8 @@ class VMCIteration:
 
     def __init__(self, model, theta, R, S, *, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
                  lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, clip_k=5.0, n_spin_flips=2,
-                 seed=0, counter=0, precision="fp64", gram=None, n_refine=None, ext_field=None):
+                 seed=0, counter=0, precision="fp64", gram=None, n_refine=None, ext_field=None,
+                 checkpoint_blocks=False):
         from . import _lib
         from .psiformer import _prec, as_batch
         _lib.require_cuda()
@@ -263,6 +264,7 @@ class VMCIteration:
         self.seed, self.counter = int(seed), int(counter)
         self.prec_name = precision
         self.prec = _prec(precision)
+        self.checkpoint_blocks = bool(checkpoint_blocks)
         self.gram = gram or ("fp64" if self.prec == _lib.PREC_FP64 else "bf16")
         self.n_refine = int(n_refine if n_refine is not None
                             else (1 if self.gram == "fp64" else PCG_MAX_ITERS))
@@ -284,8 +286,9 @@ class VMCIteration:
                       if ext_field is not None else None)
         h = model.native().handle
         self.h = h
+        op_o = _lib.OP_PER_SAMPLE_O_CKPT if self.checkpoint_blocks else _lib.OP_PER_SAMPLE_O
         sizes = [_lib.workspace_for(h, op, self.W, self.prec)[1]
-                 for op in (_lib.OP_MCMC, _lib.OP_LOCAL_E, _lib.OP_PER_SAMPLE_O)]
+                 for op in (_lib.OP_MCMC, _lib.OP_LOCAL_E, op_o)]
         sizes.append(ctypes_size(self.W, self.P, 0 if self.o_dtype == torch.float64 else 1,
                                  _GRAM[self.gram]))
         self.ws = _lib.workspace.get(max(sizes))
@@ -339,11 +342,18 @@ class VMCIteration:
                 "nqs_local_energy_field")
 
     def jacobian(self):
+        """The per-sample Jacobian O (nqs_per_sample_O_ex; with checkpoint_blocks the reverse
+        pass recomputes each block's activations instead of storing them)."""
         from . import _lib
-        _lib.check(_lib.lib().nqs_per_sample_O(
+        _lib.check(_lib.lib().nqs_per_sample_O_ex(
             self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), self.W,
             _lib.ptr(self.O), 0 if self.o_dtype == torch.float64 else 1, self.prec,
-            _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()), "nqs_per_sample_O")
+            int(self.checkpoint_blocks), _lib.ptr(self.ws), self.ws.numel(), _lib.stream_ptr()),
+            "nqs_per_sample_O_ex")
+
+    def release_jacobian(self):
+        """Free the [2W][P] Jacobian buffer (it is reallocated by the next jacobian())."""
+        self._O = None
 
     def update(self):
         from . import _lib
