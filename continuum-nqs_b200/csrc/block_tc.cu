@@ -16,6 +16,11 @@
 // group's math hides the other's MMA and load latency) and its own TMEM columns; thread 0 of a
 // group issues that group's MMAs and commits them to the group's mbarrier. All waits are bounded
 // (tc_common.cuh); a timed-out wait aborts the CTA and sets *err.
+//
+// Operand precision: TF32 (float32 operand tiles and W^T, kind::tf32) or BF16 (the threads write
+// the operand tiles in BF16 and W^T is staged in BF16, both rounded to nearest even; kind::f16,
+// float32 accumulation; width 64 only, where every K is a multiple of 64).
+#include <cuda_bf16.h>
 #include <cstdio>
 #include <algorithm>
 #include <vector>
@@ -26,11 +31,13 @@
 namespace nqs {
 namespace tc {
 
-template <int D, int HD>
+template <int D, int HD, bool BF = false>
 struct BlkCfg {
   static constexpr int FF = 2 * D, H = D / HD, NQKV = 3 * D;
-  static constexpr int KB = D / 32;                    // 128-byte K-blocks of a D-wide operand
-  static constexpr int W_QKV = NQKV * D * 4, W_O = D * D * 4, W_0 = FF * D * 4, W_1 = D * FF * 4;
+  static constexpr int ES = BF ? 2 : 4;                // operand element bytes
+  static constexpr int KB = D * ES / 128;              // 128-byte K-blocks of a D-wide operand
+  static constexpr int W_QKV = NQKV * D * ES, W_O = D * D * ES, W_0 = FF * D * ES,
+                       W_1 = D * FF * ES;
   static constexpr int W_BYTES = W_QKV + W_O + W_0 + W_1;
   static constexpr int A_BYTES = 128 * D * 4;          // operand tile / row staging
   static constexpr int KV_BYTES = 2 * 128 * HD * 4;    // one head's K and V rows
@@ -151,6 +158,32 @@ __device__ __forceinline__ void load_wt(uint8_t* dst, const float* __restrict__ 
   }
 }
 
+// eight float32 values -> one 16-byte chunk of BF16 (round to nearest even)
+__device__ __forceinline__ uint4 pack8_bf16(float a0, float a1, float a2, float a3, float a4,
+                                            float a5, float a6, float a7) {
+  __nv_bfloat162 h[4];
+  h[0] = __floats2bfloat162_rn(a0, a1);
+  h[1] = __floats2bfloat162_rn(a2, a3);
+  h[2] = __floats2bfloat162_rn(a4, a5);
+  h[3] = __floats2bfloat162_rn(a6, a7);
+  return *reinterpret_cast<const uint4*>(h);
+}
+// 16-byte BF16 chunk j (0..7, eight elements) of row r in K-block kb (64 elements per row)
+__device__ __forceinline__ uint4* sw_chunk16(uint8_t* base, int nrows, int kb, int r, int j) {
+  return reinterpret_cast<uint4*>(base + (size_t)kb * nrows * 128 + r * 128 + ((j ^ (r & 7)) << 4));
+}
+// W^T [nrows][K] float32 -> swizzled BF16 shared operand
+__device__ __forceinline__ void load_wt16(uint8_t* dst, const float* __restrict__ src, int nrows,
+                                          int K) {
+  const int q8 = K / 8, n8 = nrows * q8;
+  for (int c = threadIdx.x; c < n8; c += blockDim.x) {
+    const int n = c / q8, q = c - n * q8;
+    const float4 a = __ldg(reinterpret_cast<const float4*>(src) + 2 * c);
+    const float4 b = __ldg(reinterpret_cast<const float4*>(src) + 2 * c + 1);
+    *sw_chunk16(dst, nrows, q >> 3, n, q & 7) = pack8_bf16(a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w);
+  }
+}
+
 // row-major staging of a warp's 32 rows of width D (coalesced global <-> per-thread rows),
 // chunk c of row r at r * D * 4 + 16 (c ^ (r mod D/4)) bytes
 template <int D>
@@ -166,23 +199,25 @@ __device__ __forceinline__ uint64_t desc_u32(uint32_t u) {
   return (uint64_t)((u & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
          (2ull << 61);
 }
+// (BF: BF16 operands, kind::f16, K = 16 per MMA; otherwise TF32, K = 8: 32 bytes either way)
+template <bool BF = false>
 __device__ __forceinline__ void issue_chain(uint32_t tmem_d, const uint8_t* sa, const uint8_t* sw,
                                             int nrows, int kb0, int KBn, bool accumulate) {
   uint32_t ua = smem_u32(sa), ub = smem_u32(sw) + (uint32_t)(kb0 * nrows * 128);
   asm volatile("" : "+r"(ua), "+r"(ub));
-  const uint32_t id = make_idesc(1, 128, nrows);
+  const uint32_t id = make_idesc(BF ? 0 : 1, 128, nrows);
 #pragma unroll 1
   for (int kb = 0; kb < KBn; ++kb)
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk)
-      mma<1>(tmem_d, desc_u32(ua + (uint32_t)(kb * 128 * 128 + kk * 32)),
-             desc_u32(ub + (uint32_t)(kb * nrows * 128 + kk * 32)), id,
-             (accumulate || kb || kk) ? 1u : 0u);
+      mma<BF ? 0 : 1>(tmem_d, desc_u32(ua + (uint32_t)(kb * 128 * 128 + kk * 32)),
+                      desc_u32(ub + (uint32_t)(kb * nrows * 128 + kk * 32)), id,
+                      (accumulate || kb || kk) ? 1u : 0u);
 }
 
-template <int D, int HD>
+template <int D, int HD, bool BF>
 __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
-  using Cfg = BlkCfg<D, HD>;
+  using Cfg = BlkCfg<D, HD, BF>;
   constexpr int FF = Cfg::FF, H = Cfg::H, KB = Cfg::KB;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -210,10 +245,17 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
                  "r"(2 * Cfg::TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  load_wt(sWqkv, a.wqkv, Cfg::NQKV, D);
-  load_wt(sWo, a.wo, D, D);
-  load_wt(sW0, a.w0, FF, D);
-  load_wt(sW1, a.w1, D, FF);
+  if constexpr (BF) {
+    load_wt16(sWqkv, a.wqkv, Cfg::NQKV, D);
+    load_wt16(sWo, a.wo, D, D);
+    load_wt16(sW0, a.w0, FF, D);
+    load_wt16(sW1, a.w1, D, FF);
+  } else {
+    load_wt(sWqkv, a.wqkv, Cfg::NQKV, D);
+    load_wt(sWo, a.wo, D, D);
+    load_wt(sW0, a.w0, FF, D);
+    load_wt(sW1, a.w1, D, FF);
+  }
   proxy_fence();
   fence_before();
   __syncthreads();
@@ -253,15 +295,30 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
 #pragma unroll
     for (int f = 0; f < D; ++f) var += (x[f] - mu) * (x[f] - mu);
     const float rho = 1.0f / sqrtf(var * inv_d + 1e-6f);  // flax LayerNorm epsilon
+    if constexpr (BF) {
 #pragma unroll
-    for (int q = 0; q < D / 4; ++q) {
-      float4 o;
-      const float4 sg = ldp4(s + 4 * q), sb = ldp4(b + 4 * q);
-      o.x = ((x[4 * q] - mu) * rho) * sg.x + sb.x;
-      o.y = ((x[4 * q + 1] - mu) * rho) * sg.y + sb.y;
-      o.z = ((x[4 * q + 2] - mu) * rho) * sg.z + sb.z;
-      o.w = ((x[4 * q + 3] - mu) * rho) * sg.w + sb.w;
-      *sw_chunk(op, 128, q >> 3, r, q & 7) = o;
+      for (int q = 0; q < D / 8; ++q) {
+        float o[8];
+        const float4 sg0 = ldp4(s + 8 * q), sg1 = ldp4(s + 8 * q + 4);
+        const float4 sb0 = ldp4(b + 8 * q), sb1 = ldp4(b + 8 * q + 4);
+        const float sg[8] = {sg0.x, sg0.y, sg0.z, sg0.w, sg1.x, sg1.y, sg1.z, sg1.w};
+        const float sb[8] = {sb0.x, sb0.y, sb0.z, sb0.w, sb1.x, sb1.y, sb1.z, sb1.w};
+#pragma unroll
+        for (int e = 0; e < 8; ++e) o[e] = ((x[8 * q + e] - mu) * rho) * sg[e] + sb[e];
+        *sw_chunk16(op, 128, q >> 3, r, q & 7) =
+            pack8_bf16(o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < D / 4; ++q) {
+        float4 o;
+        const float4 sg = ldp4(s + 4 * q), sb = ldp4(b + 4 * q);
+        o.x = ((x[4 * q] - mu) * rho) * sg.x + sb.x;
+        o.y = ((x[4 * q + 1] - mu) * rho) * sg.y + sb.y;
+        o.z = ((x[4 * q + 2] - mu) * rho) * sg.z + sb.z;
+        o.w = ((x[4 * q + 3] - mu) * rho) * sg.w + sb.w;
+        *sw_chunk(op, 128, q >> 3, r, q & 7) = o;
+      }
     }
   };
 
@@ -303,7 +360,7 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
     ln_to_operand(x, a.ln0_s, a.ln0_b, sAl);
     publish();
     if (issuer) {
-      issue_chain(tm, sAl, sWqkv, Cfg::NQKV, 0, KB, false);
+      issue_chain<BF>(tm, sAl, sWqkv, Cfg::NQKV, 0, KB, false);
       mma_commit(bar);
     }
     if (!wait_mma()) break;
@@ -388,17 +445,27 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
         }
       }
       // head output -> operand columns [h HD, (h + 1) HD) of the projection
+      if constexpr (BF) {
 #pragma unroll
-      for (int c = 0; c < HD / 4; ++c) {
-        const int col = h * HD + 4 * c;
-        *sw_chunk(sAl, 128, col >> 5, r, (col & 31) >> 2) =
-            make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+        for (int c = 0; c < HD / 8; ++c) {
+          const int col = h * HD + 8 * c;
+          *sw_chunk16(sAl, 128, col >> 6, r, (col & 63) >> 3) =
+              pack8_bf16(o[8 * c], o[8 * c + 1], o[8 * c + 2], o[8 * c + 3], o[8 * c + 4],
+                         o[8 * c + 5], o[8 * c + 6], o[8 * c + 7]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < HD / 4; ++c) {
+          const int col = h * HD + 4 * c;
+          *sw_chunk(sAl, 128, col >> 5, r, (col & 31) >> 2) =
+              make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+        }
       }
       group_bar(g);  // K / V rows of this head are no longer read
     }
     publish();
     if (issuer) {
-      issue_chain(tm + Cfg::C_O, sAl, sWo, D, 0, KB, false);
+      issue_chain<BF>(tm + Cfg::C_O, sAl, sWo, D, 0, KB, false);
       mma_commit(bar);
     }
     if (!wait_mma()) break;
@@ -422,7 +489,7 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
     ln_to_operand(x, a.ln1_s, a.ln1_b, sAl);
     publish();
     if (issuer) {
-      issue_chain(tm + Cfg::C_UP, sAl, sW0, FF, 0, KB, false);
+      issue_chain<BF>(tm + Cfg::C_UP, sAl, sW0, FF, 0, KB, false);
       mma_commit(bar);
     }
     if (!wait_mma()) break;
@@ -444,14 +511,24 @@ __global__ void __launch_bounds__(256, 1) k_block_value_tc(BlkArgs a) {
           t[4 * j + 2] = gelu_sig(t[4 * j + 2] + bb[j].z);
           t[4 * j + 3] = gelu_sig(t[4 * j + 3] + bb[j].w);
         }
+        if constexpr (BF) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          *sw_chunk(sAl, 128, c0 >> 5, r, j) =
-              make_float4(t[4 * j], t[4 * j + 1], t[4 * j + 2], t[4 * j + 3]);
+          for (int j = 0; j < 4; ++j) {
+            const int col = c0 + 8 * j;
+            *sw_chunk16(sAl, 128, col >> 6, r, (col & 63) >> 3) =
+                pack8_bf16(t[8 * j], t[8 * j + 1], t[8 * j + 2], t[8 * j + 3], t[8 * j + 4],
+                           t[8 * j + 5], t[8 * j + 6], t[8 * j + 7]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            *sw_chunk(sAl, 128, c0 >> 5, r, j) =
+                make_float4(t[4 * j], t[4 * j + 1], t[4 * j + 2], t[4 * j + 3]);
+        }
       }
       publish();
       if (issuer) {
-        issue_chain(tm + Cfg::C_DN, sAl, sW1, D, half * KB, KB, half != 0);
+        issue_chain<BF>(tm + Cfg::C_DN, sAl, sW1, D, half * KB, KB, half != 0);
         mma_commit(bar);
       }
       if (!wait_mma()) {
@@ -545,13 +622,13 @@ bool block_value_tc_ok(int N, int d, int H, int ff) {
   return N >= 1 && N <= 16 && ff == 2 && ((d == 64 && (H == 4 || H == 8)) || (d == 32 && H == 4));
 }
 
-template <int D, int HD>
+template <int D, int HD, bool BF>
 static int launch_block_value(const tc::BlkArgs& a, cudaStream_t st) {
-  using Cfg = tc::BlkCfg<D, HD>;
+  using Cfg = tc::BlkCfg<D, HD, BF>;
   static int nsm = 0;
   if (!nsm) {
-    cudaFuncSetAttribute(tc::k_block_value_tc<D, HD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         Cfg::SMEM);
+    cudaFuncSetAttribute(tc::k_block_value_tc<D, HD, BF>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -569,7 +646,7 @@ static int launch_block_value(const tc::BlkArgs& a, cudaStream_t st) {
     }
     cudaEventRecord(g_blk_ev[2 * g_blk_n], st);
   }
-  tc::k_block_value_tc<D, HD><<<grid, 256, Cfg::SMEM, st>>>(a);
+  tc::k_block_value_tc<D, HD, BF><<<grid, 256, Cfg::SMEM, st>>>(a);
   if (prof) {
     cudaEventRecord(g_blk_ev[2 * g_blk_n + 1], st);
     ++g_blk_n;
@@ -609,9 +686,11 @@ int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, 
     al |= reinterpret_cast<uintptr_t>(q);
   if ((al & 15) || !block_value_tc_ok(N, d, H, 2)) return NQS_OK;
   *done = true;
-  if (d == 64 && H == 4) return launch_block_value<64, 16>(a, st);
-  if (d == 64 && H == 8) return launch_block_value<64, 8>(a, st);
-  return launch_block_value<32, 8>(a, st);
+  if (d == 64 && H == 4)
+    return tcn.bf16 ? launch_block_value<64, 16, true>(a, st) : launch_block_value<64, 16, false>(a, st);
+  if (d == 64 && H == 8)
+    return tcn.bf16 ? launch_block_value<64, 8, true>(a, st) : launch_block_value<64, 8, false>(a, st);
+  return launch_block_value<32, 8, false>(a, st);
 }
 
 }  // namespace nqs

@@ -1,11 +1,16 @@
 // gemm_tc.cu — network row GEMMs of the mixed-precision path on the tcgen05 tensor cores.
 //
 // Y[r, n] = sum_k X[r, k] W[k, n] (+ bias[n] on value rows r % C == 0) (+ Res[r, n]) with X the
-// float32 activations read by TMA as TF32 operands (kind::tf32, float32 accumulation in TMEM) and W
-// pre-transposed to K-major W^T[n][k] once per call. Persistent CTAs (one per SM) keep W^T
-// resident in shared memory and stream 128-row tiles of X through a TMA ring; each tile's MMA
-// covers the whole output width (N <= 256, padded to a multiple of 16) and K <= 128. Waits are
-// bounded (tc_common.cuh); an abort is recorded in *err.
+// float32 activations read by TMA and W pre-transposed to K-major W^T[n][k] once per call.
+// Persistent CTAs (one per SM) keep W^T resident in shared memory and stream 128-row tiles of X
+// through a TMA ring; each tile's MMA covers the whole output width (N <= 256, padded to a
+// multiple of 16) and K <= 128, float32 accumulation in TMEM. Two operand precisions:
+//   TF32: the tensor core reads the float32 tiles as TF32 (kind::tf32);
+//   BF16: W^T is a BF16 copy, and the MMA warp converts each float32 X tile into a BF16
+//         operand tile (round to nearest even, K-major, 128B swizzle) before issuing
+//         kind::f16 MMAs (K a multiple of 64).
+// Waits are bounded (tc_common.cuh); an abort is recorded in *err.
+#include <cuda_bf16.h>
 #include <cstdio>
 #include <algorithm>
 #include <vector>
@@ -45,6 +50,30 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// float32 tile (K-blocks of 32 floats, 128B swizzle) -> BF16 operand tile (K-blocks of 64, 128B
+// swizzle), by one warp: lane l converts 16-byte chunk j of rows l, l + 32, ... (consecutive lanes
+// take consecutive rows, so each phase of 8 lanes touches 8 different bank groups)
+__device__ __forceinline__ void tile_to_bf16(const uint8_t* __restrict__ src, uint8_t* dst,
+                                             int nkb16, int lane) {
+  const int n = nkb16 * RG_BM * 8;
+#pragma unroll 4
+  for (int q = lane; q < n; q += 32) {
+    const int row = q & (RG_BM - 1), j = (q >> 7) & 7, kb = q >> 10;
+    const uint8_t* s32 = src + (size_t)(2 * kb + (j >> 2)) * RG_BM * 128 + row * 128;
+    const int c0 = 2 * (j & 3);
+    const float4 a = *reinterpret_cast<const float4*>(s32 + ((c0 ^ (row & 7)) << 4));
+    const float4 b = *reinterpret_cast<const float4*>(s32 + (((c0 + 1) ^ (row & 7)) << 4));
+    __nv_bfloat162 h[4];
+    h[0] = __floats2bfloat162_rn(a.x, a.y);
+    h[1] = __floats2bfloat162_rn(a.z, a.w);
+    h[2] = __floats2bfloat162_rn(b.x, b.y);
+    h[3] = __floats2bfloat162_rn(b.z, b.w);
+    *reinterpret_cast<uint4*>(dst + (size_t)kb * RG_BM * 128 + row * 128 + ((j ^ (row & 7)) << 4)) =
+        *reinterpret_cast<const uint4*>(h);
+  }
+}
+
+template <bool BF>
 __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_constant__ CUtensorMap tA,
                                                               const __grid_constant__ CUtensorMap tB,
                                                               const __grid_constant__ CUtensorMap tY,
@@ -53,17 +82,22 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~(uintptr_t)1023);
   const int nkb = g.K / RG_KB, S = g.stages;
+  const int nkb16 = g.K / 64;  // BF16 K-blocks (BF only)
   const int a_bytes = RG_BM * 128, b_bytes = g.Npad * 128;
   const int stage_bytes = nkb * a_bytes;
+  // BF16 resident W^T: nkb16 blocks of Npad rows x 128 bytes (half the float32 panel)
+  const int bpanel = BF ? nkb16 * b_bytes : nkb * b_bytes;
   uint8_t* sB = smem;
-  uint8_t* sA = smem + nkb * b_bytes;  // S stages
-  uint8_t* stage_out = sA + S * stage_bytes;  // 4 warps x 2 x (32 x 32 floats, 128B-swizzled)
+  uint8_t* sA = smem + bpanel;  // S stages of float32 tiles
+  uint8_t* sC = sA + S * stage_bytes;  // BF16 operand tile (BF only)
+  uint8_t* stage_out = sC + (BF ? nkb16 * a_bytes : 0);  // 4 warps x 2 x (32 x 32 floats)
   uint64_t* bfull = reinterpret_cast<uint64_t*>(stage_out + 4 * 2 * 4096);
   uint64_t* afull = bfull + 1;
   uint64_t* aempty = afull + S;
   uint64_t* accfull = aempty + S;
   uint64_t* accempty = accfull + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accempty + 2);
+  uint64_t* cempty = accempty + 2;  // BF16 operand tile free again (BF only)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cempty + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t ncols = g.Npad <= 32 ? 32u : g.Npad <= 64 ? 64u : g.Npad <= 128 ? 128u : 256u;
@@ -80,6 +114,7 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
       mbar_init(&accfull[b], 1);
       mbar_init(&accempty[b], 4);
     }
+    mbar_init(cempty, 1);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -96,8 +131,12 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
 
   if (warp == 0) {
     if (lane == 0) {
-      mbar_expect_tx(bfull, (uint32_t)(nkb * b_bytes));
-      for (int kb = 0; kb < nkb; ++kb) tma_load_2d(sB + kb * b_bytes, &tB, kb * RG_KB, 0, bfull);
+      mbar_expect_tx(bfull, (uint32_t)bpanel);
+      if (BF) {
+        for (int kb = 0; kb < nkb16; ++kb) tma_load_2d(sB + kb * b_bytes, &tB, kb * 64, 0, bfull);
+      } else {
+        for (int kb = 0; kb < nkb; ++kb) tma_load_2d(sB + kb * b_bytes, &tB, kb * RG_KB, 0, bfull);
+      }
       int issued = 0;
       for (int i = 0; i < my_tiles; ++i) {
         const int s = i % S;
@@ -112,6 +151,39 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
       mbar_wait(bfull, 0, abort, g.wait_limit);
       for (int i = max(0, issued - S); i < issued; ++i)
         mbar_wait(&afull[i % S], (i / S) & 1, abort, g.wait_limit);
+    }
+  } else if (warp == 1 && BF) {
+    // the whole warp converts tile i's float32 rows into the BF16 operand tile once the MMAs of
+    // tile i - 1 have read it; lane 0 then frees the float32 stage and issues the BF16 MMAs
+    const uint32_t id = make_idesc(0, RG_BM, g.Npad);
+    bool ok = mbar_wait(bfull, 0, abort, g.wait_limit);
+    for (int i = 0; i < my_tiles; ++i) {
+      if (!__all_sync(0xffffffffu, ok)) break;
+      const int s = i % S, b = i & 1;
+      ok = mbar_wait(&afull[s], (i / S) & 1, abort, g.wait_limit);
+      if (ok && i >= 1) ok = mbar_wait(cempty, (i - 1) & 1, abort, g.wait_limit);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      fence_after();
+      tile_to_bf16(sA + s * stage_bytes, sC, nkb16, lane);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&aempty[s]))
+                     : "memory");
+        if (i >= 2) ok = mbar_wait(&accempty[b], ((i >> 1) - 1) & 1, abort, g.wait_limit);
+        if (ok) {
+          fence_after();
+          const uint32_t td = tmem + (uint32_t)b * ncols;
+          for (int kb = 0; kb < nkb16; ++kb)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)  // 4 x (K=16 BF16 = 32 bytes) per 128-byte row
+              mma<0>(td, make_desc(sC + kb * a_bytes + kk * 32),
+                     make_desc(sB + kb * b_bytes + kk * 32), id, (kb | kk) != 0 ? 1u : 0u);
+          mma_commit(cempty);
+          mma_commit(&accfull[b]);
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -229,10 +301,18 @@ bool rowgemm_tc_ok(int K, int ldx, int Nout) {
   return K % tc::RG_KB == 0 && K <= 128 && ldx % 4 == 0 && Nout >= 1 && Nout <= 256;
 }
 
+// float32 -> BF16 (round to nearest even) copy of n values
+__global__ void k_f32_to_bf16(const float* __restrict__ x, __nv_bfloat16* __restrict__ y,
+                              size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+}
+
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
-               cudaStream_t st, int act) {
+               cudaStream_t st, int act, const uint16_t* WT16) {
   if (rows <= 0) return NQS_OK;
+  const bool bf = WT16 != nullptr && K % 64 == 0;
   if (act && C != 1) {
     set_error("rowgemm_tc: the fused activation needs single-channel rows");
     return NQS_ERR_INVALID_ARG;
@@ -260,13 +340,18 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
       return NQS_ERR_CUDA;
     }
   }
+  if (bf && (reinterpret_cast<uintptr_t>(WT16) & 15)) {
+    set_error("rowgemm_tc: BF16 weights not 16-byte aligned");
+    return NQS_ERR_INVALID_ARG;
+  }
   {
     const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)Npad};
-    const cuuint64_t strides[1] = {(cuuint64_t)K * 4};
-    const cuuint32_t box[2] = {(cuuint32_t)tc::RG_KB, (cuuint32_t)Npad};
-    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(WT), dims, strides, box,
-            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+    const cuuint64_t strides[1] = {(cuuint64_t)K * (bf ? 2 : 4)};
+    const cuuint32_t box[2] = {(cuuint32_t)(bf ? 64 : tc::RG_KB), (cuuint32_t)Npad};
+    if (enc(&tb, bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+            bf ? (void*)WT16 : (void*)WT, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
       set_error("rowgemm_tc: tensor map (weights)");
       return NQS_ERR_CUDA;
     }
@@ -294,10 +379,13 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     }
   }
   const int nkb = K / tc::RG_KB;
-  // shared memory: resident W^T, S stages of A tiles, epilogue staging, barriers
-  const size_t fixed = (size_t)nkb * Npad * 128 + 4 * 2 * 4096 + 256 + 1024;
+  // shared memory: resident W^T, S stages of A tiles, (BF16: the converted operand tile),
+  // epilogue staging, barriers
+  const size_t panel = bf ? (size_t)(K / 64) * Npad * 128 : (size_t)nkb * Npad * 128;
+  const size_t conv = bf ? (size_t)(K / 64) * tc::RG_BM * 128 : 0;
+  const size_t fixed = panel + conv + 4 * 2 * 4096 + 256 + 1024;
   const size_t stage = (size_t)nkb * tc::RG_BM * 128;
-  const size_t cap = 200 * 1024;
+  const size_t cap = bf ? 227 * 1024 : 200 * 1024;
   int S = (int)std::min<size_t>(4, (cap - fixed) / stage);
   if (S < 2) {
     set_error("rowgemm_tc: K=%d, N=%d leave room for %d pipeline stages", K, Npad, S);
@@ -307,7 +395,10 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
   static bool attr = false;
   static int nsm = 0;
   if (!attr) {
-    cudaFuncSetAttribute(tc::k_rowgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+    cudaFuncSetAttribute(tc::k_rowgemm_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(tc::k_rowgemm_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -327,7 +418,12 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     }
     cudaEventRecord(g_gemm_ev[2 * g_gemm_n], st);
   }
-  tc::k_rowgemm_tc<<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(ta, tb, ty, a);
+  if (bf)
+    tc::k_rowgemm_tc<true><<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(
+        ta, tb, ty, a);
+  else
+    tc::k_rowgemm_tc<false><<<std::min(ntiles, std::max(nsm, 1)), tc::RG_THREADS, sm, st>>>(
+        ta, tb, ty, a);
   if (prof) {
     cudaEventRecord(g_gemm_ev[2 * g_gemm_n + 1], st);
     ++g_gemm_n;
@@ -397,15 +493,26 @@ int transpose_batch(const TransJob* jobs, int n, cudaStream_t st) {
 
 static inline int pad16(int n) { return (n + 15) / 16 * 16; }
 
-size_t tc_weights_bytes(const NqsModelDesc& d) {
+size_t tc_weights_bytes(const NqsModelDesc& d, bool bf16) {
   const size_t dd = d.embed_dim, D = (size_t)d.ff_mult * dd, KN = (size_t)d.n_dets * d.n_elec;
   const size_t per_block = (size_t)pad16(3 * (int)dd) * dd + 3 * dd + dd * dd + D * dd + dd * D;
-  return sizeof(float) * ((size_t)d.depth * per_block + (size_t)pad16(2 * (int)KN) * dd) +
+  const size_t wts = (size_t)d.depth * per_block + (size_t)pad16(2 * (int)KN) * dd;
+  return sizeof(float) * wts + (bf16 ? sizeof(uint16_t) * wts + (size_t)(5 * d.depth + 1) * 256
+                                      : 0) +
          (size_t)(4 * d.depth + 4) * 256 + 64;
 }
 
+// BF16 copy of n float32 values in the workspace (nullptr when it does not fit)
+static const uint16_t* bf16_copy(const float* x, size_t n, Arena& ws, cudaStream_t st) {
+  __nv_bfloat16* y = reinterpret_cast<__nv_bfloat16*>(ws.take<uint16_t>(n));
+  if (!y) return nullptr;
+  k_f32_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, y, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return reinterpret_cast<const uint16_t*>(y);
+}
+
 int build_tc_weights(const NqsModelDesc& d, const float* th, Arena& ws, TcNet* out,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool bf16) {
   TcNet t{};
   const int dd = d.embed_dim, D = d.ff_mult * dd, KN = d.n_dets * d.n_elec;
   t.npad_qkv = pad16(3 * dd);
@@ -455,6 +562,20 @@ int build_tc_weights(const NqsModelDesc& d, const float* th, Arena& ws, TcNet* o
   if (!t.err) return NQS_ERR_WORKSPACE;
   cudaMemsetAsync(t.err, 0, sizeof(int), st);
   NQS_TRY(transpose_batch(jobs.data(), (int)jobs.size(), st));
+  if (bf16) {
+    for (int b = 0; b < d.depth; ++b) {
+      t.wqkv16[b] = bf16_copy(t.wqkv[b], (size_t)t.npad_qkv * dd, ws, st);
+      t.wo16[b] = bf16_copy(t.wo[b], (size_t)dd * dd, ws, st);
+      t.w016[b] = bf16_copy(t.w0[b], (size_t)D * dd, ws, st);
+      t.w116[b] = bf16_copy(t.w1[b], (size_t)dd * D, ws, st);
+      if (!t.w116[b]) return NQS_ERR_WORKSPACE;
+    }
+    t.wbf16 = bf16_copy(t.wbf, (size_t)t.npad_bf * dd, ws, st);
+    if (!t.wbf16) return NQS_ERR_WORKSPACE;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "k_f32_to_bf16");
+    t.bf16 = 1;
+  }
   t.on = 1;
   *out = t;
   return NQS_OK;

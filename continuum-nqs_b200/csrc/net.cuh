@@ -14,12 +14,16 @@ struct BlockW {
   const T *w0, *b0, *w1, *b1;
 };
 
-// K-major float32 weight copies for the tensor-core row GEMMs of the mixed path.
+// K-major float32 weight copies for the tensor-core row GEMMs of the mixed path, and (BF16
+// operands) their BF16 copies (raw bits, round to nearest even).
 struct TcNet {
   int on;
+  int bf16;  // Dense layers with BF16 operands where K is a multiple of 64
   const float *wqkv[NQS_MAX_DEPTH], *bqkv[NQS_MAX_DEPTH], *wo[NQS_MAX_DEPTH];
   const float *w0[NQS_MAX_DEPTH], *w1[NQS_MAX_DEPTH];
   const float *wbf;
+  const uint16_t *wqkv16[NQS_MAX_DEPTH], *wo16[NQS_MAX_DEPTH], *w016[NQS_MAX_DEPTH],
+      *w116[NQS_MAX_DEPTH], *wbf16;
   int npad_qkv, npad_bf;
   int* err;
 };
@@ -109,9 +113,11 @@ int logpsi_vjp_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
 
 // tensor-core row GEMM (gemm_tc.cu)
 bool rowgemm_tc_ok(int K, int ldx, int Nout);
+// act 1: tanh-GELU on the output (C == 1 only); WT16 (nullable): BF16 copy of W^T, which makes
+// the operands BF16 (kind::f16) when K is a multiple of 64
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
-               cudaStream_t st, int act = 0);  // act 1: tanh-GELU on the output (C == 1 only)
+               cudaStream_t st, int act = 0, const uint16_t* WT16 = nullptr);
 // one whole transformer block of single-channel rows in one launch (block_tc.cu); *done is false
 // when the shape or the operand alignment is not covered and the caller runs the unfused block
 bool block_value_tc_ok(int N, int d, int H, int ff);
@@ -119,9 +125,9 @@ int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, 
                    const BlockW<float>& bw, cudaStream_t st, bool* done);
 extern bool g_block_fusion;
 bool profiling_enabled();  // nqs_profile_gemm(1) is in force
-size_t tc_weights_bytes(const NqsModelDesc& d);
+size_t tc_weights_bytes(const NqsModelDesc& d, bool bf16);
 int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,
-                     cudaStream_t st);
+                     cudaStream_t st, bool bf16);
 
 // Default row budget of one network chunk.
 constexpr size_t kMaxRows = (size_t)1 << 19;

@@ -105,7 +105,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       GemmArgs<T> g{};
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wqkv[b], w.tc.npad_qkv, 3 * d,
-                           w.tc.bqkv[b], C, nullptr, 0, (float*)Big, 3 * d, w.tc.err, st));
+                           w.tc.bqkv[b], C, nullptr, 0, (float*)Big, 3 * d, w.tc.err, st, 0,
+                           w.tc.bf16 ? w.tc.wqkv16[b] : nullptr));
       } else {
         g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
         g.Y = Big; g.ldy = 3 * d; g.Res = nullptr; g.ldr = 0; g.trans_w = 0; g.nseg = 3;
@@ -117,7 +118,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       NQS_TRY(launch_attention<T>(cb.n_jobs, N, C, cb.n_tan, cb.has_lap, d, mc.H, Big, Att, st));
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Att, d, rows, d, w.tc.wo[b], d, d, (const float*)bw.bo,
-                           C, (const float*)X, d, (float*)X, d, w.tc.err, st));
+                           C, (const float*)X, d, (float*)X, d, w.tc.err, st, 0,
+                           w.tc.bf16 ? w.tc.wo16[b] : nullptr));
       } else {
         g = GemmArgs<T>{};
         g.X = Att; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
@@ -132,7 +134,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       const bool fuse_act = tcn && C == 1;
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.w0[b], D, D, (const float*)bw.b0, C,
-                           nullptr, 0, (float*)Big, D, w.tc.err, st, fuse_act ? 1 : 0));
+                           nullptr, 0, (float*)Big, D, w.tc.err, st, fuse_act ? 1 : 0,
+                           w.tc.bf16 ? w.tc.w016[b] : nullptr));
       } else {
         g = GemmArgs<T>{};
         g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;
@@ -148,7 +151,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       }
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Big, D, rows, D, w.tc.w1[b], d, d, (const float*)bw.b1,
-                           C, (const float*)X, d, (float*)X, d, w.tc.err, st));
+                           C, (const float*)X, d, (float*)X, d, w.tc.err, st, 0,
+                           w.tc.bf16 ? w.tc.w116[b] : nullptr));
       } else {
         g = GemmArgs<T>{};
         g.X = Big; g.ldx = D; g.rows = rows; g.K = D; g.C = C;
@@ -162,7 +166,7 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
     if (tcn) {
       NQS_TRY(rowgemm_tc((const float*)Hb, d, rows, d, w.tc.wbf, w.tc.npad_bf, 2 * KN,
                          (const float*)w.bf_b_re, C, nullptr, 0, (float*)Big, 2 * KN, w.tc.err,
-                         st));
+                         st, 0, w.tc.bf16 ? w.tc.wbf16 : nullptr));
     } else {
       GemmArgs<T> g{};
       g.X = Hb; g.ldx = d; g.rows = rows; g.K = d; g.C = C;

@@ -429,7 +429,8 @@ size_t plan_bytes(const NqsModel* m, int op, int W, int prec) {
   const int N = mc.N;
   Plan p;
   if (prec != NQS_PREC_FP64) p.add(sizeof(float) * m->hm.desc.n_params);
-  if (prec == NQS_PREC_MIXED) p.add(tc_weights_bytes(m->hm.desc));
+  if (prec == NQS_PREC_MIXED || prec == NQS_PREC_MIXED_BF16)
+    p.add(tc_weights_bytes(m->hm.desc, prec == NQS_PREC_MIXED_BF16));
   switch (op) {
     case NQS_OP_LOGPSI:
       p.add(net_bytes(mc, prec, chunk_rows(JOB_VALUE, W, N, 1, kMaxRows)));
@@ -477,7 +478,8 @@ int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cud
     set_error("null model or theta");
     return NQS_ERR_INVALID_ARG;
   }
-  if (prec != NQS_PREC_FP64 && prec != NQS_PREC_MIXED && prec != NQS_PREC_MIXED_SIMT) {
+  if (prec != NQS_PREC_FP64 && prec != NQS_PREC_MIXED && prec != NQS_PREC_MIXED_SIMT &&
+      prec != NQS_PREC_MIXED_BF16) {
     set_error("unknown precision %d", prec);
     return NQS_ERR_INVALID_ARG;
   }
@@ -494,7 +496,9 @@ int begin(NqsModel* m, const double* theta, int prec, void* wsp, size_t wsb, cud
     c->theta32 = t32;
   }
   c->tc = TcNet{};
-  if (prec == NQS_PREC_MIXED) NQS_TRY(build_tc_weights(m->hm.desc, c->theta32, c->ws, &c->tc, st));
+  if (prec == NQS_PREC_MIXED || prec == NQS_PREC_MIXED_BF16)
+    NQS_TRY(build_tc_weights(m->hm.desc, c->theta32, c->ws, &c->tc, st,
+                             prec == NQS_PREC_MIXED_BF16));
   return NQS_OK;
 }
 

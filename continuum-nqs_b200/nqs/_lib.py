@@ -28,6 +28,7 @@ NQS_ERR_NOT_SPD = 7
 PREC_FP64 = 0
 PREC_MIXED = 1
 PREC_MIXED_SIMT = 2
+PREC_MIXED_BF16 = 3
 
 OP_LOGPSI, OP_LOCAL_E, OP_MCMC, OP_PER_SAMPLE_O = 0, 1, 2, 3
 OP_PER_SAMPLE_O_CKPT, OP_LOGPSI_VJP, OP_LOGPSI_VJP_CKPT = 4, 5, 6

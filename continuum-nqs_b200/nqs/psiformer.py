@@ -249,6 +249,8 @@ def _prec(precision) -> int:
         return _lib.PREC_MIXED
     if precision in (2, "mixed_simt", "fp32"):
         return _lib.PREC_MIXED_SIMT
+    if precision in (3, "mixed_bf16", "bf16"):
+        return _lib.PREC_MIXED_BF16
     raise ValueError(f"unknown precision {precision!r}")
 
 

@@ -53,6 +53,9 @@ extern "C" {
                                cores (TF32 operands, float32 accumulation) where the shapes
                                allow; determinants, LU pivots, log-space sums, energies float64 */
 #define NQS_PREC_MIXED_SIMT 2  /* as NQS_PREC_MIXED with every GEMM on the float32 SIMT cores  */
+#define NQS_PREC_MIXED_BF16 3  /* as NQS_PREC_MIXED with BF16 operands (kind::f16, float32
+                                  accumulation) for the Dense layers whose K is a multiple of
+                                  64 (the rest TF32); activations stay float32 in memory    */
 
 /* ---- compiled limits ---------------------------------------------------------------------- */
 #define NQS_MAX_DEPTH     16

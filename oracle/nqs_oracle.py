@@ -78,7 +78,15 @@ def gelu_tanh(x):
     return 0.5 * x * (1.0 + torch.tanh(math.sqrt(2.0 / math.pi) * (x + 0.044715 * x ** 3)))
 
 
+# Emulation hook for tests of the tensor-core precisions: when set to a function f, the operands
+# of every Dense product whose K (input width) is a multiple of 64, and of the backflow product,
+# become f(x) and f(kernel) (e.g. rounding to BF16); the products themselves stay float64.
+OPERAND_ROUND: Callable | None = None
+
+
 def dense(x, p):
+    if OPERAND_ROUND is not None and x.shape[-1] % 64 == 0:
+        return OPERAND_ROUND(x) @ OPERAND_ROUND(p["kernel"]) + p["bias"]
     return x @ p["kernel"] + p["bias"]
 
 
@@ -127,7 +135,12 @@ def logpsi(spec, params, R, S):
     for b in range(spec.depth):
         x = transformer_block(x, p[f"TransformerBlock_{b}"], spec.n_heads)
     x = layer_norm(x, p["LayerNorm_0"])
-    bf = x.to(C128) @ p["backflow"]["kernel"] + p["backflow"]["bias"]     # (N, K*N)
+    if OPERAND_ROUND is not None and x.shape[-1] % 64 == 0:
+        kb = p["backflow"]["kernel"]
+        kr = torch.complex(OPERAND_ROUND(kb.real), OPERAND_ROUND(kb.imag))
+        bf = OPERAND_ROUND(x).to(C128) @ kr + p["backflow"]["bias"]
+    else:
+        bf = x.to(C128) @ p["backflow"]["kernel"] + p["backflow"]["bias"]  # (N, K*N)
     bf = bf.reshape(N, spec.n_dets, N).permute(1, 2, 0)                  # (K, n_orb, N)
     phase = torch.exp(1j * (Gs @ R.T))                                    # (n_G, N)
     Ws = W[:, :, S.long()]                                                # (n_orb, n_G, N)
