@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sample work")
+    ap.add_argument("--bf16-steps", type=int, default=2)
+    ap.add_argument("--no-bf16", action="store_true",
+                    help="skip the BF16-operand network variant")
     ap.add_argument("--trajectory", type=int, default=5,
                     help="iterations of the mixed-vs-float64 trajectory comparison (0: skip)")
     return ap.parse_args()
@@ -254,38 +257,54 @@ def run_ours(a, rank, world):
     # ------------------------------------------------ plain float64 GPU path + accuracy gates
     fp64 = None
     acc = None
+    bf16net = None
     if not a.no_fp64 and a.fp64_steps > 0:
         from nqs.minsr import minsr_step
-        # accuracy of the mixed path against float64 on identical walkers and parameters, both
+        # accuracy of the mixed paths against float64 on identical walkers and parameters, all
         # solved at the configured damping lam; one Jacobian resident at a time (configuration
         # 5's float64 Jacobian alone is 118 GB)
-        it.energies()
-        em, e_mixed = it.e.real.double().clone(), it.e.clone()
-        it.jacobian()
-        delta = torch.zeros(1, dtype=torch.float64, device=dev)
-        info = torch.zeros(5, dtype=torch.int32, device=dev)
-        d_mixed = minsr_step(it.O, e_mixed, su.lam, "bf16", n_refine=it.n_refine,
-                             damping_out=delta, info=info)
-        it.release_jacobian()
-        torch.cuda.empty_cache()
+        def mixed_direction(r):
+            r.energies()
+            e_r = r.e.clone()
+            r.jacobian()
+            dl = torch.zeros(1, dtype=torch.float64, device=dev)
+            inf_ = torch.zeros(5, dtype=torch.int32, device=dev)
+            d_r = minsr_step(r.O, e_r, su.lam, "bf16", n_refine=r.n_refine, damping_out=dl,
+                             info=inf_)
+            r.release_jacobian()
+            torch.cuda.empty_cache()
+            return e_r.real.double(), d_r, float(dl.item()), inf_.tolist()
+
+        em, d_mixed, dshift, inf = mixed_direction(it)
+        itb = None
+        if not a.no_bf16:
+            itb = VMCIteration(model, it.theta, it.R, it.S, precision="mixed_bf16", **common)
+            eb, d_bf, _, infb = mixed_direction(itb)
         it64 = VMCIteration(model, it.theta, it.R, it.S, precision="fp64", **common)
         it64.energies()
         e64 = it64.e.real.double()
         it64.jacobian()
         d_64 = minsr_step(it64.O, it64.e, su.lam, "fp64")
         n64 = float(d_64.norm())
-        inf = info.tolist()
-        acc = {"dE_per_electron": float((em.mean() - e64.mean()).abs()) / su.N,
-               "dE_target": 1e-4,
-               "dvar_rel": float((em.var() - e64.var()).abs() / e64.var()),
-               "dvar_target": 0.05,
-               "lam": su.lam,
-               "dtheta_rel_vs_fp64_lam": float((d_mixed - d_64).norm()) / n64,
-               "dtheta_cos_vs_fp64_lam": float((d_mixed * d_64).sum()) / (float(d_mixed.norm()) * n64),
-               "dtheta_target": 1e-2,
-               "bf16_preconditioner_shift": float(delta.item()),
-               "pcg_iterations": inf[3], "pcg_stop": ["limit", "converged", "breakdown"][inf[4]],
-               "E_fp64": float(e64.mean()), "E_mixed": float(em.mean())}
+
+        def gates(e_r, d_r, inf_):
+            return {"dE_per_electron": float((e_r.mean() - e64.mean()).abs()) / su.N,
+                    "dE_target": 1e-4,
+                    "dvar_rel": float((e_r.var() - e64.var()).abs() / e64.var()),
+                    "dvar_target": 0.05,
+                    "lam": su.lam,
+                    "dtheta_rel_vs_fp64_lam": float((d_r - d_64).norm()) / n64,
+                    "dtheta_cos_vs_fp64_lam": float((d_r * d_64).sum()) / (float(d_r.norm()) * n64),
+                    "dtheta_target": 1e-2,
+                    "pcg_iterations": inf_[3],
+                    "pcg_stop": ["limit", "converged", "breakdown"][inf_[4]]}
+
+        acc = gates(em, d_mixed, inf)
+        acc.update(bf16_preconditioner_shift=dshift, E_fp64=float(e64.mean()),
+                   E_mixed=float(em.mean()))
+        if itb is not None:
+            acc_bf = gates(eb, d_bf, infb)
+            acc_bf["E_mixed_bf16"] = float(eb.mean())
         it64.step()
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -299,6 +318,25 @@ def run_ours(a, rank, world):
                 "mixed_speedup": ms64 / ms, "E": float(it64.stats[0])}
         del it64
         torch.cuda.empty_cache()
+        if itb is not None:
+            # the same iteration with BF16 operands in the network's Dense layers (TF32 is the
+            # headline's comparison precision)
+            itb.step()
+            torch.cuda.synchronize()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record()
+            for _ in range(a.bf16_steps):
+                itb.step()
+            b1.record()
+            torch.cuda.synchronize()
+            msb = b0.elapsed_time(b1) / a.bf16_steps
+            bf16net = {"ms_per_step": msb, "VMC_iter_per_s": 1000.0 / msb,
+                       "speedup_vs_fp64": ms64 / msb, "accuracy_vs_fp64": acc_bf,
+                       "network": "Dense layers with BF16 operands on tcgen05 kind::f16 "
+                                  "(float32 accumulation); the rest as the mixed path"}
+            del itb
+            torch.cuda.empty_cache()
+
     traj = None
     if not a.no_fp64 and a.trajectory > 0:
         if 2 * su.n_walkers * it.P * 12 < 100e9:  # both runs' Jacobians resident at once
@@ -357,7 +395,8 @@ def run_ours(a, rank, world):
                  "algorithmic_flops": gflop}
     return dict(ms=ms, phases=phases, stats=stats, e2e=e2e, fp64=fp64, roofline=roof,
                 roofline_second=roof_other, roofline_gram=roof_gram, clocks=clk,
-                launches=launches, su=su, model=model, P=it.P, acc=acc, traj=traj)
+                launches=launches, su=su, model=model, P=it.P, acc=acc, traj=traj,
+                bf16net=bf16net)
 
 
 def trajectories(model, it, common, n_iter, su):
@@ -604,7 +643,8 @@ def main():
         "eloc_evals_per_s": world * W / (ph["local_energy_ms"] * 1e-3),
         "phases_ms": ph, "energy": {"mean": r["stats"][0], "err": r["stats"][1],
                                     "var": r["stats"][2]},
-        "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "trajectory_vs_fp64": r["traj"],
+        "fp64_plain": r["fp64"], "accuracy_vs_fp64": r["acc"], "bf16_network": r["bf16net"],
+        "trajectory_vs_fp64": r["traj"],
         "roofline": r["roofline"],
         "roofline_second": r["roofline_second"], "roofline_gram": r["roofline_gram"],
         "cpu_baseline": cpu,
