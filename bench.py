@@ -599,6 +599,88 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_multi(a, rank, world):
+    """Configuration 4: 64 independent VMC instances (electron counts 6..26, walkers 512..4096,
+    their own r_s, Rashba and Zeeman) advanced together; one step = one VMC iteration of every
+    instance, captured once as a CUDA graph (knobs per (N, W) bucket from the autotuner)."""
+    from nqs import _lib
+    from nqs.batched import MultiVMC, tuning_table, walker_steps
+    from nqs.configs import config4_instances
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    inst = config4_instances(64, seed=rank)
+    t0 = time.perf_counter()
+    mv = MultiVMC(inst, precision="mixed", use_graph=True)
+    for it in mv.its:
+        it.sample(20)  # thermalise once
+    rep = mv.autotune()
+    t_tune = time.perf_counter() - t0
+    L = _lib.lib()
+    c0 = L.nqs_kernel_launches()
+    mv.capture(warmup=1)  # one eager step + the captured one: the kernels of a step, twice
+    per_step_kernels = (L.nqs_kernel_launches() - c0) // 2
+    for _ in range(max(0, a.warmup - 1)):
+        mv.step()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev.index)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        mv.step()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / a.steps, dev)
+    # end to end: every instance's walkers and theta from pinned host memory before the step,
+    # and back (with the energy statistics) after it
+    hs = [(it.R.cpu().pin_memory(), it.S.cpu().pin_memory(), it.theta.cpu().pin_memory(),
+           torch.empty(5, dtype=torch.float64).pin_memory()) for it in mv.its]
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(a.steps):
+        for it, (Rh, Sh, Th, _) in zip(mv.its, hs):
+            it.R.copy_(Rh, non_blocking=True)
+            it.S.copy_(Sh, non_blocking=True)
+            it.theta.copy_(Th, non_blocking=True)
+        mv.step()
+        for it, (Rh, Sh, Th, sth) in zip(mv.its, hs):
+            Rh.copy_(it.R, non_blocking=True)
+            Sh.copy_(it.S, non_blocking=True)
+            Th.copy_(it.theta, non_blocking=True)
+            sth.copy_(it.stats, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / a.steps, dev)
+    h2d = sum(Rh.numel() * 8 + Sh.numel() * 4 + Th.numel() * 8 for Rh, Sh, Th, _ in hs)
+    wsteps = walker_steps(mv.its)
+    line = {
+        "metric": "VMC iter/s", "value": job_throughput(ms, world), "unit": "VMC iter/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/bf16+f64",
+        "data": "synthetic (seeded uniform walkers, N(0,0.02^2) weights)",
+        "config": {"workload": "config4: 64 independent VMC instances, N in {6..26}, W in "
+                               "{512..4096}, width 64, 3 blocks, K=2; one step = one iteration "
+                               "of every instance (one CUDA graph launch)",
+                   "instances": len(mv.its), "walkers": sum(it.W for it in mv.its),
+                   "electrons": [it.N for it in mv.its]},
+        "walker_steps_per_s": world * wsteps / (ms * 1e-3),
+        "instances": [{"N": it.N, "W": it.W, "E": float(it.stats[0])} for it in mv.its],
+        "autotune": {"table": tuning_table(rep), "seconds": t_tune},
+        "e2e": {"value": job_throughput(e2e_ms, world), "unit": "VMC iter/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d + 40 * len(hs),
+                "ms_per_step": e2e_ms},
+        "clocks": clk, "gpu_launches": int(per_step_kernels),
+        "gpu_launches_note": "kernels of one step (counted while it was enqueued for capture); "
+                             "each timed step replays them as one CUDA graph launch",
+    }
+    return line
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -610,6 +692,14 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if a.config == 4:
+        line = run_multi(a, rank, world)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     r = run_ours(a, rank, world)
     su = r["su"]
     cpu = None

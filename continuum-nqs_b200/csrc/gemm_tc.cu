@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 #include <cstdio>
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "net.cuh"
@@ -286,7 +287,8 @@ __global__ void __launch_bounds__(RG_THREADS, 1) k_rowgemm_tc(const __grid_const
 
 }  // namespace tc
 
-// ---- optional per-launch timing (nqs_profile_gemm) ----
+// ---- pipeline depth cap (nqs_set_rowgemm_stages) and optional per-launch timing ----
+std::atomic<int> g_rowgemm_stages{4};
 namespace {
 constexpr int kGemmProfCap = 16384;
 bool g_gemm_prof = false;
@@ -386,7 +388,7 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
   const size_t fixed = panel + conv + 4 * 2 * 4096 + 256 + 1024;
   const size_t stage = (size_t)nkb * tc::RG_BM * 128;
   const size_t cap = bf ? 227 * 1024 : 200 * 1024;
-  int S = (int)std::min<size_t>(4, (cap - fixed) / stage);
+  int S = (int)std::min<size_t>((size_t)g_rowgemm_stages.load(), (cap - fixed) / stage);
   if (S < 2) {
     set_error("rowgemm_tc: K=%d, N=%d leave room for %d pipeline stages", K, Npad, S);
     return NQS_ERR_UNSUPPORTED;
@@ -431,6 +433,15 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     g_gemm_bytes += 4.0 * ((double)rows * K + (double)Npad * K + (double)rows * Nout * (Res ? 2 : 1));
   }
   NQS_CHECK_LAUNCH("k_rowgemm_tc");
+  return NQS_OK;
+}
+
+extern "C" int nqs_set_rowgemm_stages(int max_stages) {
+  if (max_stages != 0 && (max_stages < 2 || max_stages > 4)) {
+    set_error("nqs_set_rowgemm_stages: %d is not 0 or 2..4", max_stages);
+    return NQS_ERR_INVALID_ARG;
+  }
+  g_rowgemm_stages.store(max_stages ? max_stages : 4);
   return NQS_OK;
 }
 

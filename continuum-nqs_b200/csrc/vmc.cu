@@ -61,6 +61,7 @@ struct McArgs {
   double step;
   uint64_t seed, sweep;  // global sweep index = counter + s
   int s;                 // sweep index within the call (for injected buffers)
+  const uint64_t* counter_dev;  // nullable: sweep = *counter_dev + s, read at run time
   double A[4], Ainv[4];
   const double* inj_normals;
   const double* inj_u_pos;
@@ -69,8 +70,12 @@ struct McArgs {
 };
 
 __device__ __forceinline__ u32x4 mc_draw(const McArgs& a, int w, uint32_t draw) {
-  return philox4x32_10(u32x4{(uint32_t)w, draw, (uint32_t)a.sweep, (uint32_t)(a.sweep >> 32)},
-                       a.seed);
+  const uint64_t sw = a.counter_dev ? *a.counter_dev + (uint64_t)a.s : a.sweep;
+  return philox4x32_10(u32x4{(uint32_t)w, draw, (uint32_t)sw, (uint32_t)(sw >> 32)}, a.seed);
+}
+
+__global__ void k_counter_add(uint64_t* c, uint64_t n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *c += n;
 }
 
 __global__ void k_propose_pos(McArgs a, const double* __restrict__ R, double* __restrict__ Rp) {
@@ -668,13 +673,13 @@ int nqs_grad_laplacian(NqsModel* m, const double* theta, const double* R, const 
                            false);
 }
 
-int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, double* logpsi_io,
-                    int W, int n_sweeps, int n_flips, double step, uint64_t seed,
-                    uint64_t counter, const double* inj_normals, const double* inj_u_pos,
-                    const int32_t* inj_flip_idx, const double* inj_u_flip, double* out_acc_pos,
-                    double* out_acc_spin, double* out_d, int prec, void* wsp, size_t wsb,
-                    void* stream) {
-  cudaStream_t st = (cudaStream_t)stream;
+static int mcmc_impl(NqsModel* m, const double* theta, double* R, int32_t* S,
+                     double* logpsi_io, int W, int n_sweeps, int n_flips, double step,
+                     uint64_t seed, uint64_t counter, uint64_t* counter_dev,
+                     const double* inj_normals, const double* inj_u_pos,
+                     const int32_t* inj_flip_idx, const double* inj_u_flip, double* out_acc_pos,
+                     double* out_acc_spin, double* out_d, int prec, void* wsp, size_t wsb,
+                     cudaStream_t st) {
   if (W < 0 || n_sweeps < 0 || n_flips < 0 || (W > 0 && (!R || !S))) return NQS_ERR_INVALID_ARG;
   if (W == 0) return NQS_OK;
   NQS_TRY(check_ws(m, NQS_OP_MCMC, W, prec, wsb));
@@ -700,6 +705,7 @@ int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, dou
   a.inj_u_pos = inj_u_pos;
   a.inj_flip = inj_flip_idx;
   a.inj_u_flip = inj_u_flip;
+  a.counter_dev = counter_dev;
   if (out_acc_pos) cudaMemsetAsync(out_acc_pos, 0, sizeof(double) * W, st);
   if (out_acc_spin) cudaMemsetAsync(out_acc_spin, 0, sizeof(double) * W, st);
   // current log psi (the reference recomputes it per proposal; the forward is deterministic,
@@ -740,7 +746,35 @@ int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, dou
                                           cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return cuda_status(e, "nqs_mcmc_sweeps: copy");
   }
+  if (counter_dev && n_sweeps > 0) {
+    k_counter_add<<<1, 32, 0, st>>>(counter_dev, (uint64_t)n_sweeps);
+    NQS_CHECK_LAUNCH("k_counter_add");
+  }
   return NQS_OK;
+}
+
+int nqs_mcmc_sweeps(NqsModel* m, const double* theta, double* R, int32_t* S, double* logpsi_io,
+                    int W, int n_sweeps, int n_flips, double step, uint64_t seed,
+                    uint64_t counter, const double* inj_normals, const double* inj_u_pos,
+                    const int32_t* inj_flip_idx, const double* inj_u_flip, double* out_acc_pos,
+                    double* out_acc_spin, double* out_d, int prec, void* wsp, size_t wsb,
+                    void* stream) {
+  return mcmc_impl(m, theta, R, S, logpsi_io, W, n_sweeps, n_flips, step, seed, counter, nullptr,
+                   inj_normals, inj_u_pos, inj_flip_idx, inj_u_flip, out_acc_pos, out_acc_spin,
+                   out_d, prec, wsp, wsb, (cudaStream_t)stream);
+}
+
+int nqs_mcmc_sweeps_devctr(NqsModel* m, const double* theta, double* R, int32_t* S,
+                           double* logpsi_io, int W, int n_sweeps, int n_flips, double step,
+                           uint64_t seed, uint64_t* counter_dev, double* out_acc_pos,
+                           double* out_acc_spin, int prec, void* wsp, size_t wsb, void* stream) {
+  if (!counter_dev) {
+    set_error("nqs_mcmc_sweeps_devctr: null counter");
+    return NQS_ERR_INVALID_ARG;
+  }
+  return mcmc_impl(m, theta, R, S, logpsi_io, W, n_sweeps, n_flips, step, seed, 0, counter_dev,
+                   nullptr, nullptr, nullptr, nullptr, out_acc_pos, out_acc_spin, nullptr, prec,
+                   wsp, wsb, (cudaStream_t)stream);
 }
 
 }  // extern "C"

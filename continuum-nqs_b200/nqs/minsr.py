@@ -243,7 +243,7 @@ class VMCIteration:
     def __init__(self, model, theta, R, S, *, m_star=1.0, lambda_r=1.0, h_z=0.0, coulomb=None,
                  lr=0.05, lam=1e-3, n_sweeps=10, step_size=0.4, clip_k=5.0, n_spin_flips=2,
                  seed=0, counter=0, precision="fp64", gram=None, n_refine=None, ext_field=None,
-                 checkpoint_blocks=False):
+                 checkpoint_blocks=False, device_counter=False, O_buffer=None):
         from . import _lib
         from .psiformer import _prec, as_batch
         _lib.require_cuda()
@@ -271,6 +271,14 @@ class VMCIteration:
         dev = self.R.device
         self.o_dtype = torch.float64 if self.prec == _lib.PREC_FP64 else torch.float32
         self._O = None  # the [2W][P] Jacobian, allocated on first use
+        if O_buffer is not None:  # a caller-owned buffer (several iterations may share one)
+            if O_buffer.dtype != self.o_dtype or O_buffer.numel() < 2 * self.W * self.P:
+                raise ValueError("O_buffer: wrong dtype or too small")
+            self._O = O_buffer.view(-1)[:2 * self.W * self.P].view(2 * self.W, self.P)
+        # the random stream's sweep counter in device memory (CUDA-graph replay draws fresh
+        # proposals each time); the host counter is then not advanced
+        self.counter_dev = (torch.tensor([self.counter], dtype=torch.int64, device=dev)
+                            if device_counter else None)
         self.e = torch.empty(self.W, dtype=torch.complex128, device=dev)
         self.e_clip = torch.empty_like(self.e)
         self.stats = torch.zeros(5, dtype=F64, device=dev)
@@ -307,6 +315,15 @@ class VMCIteration:
         from . import _lib
         L = _lib.lib()
         n = self.n_sweeps if n_sweeps is None else n_sweeps
+        if self.counter_dev is not None:
+            if inject is not None:
+                raise ValueError("injected randomness needs the host counter")
+            _lib.check(L.nqs_mcmc_sweeps_devctr(
+                self.h, _lib.ptr(self.theta), _lib.ptr(self.R), _lib.ptr(self.S), None, self.W,
+                n, self.n_flips, self.step_size, self.seed, _lib.ptr(self.counter_dev),
+                _lib.ptr(self.acc_pos), _lib.ptr(self.acc_spin), self.prec, _lib.ptr(self.ws),
+                self.ws.numel(), _lib.stream_ptr()), "nqs_mcmc_sweeps_devctr")
+            return
         inj = [None] * 4
         if inject is not None:
             dev = self.R.device
@@ -377,8 +394,9 @@ class VMCIteration:
     def state_dict(self):
         """What a resume needs beyond the constructor arguments: theta, the walkers and the
         position of the Metropolis random stream (seed, sweep counter), as host copies."""
+        counter = int(self.counter_dev.item()) if self.counter_dev is not None else self.counter
         return {"theta": self.theta.cpu(), "R": self.R.cpu(), "S": self.S.cpu(),
-                "seed": self.seed, "counter": self.counter}
+                "seed": self.seed, "counter": counter}
 
     def load_state_dict(self, st):
         """Restore a state_dict (shapes must match this iteration's model and walker count); the
@@ -392,6 +410,8 @@ class VMCIteration:
         self.R.copy_(R)
         self.S.copy_(S.to(self.S.dtype))
         self.seed, self.counter = int(st["seed"]), int(st["counter"])
+        if self.counter_dev is not None:
+            self.counter_dev.fill_(self.counter)
 
 
 def save_checkpoint(path, it):

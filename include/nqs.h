@@ -134,6 +134,10 @@ int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches);
  * runs as separate LayerNorm / GEMM / attention / GEMM launches. Both compute the same function
  * with the same TF32 products; the switch exists so that the two can be compared. */
 int nqs_set_block_fusion(int enable);
+/* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
+ * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;
+ * 0 restores the default (4). A tuning knob of the multi-instance autotuner. */
+int nqs_set_rowgemm_stages(int max_stages);
 /* Per-launch timing of the fused value-pass blocks (profiling aid, no reference counterpart),
  * recorded while nqs_profile_gemm(1) is in force: summed kernel time (ms), algorithmic HBM bytes
  * (rows in and out, weights once), tensor-core and attention flops, and the launch count since
@@ -211,6 +215,16 @@ int nqs_mcmc_sweeps(NqsModel* model, const double* theta, double* R_io, int32_t*
                     const int32_t* inj_flip_idx, const double* inj_u_flip,
                     double* out_acc_pos, double* out_acc_spin, double* out_d,
                     int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* nqs_mcmc_sweeps with the random stream's sweep counter in device memory (uint64, read when
+ * the kernels run and advanced by n_sweeps on the device at the end), for a sequence of calls
+ * captured once in a CUDA graph and replayed: each replay draws fresh proposals. No injected
+ * randomness. */
+int nqs_mcmc_sweeps_devctr(NqsModel* model, const double* theta, double* R_io, int32_t* S_io,
+                           double* logpsi_io, int n_walkers, int n_sweeps, int n_spin_flips,
+                           double step, uint64_t seed, uint64_t* counter_dev,
+                           double* out_acc_pos, double* out_acc_spin, int precision,
+                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* Per-sample Jacobian O[w][k] = d log psi(R_w,S_w) / d theta_k written as two real rows:
  * out_O is [2W][P] with rows 0..W-1 = Re O and rows W..2W-1 = Im O, dtype f64 (out_dtype 0)
