@@ -214,41 +214,50 @@ __global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, 
         dus[tt][q] = (t0 + tt < n_tan && f < d) ? xt[f] : T(0);
       }
     }
+    // the TP rows' sums reduce together: one butterfly for their means, one for their
+    // (u . du, du . du) pairs (the same two-pass arithmetic per row as one row at a time)
+    T mt[TP], s23[2 * TP];
 #pragma unroll
     for (int tt = 0; tt < TP; ++tt) {
-      const int t = t0 + tt;
-      if (t >= n_tan) break;  // warp-uniform
-      T du[Q];
-      s = 0;
+      mt[tt] = 0;
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        du[q] = dus[tt][q];
-        s += du[q];
-      }
-      const T mt = warp_sum(s) * inv_d;
+      for (int q = 0; q < Q; ++q) mt[tt] += dus[tt][q];
+    }
+    warp_sum_n<T, TP>(mt);
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) {
+      mt[tt] *= inv_d;
       T s2 = 0, s3 = 0;
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int f = lane + 32 * q;
         if (f < d) {
-          du[q] -= mt;
-          s2 += u[q] * du[q];
-          s3 += du[q] * du[q];
+          dus[tt][q] -= mt[tt];
+          s2 += u[q] * dus[tt][q];
+          s3 += dus[tt][q] * dus[tt][q];
         }
       }
-      const T dv = T(2) * warp_sum(s2) * inv_d;
+      s23[2 * tt] = s2;
+      s23[2 * tt + 1] = s3;
+    }
+    warp_sum_n<T, 2 * TP>(s23);
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) {
+      const int t = t0 + tt;
+      if (t >= n_tan) break;  // warp-uniform
+      const T dv = T(2) * s23[2 * tt] * inv_d;
       const T drho = T(-0.5) * rho3 * dv;
       T* yt = y + (size_t)(1 + t) * d;
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int f = lane + 32 * q;
         if (f < d) {
-          yt[f] = (du[q] * rho + u[q] * drho) * gm[q];
-          acc[q] += du[q] * drho;
+          yt[f] = (dus[tt][q] * rho + u[q] * drho) * gm[q];
+          acc[q] += dus[tt][q] * drho;
         }
       }
       S1 += dv * dv;
-      S2 += warp_sum(s3) * inv_d;
+      S2 += s23[2 * tt + 1] * inv_d;
     }
   }
   if (has_lap) {

@@ -178,3 +178,12 @@ __device__ __forceinline__ T warp_sum(T v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// K independent warp sums in one butterfly (the same order per value as warp_sum)
+template <typename T, int K>
+__device__ __forceinline__ void warp_sum_n(T (&v)[K]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+}
