@@ -43,78 +43,109 @@ def h0(k, m_star, lambda_r, h_z):
     return out - 0.5 * h_z * _SZ
 
 
-def sector_ground_energy(A, m_vec, n_cut, m_star=1.0, lambda_r=1.0, h_z=0.0, alpha=1.0,
-                         twist=(0.0, 0.0), zeta_M=0.0, tol=1e-12, shift=1.0e4, offset=10.0):
-    A = np.asarray(A, float)
-    Ainv = np.linalg.inv(A)
-    B = 2.0 * np.pi * Ainv.T
-    kt = Ainv.T @ np.asarray(twist, float)
-    area = float(abs(np.linalg.det(A)))
-    n1 = np.arange(-n_cut, n_cut + 1)
-    nx, ny = np.meshgrid(n1, n1, indexing="ij")
-    n = np.stack([nx, ny], -1).astype(float)                   # (S, S, 2)
-    S = 2 * n_cut + 1
-    m_vec = np.asarray(m_vec, float)
-    k1 = n @ B.T + kt
-    K = B @ m_vec + 2.0 * kt
-    k2 = K - k1
-    n2 = m_vec - n
-    valid = (np.abs(n2) <= n_cut).all(-1)                      # particle 2 inside the box too
-    # one-body part: h0(k1) x I + I x h0(k2), a 4x4 block per n (index s1 * 2 + s2)
-    H1 = np.einsum("xyab,cd->xyacbd", h0(k1, m_star, lambda_r, h_z), np.eye(2))
-    H1 = H1 + np.einsum("ab,xycd->xyacbd", np.eye(2), h0(k2, m_star, lambda_r, h_z))
-    H1 = H1.reshape(S, S, 4, 4)
-    # Coulomb kernel over differences d in [-2 n_cut, 2 n_cut]^2, zero-padded FFT convolution
-    P = 4 * n_cut + 2
-    d1 = np.arange(-2 * n_cut, 2 * n_cut + 1)
-    dx, dy = np.meshgrid(d1, d1, indexing="ij")
-    q = np.stack([dx, dy], -1).astype(float) @ B.T
-    qn = np.linalg.norm(q, axis=-1)
-    ker = np.where(qn > 0, 2.0 * np.pi * alpha / (area * np.where(qn > 0, qn, 1.0)), 0.0)
-    kpad = np.zeros((P, P))
-    kpad[:4 * n_cut + 1, :4 * n_cut + 1] = ker
-    kf = np.fft.fft2(kpad)
-    const = zeta_M  # N zeta_M / 2 with N = 2
-    mask = valid[..., None].astype(float)                      # (S, S, 1)
-    perm = np.array([0, 2, 1, 3])                              # (s1, s2) -> (s2, s1)
+class Sector:
+    """The two-electron Hamiltonian restricted to total momentum K = B m + 2 A^-T twist: the
+    amplitudes c(n_1, s_1, s_2) (shape (S, S, 4), S = 2 n_cut + 1, spin index s_1 * 2 + s_2) with
+    k_2 = K - k(n_1), both particles inside the box."""
 
-    def exch(c):  # c(n, s1, s2) -> c(m - n, s2, s1): n -> m - n reverses the box about m / 2
+    def __init__(self, A, m_vec, n_cut, m_star=1.0, lambda_r=1.0, h_z=0.0, alpha=1.0,
+                 twist=(0.0, 0.0), zeta_M=0.0):
+        A = np.asarray(A, float)
+        Ainv = np.linalg.inv(A)
+        B = 2.0 * np.pi * Ainv.T
+        kt = Ainv.T @ np.asarray(twist, float)
+        area = float(abs(np.linalg.det(A)))
+        n1 = np.arange(-n_cut, n_cut + 1)
+        nx, ny = np.meshgrid(n1, n1, indexing="ij")
+        self.n = np.stack([nx, ny], -1).astype(float)               # (S, S, 2)
+        self.S = S = 2 * n_cut + 1
+        self.n_cut = n_cut
+        self.m_vec = m_vec = np.asarray(m_vec, float)
+        k1 = self.n @ B.T + kt
+        K = B @ m_vec + 2.0 * kt
+        k2 = K - k1
+        n2 = m_vec - self.n
+        self.valid = (np.abs(n2) <= n_cut).all(-1)                  # particle 2 inside the box
+        # one-body part: h0(k1) x I + I x h0(k2), a 4x4 block per n (index s1 * 2 + s2)
+        H1 = np.einsum("xyab,cd->xyacbd", h0(k1, m_star, lambda_r, h_z), np.eye(2))
+        H1 = H1 + np.einsum("ab,xycd->xyacbd", np.eye(2), h0(k2, m_star, lambda_r, h_z))
+        self.H1 = H1.reshape(S, S, 4, 4)
+        # Coulomb kernel over differences d in [-2 n_cut, 2 n_cut]^2, zero-padded FFT convolution
+        self.P = P = 4 * n_cut + 2
+        d1 = np.arange(-2 * n_cut, 2 * n_cut + 1)
+        dx, dy = np.meshgrid(d1, d1, indexing="ij")
+        q = np.stack([dx, dy], -1).astype(float) @ B.T
+        qn = np.linalg.norm(q, axis=-1)
+        ker = np.where(qn > 0, 2.0 * np.pi * alpha / (area * np.where(qn > 0, qn, 1.0)), 0.0)
+        kpad = np.zeros((P, P))
+        kpad[:4 * n_cut + 1, :4 * n_cut + 1] = ker
+        self.kf = np.fft.fft2(kpad)
+        self.const = zeta_M  # N zeta_M / 2 with N = 2
+        self.mask = self.valid[..., None].astype(float)             # (S, S, 1)
+        self.perm = np.array([0, 2, 1, 3])                          # (s1, s2) -> (s2, s1)
+
+    def exch(self, c):  # c(n, s1, s2) -> c(m - n, s2, s1): n -> m - n reverses the box about m/2
         out = np.zeros_like(c)
+        n_cut, n, m_vec, ok = self.n_cut, self.n, self.m_vec, self.valid
         ix = (m_vec[0] - n[..., 0] + n_cut).astype(int)
         iy = (m_vec[1] - n[..., 1] + n_cut).astype(int)
-        ok = valid
-        out[ok] = c[ix[ok], iy[ok]][:, perm]
+        out[ok] = c[ix[ok], iy[ok]][:, self.perm]
         return out
 
-    def proj(c):  # antisymmetric part, inside the box
-        c = c * mask
-        return 0.5 * (c - exch(c))
+    def proj(self, c):  # antisymmetric part, inside the box
+        c = c * self.mask
+        return 0.5 * (c - self.exch(c))
 
-    def apply_H(c):
-        out = np.einsum("xyab,xyb->xya", H1, c) + const * c
+    def apply_H(self, c):
+        S, P, n_cut = self.S, self.P, self.n_cut
+        out = np.einsum("xyab,xyb->xya", self.H1, c) + self.const * c
         cp = np.zeros((P, P, 4), dtype=complex)
         cp[:S, :S] = c
-        conv = np.fft.ifft2(np.fft.fft2(cp, axes=(0, 1)) * kf[..., None], axes=(0, 1))
-        out = out + conv[2 * n_cut:2 * n_cut + S, 2 * n_cut:2 * n_cut + S]
-        return out
+        conv = np.fft.ifft2(np.fft.fft2(cp, axes=(0, 1)) * self.kf[..., None], axes=(0, 1))
+        return out + conv[2 * n_cut:2 * n_cut + S, 2 * n_cut:2 * n_cut + S]
 
+
+def sector_ground_energy(A, m_vec, n_cut, m_star=1.0, lambda_r=1.0, h_z=0.0, alpha=1.0,
+                         twist=(0.0, 0.0), zeta_M=0.0, tol=1e-12, shift=1.0e4, offset=10.0):
+    sec = Sector(A, m_vec, n_cut, m_star, lambda_r, h_z, alpha, twist, zeta_M)
+    S = sec.S
     dim = S * S * 4
 
     # `offset` keeps the sought eigenvalue away from 0, where ARPACK's relative residual test
     # cannot converge; it is removed from the result
     def mv(x):
         c = x.reshape(S, S, 4)
-        pc = proj(c)
-        y = proj(apply_H(pc)) + offset * pc + shift * (c - pc)
+        pc = sec.proj(c)
+        y = sec.proj(sec.apply_H(pc)) + offset * pc + shift * (c - pc)
         return y.reshape(-1)
 
     op = LinearOperator((dim, dim), matvec=mv, dtype=complex)
     rng = np.random.default_rng(0)
-    v0 = proj((rng.standard_normal((S, S, 4)) + 1j * rng.standard_normal((S, S, 4)))).reshape(-1)
+    v0 = sec.proj((rng.standard_normal((S, S, 4)) + 1j * rng.standard_normal((S, S, 4)))).reshape(-1)
     w = eigsh(op, k=1, which="SA", v0=v0, tol=tol, maxiter=20000, return_eigenvectors=False)
     return float(w[0]) - offset
 
 
+def expectation(A, coeff, n_cut, m_star=1.0, lambda_r=1.0, h_z=0.0, alpha=1.0,
+                twist=(0.0, 0.0), ewald_alpha=None):
+    """<psi|H|psi> / <psi|psi> of a two-electron state given by its plane-wave amplitudes
+    coeff[n1x, n1y, n2x, n2y, s1, s2] (indices n + n_cut, |n| <= n_cut per component), with
+    every total-momentum sector's Hamiltonian (the same H as ground_energy). The exact
+    variational energy of the state truncated to the basis; no sampling, no local energy."""
+    ew = O.Ewald(A, alpha=alpha, ewald_alpha=ewald_alpha, n_real=6, n_recip=12)
+    S = 2 * n_cut + 1
+    num, den = 0.0, 0.0
+    for mx in range(-2 * n_cut, 2 * n_cut + 1):
+        for my in range(-2 * n_cut, 2 * n_cut + 1):
+            sec = Sector(A, (mx, my), n_cut, m_star, lambda_r, h_z, alpha, twist, ew.zeta_M)
+            n = sec.n.astype(int)
+            ix2, iy2 = mx - n[..., 0] + n_cut, my - n[..., 1] + n_cut
+            ok = sec.valid
+            c = np.zeros((S, S, 4), dtype=complex)
+            c[ok] = coeff[n[ok][:, 0] + n_cut, n[ok][:, 1] + n_cut, ix2[ok], iy2[ok]].reshape(-1, 4)
+            den += float(np.vdot(c, c).real)
+            num += float(np.vdot(c, sec.apply_H(c)).real)
+    return num / den
 def ground_energy(A, n_cut, m_star=1.0, lambda_r=1.0, h_z=0.0, alpha=1.0, twist=(0.0, 0.0),
                   ewald_alpha=None, m_range=1):
     """Two-electron ground-state energy: the lowest over total-momentum sectors

@@ -228,6 +228,49 @@ def test_ed2_noninteracting_limit_and_convergence():
     assert e10 - g["E_ed_ncut24"] < 3e-5
 
 
+def slater_pair_on_grid(L, G, na, nb, lambda_r, h_z):
+    """A two-electron Slater determinant of Rashba eigen-spinors at plane waves k(na), k(nb),
+    sampled on a G^4 grid of (r_1, r_2) and its amplitudes by FFT (the projection the ED check
+    applies to the trained network), with its energy in closed form: band energies + zeta_M +
+    the exchange term -(2 pi / (A |k_a - k_b|)) |<chi_a|chi_b>|^2."""
+    from oracle import ed2
+    A = np.diag([L, L])
+    B = 2.0 * np.pi * np.linalg.inv(A).T
+    ka, kb = B @ np.asarray(na, float), B @ np.asarray(nb, float)
+    ea, va = np.linalg.eigh(ed2.h0(ka, 1.0, lambda_r, h_z))
+    eb, vb = np.linalg.eigh(ed2.h0(kb, 1.0, lambda_r, h_z))
+    xa, xb = va[:, 0], vb[:, 1]
+    f = np.arange(G) * L / G
+    x1, y1, x2, y2 = np.meshgrid(f, f, f, f, indexing="ij")
+    pw = lambda k, x, y: np.exp(1j * (k[0] * x + k[1] * y))  # noqa: E731
+    psi = np.empty((G, G, G, G, 2, 2), complex)
+    for s1 in range(2):
+        for s2 in range(2):
+            psi[..., s1, s2] = (pw(ka, x1, y1) * xa[s1] * pw(kb, x2, y2) * xb[s2]
+                                - pw(kb, x1, y1) * xb[s1] * pw(ka, x2, y2) * xa[s2])
+    coeff = np.fft.fftn(psi, axes=(0, 1, 2, 3)) / G ** 4
+    exch = -2.0 * np.pi / (L * L * np.linalg.norm(ka - kb)) * abs(np.vdot(xa, xb)) ** 2
+    return coeff, ea[0] + eb[1] + exch
+
+
+def test_ed2_expectation_of_a_projected_slater_determinant():
+    """oracle/ed2.expectation (<H> of plane-wave amplitudes, every total-momentum sector) on a
+    Slater determinant sampled on a grid and Fourier transformed: equals the closed-form energy
+    to 1e-12, which pins the FFT sign, the spin index order and the Coulomb / Madelung terms of
+    the projection that measures the trained network's variational energy."""
+    import json
+    from oracle import ed2
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ed2_config1.json")))
+    L, nc, G = g["L"], 3, 8
+    for na, nb in (((1, 0), (0, -1)), ((0, 0), (1, 1))):
+        coeff, e_ref = slater_pair_on_grid(L, G, na, nb, g["lambda_r"], g["h_z"])
+        idx = np.arange(-nc, nc + 1) % G
+        c = coeff[idx][:, idx][:, :, idx][:, :, :, idx]
+        e = ed2.expectation(np.diag([L, L]), c, nc, 1.0, g["lambda_r"], g["h_z"], alpha=1.0,
+                            ewald_alpha=5.0 / L)
+        assert abs(e - (e_ref + g["zeta_M"])) < 1e-12, (e, e_ref + g["zeta_M"])
+
+
 def test_slater_model_is_the_slater_determinant():
     """The network behind nqs.slater (zero backflow, no Jastrow, one determinant) reproduces the
     spinor Slater determinant of the reference (slater_reference.py:21-37) on the oracle."""
