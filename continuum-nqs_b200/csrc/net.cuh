@@ -124,6 +124,7 @@ bool block_value_tc_ok(int N, int d, int H, int ff);
 int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, int b,
                    const BlockW<float>& bw, cudaStream_t st, bool* done);
 extern bool g_block_fusion;
+extern bool g_head_lg;
 bool profiling_enabled();  // nqs_profile_gemm(1) is in force
 size_t tc_weights_bytes(const NqsModelDesc& d, bool bf16);
 int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,

@@ -14,6 +14,7 @@
 
 #include "net_kernels.cuh"
 #include "head_rt.cuh"
+#include "head_lg.cuh"
 
 namespace nqs {
 
@@ -25,6 +26,46 @@ size_t net_scratch_bytes(const ModelConst& mc, size_t rows) {
   const size_t d = mc.d;
   const size_t big = std::max({3 * d, (size_t)mc.ff * d, (size_t)2 * mc.K * mc.N});
   return rows * (3 * d + big) * sizeof(T) + 4 * 256;
+}
+
+bool g_head_lg = true;
+
+extern "C" int nqs_set_head_lg(int enable) {
+  g_head_lg = enable != 0;
+  return NQS_OK;
+}
+
+// one CTA per job for 16 < N (head_lg.cuh); false when the job's tables do not fit
+template <typename T>
+static bool launch_head_lg(const ModelConst& mc, const JobBatch& cb, const T* BF, int ldbf,
+                           const HeadParams& hp, const HeadOut& out, int jout, cudaStream_t st) {
+  const int N = cb.N;
+  const bool tan = cb.n_tan > 0, lap = tan && cb.has_lap;
+  const int mode = lap ? 2 : (tan ? 1 : 0);
+  const int ts = head_lg_ts(N);
+  if (N > kHeadLgMaxN || (lap && N > kHeadLgMaxNLap) || mc.K > NQS_MAX_DETS) return false;
+  const HeadLgLayout lay = head_lg_layout(N, mc.nG, mc.K, cb.n_tan, mode, mode == 2 ? ts : 1);
+  if (lay.total + kHeadLgStaticBytes > 227 * 1024) return false;
+  static bool attr = false;  // one-time opt-in to large dynamic shared memory, per instantiation
+  if (!attr) {
+    const int mx = 227 * 1024 - (int)kHeadLgStaticBytes;
+    cudaFuncSetAttribute(k_head_lg<T, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_head_lg<T, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_head_lg<T, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_head_lg<T, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    attr = true;
+  }
+  const unsigned grid = (unsigned)cb.n_jobs;
+  const size_t sm = lay.total;
+  if (mode == 0)
+    k_head_lg<T, 0, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+  else if (mode == 1)
+    k_head_lg<T, 1, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+  else if (ts == 2)
+    k_head_lg<T, 2, 2><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+  else
+    k_head_lg<T, 2, 3><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+  return true;
 }
 
 template <typename T>
@@ -194,6 +235,10 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         k_head_rt<T, false, false><<<rg, 64, rp.bytes, st>>>(cb, mc, Big, 2 * KN, hp, out, jout,
                                                              rp.jpc, rp.job_bytes, rp.hw_bytes);
       NQS_CHECK_LAUNCH("k_head_rt");
+      continue;
+    }
+    if (g_head_lg && launch_head_lg<T>(mc, cb, Big, 2 * KN, hp, out, jout, st)) {
+      NQS_CHECK_LAUNCH("k_head_lg");
       continue;
     }
     const HeadPlan hpl = head_plan(N, mc.nG, mc.K, cb.n_tan, tan);

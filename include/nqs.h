@@ -134,6 +134,12 @@ int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches);
  * runs as separate LayerNorm / GEMM / attention / GEMM launches. Both compute the same function
  * with the same TF32 products; the switch exists so that the two can be compared. */
 int nqs_set_block_fusion(int enable);
+/* Implementation selection (no reference counterpart; process-wide, default on): with it on,
+ * the determinant head of more than 16 electrons runs one 256-thread CTA per job (every
+ * elimination step and every tangent product spread over the CTA; up to 64 electrons, 48 with
+ * the Laplacian); off, one warp per (job, determinant). Same function, same pivot rule; the
+ * switch exists so that the two can be compared. */
+int nqs_set_head_lg(int enable);
 /* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
  * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;
  * 0 restores the default (4). A tuning knob of the multi-instance autotuner. */

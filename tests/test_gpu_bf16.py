@@ -61,16 +61,19 @@ def test_bf16_logpsi_follows_bf16_rounding(fused):
 
 
 def test_bf16_local_energy_close_to_fp64():
-    """Forward-Laplacian and spin-orbit batches through the BF16 row GEMMs: local energies within
-    BF16-level errors of the float64 path (median per-walker error below 1e-2 Ha, mean energy
-    within 1e-2 Ha)."""
+    """Forward-Laplacian and spin-orbit batches through the BF16 row GEMMs: per-walker local
+    energy errors against the float64 path scale like the operand rounding. BF16 keeps 8
+    significant bits and TF32 11, so the BF16 errors are expected ~8x the TF32 ones: the median
+    BF16 error lies between the TF32 median and 32x it, and below 5% of the median |E_loc|."""
     from nqs.local_energy import make_local_energy
     from nqs.psiformer import make_logpsi
     model, p = _model()
     R, S = configs(model.n_elec, model.L, 64, 93)
-    eb = make_local_energy(make_logpsi(model, p, precision="mixed_bf16"), 1.0, 1.0, 0.5)(R, S)
-    e64 = make_local_energy(make_logpsi(model, p), 1.0, 1.0, 0.5)(R, S)
-    d = (eb - e64).abs().cpu()
-    assert torch.isfinite(eb).all()
-    assert float(d.median()) < 1e-2, float(d.median())
-    assert abs(float((eb.real - e64.real).mean())) < 1e-2
+    el = {prec: make_local_energy(make_logpsi(model, p, precision=prec), 1.0, 1.0, 0.5)(R, S).cpu()
+          for prec in ("mixed_bf16", "mixed", "fp64")}
+    assert torch.isfinite(el["mixed_bf16"]).all()
+    d_bf = float((el["mixed_bf16"] - el["fp64"]).abs().median())
+    d_tf = float((el["mixed"] - el["fp64"]).abs().median())
+    scale = float(el["fp64"].abs().median())
+    assert d_tf < d_bf < 32.0 * d_tf, (d_bf, d_tf, scale)
+    assert d_bf < 0.05 * scale, (d_bf, d_tf, scale)

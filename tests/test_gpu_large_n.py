@@ -62,3 +62,47 @@ def test_per_sample_O_n18_matches_oracle():
     ot, ou = O.real_ravel(p["params"])
     Oo = O.per_sample_O(model, ot, ou, R, S)
     assert (Og - Oo).abs().max() < 1e-10 * max(1.0, float(Oo.abs().max()))
+
+
+def test_local_energy_n40_matches_oracle():
+    """N = 40 (the CTA-per-job head with 3 x 3 tiles of the tangent products per thread): the
+    local energy, forward Laplacian and spin-orbit flips included, against the dense-Hessian
+    oracle."""
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import make_logpsi
+    g, model = build(N=40, L=12.0, embed=16, depth=1, heads=4, n_dets=2, use_jastrow=True,
+                     n_knots=4)
+    p = perturb(model.init(0), 0.05, 47)
+    R, S = configs(model.n_elec, model.L, 2, 48)
+    e = make_local_energy(make_logpsi(model, p), 1.0, 1.0, 0.5)(R, S).cpu()
+    for w in range(2):
+        ref = O.local_energy(lambda r, s: O.logpsi(model, p, r, s), R[w], S[w], 1.0, 1.0, 0.5)
+        assert abs(complex(e[w]) - complex(ref)) < 1e-9 * max(1.0, abs(complex(ref)))
+
+
+@pytest.mark.parametrize("N,K,prec", [(24, 3, "fp64"), (40, 2, "fp64"), (24, 3, "mixed"),
+                                      (33, 2, "mixed")])
+def test_cta_head_equals_warp_head(N, K, prec):
+    """The CTA-per-job determinant head (default past 16 electrons) against the warp-per-
+    determinant head it replaces (nqs_set_head_lg(0)), on the same network outputs: log psi,
+    local energies (forward-Laplacian batch and spin-orbit flips) and spin estimators agree to
+    rounding (1e-10 relative; the two sum in different orders)."""
+    from nqs import _lib
+    from nqs.local_energy import make_local_energy
+    from nqs.psiformer import make_logpsi
+    g, model = build(N=N, L=1.9 * np.sqrt(N), embed=32, depth=2, heads=4, n_dets=K,
+                     use_jastrow=True, n_knots=6)
+    p = perturb(model.init(0), 0.05, 50 + N)
+    R, S = configs(model.n_elec, model.L, 37, 51 + N)
+    out = {}
+    for on in (1, 0):
+        _lib.lib().nqs_set_head_lg(on)
+        try:
+            lp = make_logpsi(model, p, precision=prec)
+            out[on] = (lp(R, S).cpu(), make_local_energy(lp, 1.0, 0.7, 0.3)(R, S).cpu())
+        finally:
+            _lib.lib().nqs_set_head_lg(1)
+    for a, b in zip(out[1], out[0]):
+        d = a - b
+        d = d.real.abs() + ((d.imag + np.pi) % (2 * np.pi) - np.pi).abs()
+        assert float((d / b.abs().clamp(min=1.0)).max()) < 1e-10, float(d.max())
