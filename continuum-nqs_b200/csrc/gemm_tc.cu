@@ -299,10 +299,6 @@ double g_gemm_bytes = 0.0;
 
 bool profiling_enabled() { return g_gemm_prof; }
 
-bool rowgemm_tc_ok(int K, int ldx, int Nout) {
-  return K % tc::RG_KB == 0 && K <= 128 && ldx % 4 == 0 && Nout >= 1 && Nout <= 256;
-}
-
 // float32 -> BF16 (round to nearest even) copy of n values
 __global__ void k_f32_to_bf16(const float* __restrict__ x, __nv_bfloat16* __restrict__ y,
                               size_t n) {
@@ -310,9 +306,11 @@ __global__ void k_f32_to_bf16(const float* __restrict__ x, __nv_bfloat16* __rest
   if (i < n) y[i] = __float2bfloat16_rn(x[i]);
 }
 
-int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
-               const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
-               cudaStream_t st, int act, const uint16_t* WT16) {
+// one launch: K <= 128, Npad <= 256; W^T rows (K-major) have stride ldw elements
+static int rowgemm_tc_piece(const float* X, int ldx, int rows, int K, const float* WT, int ldw,
+                            int Npad, int Nout, const float* bias, int C, const float* Res,
+                            int ldr, float* Y, int ldy, int* err, cudaStream_t st, int act,
+                            const uint16_t* WT16) {
   if (rows <= 0) return NQS_OK;
   const bool bf = WT16 != nullptr && K % 64 == 0;
   if (act && C != 1) {
@@ -348,7 +346,7 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
   }
   {
     const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)Npad};
-    const cuuint64_t strides[1] = {(cuuint64_t)K * (bf ? 2 : 4)};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldw * (bf ? 2 : 4)};
     const cuuint32_t box[2] = {(cuuint32_t)(bf ? 64 : tc::RG_KB), (cuuint32_t)Npad};
     if (enc(&tb, bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
             bf ? (void*)WT16 : (void*)WT, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -433,6 +431,39 @@ int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Np
     g_gemm_bytes += 4.0 * ((double)rows * K + (double)Npad * K + (double)rows * Nout * (Res ? 2 : 1));
   }
   NQS_CHECK_LAUNCH("k_rowgemm_tc");
+  return NQS_OK;
+}
+
+// Any K (a multiple of 32) and any output width: pieces of at most 128 K-columns and 256 output
+// columns, one launch each. The first K piece of an output slice stores (with the bias) or, when
+// a residual is given, adds into Y; later K pieces add their partial products into Y with the
+// bulk reduction. The fused activation needs a single K piece.
+int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
+               const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
+               cudaStream_t st, int act, const uint16_t* WT16) {
+  constexpr int kMaxK = 128, kMaxN = 256;
+  if (K <= kMaxK && Npad <= kMaxN)
+    return rowgemm_tc_piece(X, ldx, rows, K, WT, K, Npad, Nout, bias, C, Res, ldr, Y, ldy, err,
+                            st, act, WT16);
+  if (act && K > kMaxK) {
+    set_error("rowgemm_tc: the fused activation needs K <= %d", kMaxK);
+    return NQS_ERR_INVALID_ARG;
+  }
+  if (Res && (Res != Y || ldr != ldy)) {
+    set_error("rowgemm_tc: the residual must be the output itself (in-place Y += X W)");
+    return NQS_ERR_INVALID_ARG;
+  }
+  for (int n0 = 0; n0 < Npad && n0 < Nout; n0 += kMaxN) {
+    const int np = std::min(kMaxN, Npad - n0), no = std::min(np, Nout - n0);
+    for (int k0 = 0; k0 < K; k0 += kMaxK) {
+      const int kp = std::min(kMaxK, K - k0);
+      const bool first = k0 == 0;
+      const float* res = (Res || !first) ? Y + n0 : nullptr;
+      NQS_TRY(rowgemm_tc_piece(X + k0, ldx, rows, kp, WT + (size_t)n0 * K + k0, K, np, no,
+                               first && bias ? bias + n0 : nullptr, C, res, ldy, Y + n0, ldy,
+                               err, st, act, WT16 ? WT16 + (size_t)n0 * K + k0 : nullptr));
+    }
+  }
   return NQS_OK;
 }
 
@@ -528,8 +559,8 @@ int build_tc_weights(const NqsModelDesc& d, const float* th, Arena& ws, TcNet* o
   const int dd = d.embed_dim, D = d.ff_mult * dd, KN = d.n_dets * d.n_elec;
   t.npad_qkv = pad16(3 * dd);
   t.npad_bf = pad16(2 * KN);
-  if (!rowgemm_tc_ok(dd, dd, t.npad_qkv) || !rowgemm_tc_ok(D, D, dd) || !rowgemm_tc_ok(dd, dd, D) ||
-      !rowgemm_tc_ok(dd, dd, t.npad_bf)) {
+  // every Dense layer runs as row-GEMM pieces of K <= 128 and N <= 256 (rowgemm_tc)
+  if (dd % tc::RG_KB || D % tc::RG_KB) {
     t.on = 0;
     *out = t;
     return NQS_OK;

@@ -1694,7 +1694,7 @@ __global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W
 // ============================================================================================
 // relative reduction of the preconditioned residual sqrt(r.z / r0.z0) at which the conjugate
 // gradients stop by default
-constexpr double kPcgDefaultTol = 1e-3;
+constexpr double kPcgDefaultTol = 1e-2;
 
 // caller-facing status from the internal slots: [0] non-positive pivot, [1] Gram timeout,
 // [2] floored pivots, [3] PCG iterations, [4] PCG stop reason (0 iteration limit, 1 converged,

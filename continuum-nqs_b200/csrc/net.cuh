@@ -111,10 +111,10 @@ int logpsi_vjp_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
                    const double* R, const int32_t* S, int W, const cplx* ct, double* grad,
                    bool ckpt, Arena& ws, cudaStream_t st);
 
-// tensor-core row GEMM (gemm_tc.cu)
-bool rowgemm_tc_ok(int K, int ldx, int Nout);
-// act 1: tanh-GELU on the output (C == 1 only); WT16 (nullable): BF16 copy of W^T, which makes
-// the operands BF16 (kind::f16) when K is a multiple of 64
+// tensor-core row GEMM (gemm_tc.cu): K a multiple of 32, any width (pieces of K <= 128 and
+// N <= 256, one launch each); act 1: tanh-GELU on the output (C == 1 and K <= 128 only); WT16
+// (nullable): BF16 copy of W^T, which makes the operands BF16 (kind::f16) when K is a multiple
+// of 64
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
                cudaStream_t st, int act = 0, const uint16_t* WT16 = nullptr);
@@ -124,7 +124,6 @@ bool block_value_tc_ok(int N, int d, int H, int ff);
 int block_value_tc(float* X, int n_jobs, int N, int d, int H, const TcNet& tcn, int b,
                    const BlockW<float>& bw, cudaStream_t st, bool* done);
 extern bool g_block_fusion;
-extern bool g_head_lg;
 bool profiling_enabled();  // nqs_profile_gemm(1) is in force
 size_t tc_weights_bytes(const NqsModelDesc& d, bool bf16);
 int build_tc_weights(const NqsModelDesc& d, const float* theta32, Arena& ws, TcNet* out,

@@ -28,10 +28,10 @@ size_t net_scratch_bytes(const ModelConst& mc, size_t rows) {
   return rows * (3 * d + big) * sizeof(T) + 4 * 256;
 }
 
-bool g_head_lg = true;
+bool g_large_n_cta = true;
 
-extern "C" int nqs_set_head_lg(int enable) {
-  g_head_lg = enable != 0;
+extern "C" int nqs_set_large_n_kernels(int enable) {
+  g_large_n_cta = enable != 0;
   return NQS_OK;
 }
 
@@ -237,7 +237,7 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       NQS_CHECK_LAUNCH("k_head_rt");
       continue;
     }
-    if (g_head_lg && launch_head_lg<T>(mc, cb, Big, 2 * KN, hp, out, jout, st)) {
+    if (g_large_n_cta && launch_head_lg<T>(mc, cb, Big, 2 * KN, hp, out, jout, st)) {
       NQS_CHECK_LAUNCH("k_head_lg");
       continue;
     }

@@ -7,6 +7,11 @@
 
 namespace nqs {
 
+// kernels of more than 16 electrons: one CTA per job (head) and per (job, head) (attention);
+// off, the warp-per-task kernels (nqs_set_large_n_kernels)
+extern bool g_large_n_cta;
+
+
 constexpr double kPi = 3.141592653589793;
 constexpr double kLnEps = 1e-6;  // flax.linen.LayerNorm default epsilon
 
@@ -907,6 +912,267 @@ inline int launch_attention_rt(int n_jobs, int N, int C, int n_tan, int has_lap,
   return NQS_OK;
 }
 
+// --------------------------------------------------------------------------------------------
+// Attention for 16 < N <= 64 tokens: one CTA (256 threads) per (job, head), same arithmetic as
+// k_attention. Thread (ty, tx) = (tid / 16, tid % 16) owns the score / probability entries of
+// rows ty + 16u and columns tx + 16w (u, w < TS); a half-warp holds whole rows, so the softmax
+// and every row sum (d_t lse, Lap lse) are 16-lane shuffles. P_qk and P_sq stay in the owners'
+// registers across the channels, and so does P_av for the output entries: thread
+// (tid / (HD/4), tid % (HD/4)) writes features 4 (tid % (HD/4)) .. + 3 of one token. Per channel:
+// stage Q_c, K_c, V_c head tiles (rows past N are zero), scores, one barrier, outputs.
+// Rows of the K-type tiles are HD + 4 long (16 rows of a half-warp fall in different banks); the
+// probability tiles have an odd row length.
+// --------------------------------------------------------------------------------------------
+template <int HD>
+constexpr int attn_cta_hdp() { return HD + 4; }
+
+template <typename T, int TS, int HD>
+__host__ __device__ constexpr size_t attention_cta_bytes() {
+  return sizeof(T) * (6 * (size_t)(16 * TS) * attn_cta_hdp<HD>() +
+                      2 * (size_t)(16 * TS) * (16 * TS + 1));
+}
+
+template <typename T>
+__device__ __forceinline__ T hw_sum16(T v) {
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T hw_max16(T v) {
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <typename T, int TS, int HD>
+__global__ void __launch_bounds__(256) k_attention_cta(int n_jobs, int N, int C, int n_tan,
+                                                       int has_lap, int d, int H,
+                                                       const T* __restrict__ QKV,
+                                                       T* __restrict__ OUT) {
+  constexpr int NP = 16 * TS, HDP = attn_cta_hdp<HD>(), LDA = NP + 1, NQ = HD / 4;
+  const int pair = blockIdx.x;
+  const int job = pair / H, h = pair - job * H;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* q = reinterpret_cast<T*>(smraw);
+  T* k = q + NP * HDP;
+  T* v = k + NP * HDP;
+  T* qt = v + NP * HDP;
+  T* kt = qt + NP * HDP;
+  T* vt = kt + NP * HDP;
+  T* A = vt + NP * HDP;
+  T* ST = A + NP * LDA;
+  const T sc = T(1) / sqrt(T(HD));
+  const int ld = 3 * d;
+  auto row = [&](int i, int c) -> size_t { return ((size_t)job * N + i) * C + c; };
+  // Q, K, V head tiles of channel c (rows >= N zero)
+  auto stage = [&](int c, T* dq, T* dk, T* dv) {
+    for (int idx = tid; idx < NP * HD; idx += 256) {
+      const int i = idx / HD, e = idx - i * HD;
+      T a = T(0), b = T(0), cc = T(0);
+      if (i < N) {
+        const T* p = QKV + row(i, c) * ld + h * HD + e;
+        a = p[0];
+        b = p[d];
+        cc = p[2 * d];
+      }
+      dq[i * HDP + e] = a;
+      dk[i * HDP + e] = b;
+      dv[i * HDP + e] = cc;
+    }
+  };
+  // output thread: token oi, features 4 oq .. 4 oq + 3
+  const int oi = tid / NQ, oq = tid - (tid / NQ) * NQ;
+  const bool out_on = oi < N;
+  // sum_j P1[oi][j] V1[j][f] + P2[oi][j] V2[j][f] (and sum_j P1 V2 into pav when acc)
+  auto outputs = [&](const T* P1, const T* V1, const T* P2, const T* V2, T (&o)[4], T* pav) {
+#pragma unroll
+    for (int f = 0; f < 4; ++f) o[f] = T(0);
+    if (!out_on) return;
+    const T* p1 = P1 + oi * LDA;
+    const T* p2 = P2 ? P2 + oi * LDA : nullptr;
+    for (int j = 0; j < N; ++j) {
+      const T a1 = p1[j];
+      const T* v1 = V1 + j * HDP + 4 * oq;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) o[f] = fma(a1, v1[f], o[f]);
+      if (p2) {
+        const T a2 = p2[j];
+        const T* v2 = V2 + j * HDP + 4 * oq;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          o[f] = fma(a2, v2[f], o[f]);
+          if (pav) pav[f] = fma(a1, v2[f], pav[f]);
+        }
+      }
+    }
+  };
+  auto store = [&](int c, const T (&o)[4]) {
+    if (!out_on) return;
+    T* p = OUT + row(oi, c) * d + h * HD + 4 * oq;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) p[f] = o[f];
+  };
+  // ---- value channel: probabilities a (registers and shared), output ----
+  stage(0, q, k, v);
+  __syncthreads();
+  T a[TS][TS];
+#pragma unroll
+  for (int u = 0; u < TS; ++u) {
+    const int i = ty + 16 * u;
+    T sv[TS];
+#pragma unroll
+    for (int w = 0; w < TS; ++w) sv[w] = T(0);
+#pragma unroll
+    for (int e = 0; e < HD; ++e) {
+      const T qe = q[i * HDP + e];
+#pragma unroll
+      for (int w = 0; w < TS; ++w) sv[w] = fma(qe, k[(tx + 16 * w) * HDP + e], sv[w]);
+    }
+    T mx = -INFINITY;
+#pragma unroll
+    for (int w = 0; w < TS; ++w) {
+      sv[w] = (tx + 16 * w < N) ? sv[w] * sc : T(-INFINITY);
+      mx = max(mx, sv[w]);
+    }
+    mx = hw_max16(mx);
+    T ssum = T(0);
+#pragma unroll
+    for (int w = 0; w < TS; ++w) {
+      sv[w] = (tx + 16 * w < N) ? exp(sv[w] - mx) : T(0);
+      ssum += sv[w];
+    }
+    ssum = hw_sum16(ssum);
+#pragma unroll
+    for (int w = 0; w < TS; ++w) {
+      a[u][w] = sv[w] / ssum;
+      A[i * LDA + tx + 16 * w] = a[u][w];
+    }
+  }
+  __syncthreads();
+  T o[4];
+  outputs(A, v, nullptr, nullptr, o, nullptr);
+  store(0, o);
+  if (C == 1) return;
+  T pqk[TS][TS], psq[TS][TS], pav[4];
+#pragma unroll
+  for (int u = 0; u < TS; ++u)
+#pragma unroll
+    for (int w = 0; w < TS; ++w) pqk[u][w] = psq[u][w] = T(0);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) pav[f] = T(0);
+  // scores of a channel: s1 = qt.k + q.kt (and s2 = qt.kt)
+  auto scores = [&](T (&s1)[TS][TS], T (&s2)[TS][TS], bool want_s2) {
+#pragma unroll
+    for (int u = 0; u < TS; ++u)
+#pragma unroll
+      for (int w = 0; w < TS; ++w) s1[u][w] = s2[u][w] = T(0);
+#pragma unroll 4
+    for (int e = 0; e < HD; ++e) {
+      T qa[TS], qb[TS], ka[TS], kb[TS];
+#pragma unroll
+      for (int u = 0; u < TS; ++u) {
+        qa[u] = qt[(ty + 16 * u) * HDP + e];
+        qb[u] = q[(ty + 16 * u) * HDP + e];
+      }
+#pragma unroll
+      for (int w = 0; w < TS; ++w) {
+        ka[w] = k[(tx + 16 * w) * HDP + e];
+        kb[w] = kt[(tx + 16 * w) * HDP + e];
+      }
+#pragma unroll
+      for (int u = 0; u < TS; ++u)
+#pragma unroll
+        for (int w = 0; w < TS; ++w) {
+          s1[u][w] = fma(qa[u], ka[w], fma(qb[u], kb[w], s1[u][w]));
+          if (want_s2) s2[u][w] = fma(qa[u], kb[w], s2[u][w]);
+        }
+    }
+  };
+  for (int t = 0; t < n_tan; ++t) {
+    __syncthreads();  // the previous channel's outputs no longer read ST / vt
+    stage(1 + t, qt, kt, vt);
+    __syncthreads();
+    T s1[TS][TS], s2[TS][TS];
+    scores(s1, s2, has_lap != 0);
+#pragma unroll
+    for (int u = 0; u < TS; ++u) {
+      T l = T(0);
+#pragma unroll
+      for (int w = 0; w < TS; ++w) {
+        s1[u][w] *= sc;
+        l = fma(a[u][w], s1[u][w], l);
+      }
+      l = hw_sum16(l);
+#pragma unroll
+      for (int w = 0; w < TS; ++w) {
+        const T ds = s1[u][w] - l;
+        if (has_lap) {
+          pqk[u][w] += s2[u][w];
+          psq[u][w] = fma(ds, ds, psq[u][w]);
+        }
+        ST[(ty + 16 * u) * LDA + tx + 16 * w] = a[u][w] * ds;
+      }
+    }
+    __syncthreads();
+    outputs(ST, v, A, vt, o, has_lap ? pav : nullptr);
+    store(1 + t, o);
+  }
+  if (!has_lap) return;
+  __syncthreads();
+  stage(C - 1, qt, kt, vt);
+  __syncthreads();
+  {
+    T s1[TS][TS], s2[TS][TS];
+    scores(s1, s2, false);
+#pragma unroll
+    for (int u = 0; u < TS; ++u) {
+      T l = T(0);
+#pragma unroll
+      for (int w = 0; w < TS; ++w) {
+        s1[u][w] = (s1[u][w] + T(2) * pqk[u][w]) * sc;
+        l = fma(a[u][w], s1[u][w] + psq[u][w], l);
+      }
+      l = hw_sum16(l);
+#pragma unroll
+      for (int w = 0; w < TS; ++w)
+        ST[(ty + 16 * u) * LDA + tx + 16 * w] = a[u][w] * (psq[u][w] + s1[u][w] - l);
+    }
+  }
+  __syncthreads();
+  outputs(ST, v, A, vt, o, nullptr);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) o[f] += T(2) * pav[f];
+  store(C - 1, o);
+}
+
+template <typename T, int TS, int HD>
+inline int launch_attention_cta(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
+                                const T* QKV, T* OUT, cudaStream_t st) {
+  constexpr size_t sm = attention_cta_bytes<T, TS, HD>();
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_attention_cta<T, TS, HD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    attr = true;
+  }
+  k_attention_cta<T, TS, HD><<<(unsigned)((long long)n_jobs * H), 256, sm, st>>>(
+      n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT);
+  NQS_CHECK_LAUNCH("k_attention_cta");
+  return NQS_OK;
+}
+
+template <typename T, int HD>
+inline int launch_attention_cta_ts(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
+                                   const T* QKV, T* OUT, cudaStream_t st) {
+  if (N <= 32)
+    return launch_attention_cta<T, 2, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+  if (N <= 48)
+    return launch_attention_cta<T, 3, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+  return launch_attention_cta<T, 4, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+}
+
 template <typename T>
 inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
                             const T* QKV, T* OUT, cudaStream_t st) {
@@ -918,6 +1184,12 @@ inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, in
     if (hd == 8) return launch_attention_rt<T, 8>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
     if (hd == 4)
       return launch_attention_rt<T, 4>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+  }
+  if (g_large_n_cta && N > kAttnTok && N <= 64 && C == 1 + n_tan + has_lap) {
+    if (hd == 16)
+      return launch_attention_cta_ts<T, 16>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+    if (hd == 8)
+      return launch_attention_cta_ts<T, 8>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
   }
   static bool attr = false;
   if (!attr) {

@@ -104,7 +104,7 @@ _GRAM = {"fp64": 0, "bf16": 1, "tf32": 2}
 
 
 PCG_MAX_ITERS = 24  # conjugate-gradient iterations allowed to a tensor-core Gram's solve
-PCG_TOL = 1e-3      # ... and the preconditioned-residual reduction at which it stops
+PCG_TOL = 1e-2      # ... and the preconditioned-residual reduction at which it stops
 
 
 def minsr_step(O_rows, eps, lam, gram="fp64", theta=None, lr=0.0, want_direction=True,

@@ -135,11 +135,12 @@ int nqs_profile_gemm_read(double* ms, double* bytes, long long* launches);
  * with the same TF32 products; the switch exists so that the two can be compared. */
 int nqs_set_block_fusion(int enable);
 /* Implementation selection (no reference counterpart; process-wide, default on): with it on,
- * the determinant head of more than 16 electrons runs one 256-thread CTA per job (every
- * elimination step and every tangent product spread over the CTA; up to 64 electrons, 48 with
- * the Laplacian); off, one warp per (job, determinant). Same function, same pivot rule; the
- * switch exists so that the two can be compared. */
-int nqs_set_head_lg(int enable);
+ * the kernels of more than 16 electrons run one 256-thread CTA per job (determinant head: every
+ * elimination step and tangent product spread over the CTA; up to 64 electrons, 48 with the
+ * Laplacian) and per (job, head) (attention: up to 64 tokens, head width 8 or 16); off, one
+ * warp per (job, determinant) and per (job, head). Same functions, same pivot rule; the switch
+ * exists so that the two can be compared. */
+int nqs_set_large_n_kernels(int enable);
 /* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
  * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;
  * 0 restores the default (4). A tuning knob of the multi-instance autotuner. */
@@ -288,7 +289,7 @@ int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int n_walker
                            double* out_dtheta, double* theta_io, double lr, int* info_dev,
                            double* damping_out, void* workspace, size_t workspace_bytes,
                            void* stream);
-/* The same with tol = 1e-3, max_iters = n_refine and status_dev (nullable, device int[3]) =
+/* The same with tol = 1e-2, max_iters = n_refine and status_dev (nullable, device int[3]) =
  * info_dev[0..2]. */
 int nqs_minsr_direction(void* O, int o_dtype, const double* eps, int n_walkers,
                         int64_t n_params, double lam, int gram_prec, int n_refine,
