@@ -716,6 +716,16 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
   return NQS_OK;
 }
 
+// the task-graph factorization (chol_dag.cu) where its operand layout and scratch allow, the
+// launch-per-panel one otherwise (or when switched off)
+static int cholesky_any(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
+                        int nsm, cudaStream_t st, const double* floor_p = nullptr) {
+  if (g_chol_dag && lda % 2 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 &&
+      part_elems >= cholesky_dag_scratch_elems(n))
+    return cholesky_dag(A, lda, n, bad, part, part_elems, nsm, st, floor_p);
+  return cholesky_lower(A, lda, n, bad, part, part_elems, nsm, st, floor_p);
+}
+
 // Inverses of the 64x64 diagonal blocks of a lower-triangular L: dinv[s] = L_ss^-1 (row-major
 // 64x64 per block, zero-padded past n). One CTA per block, one thread per column of the inverse
 // (forward substitution against e_j in shared memory).
@@ -1841,7 +1851,7 @@ static int minsr_direction_impl(void* O, int o_dtype, const double* eps, int W, 
     floor_p = fl;
     if (damping_out) cudaMemcpyAsync(damping_out, fl + 1, sizeof(double), cudaMemcpyDeviceToDevice, st);
   }
-  NQS_TRY(cholesky_lower(T, n, n, bad, part, part_elems, nsm, st, floor_p));
+  NQS_TRY(cholesky_any(T, n, n, bad, part, part_elems, nsm, st, floor_p));
   double* z = zpq;
   double* pp = zpq + n;
   double* q = zpq + 2 * (size_t)n;
@@ -1889,6 +1899,11 @@ int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int W, int64
   return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, max_iters, tol, out_dtheta,
                               theta_io, lr, info_dev, 5, damping_out, wsp, wsb,
                               (cudaStream_t)stream);
+}
+
+int nqs_set_cholesky_dag(int enable) {
+  g_chol_dag = enable != 0;
+  return NQS_OK;
 }
 
 int nqs_selftest_bounded_wait(const double* L, int n, int dead_block, unsigned wait_limit,
@@ -1946,7 +1961,7 @@ int nqs_gram_solve(const double* A, int M, int64_t K, double lam, const double* 
   NQS_TRY(dsyrk_lower(A, K, M, K, 1.0, 0.0, T, M, part, pe, nsm, st));
   k_add_diag<<<(M + 255) / 256, 256, 0, st>>>(T, M, M, lam);
   NQS_CHECK_LAUNCH("k_add_diag");
-  NQS_TRY(cholesky_lower(T, M, M, bad, part, pe, nsm, st));
+  NQS_TRY(cholesky_any(T, M, M, bad, part, pe, nsm, st));
   double* xb = ws.take<double>(trsv_elems(M));
   if (!xb) return NQS_ERR_WORKSPACE;
   NQS_TRY(solve_refined<double>(T, M, M, K, A, nullptr, lam, nullptr, rhs, x, r, tmpK, tmpK_lo, xb,

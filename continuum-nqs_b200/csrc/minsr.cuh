@@ -14,6 +14,13 @@ int dsyrk_lower(const double* A, int64_t lda, int M, int64_t K, double alpha, do
 size_t gram_tc_workspace(int W, int64_t P, int prec);
 int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int prec, double* T,
             Arena& ws, int nsm, cudaStream_t st, int* err);
+// float64 Cholesky of the lower triangle in place as one persistent task-graph kernel of
+// 128 x 128 tiles (chol_dag.cu); scratch: cholesky_dag_scratch_elems(n) doubles (tile counters)
+size_t cholesky_dag_scratch_elems(int n);
+int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_t scratch_elems,
+                 int nsm, cudaStream_t st, const double* floor_p);
+extern bool g_chol_dag;  // nqs_set_cholesky_dag
+
 int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, double* T, int64_t ldt,
                    int* err, cudaStream_t st);
 

@@ -84,9 +84,12 @@ def test_local_energy_n40_matches_oracle():
                                       (33, 2, "mixed")])
 def test_cta_kernels_equal_warp_kernels(N, K, prec):
     """The CTA-per-job determinant head and CTA-per-(job, head) attention (default past 16
-    electrons) against the warp-per-task kernels they replace (nqs_set_large_n_kernels(0)): log
-    psi and local energies (forward-Laplacian batch and spin-orbit flips) agree to rounding
-    (1e-10 relative in float64; the float32 network of the mixed path to 1e-4)."""
+    electrons) against the warp-per-task kernels they replace (nqs_set_large_n_kernels(0)).
+    Float64: log psi and local energies (forward-Laplacian batch and spin-orbit flips) agree to
+    1e-10 relative (the two sum in different orders). Mixed: the float32 attention's summation
+    order changes the float32 rounding, so each is compared with the float64 path: log psi to
+    1e-5 of each other, and the new kernels' median local-energy error no larger than 2 x the
+    old kernels'."""
     from nqs import _lib
     from nqs.local_energy import make_local_energy
     from nqs.psiformer import make_logpsi
@@ -94,19 +97,33 @@ def test_cta_kernels_equal_warp_kernels(N, K, prec):
                      use_jastrow=True, n_knots=6)
     p = perturb(model.init(0), 0.05, 50 + N)
     R, S = configs(model.n_elec, model.L, 37, 51 + N)
+
+    def run(prec_):
+        lp = make_logpsi(model, p, precision=prec_)
+        return lp(R, S).cpu(), make_local_energy(lp, 1.0, 0.7, 0.3)(R, S).cpu()
+
     out = {}
     for on in (1, 0):
         _lib.lib().nqs_set_large_n_kernels(on)
         try:
-            lp = make_logpsi(model, p, precision=prec)
-            out[on] = (lp(R, S).cpu(), make_local_energy(lp, 1.0, 0.7, 0.3)(R, S).cpu())
+            out[on] = run(prec)
         finally:
             _lib.lib().nqs_set_large_n_kernels(1)
-    tol = 1e-10 if prec == "fp64" else 1e-4
-    for a, b in zip(out[1], out[0]):
+
+    def rel(a, b):
         d = a - b
         d = d.real.abs() + ((d.imag + np.pi) % (2 * np.pi) - np.pi).abs()
-        assert float((d / b.abs().clamp(min=1.0)).max()) < tol, float(d.max())
+        return d / b.abs().clamp(min=1.0)
+
+    if prec == "fp64":
+        for a, b in zip(out[1], out[0]):
+            assert float(rel(a, b).max()) < 1e-10
+        return
+    assert float(rel(out[1][0], out[0][0]).max()) < 1e-5
+    e64 = run("fp64")[1]
+    err_new = float((out[1][1] - e64).abs().median())
+    err_old = float((out[0][1] - e64).abs().median())
+    assert err_new <= 2.0 * err_old + 1e-12, (err_new, err_old)
 
 
 def test_width128_network_runs_on_tensor_cores():
