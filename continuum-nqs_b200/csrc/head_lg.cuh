@@ -554,4 +554,237 @@ __global__ void __launch_bounds__(kHeadLgThreads, TS >= 3 ? 1 : 2) k_head_lg(Job
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Values only (log psi of single-channel jobs: the sampler's proposals, the flipped-spin values),
+// 16 < N <= 64: one CTA of 256 threads per job in four 64-thread groups, each factoring its own
+// determinants (k = group, group + 4, ...) with the same pivot rule as k_head_lg; a group
+// synchronises on its own named barrier, so four eliminations proceed at once. The phases live
+// in the groups' matrix buffers while the envelope is built. Thread (tid % 64) of a group owns
+// the entries of rows r = tid % 64 / 16 + 4 u and columns tx + 16 v of the trailing block.
+// ---------------------------------------------------------------------------------------------
+constexpr int kHeadValGroups = 4;
+// static shared arrays of k_head_val_lg (bytes), for the host's fit check
+constexpr size_t kHeadValStaticBytes = 8 * (2 * kHeadLgMaxN + kHeadLgThreads / 32 + 1) +
+                                       4 * (kHeadLgMaxN + 2 * kHeadValGroups * kHeadLgMaxN +
+                                            kHeadValGroups + NQS_MAX_DETS) +
+                                       16 * (2 * kHeadValGroups * kHeadLgMaxN + NQS_MAX_DETS) +
+                                       256;
+
+struct HeadValLayout {
+  int ld;
+  size_t env, G, total;
+};
+__host__ __device__ inline HeadValLayout head_val_layout(int N, int nG) {
+  HeadValLayout L;
+  L.ld = N + 1;
+  const size_t mat = round128(16 * (size_t)N * L.ld);
+  L.env = 0;
+  L.G = mat;
+  L.total = mat + kHeadValGroups * mat;
+  // the phases (nG x N complex) are staged in the group buffers before the envelope exists
+  const size_t ph = 16 * (size_t)nG * N;
+  if (ph > kHeadValGroups * mat) L.total = 0;  // does not fit: caller takes k_head_lg
+  return L;
+}
+
+__device__ __forceinline__ void group_bar(int id) {
+  asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(kHeadLgThreads, 1) k_head_val_lg(JobBatch jb, ModelConst mc,
+                                                                  const TIN* __restrict__ BF,
+                                                                  int ldbf, HeadParams hp,
+                                                                  HeadOut out, int j_out0) {
+  const int N = jb.N, C = jb.C, nG = mc.nG, K = mc.K;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int grp = tid >> 6, gt = tid & 63, gw = gt >> 5;  // group, thread in group, warp in group
+  const int job = blockIdx.x;
+  const HeadValLayout lay = head_val_layout(N, nG);
+  const int LD = lay.ld;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* env = reinterpret_cast<cplx*>(smraw + lay.env);
+  const size_t gstride = (lay.total - lay.G) / kHeadValGroups;
+  cplx* G = reinterpret_cast<cplx*>(smraw + lay.G + grp * gstride);
+  cplx* ph = reinterpret_cast<cplx*>(smraw + lay.G);  // phase 1 only
+  __shared__ double rx[kHeadLgMaxN], ry[kHeadLgMaxN], red[kHeadLgThreads / 32];
+  __shared__ int sp[kHeadLgMaxN];
+  __shared__ int used[kHeadValGroups][kHeadLgMaxN], piv[kHeadValGroups][kHeadLgMaxN];
+  __shared__ int s_p[kHeadValGroups], sing[NQS_MAX_DETS];
+  __shared__ __align__(16) cplx prow[kHeadValGroups][kHeadLgMaxN],
+      fcol[kHeadValGroups][kHeadLgMaxN];
+  __shared__ cplx s_ld[NQS_MAX_DETS];
+  __shared__ double s_jas;
+  const JobInfo ji = job_info(jb, job);
+  auto Weff = [&](int a, int g, int s) -> cplx {
+    const size_t o = ((size_t)a * nG + g) * 2 + s;
+    cplx w = mk(mc.W[2 * o], mc.W[2 * o + 1]);
+    if (mc.learnable_env) w = cadd(w, mk(hp.dW[o], hp.dW[(size_t)N * nG * 2 + o]));
+    return w;
+  };
+  // ---- phase 1 ----
+  for (int i = tid; i < N; i += kHeadLgThreads) {
+    const double* r = jb.R + ((size_t)ji.walker * N + i) * 2;
+    rx[i] = r[0];
+    ry[i] = r[1];
+    sp[i] = job_spin(jb, ji, i);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nG * N; idx += kHeadLgThreads) {
+    const int g = idx / N, i = idx - g * N;
+    double sn, cs;
+    sincos(mc.Gs[2 * g] * rx[i] + mc.Gs[2 * g + 1] * ry[i], &sn, &cs);
+    ph[idx] = mk(cs, sn);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * N; idx += kHeadLgThreads) {
+    const int a = idx / N, i = idx - a * N;
+    const int s = sp[i];
+    cplx e = mk(0, 0);
+#pragma unroll 4
+    for (int g = 0; g < nG; ++g) cfma(e, ph[g * N + i], Weff(a, g, s));
+    env[a * LD + i] = e;
+  }
+  double J = 0.0;
+  if (mc.use_jastrow) {
+    const int npair = N * (N - 1) / 2;
+    for (int p = tid; p < npair; p += kHeadLgThreads) {
+      int i = 0, rem = p;
+      while (rem >= N - 1 - i) {
+        rem -= N - 1 - i;
+        ++i;
+      }
+      const int jj = i + 1 + rem;
+      double dx, dy;
+      min_image(mc, rx[i] - rx[jj], ry[i] - ry[jj], &dx, &dy);
+      const double r = sqrt(dx * dx + dy * dy + 1e-12);
+      double u, u1, u2;
+      jastrow_u(mc, hp, r, sp[i] == sp[jj], &u, &u1, &u2);
+      J += u;
+    }
+    J = warp_sum(J);
+    if (lane == 0) red[tid >> 5] = J;
+  }
+  __syncthreads();  // env complete, phases no longer read: the group buffers are free
+  if (tid == 0) {
+    double t = 0.0;
+    if (mc.use_jastrow)
+      for (int w = 0; w < kHeadLgThreads / 32; ++w) t += red[w];
+    s_jas = t;
+  }
+  // ---- phase 2: determinants k = grp, grp + 4, ... ----
+  const int bar = 1 + grp;
+  const int ty = gt >> 4, tx = gt & 15;  // 4 x 16 threads over the trailing block
+  for (int k = grp; k < K; k += kHeadValGroups) {
+    for (int idx = gt; idx < N * N; idx += 64) {
+      const int i = idx / N, a = idx - i * N;
+      const TIN* pb = BF + (((size_t)job * N + i) * C) * ldbf;
+      const cplx b0 = mk((double)pb[k * N + a], (double)pb[K * N + k * N + a]);
+      G[a * LD + i] = cmul(env[a * LD + i], mk(1.0 + b0.re, b0.im));
+    }
+    for (int r = gt; r < N; r += 64) used[grp][r] = 0;
+    group_bar(bar);
+    cplx prod = mk(1.0, 0.0);
+    int pexp = 0, sg = 0;
+#pragma unroll 1
+    for (int c = 0; c < N; ++c) {
+      if (gw == 0) {
+        const int r0 = lane, r1 = lane + 32;
+        const bool u0 = r0 >= N || used[grp][r0], u1 = r1 >= N || used[grp][r1];
+        auto mag = [](cplx z) {
+          const double v = cabs1(z);
+          return v >= 0.0 ? v : 0.0;
+        };
+        double best = u0 ? -1.0 : mag(G[r0 * LD + c]);
+        int bi = r0;
+        if (!u1) {
+          const double v1 = mag(G[r1 * LD + c]);
+          if (v1 > best) {
+            best = v1;
+            bi = r1;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+          }
+        }
+        const int p = bi;
+        const cplx pv = G[p * LD + c];
+        const bool zero = pv.re == 0.0 && pv.im == 0.0;
+        const cplx ipv = zero ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
+        if (zero) {
+          sg = 1;
+        } else {
+          prod = cmul(prod, pv);
+          int ex;
+          frexp(fmax(fabs(prod.re), fabs(prod.im)), &ex);
+          prod = mk(ldexp(prod.re, -ex), ldexp(prod.im, -ex));
+          pexp += ex;
+        }
+        for (int j = c + 1 + lane; j < N; j += 32) prow[grp][j] = G[p * LD + j];
+        if (r0 < N) fcol[grp][r0] = (!u0 && r0 != p) ? cmul(G[r0 * LD + c], ipv) : mk(0.0, 0.0);
+        if (r1 < N) fcol[grp][r1] = (!u1 && r1 != p) ? cmul(G[r1 * LD + c], ipv) : mk(0.0, 0.0);
+        __syncwarp();
+        if (lane == 0) {
+          piv[grp][c] = p;
+          used[grp][p] = 1;
+          s_p[grp] = p;
+        }
+      }
+      group_bar(bar);
+      // rows not used yet, columns c + 1 .. N - 1
+      for (int r = ty; r < N; r += 4) {
+        const cplx f = fcol[grp][r];
+        if (f.re == 0.0 && f.im == 0.0) continue;
+        for (int j = c + 1 + tx; j < N; j += 16) G[r * LD + j] = csub(G[r * LD + j], cmul(f, prow[grp][j]));
+      }
+      group_bar(bar);
+    }
+    if (gw == 0) {
+      int inv_cnt = 0;
+      for (int c = lane; c < N; c += 32)
+        for (int c2 = c + 1; c2 < N; ++c2)
+          if (piv[grp][c] > piv[grp][c2]) ++inv_cnt;
+      inv_cnt = warp_sum(inv_cnt);
+      if (inv_cnt & 1) prod = mk(-prod.re, -prod.im);
+      if (lane == 0) {
+        s_ld[k] = sg ? mk(-INFINITY, 0.0)
+                     : mk(log(hypot(prod.re, prod.im)) + pexp * 0.6931471805599453,
+                          atan2(prod.im, prod.re));
+        sing[k] = sg;
+      }
+    }
+    group_bar(bar);  // piv / used / G of this group are rewritten by its next determinant
+  }
+  __syncthreads();
+  // ---- phase 3: log-sum-exp over determinants ----
+  if (tid != 0) return;
+  double mx = -INFINITY;
+  for (int k = 0; k < K; ++k) {
+    const double zr = s_ld[k].re + ((K > 1 && hp.det_logw) ? hp.det_logw[k] : 0.0);
+    if (!sing[k] && zr > mx) mx = zr;
+  }
+  cplx L;
+  if (K == 1) {
+    L = s_ld[0];
+  } else if (mx == -INFINITY) {
+    L = mk(-INFINITY, 0.0);
+  } else {
+    cplx ssum = mk(0, 0);
+    for (int k = 0; k < K; ++k) {
+      if (sing[k]) continue;
+      const cplx wk = (K > 1 && hp.det_logw) ? mk(hp.det_logw[k], hp.det_logw[K + k]) : mk(0, 0);
+      ssum = cadd(ssum, cexp_(mk(s_ld[k].re + wk.re - mx, s_ld[k].im + wk.im)));
+    }
+    L = mk(mx + log(hypot(ssum.re, ssum.im)), atan2(ssum.im, ssum.re));
+  }
+  if (mc.use_jastrow) L.re += s_jas;
+  if (out.L) out.L[j_out0 + job] = L;
+}
+
 }  // namespace nqs

