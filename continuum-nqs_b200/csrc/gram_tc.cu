@@ -34,23 +34,40 @@ __host__ __device__ constexpr uint32_t idesc() {
          ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
-// lower-triangular tile enumeration over 128-row x 256-col tiles: row tile ti needs col tiles
-// 0 .. floor(ti/2)
-__device__ __forceinline__ void tile_coords(int t, int* ti, int* tj) {
-  int i = 0, base = 0;
-  while (base + (i / 2 + 1) <= t) {
-    base += i / 2 + 1;
-    ++i;
+// lower-triangular tile enumeration over 128-row x 256-col tiles (row tile ti needs col tiles
+// 0 .. floor(ti/2)), grouped for L2 reuse: bands of 8 row tiles, inside a band column tile by
+// column tile. Consecutive tiles share their 256-row B panel and cycle through the band's eight
+// A panels, so the tiles of one launch round read a compact set of operand rows.
+constexpr int GRAM_BAND = 8;
+__device__ __forceinline__ void tile_coords(int t, int nrt, int* ti, int* tj) {
+  *ti = 0;
+  *tj = 0;
+  for (int g0 = 0; g0 < nrt; g0 += GRAM_BAND) {
+    const int g1 = min(nrt, g0 + GRAM_BAND);
+    int cnt = 0;
+    for (int i = g0; i < g1; ++i) cnt += i / 2 + 1;
+    if (t >= cnt) {
+      t -= cnt;
+      continue;
+    }
+    for (int j = 0; 2 * j < g1; ++j) {
+      const int lo = max(g0, 2 * j), c = g1 - lo;  // row tiles ti >= 2 j of the band
+      if (t < c) {
+        *ti = lo + t;
+        *tj = j;
+        return;
+      }
+      t -= c;
+    }
+    return;
   }
-  *ti = i;
-  *tj = t - base;
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUtensorMap tmap,
                                                     int M, int64_t K, double* __restrict__ T,
                                                     int64_t ldt, int* __restrict__ err,
-                                                    uint32_t wait_limit) {
+                                                    uint32_t wait_limit, int t0) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~(uintptr_t)1023);
@@ -64,7 +81,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ti, tj;
-  tile_coords(blockIdx.x, &ti, &tj);
+  tile_coords(t0 + (int)blockIdx.x, (M + BM - 1) / BM, &ti, &tj);
   const int i0 = ti * BM, j0 = tj * BN;
   constexpr int KE = (KIND == 0) ? 64 : 32;  // elements per 128-byte row
   const int nk = (int)((K + KE - 1) / KE);
@@ -289,18 +306,28 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
   for (int i = 0; i < nrt; ++i) tiles += i / 2 + 1;
   // every column tile must start inside the matrix: col tile tj <= floor(ti/2) => j0 <= i0
   if (g_prof_start) cudaEventRecord(g_prof_start, st);
-  if (prec == 1) {
+  // one launch per round of one tile per SM: the CTAs of a round start together and stream K
+  // in step, so the operand rows they share are read from DRAM about once per round
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(tc::k_gram_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
-    tc::k_gram_tc<0><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err,
-                                                         wait_limit_or(tc::WAIT_LIMIT));
-  } else {
     cudaFuncSetAttribute(tc::k_gram_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
-    tc::k_gram_tc<1><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err,
-                                                         wait_limit_or(tc::WAIT_LIMIT));
   }
-  NQS_CHECK_LAUNCH("k_gram_tc");
+  const int per = std::max(nsm, 1);
+  const uint32_t wl = wait_limit_or(tc::WAIT_LIMIT);
+  for (int t0 = 0; t0 < tiles; t0 += per) {
+    const int nt = std::min(per, tiles - t0);
+    if (prec == 1)
+      tc::k_gram_tc<0><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+    else
+      tc::k_gram_tc<1><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+    NQS_CHECK_LAUNCH("k_gram_tc");
+  }
   if (g_prof_stop) cudaEventRecord(g_prof_stop, st);
   return NQS_OK;
 }
