@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
 
 }  // namespace
 
-bool g_chol_dag = true;
+bool g_chol_dag = false;
 
 size_t cholesky_dag_scratch_elems(int n) {
   const size_t T = (size_t)(n + TB - 1) / TB;

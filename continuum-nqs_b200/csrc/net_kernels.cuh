@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256) k_layernorm(int n_tok, int C, int n_tan, 
   const T rho3 = rho * rho * rho;
   // tangent rows TP at a time: their loads are in flight before the first reduction (the narrow
   // instantiations, Q <= 2, keep the registers for this without losing occupancy)
-  constexpr int TP = Q <= 2 ? 8 : 1;
+  constexpr int TP = Q <= 2 ? 4 : 1;
   for (int t0 = 0; t0 < n_tan; t0 += TP) {
     T dus[TP][Q];
 #pragma unroll
@@ -1294,28 +1294,8 @@ __global__ void __launch_bounds__(256) k_gelu(size_t n_tok, int C, int n_tan, in
   const T w2 = c * T(6) * b3 * xv;
   const T g1 = cdf + T(0.5) * xv * sech2 * w1;
   const T g2 = sech2 * (w1 - xv * th * w1 * w1 + T(0.5) * xv * w2);
-  if (n_tan <= 32) {
-    // one pass: the tangents stay in registers between the sum of squares and the rescale
-    T v[32];
-#pragma unroll
-    for (int t = 0; t < 32; ++t)
-      if (t < n_tan) v[t] = x[(size_t)(1 + t) * D];
-    T a4[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int t = 0; t < 32; ++t)
-      if (t < n_tan) a4[t & 3] += v[t] * v[t];
-    x[0] = gelu_value(xv, th);
-#pragma unroll
-    for (int t = 0; t < 32; ++t)
-      if (t < n_tan) x[(size_t)(1 + t) * D] = g1 * v[t];
-    if (has_lap) {
-      T* p = x + (size_t)(C - 1) * D;
-      *p = g1 * (*p) + g2 * ((a4[0] + a4[1]) + (a4[2] + a4[3]));
-    }
-    return;
-  }
   // pass 1: independent loads of the tangents (sum of squares for the Laplacian); pass 2 rescales
-  // them in place
+  // them in place (the second reads hit L1)
   T acc = 0;
   if (has_lap) {
     T a4[4] = {0, 0, 0, 0};

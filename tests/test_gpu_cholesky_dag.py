@@ -1,6 +1,6 @@
-"""The task-graph float64 Cholesky (one persistent kernel over 128 x 128 tiles) against the
-launch-per-panel factorization it replaces and against a CPU float64 solve, inside the MinSR
-sample-space solve (reference src/nqs/minsr.py:76-81) and the explicit Gram solve (:84-88):
+"""The task-graph float64 Cholesky (one persistent kernel over 128 x 128 tiles; off by default,
+nqs_set_cholesky_dag) against the launch-per-panel factorization and a CPU float64 solve,
+inside the MinSR sample-space solve (reference src/nqs/minsr.py:76-81) and the explicit Gram solve (:84-88):
 sizes that are one tile, several tiles with a partial last tile, and the benchmark's 8192."""
 import numpy as np
 import pytest
@@ -26,7 +26,7 @@ def _dir(O, eps, lam, gram, dag, **kw):
         rows = O.cuda().to(torch.float64 if gram == "fp64" else torch.float32).contiguous()
         return minsr_step(rows.clone(), eps, lam, gram, **kw).cpu()
     finally:
-        _lib.lib().nqs_set_cholesky_dag(1)
+        _lib.lib().nqs_set_cholesky_dag(0)
 
 
 def _cpu_direction(O, eps, lam):
@@ -82,12 +82,12 @@ def test_dag_cholesky_gram_solve():
     for M, K in ((130, 300), (256, 900)):
         A = torch.as_tensor(rng.standard_normal((M, K)))
         rhs = torch.as_tensor(rng.standard_normal(M))
-        x = gram_solve(A.cuda(), rhs, 1e-2).cpu()
-        _lib.lib().nqs_set_cholesky_dag(0)
+        _lib.lib().nqs_set_cholesky_dag(1)
         try:
-            y = gram_solve(A.cuda(), rhs, 1e-2).cpu()
+            x = gram_solve(A.cuda(), rhs, 1e-2).cpu()
         finally:
-            _lib.lib().nqs_set_cholesky_dag(1)
+            _lib.lib().nqs_set_cholesky_dag(0)
+        y = gram_solve(A.cuda(), rhs, 1e-2).cpu()
         ref = torch.linalg.solve(A @ A.T + 1e-2 * torch.eye(M, dtype=torch.float64), rhs)
         assert float((x - ref).norm() / ref.norm()) < 1e-10
         assert float((x - y).norm() / y.norm()) < 1e-10
