@@ -8,15 +8,20 @@
 //                    their 128 columns in registers, L_kk in shared memory)
 //   UPDATE(i, j, k): A_ij -= L_ik L_jk^T, k < j <= i (128 x 128 x 128 tile product, 8 x 8 per
 //                    thread, operands staged by cp.async in a 3-stage ring)
-// dealt in one fixed topological order by an atomic ticket, with one step of look-ahead:
-//   POTRF(0), TRSM(i, 0); for k = 0 .. T-2: UPDATE(i, k+1, k) [column k+1], POTRF(k+1),
-//   TRSM(i, k+1), then UPDATE(i, j, k) for j >= k+2 [the rest of step k].
-// Tile (i, j) carries a counter of the operations applied to it (updates k = 0 .. j-1, then its
-// POTRF or TRSM). A task's thread 0 waits with acquire loads for the counters it depends on;
-// after the task (and a barrier) it publishes the tile's counter with a release store. A task
-// waits only for tasks dealt before it, and every dealt task is held by a running CTA, so the
-// graph drains. Every wait is bounded: a CTA that runs out of its limit sets the abort word
-// (every CTA then leaves), the failure flag bad[0] and a NaN in L[0][0].
+// Two queues, each consumed in order:
+//   critical: POTRF(0), TRSM(i, 0); for k = 0 .. T-2: UPDATE(i, k+1, k) [column k+1],
+//             POTRF(k+1), TRSM(i, k+1)                         -- the factorization's spine
+//   bulk:     UPDATE(i, j, k), j >= k+2, by k, then column j, then row i
+// A CTA (its thread 0) takes the head of the critical queue when that task's inputs are complete,
+// otherwise the head of the bulk queue once the two panel solves it reads have been taken, so the
+// spine runs as soon as it can and the bulk fills the SMs around it. Tile (i, j) carries a counter
+// of the operations applied to it (updates k = 0 .. j-1, then its POTRF or TRSM): a critical task
+// is taken only when its counters are reached (acquire loads), a bulk task waits (bounded) for
+// counters of tasks already taken; a finished task publishes its tile's counter with a release
+// store after a barrier. Every task a CTA waits for is held by a running CTA whose own inputs are
+// complete or in flight, so the graph drains. Every wait and every idle spin is bounded: a CTA
+// that runs out of its limit sets the abort word (every CTA then leaves), the failure flag bad[0]
+// and a NaN in L[0][0].
 // Pivots below *floor_p are raised to it (counted in bad[2]); a non-positive pivot sets bad[0].
 #include <cstdio>
 #include <algorithm>
@@ -38,29 +43,43 @@ struct DagTask {
   int type, k, i, j;  // type 0 POTRF, 1 TRSM, 2 UPDATE; -1 none
 };
 
-__host__ __device__ inline long long dag_ntasks(int T) {
-  long long c = T;
-  for (int k = 0; k + 1 < T; ++k)
-    c += 2LL * (T - 1 - k) + (long long)(T - k - 2) * (T - k - 1) / 2;
+__host__ __device__ inline int dag_ncrit(int T) { return T * T; }
+__host__ __device__ inline int dag_nbulk(int T) {
+  int c = 0;
+  for (int k = 0; k + 2 < T; ++k) c += (T - k - 2) * (T - k - 1) / 2;
   return c;
 }
 
-__device__ DagTask dag_task(int T, long long id) {
-  if (id < T) return id == 0 ? DagTask{0, 0, 0, 0} : DagTask{1, 0, (int)id, 0};
+__device__ DagTask dag_crit_task(int T, int id) {
+  if (id < T) return id == 0 ? DagTask{0, 0, 0, 0} : DagTask{1, 0, id, 0};
   id -= T;
   for (int k = 0; k + 1 < T; ++k) {
-    const long long a = T - 1 - k;
-    if (id < a) return DagTask{2, k, k + 1 + (int)id, k + 1};
+    const int a = T - 1 - k;
+    if (id < a) return DagTask{2, k, k + 1 + id, k + 1};
     id -= a;
-    if (id < a)
-      return id == 0 ? DagTask{0, k + 1, k + 1, k + 1} : DagTask{1, k + 1, k + 1 + (int)id, k + 1};
-    id -= a;
+    if (id == 0) return DagTask{0, k + 1, k + 1, k + 1};
+    id -= 1;
+    if (id < a - 1) return DagTask{1, k + 1, k + 2 + id, k + 1};
+    id -= a - 1;
+  }
+  return DagTask{-1, 0, 0, 0};
+}
+
+// position of TRSM(i, k) in the critical queue
+__device__ int dag_trsm_index(int T, int i, int k) {
+  if (k == 0) return i;
+  int idx = T;
+  for (int m = 0; m + 1 < k; ++m) idx += 2 * (T - 1 - m);
+  return idx + (T - k) + 1 + (i - k - 1);
+}
+
+__device__ DagTask dag_bulk_task(int T, int id) {
+  for (int k = 0; k + 2 < T; ++k)
     for (int j = k + 2; j < T; ++j) {
-      const long long c = T - j;
-      if (id < c) return DagTask{2, k, j + (int)id, j};
+      const int c = T - j;
+      if (id < c) return DagTask{2, k, j + id, j};
       id -= c;
     }
-  }
   return DagTask{-1, 0, 0, 0};
 }
 
@@ -81,6 +100,17 @@ __device__ int dag_wait(const int* p, int target, const int* abort_w, uint32_t l
     if (w > 32) __nanosleep(w > 4096 ? 256 : 64);
   }
   return 0;
+}
+
+// inputs of a task complete (acquire loads, no waiting)
+__device__ bool dag_ready(const int* state, int T, DagTask t) {
+  if (t.type == 0) return dag_ld_acquire(state + t.k * T + t.k) >= t.k;
+  if (t.type == 1)
+    return dag_ld_acquire(state + t.k * T + t.k) >= t.k + 1 &&
+           dag_ld_acquire(state + t.i * T + t.k) >= t.k;
+  return dag_ld_acquire(state + t.i * T + t.j) >= t.k &&
+         dag_ld_acquire(state + t.i * T + t.k) >= t.k + 1 &&
+         dag_ld_acquire(state + t.j * T + t.k) >= t.k + 1;
 }
 
 __device__ __forceinline__ void cp16_zfill(void* smem, const void* gmem, int n_src) {
@@ -301,43 +331,84 @@ __device__ void dag_update(double* C, const double* X, const double* Y, int64_t 
 
 __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int64_t lda, int n,
                                                      int T, int* __restrict__ state,
-                                                     unsigned long long* __restrict__ ticket,
+                                                     int* __restrict__ tickets,
                                                      int* __restrict__ abort_w,
                                                      int* __restrict__ bad,
                                                      const double* __restrict__ floor_p,
-                                                     uint32_t wait_limit, long long ntasks) {
+                                                     uint32_t wait_limit) {
   extern __shared__ __align__(16) double dsm[];
-  __shared__ long long s_id;
-  __shared__ int s_st;
+  __shared__ int s_task[5];  // type, k, i, j, stop
   __shared__ double dval[TB], dinv[TB];
   const int tid = threadIdx.x;
+  const int n_crit = dag_ncrit(T), n_bulk = dag_nbulk(T);
+  int* crit = tickets;
+  int* bulk = tickets + 1;
   for (;;) {
-    if (tid == 0) s_id = (long long)atomicAdd(ticket, 1ULL);
-    __syncthreads();
-    const long long id = s_id;
-    if (id >= ntasks) break;
-    const DagTask t = dag_task(T, id);
     if (tid == 0) {
-      int st = 0;
-      if (t.type == 0) {
-        st = dag_wait(state + t.k * T + t.k, t.k, abort_w, wait_limit);
-      } else if (t.type == 1) {
-        st = dag_wait(state + t.k * T + t.k, t.k + 1, abort_w, wait_limit);
-        if (!st) st = dag_wait(state + t.i * T + t.k, t.k, abort_w, wait_limit);
-      } else {
-        st = dag_wait(state + t.i * T + t.j, t.k, abort_w, wait_limit);
-        if (!st) st = dag_wait(state + t.i * T + t.k, t.k + 1, abort_w, wait_limit);
-        if (!st) st = dag_wait(state + t.j * T + t.k, t.k + 1, abort_w, wait_limit);
+      DagTask pick{-1, 0, 0, 0};
+      int stop = 0;
+      uint32_t idle = 0;
+      for (;;) {
+        if (dag_ld_acquire(abort_w) != 0) {
+          stop = 1;
+          break;
+        }
+        const int c = dag_ld_acquire(crit), b = dag_ld_acquire(bulk);
+        if (c >= n_crit && b >= n_bulk) {
+          stop = 1;
+          break;
+        }
+        if (c < n_crit) {
+          const DagTask t = dag_crit_task(T, c);
+          if (dag_ready(state, T, t)) {
+            if (atomicCAS(crit, c, c + 1) == c) {
+              pick = t;
+              break;
+            }
+            continue;
+          }
+        }
+        if (b < n_bulk) {
+          const DagTask t = dag_bulk_task(T, b);
+          if (c > dag_trsm_index(T, t.i, t.k)) {  // both panel solves it reads are taken
+            if (atomicCAS(bulk, b, b + 1) == b) {
+              const int st =
+                  dag_wait(state + t.i * T + t.j, t.k, abort_w, wait_limit) ? 1
+                  : dag_wait(state + t.i * T + t.k, t.k + 1, abort_w, wait_limit) ? 1
+                  : dag_wait(state + t.j * T + t.k, t.k + 1, abort_w, wait_limit);
+              if (st) {
+                if (dag_ld_acquire(abort_w) == 0) {  // this CTA's own limit ran out
+                  atomicExch(abort_w, 1);
+                  atomicExch(bad, 1);
+                  A[0] = __longlong_as_double(0x7ff8000000000000ll);
+                }
+                stop = 1;
+              } else {
+                pick = t;
+              }
+              break;
+            }
+            continue;
+          }
+        }
+        if (++idle >= wait_limit) {  // nothing admissible for too long
+          atomicExch(abort_w, 1);
+          atomicExch(bad, 1);
+          A[0] = __longlong_as_double(0x7ff8000000000000ll);
+          stop = 1;
+          break;
+        }
+        if (idle > 32) __nanosleep(idle > 4096 ? 256 : 64);
       }
-      if (st == 1) {  // this CTA's limit ran out: stop everyone, flag and poison the factor
-        atomicExch(abort_w, 1);
-        atomicExch(bad, 1);
-        A[0] = __longlong_as_double(0x7ff8000000000000ll);
-      }
-      s_st = st;
+      s_task[0] = pick.type;
+      s_task[1] = pick.k;
+      s_task[2] = pick.i;
+      s_task[3] = pick.j;
+      s_task[4] = stop;
     }
     __syncthreads();
-    if (s_st) break;
+    if (s_task[4]) break;
+    const DagTask t{s_task[0], s_task[1], s_task[2], s_task[3]};
     int tile;
     if (t.type == 0) {
       dag_potrf(A, lda, t.k * TB, min(TB, n - t.k * TB), dsm, dval, dinv, bad, floor_p);
@@ -366,7 +437,7 @@ bool g_chol_dag = false;
 
 size_t cholesky_dag_scratch_elems(int n) {
   const size_t T = (size_t)(n + TB - 1) / TB;
-  return 2 + (T * T + 1) / 2;  // ticket, abort word + pad, T^2 tile counters (in doubles)
+  return 2 + (T * T + 1) / 2;  // two queue tickets, abort word + pad, T^2 tile counters (doubles)
 }
 
 int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_t scratch_elems,
@@ -382,7 +453,7 @@ int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_
               cholesky_dag_scratch_elems(n));
     return NQS_ERR_WORKSPACE;
   }
-  unsigned long long* ticket = reinterpret_cast<unsigned long long*>(scratch);
+  int* tickets = reinterpret_cast<int*>(scratch);  // [0] critical, [1] bulk
   int* abort_w = reinterpret_cast<int*>(scratch + 1);
   int* state = reinterpret_cast<int*>(scratch + 2);
   cudaMemsetAsync(scratch, 0, sizeof(double) * cholesky_dag_scratch_elems(n), st);
@@ -391,14 +462,14 @@ int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_
     cudaFuncSetAttribute(k_chol_dag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDagSmem);
     attr = true;
   }
-  const long long ntasks = dag_ntasks(T);
-  int grid = (int)std::min<long long>(std::max(nsm, 1), ntasks);
+  const int ntasks = dag_ncrit(T) + dag_nbulk(T);
+  int grid = std::min(std::max(nsm, 1), ntasks);
   uint32_t wl = wait_limit_or(kDagWaitLimit);
   int nn = n;
   int TT = T;
-  void* args[] = {(void*)&A,    (void*)&lda,     (void*)&nn,  (void*)&TT,
-                  (void*)&state, (void*)&ticket, (void*)&abort_w, (void*)&bad,
-                  (void*)&floor_p, (void*)&wl,   (void*)&ntasks};
+  void* args[] = {(void*)&A,      (void*)&lda,     (void*)&nn,  (void*)&TT,
+                  (void*)&state,  (void*)&tickets, (void*)&abort_w, (void*)&bad,
+                  (void*)&floor_p, (void*)&wl};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_chol_dag, grid, 256, args,
                                                     kDagSmem, st);
   if (e != cudaSuccess) return cuda_status(e, "k_chol_dag");

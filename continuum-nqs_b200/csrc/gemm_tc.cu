@@ -434,29 +434,58 @@ static int rowgemm_tc_piece(const float* X, int ldx, int rows, int K, const floa
   return NQS_OK;
 }
 
+// pipeline stages that fit one launch of K-piece kp and N-piece np (0: does not fit)
+static int rowgemm_stages_for(int kp, int np, bool bf) {
+  const size_t panel = bf ? (size_t)(kp / 64) * np * 128 : (size_t)(kp / tc::RG_KB) * np * 128;
+  const size_t conv = bf ? (size_t)(kp / 64) * tc::RG_BM * 128 : 0;
+  const size_t fixed = panel + conv + 4 * 2 * 4096 + 256 + 1024;
+  const size_t stage = (size_t)(kp / tc::RG_KB) * tc::RG_BM * 128;
+  const size_t cap = bf ? 227 * 1024 : 200 * 1024;
+  if (fixed + 2 * stage > cap) return 0;
+  return (int)std::min<size_t>((size_t)g_rowgemm_stages.load(), (cap - fixed) / stage);
+}
+
 // Any K (a multiple of 32) and any output width: pieces of at most 128 K-columns and 256 output
-// columns, one launch each. The first K piece of an output slice stores (with the bias) or, when
-// a residual is given, adds into Y; later K pieces add their partial products into Y with the
-// bulk reduction. The fused activation needs a single K piece.
+// columns, one launch each, chosen among the splits that leave room for at least two pipeline
+// stages by their HBM traffic (X is read once per N piece; Y is stored once and read + written
+// again by every further K piece). The first K piece of an output slice stores (with the bias)
+// or, when a residual is given, adds into Y; later K pieces add their partial products into Y
+// with the bulk reduction. The fused activation needs a single K piece.
 int rowgemm_tc(const float* X, int ldx, int rows, int K, const float* WT, int Npad, int Nout,
                const float* bias, int C, const float* Res, int ldr, float* Y, int ldy, int* err,
                cudaStream_t st, int act, const uint16_t* WT16) {
-  constexpr int kMaxK = 128, kMaxN = 256;
-  if (K <= kMaxK && Npad <= kMaxN)
+  const bool bf_all = WT16 != nullptr && K % 64 == 0;
+  if (K <= 128 && Npad <= 256 && rowgemm_stages_for(K, Npad, bf_all) >= 2)
     return rowgemm_tc_piece(X, ldx, rows, K, WT, K, Npad, Nout, bias, C, Res, ldr, Y, ldy, err,
                             st, act, WT16);
-  if (act && K > kMaxK) {
-    set_error("rowgemm_tc: the fused activation needs K <= %d", kMaxK);
-    return NQS_ERR_INVALID_ARG;
-  }
   if (Res && (Res != Y || ldr != ldy)) {
     set_error("rowgemm_tc: the residual must be the output itself (in-place Y += X W)");
     return NQS_ERR_INVALID_ARG;
   }
-  for (int n0 = 0; n0 < Npad && n0 < Nout; n0 += kMaxN) {
-    const int np = std::min(kMaxN, Npad - n0), no = std::min(np, Nout - n0);
-    for (int k0 = 0; k0 < K; k0 += kMaxK) {
-      const int kp = std::min(kMaxK, K - k0);
+  int best_k = 0, best_n = 0;
+  double best = 0.0;
+  for (int kp = 128; kp >= tc::RG_KB; kp -= tc::RG_KB) {
+    if (act && kp < K) continue;
+    for (int np = 256; np >= 16; np -= 16) {
+      const bool bf = WT16 != nullptr && kp % 64 == 0;
+      if (rowgemm_stages_for(kp, np, bf) < 2) continue;
+      const int nk = (K + kp - 1) / kp, nn = (Npad + np - 1) / np;
+      const double t = (double)K * nn + (double)Nout * (2 * nk - 1) + 1e-3 * nk * nn;
+      if (!best_k || t < best) {
+        best = t;
+        best_k = kp;
+        best_n = np;
+      }
+    }
+  }
+  if (!best_k) {
+    set_error("rowgemm_tc: no piece of K=%d, N=%d fits shared memory", K, Npad);
+    return NQS_ERR_UNSUPPORTED;
+  }
+  for (int n0 = 0; n0 < Npad && n0 < Nout; n0 += best_n) {
+    const int np = std::min(best_n, Npad - n0), no = std::min(np, Nout - n0);
+    for (int k0 = 0; k0 < K; k0 += best_k) {
+      const int kp = std::min(best_k, K - k0);
       const bool first = k0 == 0;
       const float* res = (Res || !first) ? Y + n0 : nullptr;
       NQS_TRY(rowgemm_tc_piece(X + k0, ldx, rows, kp, WT + (size_t)n0 * K + k0, K, np, no,
