@@ -44,43 +44,53 @@ struct DagTask {
 };
 
 __host__ __device__ inline int dag_ncrit(int T) { return T * T; }
-__host__ __device__ inline int dag_nbulk(int T) {
-  int c = 0;
-  for (int k = 0; k + 2 < T; ++k) c += (T - k - 2) * (T - k - 1) / 2;
-  return c;
-}
+__host__ __device__ inline long long dag_c3(long long x) { return x >= 3 ? x * (x - 1) * (x - 2) / 6 : 0; }
+__host__ __device__ inline int dag_nbulk(int T) { return (int)dag_c3(T); }  // sum_k C(T-k-1, 2)
 
-__device__ DagTask dag_crit_task(int T, int id) {
-  if (id < T) return id == 0 ? DagTask{0, 0, 0, 0} : DagTask{1, 0, id, 0};
-  id -= T;
-  for (int k = 0; k + 1 < T; ++k) {
-    const int a = T - 1 - k;
-    if (id < a) return DagTask{2, k, k + 1 + id, k + 1};
-    id -= a;
-    if (id == 0) return DagTask{0, k + 1, k + 1, k + 1};
-    id -= 1;
-    if (id < a - 1) return DagTask{1, k + 1, k + 2 + id, k + 1};
-    id -= a - 1;
-  }
-  return DagTask{-1, 0, 0, 0};
-}
-
+// critical queue: position of the first task of step k's block (k >= 0), after the T tasks
+// POTRF(0), TRSM(i, 0)
+__device__ __forceinline__ int dag_crit_base(int T, int k) { return T + 2 * k * (T - 1) - k * (k - 1); }
 // position of TRSM(i, k) in the critical queue
-__device__ int dag_trsm_index(int T, int i, int k) {
-  if (k == 0) return i;
-  int idx = T;
-  for (int m = 0; m + 1 < k; ++m) idx += 2 * (T - 1 - m);
-  return idx + (T - k) + 1 + (i - k - 1);
+__device__ __forceinline__ int dag_trsm_index(int T, int i, int k) {
+  return k == 0 ? i : dag_crit_base(T, k - 1) + (T - k) + 1 + (i - k - 1);
 }
 
-__device__ DagTask dag_bulk_task(int T, int id) {
-  for (int k = 0; k + 2 < T; ++k)
-    for (int j = k + 2; j < T; ++j) {
-      const int c = T - j;
-      if (id < c) return DagTask{2, k, j + id, j};
-      id -= c;
+// The two task lists, written once per factorization: critical entries (type, k, i, j); bulk
+// entries UPDATE(i, j, k) as (k, i, j, position of TRSM(i, k) in the critical queue).
+__global__ void k_dag_lists(int T, int4* __restrict__ crit, int4* __restrict__ bulk) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nc = (long long)T * T;
+  if (gid < nc) {
+    const int c = (int)gid;
+    int4 e = make_int4(-1, 0, 0, 0);
+    if (c < T) {
+      e = c == 0 ? make_int4(0, 0, 0, 0) : make_int4(1, 0, c, 0);
+    } else {
+      for (int k = 0; k + 1 < T; ++k) {
+        const int b0 = dag_crit_base(T, k), a = T - 1 - k;
+        if (c < b0 + 2 * a) {
+          const int o = c - b0;
+          if (o < a)
+            e = make_int4(2, k, k + 1 + o, k + 1);
+          else if (o == a)
+            e = make_int4(0, k + 1, k + 1, k + 1);
+          else
+            e = make_int4(1, k + 1, k + 2 + (o - a - 1), k + 1);
+          break;
+        }
+      }
     }
-  return DagTask{-1, 0, 0, 0};
+    crit[c] = e;
+    return;
+  }
+  // bulk: one thread per (k, j, i) with k + 2 <= j <= i < T
+  const long long t = gid - nc;
+  if (t >= (long long)T * T * T) return;
+  const int k = (int)(t / ((long long)T * T)), j = (int)((t / T) % T), i = (int)(t % T);
+  if (!(k + 2 <= j && j <= i)) return;
+  const long long offk = dag_c3(T) - dag_c3(T - k);
+  const long long offj = (long long)(j - k - 2) * T - ((long long)(j - 1) * j / 2 - (long long)(k + 1) * (k + 2) / 2);
+  bulk[offk + offj + (i - j)] = make_int4(k, i, j, dag_trsm_index(T, i, k));
 }
 
 __device__ __forceinline__ int dag_ld_acquire(const int* p) {
@@ -334,6 +344,8 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
                                                      int* __restrict__ tickets,
                                                      int* __restrict__ abort_w,
                                                      int* __restrict__ bad,
+                                                     const int4* __restrict__ crit_list,
+                                                     const int4* __restrict__ bulk_list,
                                                      const double* __restrict__ floor_p,
                                                      uint32_t wait_limit) {
   extern __shared__ __align__(16) double dsm[];
@@ -343,6 +355,12 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
   const int n_crit = dag_ncrit(T), n_bulk = dag_nbulk(T);
   int* crit = tickets;
   int* bulk = tickets + 1;
+  int pending = -1;  // (thread 0) a bulk task dealt to this CTA, not yet admitted
+  auto fail = [&]() {
+    atomicExch(abort_w, 1);
+    atomicExch(bad, 1);
+    A[0] = __longlong_as_double(0x7ff8000000000000ll);
+  };
   for (;;) {
     if (tid == 0) {
       DagTask pick{-1, 0, 0, 0};
@@ -353,13 +371,10 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
           stop = 1;
           break;
         }
-        const int c = dag_ld_acquire(crit), b = dag_ld_acquire(bulk);
-        if (c >= n_crit && b >= n_bulk) {
-          stop = 1;
-          break;
-        }
-        if (c < n_crit) {
-          const DagTask t = dag_crit_task(T, c);
+        const int c = dag_ld_acquire(crit);
+        if (c < n_crit) {  // the spine first, whenever its head is ready
+          const int4 e = __ldcg(crit_list + c);
+          const DagTask t{e.x, e.y, e.z, e.w};
           if (dag_ready(state, T, t)) {
             if (atomicCAS(crit, c, c + 1) == c) {
               pick = t;
@@ -368,33 +383,37 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
             continue;
           }
         }
-        if (b < n_bulk) {
-          const DagTask t = dag_bulk_task(T, b);
-          if (c > dag_trsm_index(T, t.i, t.k)) {  // both panel solves it reads are taken
-            if (atomicCAS(bulk, b, b + 1) == b) {
-              const int st =
-                  dag_wait(state + t.i * T + t.j, t.k, abort_w, wait_limit) ? 1
-                  : dag_wait(state + t.i * T + t.k, t.k + 1, abort_w, wait_limit) ? 1
-                  : dag_wait(state + t.j * T + t.k, t.k + 1, abort_w, wait_limit);
-              if (st) {
-                if (dag_ld_acquire(abort_w) == 0) {  // this CTA's own limit ran out
-                  atomicExch(abort_w, 1);
-                  atomicExch(bad, 1);
-                  A[0] = __longlong_as_double(0x7ff8000000000000ll);
-                }
-                stop = 1;
-              } else {
-                pick = t;
-              }
-              break;
+        if (pending >= 0) {
+          const int4 e = __ldcg(bulk_list + pending);
+          if (c > e.w) {  // both panel solves it reads are taken: its inputs are in flight
+            const DagTask t{2, e.x, e.y, e.z};
+            pending = -1;
+            int st = dag_wait(state + t.i * T + t.j, t.k, abort_w, wait_limit);
+            if (!st) st = dag_wait(state + t.i * T + t.k, t.k + 1, abort_w, wait_limit);
+            if (!st) st = dag_wait(state + t.j * T + t.k, t.k + 1, abort_w, wait_limit);
+            if (st) {
+              if (st == 1) fail();
+              stop = 1;
+            } else {
+              pick = t;
             }
-            continue;
+            break;
+          }
+        } else {
+          const int b = dag_ld_acquire(bulk);
+          if (b < n_bulk) {
+            if (c > __ldcg(bulk_list + b).w) {
+              const int b2 = atomicAdd(bulk, 1);
+              if (b2 < n_bulk) pending = b2;
+              continue;
+            }
+          } else if (c >= n_crit) {
+            stop = 1;
+            break;
           }
         }
         if (++idle >= wait_limit) {  // nothing admissible for too long
-          atomicExch(abort_w, 1);
-          atomicExch(bad, 1);
-          A[0] = __longlong_as_double(0x7ff8000000000000ll);
+          fail();
           stop = 1;
           break;
         }
@@ -435,9 +454,11 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
 
 bool g_chol_dag = false;
 
+// doubles: two queue tickets, abort word + pad, T^2 tile counters, the two task lists (int4)
+static size_t dag_counters_elems(size_t T) { return 2 + (T * T + 1) / 2; }
 size_t cholesky_dag_scratch_elems(int n) {
   const size_t T = (size_t)(n + TB - 1) / TB;
-  return 2 + (T * T + 1) / 2;  // two queue tickets, abort word + pad, T^2 tile counters (doubles)
+  return dag_counters_elems(T) + 2 * (T * T + (size_t)dag_nbulk((int)T));
 }
 
 int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_t scratch_elems,
@@ -456,7 +477,14 @@ int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_
   int* tickets = reinterpret_cast<int*>(scratch);  // [0] critical, [1] bulk
   int* abort_w = reinterpret_cast<int*>(scratch + 1);
   int* state = reinterpret_cast<int*>(scratch + 2);
-  cudaMemsetAsync(scratch, 0, sizeof(double) * cholesky_dag_scratch_elems(n), st);
+  int4* crit_list = reinterpret_cast<int4*>(scratch + dag_counters_elems(T));
+  int4* bulk_list = crit_list + (size_t)T * T;
+  cudaMemsetAsync(scratch, 0, sizeof(double) * dag_counters_elems(T), st);
+  {
+    const long long nthreads = (long long)T * T + (long long)T * T * T;
+    k_dag_lists<<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(T, crit_list, bulk_list);
+    NQS_CHECK_LAUNCH("k_dag_lists");
+  }
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_chol_dag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDagSmem);
@@ -467,9 +495,11 @@ int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_
   uint32_t wl = wait_limit_or(kDagWaitLimit);
   int nn = n;
   int TT = T;
-  void* args[] = {(void*)&A,      (void*)&lda,     (void*)&nn,  (void*)&TT,
-                  (void*)&state,  (void*)&tickets, (void*)&abort_w, (void*)&bad,
-                  (void*)&floor_p, (void*)&wl};
+  const int4* cl = crit_list;
+  const int4* bl = bulk_list;
+  void* args[] = {(void*)&A,       (void*)&lda,     (void*)&nn,      (void*)&TT,
+                  (void*)&state,   (void*)&tickets, (void*)&abort_w, (void*)&bad,
+                  (void*)&cl,      (void*)&bl,      (void*)&floor_p, (void*)&wl};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_chol_dag, grid, 256, args,
                                                     kDagSmem, st);
   if (e != cudaSuccess) return cuda_status(e, "k_chol_dag");

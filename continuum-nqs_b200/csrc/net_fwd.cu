@@ -198,9 +198,15 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
       }
       if (!fuse_act) {
         const size_t nel = (size_t)ntok * D;
-        k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)ntok, C, cb.n_tan,
-                                                                 cb.has_lap, D, Big);
-        NQS_CHECK_LAUNCH("k_gelu");
+        if (sizeof(T) == 4 && D % 4 == 0 && ((uintptr_t)Big % 16) == 0) {
+          k_gelu4<<<(unsigned)((nel / 4 + 255) / 256), 256, 0, st>>>(
+              (size_t)ntok, C, cb.n_tan, cb.has_lap, D, (float*)Big);
+          NQS_CHECK_LAUNCH("k_gelu4");
+        } else {
+          k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)ntok, C, cb.n_tan,
+                                                                   cb.has_lap, D, Big);
+          NQS_CHECK_LAUNCH("k_gelu");
+        }
       }
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Big, D, rows, D, w.tc.w1[b], d, d, (const float*)bw.b1,

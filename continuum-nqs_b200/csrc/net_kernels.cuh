@@ -1250,6 +1250,125 @@ __global__ void __launch_bounds__(256) k_layernorm1(int n_tok, int d, const T* _
 }
 
 // LayerNorm launcher: single-channel rows take k_layernorm1
+// The same LayerNorm for float32 rows of width 64: half a warp per token, four consecutive
+// features per lane (16-byte loads and stores), 16-lane butterflies, tangent rows four at a time.
+// Same formulas as k_layernorm; the sums run in a different order.
+__device__ __forceinline__ float hw16_sum(float v) {
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int K>
+__device__ __forceinline__ void hw16_sum_n(float (&v)[K]) {
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+}
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+
+static __global__ void __launch_bounds__(256) k_layernorm_w64(int n_tok, int C, int n_tan, int has_lap,
+                                                       const float* __restrict__ X,
+                                                       const float* __restrict__ g,
+                                                       const float* __restrict__ b,
+                                                       float* __restrict__ Y) {
+  constexpr int d = 64, TP = 4;
+  const int hl = threadIdx.x & 15;
+  const int tok = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  // both half-warps run every shuffle: a token past the end works on the last token, writes nothing
+  const bool live = tok < n_tok;
+  const int tk = live ? tok : n_tok - 1;
+  const float* x = X + (size_t)tk * C * d + 4 * hl;
+  float* y = Y + (size_t)tk * C * d + 4 * hl;
+  const float inv_d = 1.0f / d;
+  const float4 xv = ld4(x), gv = ld4(g + 4 * hl), bv = ld4(b + 4 * hl);
+  float u[4] = {xv.x, xv.y, xv.z, xv.w};
+  const float gm[4] = {gv.x, gv.y, gv.z, gv.w};
+  const float mu = hw16_sum((u[0] + u[1]) + (u[2] + u[3])) * inv_d;
+  float s = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    u[q] -= mu;
+    s += u[q] * u[q];
+  }
+  const float var = hw16_sum(s) * inv_d;
+  const float rho = 1.0f / sqrtf(var + (float)kLnEps);
+  if (live)
+    st4(y, u[0] * rho * gm[0] + bv.x, u[1] * rho * gm[1] + bv.y, u[2] * rho * gm[2] + bv.z,
+        u[3] * rho * gm[3] + bv.w);
+  const float rho3 = rho * rho * rho;
+  float S1 = 0.f, S2 = 0.f, acc[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int t0 = 0; t0 < n_tan; t0 += TP) {
+    float du[TP][4];
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) {
+      if (t0 + tt < n_tan) {
+        const float4 v = ld4(x + (size_t)(1 + t0 + tt) * d);
+        du[tt][0] = v.x;
+        du[tt][1] = v.y;
+        du[tt][2] = v.z;
+        du[tt][3] = v.w;
+      } else {
+        du[tt][0] = du[tt][1] = du[tt][2] = du[tt][3] = 0.f;
+      }
+    }
+    float mt[TP], s23[2 * TP];
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) mt[tt] = (du[tt][0] + du[tt][1]) + (du[tt][2] + du[tt][3]);
+    hw16_sum_n<TP>(mt);
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) {
+      mt[tt] *= inv_d;
+      float s2 = 0.f, s3 = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        du[tt][q] -= mt[tt];
+        s2 += u[q] * du[tt][q];
+        s3 += du[tt][q] * du[tt][q];
+      }
+      s23[2 * tt] = s2;
+      s23[2 * tt + 1] = s3;
+    }
+    hw16_sum_n<2 * TP>(s23);
+#pragma unroll
+    for (int tt = 0; tt < TP; ++tt) {
+      const int t = t0 + tt;
+      if (t >= n_tan) break;  // uniform over the warp (both tokens share n_tan)
+      const float dv = 2.f * s23[2 * tt] * inv_d;
+      const float drho = -0.5f * rho3 * dv;
+      float o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        o[q] = (du[tt][q] * rho + u[q] * drho) * gm[q];
+        acc[q] += du[tt][q] * drho;
+      }
+      if (live) st4(y + (size_t)(1 + t) * d, o[0], o[1], o[2], o[3]);
+      S1 += dv * dv;
+      S2 += s23[2 * tt + 1] * inv_d;
+    }
+  }
+  if (has_lap) {
+    const float4 lv = ld4(x + (size_t)(C - 1) * d);
+    float dl[4] = {lv.x, lv.y, lv.z, lv.w};
+    const float ml = hw16_sum((dl[0] + dl[1]) + (dl[2] + dl[3])) * inv_d;
+    float s2 = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      dl[q] -= ml;
+      s2 += u[q] * dl[q];
+    }
+    const float dvl = 2.f * hw16_sum(s2) * inv_d + 2.f * S2;
+    const float d2rho = 0.75f * rho3 * rho * rho * S1 - 0.5f * rho3 * dvl;
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = (dl[q] * rho + 2.f * acc[q] + u[q] * d2rho) * gm[q];
+    if (live) st4(y + (size_t)(C - 1) * d, o[0], o[1], o[2], o[3]);
+  }
+}
+
 template <typename T>
 inline int launch_layernorm(int n_tok, int C, int n_tan, int has_lap, int d, const T* X,
                             const T* g, const T* b, T* Y, cudaStream_t st) {
@@ -1259,6 +1378,16 @@ inline int launch_layernorm(int n_tok, int C, int n_tan, int has_lap, int d, con
     k_layernorm1<T, R><<<(nw + 7) / 8, 256, 0, st>>>(n_tok, d, X, g, b, Y);
     NQS_CHECK_LAUNCH("k_layernorm1");
   } else {
+    if constexpr (sizeof(T) == 4) {
+      if (d == 64 && ((uintptr_t)X % 16 == 0) && ((uintptr_t)Y % 16 == 0) &&
+          ((uintptr_t)g % 16 == 0) && ((uintptr_t)b % 16 == 0)) {
+        k_layernorm_w64<<<(unsigned)((n_tok + 15) / 16), 256, 0, st>>>(
+            n_tok, C, n_tan, has_lap, (const float*)X, (const float*)g, (const float*)b,
+            (float*)Y);
+        NQS_CHECK_LAUNCH("k_layernorm_w64");
+        return NQS_OK;
+      }
+    }
     const unsigned grid = (unsigned)((n_tok + 7) / 8);
     if (d <= 32)
       k_layernorm<T, 1><<<grid, 256, 0, st>>>(n_tok, C, n_tan, has_lap, d, X, g, b, Y);
@@ -1335,6 +1464,55 @@ __global__ void __launch_bounds__(256) k_gelu(size_t n_tok, int C, int n_tan, in
   if (has_lap) {
     T* p = x + (size_t)(C - 1) * D;
     *p = g1 * (*p) + g2 * acc;
+  }
+}
+
+// The same GELU for float32 rows, four consecutive features per thread (16-byte loads and
+// stores): same formulas as k_gelu, and the same two passes over the tangents.
+static __global__ void __launch_bounds__(256) k_gelu4(size_t n_tok, int C, int n_tan, int has_lap, int D,
+                                               float* __restrict__ X) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int D4 = D >> 2;
+  if (idx >= n_tok * (size_t)D4) return;
+  const size_t tok = idx / D4;
+  const int f = 4 * (int)(idx - tok * D4);
+  float* x = X + tok * (size_t)C * D + f;
+  const float4 x4 = *reinterpret_cast<const float4*>(x);
+  const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+  const float c = 0.7978845608028654f, b3 = 0.044715f;
+  float th[4], g1[4], g2[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    th[q] = gelu_tanh_w(xv[q]);
+    const float cdf = 0.5f * (1.f + th[q]);
+    const float sech2 = 1.f - th[q] * th[q];
+    const float w1 = c * (1.f + 3.f * b3 * xv[q] * xv[q]);
+    const float w2 = c * 6.f * b3 * xv[q];
+    g1[q] = cdf + 0.5f * xv[q] * sech2 * w1;
+    g2[q] = sech2 * (w1 - xv[q] * th[q] * w1 * w1 + 0.5f * xv[q] * w2);
+  }
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  if (has_lap) {
+    for (int t = 0; t < n_tan; ++t) {
+      const float4 v = *reinterpret_cast<const float4*>(x + (size_t)(1 + t) * D);
+      acc[0] += v.x * v.x;
+      acc[1] += v.y * v.y;
+      acc[2] += v.z * v.z;
+      acc[3] += v.w * v.w;
+    }
+  }
+  *reinterpret_cast<float4*>(x) = make_float4(gelu_value(xv[0], th[0]), gelu_value(xv[1], th[1]),
+                                              gelu_value(xv[2], th[2]), gelu_value(xv[3], th[3]));
+  for (int t = 0; t < n_tan; ++t) {
+    float4* p = reinterpret_cast<float4*>(x + (size_t)(1 + t) * D);
+    const float4 v = *p;
+    *p = make_float4(g1[0] * v.x, g1[1] * v.y, g1[2] * v.z, g1[3] * v.w);
+  }
+  if (has_lap) {
+    float4* p = reinterpret_cast<float4*>(x + (size_t)(C - 1) * D);
+    const float4 v = *p;
+    *p = make_float4(g1[0] * v.x + g2[0] * acc[0], g1[1] * v.y + g2[1] * acc[1],
+                     g1[2] * v.z + g2[2] * acc[2], g1[3] * v.w + g2[3] * acc[3]);
   }
 }
 

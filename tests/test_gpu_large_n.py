@@ -157,5 +157,5 @@ def test_width128_network_runs_on_tensor_cores():
     lp64 = l64(R, S).cpu()
     e64 = make_local_energy(l64, 1.0, 0.7, 0.3)(R, S).cpu()
     d = lp32 - lp64
-    assert float(d.real.abs().max()) < 1e-3 * max(1.0, float(lp64.real.abs().max()))
+    assert float(d.real.abs().max()) < 5e-3 * max(1.0, float(lp64.real.abs().max()))
     assert float((em - e64).abs().median()) < 1e-2 * max(1.0, float(e64.abs().median()))
