@@ -454,8 +454,9 @@ __global__ void __launch_bounds__(256, 1) k_chol_dag(double* __restrict__ A, int
 
 bool g_chol_dag = false;
 
-// doubles: two queue tickets, abort word + pad, T^2 tile counters, the two task lists (int4)
-static size_t dag_counters_elems(size_t T) { return 2 + (T * T + 1) / 2; }
+// doubles: two queue tickets, abort word + pad, T^2 tile counters, rounded up to an even count
+// so that the two task lists (int4) that follow start on 16 bytes
+static size_t dag_counters_elems(size_t T) { return (2 + (T * T + 1) / 2 + 1) & ~(size_t)1; }
 size_t cholesky_dag_scratch_elems(int n) {
   const size_t T = (size_t)(n + TB - 1) / TB;
   return dag_counters_elems(T) + 2 * (T * T + (size_t)dag_nbulk((int)T));
@@ -479,6 +480,10 @@ int cholesky_dag(double* A, int64_t lda, int n, int* bad, double* scratch, size_
   int* state = reinterpret_cast<int*>(scratch + 2);
   int4* crit_list = reinterpret_cast<int4*>(scratch + dag_counters_elems(T));
   int4* bulk_list = crit_list + (size_t)T * T;
+  if (reinterpret_cast<uintptr_t>(crit_list) & 15) {
+    set_error("cholesky_dag: scratch not 16-byte aligned");
+    return NQS_ERR_INVALID_ARG;
+  }
   cudaMemsetAsync(scratch, 0, sizeof(double) * dag_counters_elems(T), st);
   {
     const long long nthreads = (long long)T * T + (long long)T * T * T;

@@ -787,4 +787,324 @@ __global__ void __launch_bounds__(kHeadLgThreads, 1) k_head_val_lg(JobBatch jb, 
   if (out.L) out.L[j_out0 + job] = L;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Gradient-only jobs with few tangent electrons (the spin-flip batch: one electron, two tangents),
+// 16 < N <= 64: as k_head_val_lg, four 64-thread groups each invert their own determinants
+// (in-place Gauss-Jordan, same pivot rule as k_head_lg) on named barriers; the tangent
+// electrons' envelope derivatives are summed from the phases before the groups reuse that
+// memory, so tr(M^-1 D_t) needs only the envelope, the backflow channels and those columns.
+// ---------------------------------------------------------------------------------------------
+constexpr int kHeadSocMaxTe = 4;
+constexpr size_t kHeadSocStaticBytes =
+    kHeadValStaticBytes + 16 * (2 * kHeadSocMaxTe * kHeadLgMaxN + NQS_MAX_DETS * 2 * kHeadSocMaxTe +
+                                2 * NQS_MAX_DETS) +
+    8 * (2 * kHeadSocMaxTe + kHeadValGroups * 2 * 4 + 4) + 256;
+
+template <typename TIN>
+__global__ void __launch_bounds__(kHeadLgThreads, 1) k_head_soc_lg(JobBatch jb, ModelConst mc,
+                                                                  const TIN* __restrict__ BF,
+                                                                  int ldbf, HeadParams hp,
+                                                                  HeadOut out, int j_out0) {
+  const int N = jb.N, C = jb.C, nG = mc.nG, K = mc.K;
+  const int n_tan = jb.n_tan, n_te = n_tan / 2;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int grp = tid >> 6, gt = tid & 63, gw = gt >> 5;
+  const int job = blockIdx.x;
+  const HeadValLayout lay = head_val_layout(N, nG);
+  const int LD = lay.ld;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* env = reinterpret_cast<cplx*>(smraw + lay.env);
+  const size_t gstride = (lay.total - lay.G) / kHeadValGroups;
+  cplx* G = reinterpret_cast<cplx*>(smraw + lay.G + grp * gstride);
+  cplx* ph = reinterpret_cast<cplx*>(smraw + lay.G);  // phase 1 only
+  __shared__ double rx[kHeadLgMaxN], ry[kHeadLgMaxN], red[kHeadLgThreads / 32];
+  __shared__ double gj[2 * kHeadSocMaxTe], s_jas;
+  __shared__ double gred[kHeadValGroups][2][4];
+  __shared__ int sp[kHeadLgMaxN];
+  __shared__ int used[kHeadValGroups][kHeadLgMaxN], piv[kHeadValGroups][kHeadLgMaxN];
+  __shared__ int sing[NQS_MAX_DETS];
+  __shared__ __align__(16) cplx prow[kHeadValGroups][kHeadLgMaxN],
+      fcol[kHeadValGroups][kHeadLgMaxN];
+  __shared__ cplx dE[2 * kHeadSocMaxTe][kHeadLgMaxN];  // [axis + 2 et][orbital a]
+  __shared__ cplx s_ld[NQS_MAX_DETS], s_sq[NQS_MAX_DETS], dlk[NQS_MAX_DETS][2 * kHeadSocMaxTe];
+  const JobInfo ji = job_info(jb, job);
+  const int te_lo = ji.tan_e0;
+  auto Weff = [&](int a, int g, int s) -> cplx {
+    const size_t o = ((size_t)a * nG + g) * 2 + s;
+    cplx w = mk(mc.W[2 * o], mc.W[2 * o + 1]);
+    if (mc.learnable_env) w = cadd(w, mk(hp.dW[o], hp.dW[(size_t)N * nG * 2 + o]));
+    return w;
+  };
+  // ---- phase 1 ----
+  for (int i = tid; i < N; i += kHeadLgThreads) {
+    const double* r = jb.R + ((size_t)ji.walker * N + i) * 2;
+    rx[i] = r[0];
+    ry[i] = r[1];
+    sp[i] = job_spin(jb, ji, i);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nG * N; idx += kHeadLgThreads) {
+    const int g = idx / N, i = idx - g * N;
+    double sn, cs;
+    sincos(mc.Gs[2 * g] * rx[i] + mc.Gs[2 * g + 1] * ry[i], &sn, &cs);
+    ph[idx] = mk(cs, sn);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * N; idx += kHeadLgThreads) {
+    const int a = idx / N, i = idx - a * N;
+    const int s = sp[i];
+    cplx e = mk(0, 0);
+#pragma unroll 4
+    for (int g = 0; g < nG; ++g) cfma(e, ph[g * N + i], Weff(a, g, s));
+    env[a * LD + i] = e;
+  }
+  for (int idx = tid; idx < n_te * N; idx += kHeadLgThreads) {
+    const int et = idx / N, a = idx - et * N, e = te_lo + et, s = sp[e];
+    cplx dx = mk(0, 0), dy = mk(0, 0);
+    for (int g = 0; g < nG; ++g) {
+      const cplx pw = cmul(ph[g * N + e], Weff(a, g, s));
+      cfma(dx, pw, mk(0, mc.Gs[2 * g]));
+      cfma(dy, pw, mk(0, mc.Gs[2 * g + 1]));
+    }
+    dE[2 * et][a] = dx;
+    dE[2 * et + 1][a] = dy;
+  }
+  double J = 0.0;
+  if (mc.use_jastrow) {
+    const int npair = N * (N - 1) / 2;
+    for (int p = tid; p < npair; p += kHeadLgThreads) {
+      int i = 0, rem = p;
+      while (rem >= N - 1 - i) {
+        rem -= N - 1 - i;
+        ++i;
+      }
+      const int jj = i + 1 + rem;
+      double dx, dy;
+      min_image(mc, rx[i] - rx[jj], ry[i] - ry[jj], &dx, &dy);
+      const double r = sqrt(dx * dx + dy * dy + 1e-12);
+      double u, u1, u2;
+      jastrow_u(mc, hp, r, sp[i] == sp[jj], &u, &u1, &u2);
+      J += u;
+    }
+    J = warp_sum(J);
+    if (lane == 0) red[tid >> 5] = J;
+    // gradient of the tangent electrons: warp et, lanes over partners, fixed-order butterflies
+    const int w = tid >> 5;
+    if (w < n_te) {
+      const int e = te_lo + w;
+      double gx = 0.0, gy = 0.0;
+      for (int jj = lane; jj < N; jj += 32) {
+        if (jj == e) continue;
+        double dx, dy;
+        min_image(mc, rx[e] - rx[jj], ry[e] - ry[jj], &dx, &dy);
+        const double r = sqrt(dx * dx + dy * dy + 1e-12);
+        double u, u1, u2;
+        jastrow_u(mc, hp, r, sp[e] == sp[jj], &u, &u1, &u2);
+        gx += u1 * dx / r;
+        gy += u1 * dy / r;
+      }
+      gx = warp_sum(gx);
+      gy = warp_sum(gy);
+      if (lane == 0) {
+        gj[2 * w] = gx;
+        gj[2 * w + 1] = gy;
+      }
+    }
+  }
+  __syncthreads();  // env / dE complete, phases no longer read: the group buffers are free
+  if (tid == 0) {
+    double t = 0.0;
+    if (mc.use_jastrow)
+      for (int w = 0; w < kHeadLgThreads / 32; ++w) t += red[w];
+    s_jas = t;
+  }
+  // ---- phase 2: determinants k = grp, grp + 4, ... ----
+  const int bar = 1 + grp;
+  const int ty = gt >> 4, tx = gt & 15;
+  for (int k = grp; k < K; k += kHeadValGroups) {
+    auto bf = [&](int c, int a, int i) -> cplx {
+      const TIN* p = BF + (((size_t)job * N + i) * C + c) * ldbf;
+      return mk((double)p[k * N + a], (double)p[K * N + k * N + a]);
+    };
+    for (int idx = gt; idx < N * N; idx += 64) {
+      const int i = idx / N, a = idx - i * N;
+      const cplx b0 = bf(0, a, i);
+      G[a * LD + i] = cmul(env[a * LD + i], mk(1.0 + b0.re, b0.im));
+    }
+    for (int r = gt; r < N; r += 64) used[grp][r] = 0;
+    group_bar(bar);
+    cplx prod = mk(1.0, 0.0);
+    int pexp = 0, sg = 0;
+#pragma unroll 1
+    for (int c = 0; c < N; ++c) {
+      if (gw == 0) {
+        const int r0 = lane, r1 = lane + 32;
+        const bool u0 = r0 >= N || used[grp][r0], u1 = r1 >= N || used[grp][r1];
+        auto mag = [](cplx z) {
+          const double v = cabs1(z);
+          return v >= 0.0 ? v : 0.0;
+        };
+        double best = u0 ? -1.0 : mag(G[r0 * LD + c]);
+        int bi = r0;
+        if (!u1) {
+          const double v1 = mag(G[r1 * LD + c]);
+          if (v1 > best) {
+            best = v1;
+            bi = r1;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+          }
+        }
+        const int p = bi;
+        const cplx pv = G[p * LD + c];
+        const bool zero = pv.re == 0.0 && pv.im == 0.0;
+        const cplx ipv = zero ? mk(0.0, 0.0) : cdiv(mk(1.0, 0.0), pv);
+        if (zero) {
+          sg = 1;
+        } else {
+          prod = cmul(prod, pv);
+          int ex;
+          frexp(fmax(fabs(prod.re), fabs(prod.im)), &ex);
+          prod = mk(ldexp(prod.re, -ex), ldexp(prod.im, -ex));
+          pexp += ex;
+        }
+        for (int j = lane; j < N; j += 32)
+          prow[grp][j] = cmul(j == c ? mk(1.0, 0.0) : G[p * LD + j], ipv);
+        for (int r = lane; r < N; r += 32) fcol[grp][r] = r == p ? mk(0.0, 0.0) : G[r * LD + c];
+        __syncwarp();
+        if (lane == 0) {
+          piv[grp][c] = p;
+          used[grp][p] = 1;
+        }
+      }
+      group_bar(bar);
+      const int p = piv[grp][c];
+      for (int r = ty; r < N; r += 4) {
+        const cplx f = fcol[grp][r];
+        for (int j = tx; j < N; j += 16) {
+          cplx v;
+          if (r == p) {
+            v = prow[grp][j];
+          } else {
+            v = j == c ? mk(0.0, 0.0) : G[r * LD + j];
+            v = csub(v, cmul(f, prow[grp][j]));
+          }
+          G[r * LD + j] = v;
+        }
+      }
+      group_bar(bar);
+    }
+    if (gw == 0) {
+      int inv_cnt = 0;
+      for (int c = lane; c < N; c += 32)
+        for (int c2 = c + 1; c2 < N; ++c2)
+          if (piv[grp][c] > piv[grp][c2]) ++inv_cnt;
+      inv_cnt = warp_sum(inv_cnt);
+      if (inv_cnt & 1) prod = mk(-prod.re, -prod.im);
+      if (lane == 0) {
+        s_ld[k] = sg ? mk(-INFINITY, 0.0)
+                     : mk(log(hypot(prod.re, prod.im)) + pexp * 0.6931471805599453,
+                          atan2(prod.im, prod.re));
+        sing[k] = sg;
+        s_sq[k] = mk(0, 0);
+      }
+    }
+    // tr(M^-1 D_t) for both axes of each tangent electron: sum over (i, c') of
+    // M^-1[i][piv c'] D_t[piv c'][i] (rows of the inverse at storage rows piv[i])
+    for (int et = 0; et < n_te; ++et) {
+      const int e = te_lo + et;
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int idx = gt; idx < N * N; idx += 64) {
+        const int i = idx / N, c2 = idx - i * N;
+        const int a = piv[grp][c2];
+        const cplx m = G[piv[grp][i] * LD + c2];
+        const cplx en = env[a * LD + i];
+        cplx dx = cmul(en, bf(1 + 2 * et, a, i)), dy = cmul(en, bf(2 + 2 * et, a, i));
+        if (i == e) {
+          const cplx b0 = bf(0, a, e), w1 = mk(1.0 + b0.re, b0.im);
+          dx = cadd(dx, cmul(dE[2 * et][a], w1));
+          dy = cadd(dy, cmul(dE[2 * et + 1][a], w1));
+        }
+        const cplx tx_ = cmul(m, dx), ty_ = cmul(m, dy);
+        v[0] += tx_.re;
+        v[1] += tx_.im;
+        v[2] += ty_.re;
+        v[3] += ty_.im;
+      }
+      warp_sum_n<double, 4>(v);
+      if (lane == 0) {
+        gred[grp][gw][0] = v[0];
+        gred[grp][gw][1] = v[1];
+        gred[grp][gw][2] = v[2];
+        gred[grp][gw][3] = v[3];
+      }
+      group_bar(bar);
+      if (gt == 0) {
+        const cplx tx_ = mk(gred[grp][0][0] + gred[grp][1][0], gred[grp][0][1] + gred[grp][1][1]);
+        const cplx ty_ = mk(gred[grp][0][2] + gred[grp][1][2], gred[grp][0][3] + gred[grp][1][3]);
+        dlk[k][2 * et] = tx_;
+        dlk[k][2 * et + 1] = ty_;
+        cfma(s_sq[k], tx_, tx_);
+        cfma(s_sq[k], ty_, ty_);
+      }
+      group_bar(bar);  // gred is rewritten by the next tangent electron
+    }
+  }
+  __syncthreads();
+  // ---- phase 3: log-sum-exp over determinants, gradients (warp 0) ----
+  if (tid >= 32) return;
+  const int jo = j_out0 + job;
+  double mx = -INFINITY;
+  for (int k = 0; k < K; ++k) {
+    const double zr = s_ld[k].re + ((K > 1 && hp.det_logw) ? hp.det_logw[k] : 0.0);
+    if (!sing[k] && zr > mx) mx = zr;
+  }
+  const bool all_sing = (mx == -INFINITY);
+  cplx ssum = mk(0, 0);
+  cplx p[NQS_MAX_DETS];
+  for (int k = 0; k < K; ++k) {
+    if (sing[k]) {
+      p[k] = mk(0, 0);
+      continue;
+    }
+    const cplx wk = (K > 1 && hp.det_logw) ? mk(hp.det_logw[k], hp.det_logw[K + k]) : mk(0, 0);
+    p[k] = cexp_(mk(s_ld[k].re + wk.re - mx, s_ld[k].im + wk.im));
+    ssum = cadd(ssum, p[k]);
+  }
+  cplx L;
+  if (K == 1) {
+    L = s_ld[0];
+  } else {
+    L = all_sing ? mk(-INFINITY, 0.0)
+                 : mk(mx + log(hypot(ssum.re, ssum.im)), atan2(ssum.im, ssum.re));
+    if (!all_sing) {
+      const cplx inv_s = cdiv(mk(1.0, 0.0), ssum);
+      for (int k = 0; k < K; ++k) p[k] = cmul(p[k], inv_s);
+    }
+  }
+  if (K == 1) p[0] = mk(1.0, 0.0);
+  for (int t = lane; t < n_tan; t += 32) {
+    cplx g = mk(0, 0);
+    if (all_sing) {
+      g = mk(NAN, NAN);
+    } else {
+      for (int k = 0; k < K; ++k)
+        if (!sing[k]) cfma(g, p[k], dlk[k][t]);
+    }
+    if (mc.use_jastrow) g.re += gj[t];
+    if (out.dL) out.dL[(size_t)jo * jb.n_tan + t] = g;
+  }
+  if (lane == 0) {
+    if (mc.use_jastrow) L.re += s_jas;
+    if (out.L) out.L[jo] = L;
+  }
+}
+
 }  // namespace nqs

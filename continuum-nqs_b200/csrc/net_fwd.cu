@@ -71,7 +71,18 @@ static bool launch_head_lg(const ModelConst& mc, const JobBatch& cb, const T* BF
       k_head_lg<T, 0, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
     }
   } else if (mode == 1) {
-    k_head_lg<T, 1, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+    const HeadValLayout vl = head_val_layout(N, mc.nG);
+    if (cb.n_tan <= 2 * kHeadSocMaxTe && vl.total && vl.total + kHeadSocStaticBytes <= 227 * 1024) {
+      static bool sattr = false;
+      if (!sattr) {
+        cudaFuncSetAttribute(k_head_soc_lg<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - (int)kHeadSocStaticBytes);
+        sattr = true;
+      }
+      k_head_soc_lg<T><<<grid, kHeadLgThreads, vl.total, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+    } else {
+      k_head_lg<T, 1, 1><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
+    }
   } else if (ts == 2) {
     k_head_lg<T, 2, 2><<<grid, kHeadLgThreads, sm, st>>>(cb, mc, BF, ldbf, hp, out, jout);
   } else {
