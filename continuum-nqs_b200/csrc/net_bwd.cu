@@ -733,14 +733,59 @@ size_t per_sample_O_scratch(const ModelConst& mc, int W) {
   return backward_scratch<T>(mc, W, false);
 }
 
+static inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Y (+)= X W^T of a reverse-pass layer. Float32 with the tensor-core weights on: a tcgen05 row
+// GEMM that reads the stored [d_in][d_out] kernel as the K-major operand of the product (no copy);
+// otherwise, or for an operand layout the TMA cannot take, the SIMT GEMM.
+template <typename T>
+static int gemm_wt(GemmArgs<T>& g, const TcNet& tc, cudaStream_t st) {
+  if constexpr (sizeof(T) == 4) {
+    const GemmSeg<T>& s0 = g.seg[0];
+    const bool ok = tc.on && g.nseg == 1 && g.trans_w && !s0.b && s0.out_off == 0 &&
+                    s0.ldw == g.K && g.K % 32 == 0 && s0.ncols % 16 == 0 && g.ldx % 4 == 0 &&
+                    g.ldy % 4 == 0 && aligned16(g.X) && aligned16(g.Y) && aligned16(s0.W) &&
+                    (!g.Res || (g.Res == g.Y && g.ldr == g.ldy));
+    if (ok)
+      return rowgemm_tc((const float*)g.X, g.ldx, g.rows, g.K, (const float*)s0.W, s0.ncols,
+                        s0.ncols, nullptr, g.C, (const float*)g.Res, g.ldr, (float*)g.Y, g.ldy,
+                        tc.err, st);
+  }
+  return launch_gemm<T>(g, st);
+}
+
 // forward of block l from x = b.xin[l] into the block's intermediates (slot s), and, when y is
 // given, its output y = xmid + W1 GELU(W0 LN1 xmid) + b1
 template <typename T>
-static int block_forward(const ModelConst& mc, const BlockW<T>& bw, SaveBufs<T>& b, int l, int s,
-                         int nw, T* y, cudaStream_t st) {
+static int block_forward(const ModelConst& mc, const BlockW<T>& bw, const TcNet& tc,
+                         SaveBufs<T>& b, int l, int s, int nw, T* y, cudaStream_t st) {
   const int N = mc.N, d = mc.d, D = mc.ff * d, H = mc.H, nt = nw * N;
   const T* x = b.xin[l];
   NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, x, bw.ln0_s, bw.ln0_b, b.h0[s], st));
+  if constexpr (sizeof(T) == 4) {
+    if (tc.on) {  // the Dense layers on the tensor cores, as in the forward passes
+      auto w16 = [&](const uint16_t* p) { return tc.bf16 ? p : nullptr; };
+      NQS_TRY(rowgemm_tc(b.h0[s], d, nt, d, tc.wqkv[l], tc.npad_qkv, 3 * d, tc.bqkv[l], 1,
+                         nullptr, 0, b.qkv[s], 3 * d, tc.err, st, 0, w16(tc.wqkv16[l])));
+      NQS_TRY(launch_attention<T>(nw, N, 1, 0, 0, d, H, b.qkv[s], b.ao[s], st));
+      cudaMemcpyAsync(b.xmid[s], x, sizeof(T) * (size_t)nt * d, cudaMemcpyDeviceToDevice, st);
+      NQS_TRY(rowgemm_tc(b.ao[s], d, nt, d, tc.wo[l], d, d, bw.bo, 1, b.xmid[s], d, b.xmid[s], d,
+                         tc.err, st, 0, w16(tc.wo16[l])));
+      NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xmid[s], bw.ln1_s, bw.ln1_b, b.h1[s], st));
+      NQS_TRY(rowgemm_tc(b.h1[s], d, nt, d, tc.w0[l], D, D, bw.b0, 1, nullptr, 0, b.a0[s], D,
+                         tc.err, st, 0, w16(tc.w016[l])));
+      cudaMemcpyAsync(b.g0[s], b.a0[s], sizeof(T) * (size_t)nt * D, cudaMemcpyDeviceToDevice, st);
+      const size_t nel = (size_t)nt * D;
+      k_gelu<T><<<(unsigned)((nel + 255) / 256), 256, 0, st>>>((size_t)nt, 1, 0, 0, D, b.g0[s]);
+      NQS_CHECK_LAUNCH("k_gelu");
+      if (y) {
+        cudaMemcpyAsync(y, b.xmid[s], sizeof(T) * (size_t)nt * d, cudaMemcpyDeviceToDevice, st);
+        NQS_TRY(rowgemm_tc(b.g0[s], D, nt, D, tc.w1[l], d, d, bw.b1, 1, y, d, y, d, tc.err, st, 0,
+                           w16(tc.w116[l])));
+      }
+      return NQS_OK;
+    }
+  }
   GemmArgs<T> g{};
   g.X = b.h0[s]; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
   g.Y = b.qkv[s]; g.ldy = 3 * d; g.nseg = 3;
@@ -831,10 +876,18 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
     k_embed<T><<<(nt + 7) / 8, 256, 0, st>>>(jb, mc, w.emb_w, w.emb_b, mc.depth ? b.xin[0] : b.xL);
     NQS_CHECK_LAUNCH("k_embed");
     for (int l = 0; l < mc.depth; ++l)
-      NQS_TRY(block_forward<T>(mc, w.blk[l], b, l, ckpt ? 0 : l, nw,
+      NQS_TRY(block_forward<T>(mc, w.blk[l], w.tc, b, l, ckpt ? 0 : l, nw,
                                (l + 1 < mc.depth) ? b.xin[l + 1] : b.xL, st));
     NQS_TRY(launch_layernorm<T>(nt, 1, 0, 0, d, b.xL, w.lnf_s, w.lnf_b, b.hf, st));
-    {
+    bool bf_done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (w.tc.on) {
+        NQS_TRY(rowgemm_tc(b.hf, d, nt, d, w.tc.wbf, w.tc.npad_bf, 2 * KN, w.bf_b_re, 1, nullptr,
+                           0, b.bf, 2 * KN, w.tc.err, st, 0, w.tc.bf16 ? w.tc.wbf16 : nullptr));
+        bf_done = true;
+      }
+    }
+    if (!bf_done) {
       GemmArgs<T> g{};
       g.X = b.hf; g.ldx = d; g.rows = nt; g.K = d; g.C = 1;
       g.Y = b.bf; g.ldy = 2 * KN; g.nseg = 2;
@@ -851,10 +904,10 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
       g.X = b.X1; g.ldx = KN; g.rows = 2 * nt; g.K = KN; g.C = 2; g.trans_w = 1;
       g.Y = b.hb; g.ldy = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{w.bf_w_re, nullptr, KN, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      NQS_TRY(gemm_wt<T>(g, w.tc, st));
       g.X = b.X2; g.Res = b.hb; g.ldr = d;
       g.seg[0] = GemmSeg<T>{w.bf_w_im, nullptr, KN, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));
+      NQS_TRY(gemm_wt<T>(g, w.tc, st));
     }
     NQS_TRY(wgrad<T>(wr, nw, N, d, KN, b.hf, d, b.X1, KN, w0, dsc.off_backflow_kernel,
                      dsc.off_backflow_bias, 1, st));
@@ -867,13 +920,13 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
       const BlockW<T>& bw = w.blk[l];
       const int64_t* of = dsc.off_block[l];
       const int s = ckpt ? 0 : l;
-      if (ckpt) NQS_TRY(block_forward<T>(mc, bw, b, l, 0, nw, nullptr, st));  // recompute
+      if (ckpt) NQS_TRY(block_forward<T>(mc, bw, w.tc, b, l, 0, nw, nullptr, st));  // recompute
       // MLP: x_out = xmid + g0 W1 + b1
       GemmArgs<T> g{};
       g.X = b.xb; g.ldx = d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
       g.Y = b.big; g.ldy = D; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.w1, nullptr, d, D, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));  // gbar0 = xbar W1^T
+      NQS_TRY(gemm_wt<T>(g, w.tc, st));  // gbar0 = xbar W1^T
       NQS_TRY(wgrad<T>(wr, nw, N, D, d, b.g0[s], D, b.xb, d, w0, of[NQS_B_DENSE1_KERNEL],
                        of[NQS_B_DENSE1_BIAS], 0, st));
       const size_t nel = (size_t)nt * D;
@@ -883,7 +936,7 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
       g.X = b.big; g.ldx = D; g.rows = 2 * nt; g.K = D; g.C = 2; g.trans_w = 1;
       g.Y = b.hb; g.ldy = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.w0, nullptr, D, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));  // hbar1 = abar0 W0^T
+      NQS_TRY(gemm_wt<T>(g, w.tc, st));  // hbar1 = abar0 W0^T
       NQS_TRY(wgrad<T>(wr, nw, N, d, D, b.h1[s], d, b.big, D, w0, of[NQS_B_DENSE0_KERNEL],
                        of[NQS_B_DENSE0_BIAS], 0, st));
       k_ln_bwd<T, Wr><<<nw, 256, sizeof(T) * (size_t)N * d, st>>>(
@@ -895,7 +948,7 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
       g.X = b.xb; g.ldx = d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
       g.Y = b.hb; g.ldy = d; g.nseg = 1;
       g.seg[0] = GemmSeg<T>{bw.wo, nullptr, d, d, 0, 0};
-      NQS_TRY(launch_gemm<T>(g, st));  // aobar
+      NQS_TRY(gemm_wt<T>(g, w.tc, st));  // aobar
       NQS_TRY(wgrad<T>(wr, nw, N, d, d, b.ao[s], d, b.xb, d, w0, of[NQS_B_O_KERNEL],
                        of[NQS_B_O_BIAS], 0, st));
       k_attn_bwd<T><<<nw * H, 128, absm, st>>>(N, d, H, b.qkv[s], b.hb, b.big);
@@ -907,7 +960,7 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
         g.X = b.big + q * d; g.ldx = 3 * d; g.rows = 2 * nt; g.K = d; g.C = 2; g.trans_w = 1;
         g.Y = b.hb; g.ldy = d; g.Res = q ? b.hb : nullptr; g.ldr = d; g.nseg = 1;
         g.seg[0] = GemmSeg<T>{wts[q], nullptr, d, d, 0, 0};
-        NQS_TRY(launch_gemm<T>(g, st));
+        NQS_TRY(gemm_wt<T>(g, w.tc, st));
       }
       const int kk[3] = {NQS_B_Q_KERNEL, NQS_B_K_KERNEL, NQS_B_V_KERNEL};
       const int kb[3] = {NQS_B_Q_BIAS, NQS_B_K_BIAS, NQS_B_V_BIAS};
@@ -929,12 +982,24 @@ static int backward_run(const HostModel& hm, const NetW<T>& w, const HeadParams&
   return NQS_OK;
 }
 
+// a tensor-core GEMM of the pass that gave up a bounded wait recorded it in *err: the result is
+// then incomplete, and its first entry becomes NaN so that the caller sees it
+template <typename X>
+__global__ void k_poison_first_on_timeout(const int* __restrict__ err, X* p) {
+  if (*err) p[0] = (X)NAN;
+}
+
 template <typename T, typename TO>
 int per_sample_O_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
                      const double* R, const int32_t* S, int W, TO* O, bool ckpt, Arena& ws,
                      cudaStream_t st) {
   const ORows<TO> orows{O, hm.desc.n_params, W};
-  return backward_run<T, ORows<TO>>(hm, w, hp, R, S, W, orows, ckpt, ws, st);
+  NQS_TRY(backward_run<T, ORows<TO>>(hm, w, hp, R, S, W, orows, ckpt, ws, st));
+  if (w.tc.on && w.tc.err) {
+    k_poison_first_on_timeout<TO><<<1, 1, 0, st>>>(w.tc.err, O);
+    NQS_CHECK_LAUNCH("k_poison_first_on_timeout");
+  }
+  return NQS_OK;
 }
 
 template <typename T>
@@ -944,7 +1009,12 @@ int logpsi_vjp_run(const HostModel& hm, const NetW<T>& w, const HeadParams& hp,
   const cudaError_t e = cudaMemsetAsync(grad, 0, sizeof(double) * hm.desc.n_params, st);
   if (e != cudaSuccess) return cuda_status(e, "nqs_logpsi_vjp: clear");
   const VjpAcc acc{grad, ct};
-  return backward_run<T, VjpAcc>(hm, w, hp, R, S, W, acc, ckpt, ws, st);
+  NQS_TRY(backward_run<T, VjpAcc>(hm, w, hp, R, S, W, acc, ckpt, ws, st));
+  if (w.tc.on && w.tc.err) {
+    k_poison_first_on_timeout<double><<<1, 1, 0, st>>>(w.tc.err, grad);
+    NQS_CHECK_LAUNCH("k_poison_first_on_timeout");
+  }
+  return NQS_OK;
 }
 
 template size_t backward_scratch<double>(const ModelConst&, int, bool);

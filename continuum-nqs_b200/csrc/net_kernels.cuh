@@ -10,6 +10,9 @@ namespace nqs {
 // kernels of more than 16 electrons: one CTA per job (head) and per (job, head) (attention);
 // off, the warp-per-task kernels (nqs_set_large_n_kernels)
 extern bool g_large_n_cta;
+// attention of 16 tokens or fewer through the CTA-per-(job, head) kernel as well
+// (nqs_set_attention_cta_small; off by default)
+extern bool g_attn_cta_small;
 
 
 constexpr double kPi = 3.141592653589793;
@@ -1166,6 +1169,8 @@ inline int launch_attention_cta(int n_jobs, int N, int C, int n_tan, int has_lap
 template <typename T, int HD>
 inline int launch_attention_cta_ts(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
                                    const T* QKV, T* OUT, cudaStream_t st) {
+  if (N <= 16)
+    return launch_attention_cta<T, 1, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
   if (N <= 32)
     return launch_attention_cta<T, 2, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
   if (N <= 48)
@@ -1179,6 +1184,12 @@ inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, in
   const int hd = d / H;
   const bool aligned = ((uintptr_t)QKV % 16 == 0) && ((uintptr_t)OUT % 16 == 0) &&
                        ((size_t)d * sizeof(T)) % 16 == 0;
+  if (g_attn_cta_small && N <= kAttnTok && C == 1 + n_tan + has_lap) {
+    if (hd == 16)
+      return launch_attention_cta_ts<T, 16>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+    if (hd == 8)
+      return launch_attention_cta_ts<T, 8>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
+  }
   if (N <= kAttnTok && aligned && C == 1 + n_tan + has_lap) {
     if (hd == 16) return launch_attention_rt<T, 16>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
     if (hd == 8) return launch_attention_rt<T, 8>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);

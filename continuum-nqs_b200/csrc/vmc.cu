@@ -798,7 +798,8 @@ static int per_sample_O_impl(NqsModel* m, const double* theta, const double* R,
                                               st);
     return per_sample_O_run<double, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
   }
-  const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  w.tc = c.tc;  // the Dense layers of the pass on the tensor cores (TF32 / BF16 operands)
   if (out_dtype == 0)
     return per_sample_O_run<float, double>(m->hm, w, hp, R, S, W, (double*)out_O, ckpt, c.ws, st);
   return per_sample_O_run<float, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
@@ -841,6 +842,7 @@ extern "C" int nqs_logpsi_vjp(NqsModel* m, const double* theta, const double* R,
     const NetW<double> w = make_netw<double>(m->hm.desc, c.theta64, c.theta64);
     return logpsi_vjp_run<double>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
   }
-  const NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
+  w.tc = c.tc;
   return logpsi_vjp_run<float>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
 }

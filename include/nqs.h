@@ -149,6 +149,10 @@ int nqs_set_block_fusion(int enable);
  * warp per (job, determinant) and per (job, head). Same functions, same pivot rule; the switch
  * exists so that the two can be compared. */
 int nqs_set_large_n_kernels(int enable);
+/* Implementation selection (no reference counterpart; process-wide, default off): with it on,
+ * attention over 16 tokens or fewer also runs one 256-thread CTA per (job, head) instead of one
+ * warp per (job, head). Same function; the switch exists so that the two can be compared. */
+int nqs_set_attention_cta_small(int enable);
 /* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
  * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;
  * 0 restores the default (4). A tuning knob of the multi-instance autotuner. */
