@@ -779,6 +779,14 @@ int nqs_mcmc_sweeps_devctr(NqsModel* m, const double* theta, double* R, int32_t*
 
 }  // extern "C"
 
+// Dense layers of the float32 Jacobian / VJP pass on the tensor cores (nqs_set_jacobian_tc)
+static bool g_jacobian_tc = false;
+
+extern "C" int nqs_set_jacobian_tc(int enable) {
+  g_jacobian_tc = enable != 0;
+  return NQS_OK;
+}
+
 static int per_sample_O_impl(NqsModel* m, const double* theta, const double* R,
                              const int32_t* S, int W, void* out_O, int out_dtype, int prec,
                              bool ckpt, void* wsp, size_t wsb, cudaStream_t st) {
@@ -799,7 +807,7 @@ static int per_sample_O_impl(NqsModel* m, const double* theta, const double* R,
     return per_sample_O_run<double, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
   }
   NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
-  w.tc = c.tc;  // the Dense layers of the pass on the tensor cores (TF32 / BF16 operands)
+  if (g_jacobian_tc) w.tc = c.tc;  // the pass's Dense layers on the tensor cores (opt-in)
   if (out_dtype == 0)
     return per_sample_O_run<float, double>(m->hm, w, hp, R, S, W, (double*)out_O, ckpt, c.ws, st);
   return per_sample_O_run<float, float>(m->hm, w, hp, R, S, W, (float*)out_O, ckpt, c.ws, st);
@@ -843,6 +851,6 @@ extern "C" int nqs_logpsi_vjp(NqsModel* m, const double* theta, const double* R,
     return logpsi_vjp_run<double>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
   }
   NetW<float> w = make_netw<float>(m->hm.desc, c.theta32, c.theta64);
-  w.tc = c.tc;
+  if (g_jacobian_tc) w.tc = c.tc;
   return logpsi_vjp_run<float>(m->hm, w, hp, R, S, W, ct, out_grad, ckpt, c.ws, st);
 }

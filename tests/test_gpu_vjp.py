@@ -169,3 +169,24 @@ def test_adam_complex_step_matches_optax_restatement():
         tree, ost = O.optax_adam(tree, O.jax_grad_tree(ou, gv), ost, 1e-2)
     ref, _ = O.real_ravel(tree)
     assert float((th.cpu() - ref).abs().max()) < 1e-14
+
+
+def test_tensor_core_jacobian_close_to_simt():
+    """nqs_set_jacobian_tc(1): the float32 Jacobian with its Dense layers on the tensor cores
+    (TF32) against the CUDA-core float32 Jacobian, at width 64: rows agree to TF32 accuracy
+    (1e-2 of the largest entry), and the switch restores the CUDA-core result exactly."""
+    from nqs import _lib
+    from nqs.minsr import per_sample_O_rows
+    g, model = build(N=6, embed=64, depth=2, heads=4, n_dets=2, use_jastrow=True, n_knots=5)
+    theta = model.theta(perturb(model.init(0), 0.05, 61))
+    R, S = configs(model.n_elec, model.L, 32, 62)
+    a = per_sample_O_rows(model, theta, R, S, dtype=torch.float32, precision="mixed")
+    _lib.lib().nqs_set_jacobian_tc(1)
+    try:
+        b = per_sample_O_rows(model, theta, R, S, dtype=torch.float32, precision="mixed")
+    finally:
+        _lib.lib().nqs_set_jacobian_tc(0)
+    c = per_sample_O_rows(model, theta, R, S, dtype=torch.float32, precision="mixed")
+    assert torch.isfinite(b).all()
+    assert float((a - b).abs().max() / a.abs().max()) < 1e-2
+    assert torch.equal(a, c)
