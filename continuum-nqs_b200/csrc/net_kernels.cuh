@@ -13,6 +13,8 @@ extern bool g_large_n_cta;
 // attention of 16 tokens or fewer through the CTA-per-(job, head) kernel as well
 // (nqs_set_attention_cta_small; off by default)
 extern bool g_attn_cta_small;
+// attention of the multi-channel float32 batches on the tensor cores (nqs_set_attention_mma)
+extern bool g_attn_mma;
 
 
 constexpr double kPi = 3.141592653589793;
@@ -1178,12 +1180,274 @@ inline int launch_attention_cta_ts(int n_jobs, int N, int C, int n_tan, int has_
   return launch_attention_cta<T, 4, HD>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);
 }
 
+// --------------------------------------------------------------------------------------------
+// Attention of the multi-channel (forward-Laplacian, spin-flip) float32 batches on the tensor
+// cores: head width 16, N <= 64 tokens, one CTA per (job, head) with one warp per 16 query rows.
+// Every product of k_attention (Q_c K^T, Q K_c^T, Q_c K_c^T, P V, A V_c, P V_c) is a chain of
+// mma.sync m16n8k8 TF32 MMAs with float32 accumulation; the probabilities A, P_qk, P_sq and P_av
+// stay in accumulator fragments across the channels. A lane holds rows g, g + 8 (g = lane / 4) and
+// columns 2t, 2t + 1 (t = lane % 4) of every 8-key tile; used as the A operand of the next product
+// the pair (2t, 2t + 1) is read as keys (t, t + 4) of that tile, and V's rows are fetched in the
+// same order, so no fragment changes lanes. Row sums (softmax, d_t lse, Lap lse) are 4-lane
+// shuffles. Per channel: stage Q_c, K_c, V_c (rows past N zero), one barrier, products, outputs.
+// --------------------------------------------------------------------------------------------
+constexpr int kAttMmaHd = 16, kAttMmaLd = 20;  // head width; shared row stride (floats)
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int NT>  // 16-row tiles of tokens (N <= 16 NT)
+__global__ void __launch_bounds__(32 * NT) k_attention_mma(int n_jobs, int N, int C, int n_tan,
+                                                          int has_lap, int d, int H,
+                                                          const float* __restrict__ QKV,
+                                                          float* __restrict__ OUT) {
+  constexpr int NP = 16 * NT, NK = 2 * NT, LD = kAttMmaLd, HD = kAttMmaHd;
+  const int pair = blockIdx.x;
+  const int job = pair / H, h = pair - job * H;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int r0 = 16 * w;  // this warp's query rows r0 .. r0 + 15
+  __shared__ __align__(16) float sm[6 * NP * LD];
+  float* q = sm;
+  float* k = q + NP * LD;
+  float* v = k + NP * LD;
+  float* qt = v + NP * LD;
+  float* kt = qt + NP * LD;
+  float* vt = kt + NP * LD;
+  const float sc = 1.0f / sqrtf((float)HD);
+  const int ld = 3 * d;
+  auto row = [&](int i, int c) -> size_t { return ((size_t)job * N + i) * C + c; };
+  auto stage = [&](int c, float* dq, float* dk, float* dv) {
+    for (int idx = threadIdx.x; idx < NP * 4; idx += 32 * NT) {
+      const int i = idx >> 2, e4 = (idx & 3) * 4;
+      float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, cc = a;
+      if (i < N) {
+        const float* p = QKV + row(i, c) * ld + h * HD + e4;
+        a = *reinterpret_cast<const float4*>(p);
+        b = *reinterpret_cast<const float4*>(p + d);
+        cc = *reinterpret_cast<const float4*>(p + 2 * d);
+      }
+      *reinterpret_cast<float4*>(dq + i * LD + e4) = a;
+      *reinterpret_cast<float4*>(dk + i * LD + e4) = b;
+      *reinterpret_cast<float4*>(dv + i * LD + e4) = cc;
+    }
+  };
+  // A operand: rows r0.., features 8 ks .. 8 ks + 7 of X
+  auto afrag_x = [&](const float* X, int ks, uint32_t (&a)[4]) {
+    a[0] = to_tf32(X[(r0 + g) * LD + 8 * ks + t]);
+    a[1] = to_tf32(X[(r0 + g + 8) * LD + 8 * ks + t]);
+    a[2] = to_tf32(X[(r0 + g) * LD + 8 * ks + t + 4]);
+    a[3] = to_tf32(X[(r0 + g + 8) * LD + 8 * ks + t + 4]);
+  };
+  // A operand from a score-shaped fragment of key tile j: columns (2t, 2t+1) read as keys (t, t+4)
+  auto afrag_p = [&](const float (&P)[4], uint32_t (&a)[4]) {
+    a[0] = to_tf32(P[0]);
+    a[1] = to_tf32(P[2]);
+    a[2] = to_tf32(P[1]);
+    a[3] = to_tf32(P[3]);
+  };
+  // S[j] += X Y^T over the 16 features: X rows of this warp, Y rows = keys of tile j
+  auto scores = [&](const float* X, const float* Y, float (&S)[NK][4]) {
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      uint32_t a[4];
+      afrag_x(X, ks, a);
+#pragma unroll
+      for (int j = 0; j < NK; ++j) {
+        const uint32_t b0 = to_tf32(Y[(8 * j + g) * LD + 8 * ks + t]);
+        const uint32_t b1 = to_tf32(Y[(8 * j + g) * LD + 8 * ks + t + 4]);
+        mma_tf32(S[j], a, b0, b1);
+      }
+    }
+  };
+  // O[f] += P V over the keys: P score-shaped, V rows in the (t, t+4) <- (2t, 2t+1) key order
+  auto pv = [&](const float (&P)[NK][4], const float* V, float (&O)[2][4]) {
+#pragma unroll
+    for (int j = 0; j < NK; ++j) {
+      uint32_t a[4];
+      afrag_p(P[j], a);
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        const uint32_t b0 = to_tf32(V[(8 * j + 2 * t) * LD + 8 * f + g]);
+        const uint32_t b1 = to_tf32(V[(8 * j + 2 * t + 1) * LD + 8 * f + g]);
+        mma_tf32(O[f], a, b0, b1);
+      }
+    }
+  };
+  auto store = [&](int c, const float (&O)[2][4], float add_scale, const float (&Add)[2][4]) {
+    const int i0 = r0 + g, i1 = r0 + g + 8;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      const int col = h * HD + 8 * f + 2 * t;
+      if (i0 < N)
+        *reinterpret_cast<float2*>(OUT + row(i0, c) * d + col) =
+            make_float2(O[f][0] + add_scale * Add[f][0], O[f][1] + add_scale * Add[f][1]);
+      if (i1 < N)
+        *reinterpret_cast<float2*>(OUT + row(i1, c) * d + col) =
+            make_float2(O[f][2] + add_scale * Add[f][2], O[f][3] + add_scale * Add[f][3]);
+    }
+  };
+  auto quad_sum = [](float x) {
+    x += __shfl_xor_sync(0xffffffffu, x, 1);
+    x += __shfl_xor_sync(0xffffffffu, x, 2);
+    return x;
+  };
+  auto quad_max = [](float x) {
+    x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 1));
+    x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 2));
+    return x;
+  };
+  // key column of fragment element e of tile j
+  auto key = [&](int j, int e) { return 8 * j + 2 * t + (e & 1); };
+  const float zero24[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  // ---- value channel ----
+  stage(0, q, k, v);
+  __syncthreads();
+  float A[NK][4];
+#pragma unroll
+  for (int j = 0; j < NK; ++j) A[j][0] = A[j][1] = A[j][2] = A[j][3] = 0.f;
+  scores(q, k, A);
+  {
+    float mx0 = -INFINITY, mx1 = -INFINITY;
+#pragma unroll
+    for (int j = 0; j < NK; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        A[j][e] = key(j, e) < N ? A[j][e] * sc : -INFINITY;
+        if (e < 2) mx0 = fmaxf(mx0, A[j][e]); else mx1 = fmaxf(mx1, A[j][e]);
+      }
+    mx0 = quad_max(mx0);
+    mx1 = quad_max(mx1);
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int j = 0; j < NK; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float x = key(j, e) < N ? expf(A[j][e] - (e < 2 ? mx0 : mx1)) : 0.f;
+        A[j][e] = x;
+        if (e < 2) s0 += x; else s1 += x;
+      }
+    s0 = quad_sum(s0);
+    s1 = quad_sum(s1);
+    const float i0 = 1.f / s0, i1 = 1.f / s1;
+#pragma unroll
+    for (int j = 0; j < NK; ++j) {
+      A[j][0] *= i0;
+      A[j][1] *= i0;
+      A[j][2] *= i1;
+      A[j][3] *= i1;
+    }
+  }
+  float O[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  pv(A, v, O);
+  store(0, O, 0.f, zero24);
+  if (C == 1) return;
+  float Pqk[NK][4], Psq[NK][4], Pav[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int j = 0; j < NK; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) Pqk[j][e] = Psq[j][e] = 0.f;
+  for (int c = 0; c < n_tan; ++c) {
+    __syncthreads();  // the previous channel's products no longer read qt / kt / vt
+    stage(1 + c, qt, kt, vt);
+    __syncthreads();
+    float S[NK][4];
+#pragma unroll
+    for (int j = 0; j < NK; ++j) S[j][0] = S[j][1] = S[j][2] = S[j][3] = 0.f;
+    scores(qt, k, S);
+    scores(q, kt, S);
+    if (has_lap) scores(qt, kt, Pqk);
+    float l0 = 0.f, l1 = 0.f;
+#pragma unroll
+    for (int j = 0; j < NK; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        S[j][e] *= sc;
+        if (e < 2) l0 = fmaf(A[j][e], S[j][e], l0); else l1 = fmaf(A[j][e], S[j][e], l1);
+      }
+    l0 = quad_sum(l0);
+    l1 = quad_sum(l1);
+#pragma unroll
+    for (int j = 0; j < NK; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float ds = S[j][e] - (e < 2 ? l0 : l1);
+        if (has_lap) Psq[j][e] = fmaf(ds, ds, Psq[j][e]);
+        S[j][e] = A[j][e] * ds;
+      }
+    float Ot[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+    pv(S, v, Ot);
+    pv(A, vt, Ot);
+    if (has_lap) pv(S, vt, Pav);
+    store(1 + c, Ot, 0.f, zero24);
+  }
+  if (!has_lap) return;
+  __syncthreads();
+  stage(C - 1, qt, kt, vt);
+  __syncthreads();
+  float S[NK][4];
+#pragma unroll
+  for (int j = 0; j < NK; ++j) S[j][0] = S[j][1] = S[j][2] = S[j][3] = 0.f;
+  scores(qt, k, S);
+  scores(q, kt, S);
+  float l0 = 0.f, l1 = 0.f;
+#pragma unroll
+  for (int j = 0; j < NK; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      S[j][e] = (S[j][e] + 2.f * Pqk[j][e]) * sc;
+      const float x = A[j][e] * (S[j][e] + Psq[j][e]);
+      if (e < 2) l0 += x; else l1 += x;
+    }
+  l0 = quad_sum(l0);
+  l1 = quad_sum(l1);
+#pragma unroll
+  for (int j = 0; j < NK; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) S[j][e] = A[j][e] * (Psq[j][e] + S[j][e] - (e < 2 ? l0 : l1));
+  float Ol[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  pv(S, v, Ol);
+  pv(A, vt, Ol);
+  store(C - 1, Ol, 2.f, Pav);
+}
+
+template <int NT>
+inline int launch_attention_mma(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
+                                const float* QKV, float* OUT, cudaStream_t st) {
+  k_attention_mma<NT><<<(unsigned)((long long)n_jobs * H), 32 * NT, 0, st>>>(
+      n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT);
+  NQS_CHECK_LAUNCH("k_attention_mma");
+  return NQS_OK;
+}
+
 template <typename T>
 inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
                             const T* QKV, T* OUT, cudaStream_t st) {
   const int hd = d / H;
   const bool aligned = ((uintptr_t)QKV % 16 == 0) && ((uintptr_t)OUT % 16 == 0) &&
                        ((size_t)d * sizeof(T)) % 16 == 0;
+  if constexpr (sizeof(T) == 4) {
+    if (g_attn_mma && C > 1 && hd == kAttMmaHd && N <= 64 && aligned &&
+        C == 1 + n_tan + has_lap) {
+      const float* qf = (const float*)QKV;
+      float* of = (float*)OUT;
+      if (N <= 16) return launch_attention_mma<1>(n_jobs, N, C, n_tan, has_lap, d, H, qf, of, st);
+      if (N <= 32) return launch_attention_mma<2>(n_jobs, N, C, n_tan, has_lap, d, H, qf, of, st);
+      if (N <= 48) return launch_attention_mma<3>(n_jobs, N, C, n_tan, has_lap, d, H, qf, of, st);
+      return launch_attention_mma<4>(n_jobs, N, C, n_tan, has_lap, d, H, qf, of, st);
+    }
+  }
   if (g_attn_cta_small && N <= kAttnTok && C == 1 + n_tan + has_lap) {
     if (hd == 16)
       return launch_attention_cta_ts<T, 16>(n_jobs, N, C, n_tan, has_lap, d, H, QKV, OUT, st);

@@ -206,6 +206,7 @@ _SIGS.update({
     "nqs_set_large_n_kernels": ([c_int], c_int),
     "nqs_set_attention_cta_small": ([c_int], c_int),
     "nqs_set_jacobian_tc": ([c_int], c_int),
+    "nqs_set_attention_mma": ([c_int], c_int),
     "nqs_set_cholesky_dag": ([c_int], c_int),
     "nqs_set_rowgemm_stages": ([c_int], c_int),
     "nqs_mcmc_sweeps_devctr": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,

@@ -161,6 +161,13 @@ int nqs_set_attention_cta_small(int enable);
  * layers stay float32 on the CUDA cores. On a B200 at configuration 2 it saves 2.2 ms of a
  * 14.1 ms Jacobian and moves the MinSR update from 8.4e-4 to 5.2e-3 of the float64 one. */
 int nqs_set_jacobian_tc(int enable);
+/* Implementation selection (no reference counterpart; process-wide): with it on, the attention
+ * of the float32 multi-channel batches (forward-Laplacian local energies, spin-flip gradients;
+ * head width 16, up to 64 tokens) runs on the tensor cores: every product of every channel as
+ * mma.sync m16n8k8 TF32 chains, the probabilities and the Laplacian accumulators held in
+ * accumulator fragments. Value-only passes (sampling, the Jacobian's forward) keep the float32
+ * CUDA-core kernels. */
+int nqs_set_attention_mma(int enable);
 /* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
  * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;
  * 0 restores the default (4). A tuning knob of the multi-instance autotuner. */
