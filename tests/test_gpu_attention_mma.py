@@ -1,7 +1,8 @@
 """Attention of the multi-channel batches on the tensor cores (nqs_set_attention_mma: mma.sync
 TF32 products, accumulator fragments carried across the forward-Laplacian channels) against the
 float32 CUDA-core kernels and the float64 path: local energies (forward-Laplacian batch and
-spin-orbit flips) and log psi, for 16, 26 and 48 electrons (one to three 16-row query tiles)."""
+spin-orbit flips) and log psi, for 16, 26 and 48 electrons (one to three 16-row query tiles).
+The bar is the mixed path's own error against float64 (its TF32 Dense layers)."""
 import numpy as np
 import pytest
 import torch
@@ -37,7 +38,7 @@ def test_tensor_core_attention_local_energy(N, embed, heads):
     assert torch.equal(l_mma, l_f32)
     err_mma = float((e_mma - e64).abs().median())
     err_f32 = float((e_f32 - e64).abs().median())
-    scale = float(e64.abs().median())
-    # TF32 attention: within TF32 accuracy of float64, and the switch moves E_loc by at most that
-    assert err_mma < 1e-3 * max(1.0, scale), (err_mma, err_f32, scale)
-    assert float((e_mma - e_f32).abs().median()) < 1e-3 * max(1.0, scale)
+    # the mixed path's error against float64 comes mostly from its TF32 Dense layers: the TF32
+    # attention may add to it, by less than that error again
+    assert err_mma < 2.0 * err_f32, (err_mma, err_f32)
+    assert float((e_mma - e_f32).abs().median()) < err_f32, (err_mma, err_f32)
