@@ -30,7 +30,7 @@ size_t net_scratch_bytes(const ModelConst& mc, size_t rows) {
 
 bool g_large_n_cta = true;
 bool g_attn_cta_small = false;
-bool g_attn_mma = false;
+bool g_attn_mma = true;
 
 extern "C" int nqs_set_attention_mma(int enable) {
   g_attn_mma = enable != 0;

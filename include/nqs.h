@@ -161,12 +161,14 @@ int nqs_set_attention_cta_small(int enable);
  * layers stay float32 on the CUDA cores. On a B200 at configuration 2 it saves 2.2 ms of a
  * 14.1 ms Jacobian and moves the MinSR update from 8.4e-4 to 5.2e-3 of the float64 one. */
 int nqs_set_jacobian_tc(int enable);
-/* Implementation selection (no reference counterpart; process-wide): with it on, the attention
- * of the float32 multi-channel batches (forward-Laplacian local energies, spin-flip gradients;
- * head width 16, up to 64 tokens) runs on the tensor cores: every product of every channel as
- * mma.sync m16n8k8 TF32 chains, the probabilities and the Laplacian accumulators held in
- * accumulator fragments. Value-only passes (sampling, the Jacobian's forward) keep the float32
- * CUDA-core kernels. */
+/* Implementation selection (no reference counterpart; process-wide, default on): with it on, the
+ * attention of the float32 multi-channel batches (forward-Laplacian local energies, spin-flip
+ * gradients; head width 16, up to 64 tokens) runs on the tensor cores: every product of every
+ * channel as mma.sync m16n8k8 TF32 chains, the probabilities and the Laplacian accumulators held
+ * in accumulator fragments. Value-only passes (sampling, the Jacobian's forward) keep the float32
+ * CUDA-core kernels. On a B200 it takes the local energies of configuration 2 from 48.3 to
+ * 45.4 ms and of configuration 5 (512 walkers) from 454 to 365 ms at unchanged error against the
+ * float64 path; off restores the float32 kernels. */
 int nqs_set_attention_mma(int enable);
 /* Pipeline depth cap of the tensor-core row GEMMs (no reference counterpart; process-wide,
  * read when a launch is enqueued): at most max_stages (2..4) operand tiles in flight per CTA;

@@ -28,7 +28,7 @@ def test_tensor_core_attention_local_energy(N, embed, heads):
             lp = make_logpsi(model, p, precision=prec)
             return lp(R, S).cpu(), make_local_energy(lp, 1.0, 0.7, 0.3)(R, S).cpu()
         finally:
-            _lib.lib().nqs_set_attention_mma(0)
+            _lib.lib().nqs_set_attention_mma(1)
 
     l64, e64 = run("fp64", 0)
     l_mma, e_mma = run("mixed", 1)
