@@ -385,7 +385,7 @@ static int rowgemm_tc_piece(const float* X, int ldx, int rows, int K, const floa
   const size_t conv = bf ? (size_t)(K / 64) * tc::RG_BM * 128 : 0;
   const size_t fixed = panel + conv + 4 * 2 * 4096 + 256 + 1024;
   const size_t stage = (size_t)nkb * tc::RG_BM * 128;
-  const size_t cap = bf ? 227 * 1024 : 200 * 1024;
+  const size_t cap = 227 * 1024;
   int S = (int)std::min<size_t>((size_t)g_rowgemm_stages.load(), (cap - fixed) / stage);
   if (S < 2) {
     set_error("rowgemm_tc: K=%d, N=%d leave room for %d pipeline stages", K, Npad, S);
@@ -396,7 +396,7 @@ static int rowgemm_tc_piece(const float* X, int ldx, int rows, int K, const floa
   static int nsm = 0;
   if (!attr) {
     cudaFuncSetAttribute(tc::k_rowgemm_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
+                         227 * 1024);
     cudaFuncSetAttribute(tc::k_rowgemm_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          227 * 1024);
     int dev = 0;
@@ -440,7 +440,7 @@ static int rowgemm_stages_for(int kp, int np, bool bf) {
   const size_t conv = bf ? (size_t)(kp / 64) * tc::RG_BM * 128 : 0;
   const size_t fixed = panel + conv + 4 * 2 * 4096 + 256 + 1024;
   const size_t stage = (size_t)(kp / tc::RG_KB) * tc::RG_BM * 128;
-  const size_t cap = bf ? 227 * 1024 : 200 * 1024;
+  const size_t cap = 227 * 1024;
   if (fixed + 2 * stage > cap) return 0;
   return (int)std::min<size_t>((size_t)g_rowgemm_stages.load(), (cap - fixed) / stage);
 }
