@@ -10,6 +10,12 @@
 //     lower-triangular part of the tile to T in float64.
 // Every wait is bounded: on time-out the CTA records an error flag, stops issuing, drains what
 // it issued (bounded) and frees its tensor memory.
+//
+// The same pipeline, instantiated with SUB, is the trailing update T -= P P^T of the blocked
+// Cholesky that preconditions the mixed-precision MinSR solve: P's float64 rows are split into a
+// TF32 part and a float32 remainder, stored side by side as [hi | lo] (width 2K), and the k-blocks
+// run over hi hi^T, lo hi^T and hi lo^T (three TF32 products: ~2^-22 relative error against the
+// float64 update, instead of TF32's 2^-11); the epilogue subtracts from the float64 T.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdio>
@@ -63,7 +69,7 @@ __device__ __forceinline__ void tile_coords(int t, int nrt, int* ti, int* tj) {
   }
 }
 
-template <int KIND>
+template <int KIND, bool SUB>
 __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUtensorMap tmap,
                                                     int M, int64_t K, double* __restrict__ T,
                                                     int64_t ldt, int* __restrict__ err,
@@ -84,7 +90,8 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
   tile_coords(t0 + (int)blockIdx.x, (M + BM - 1) / BM, &ti, &tj);
   const int i0 = ti * BM, j0 = tj * BN;
   constexpr int KE = (KIND == 0) ? 64 : 32;  // elements per 128-byte row
-  const int nk = (int)((K + KE - 1) / KE);
+  const int nkh = (int)((K + KE - 1) / KE);  // k-blocks of one pass (SUB: of one half)
+  const int nk = SUB ? 3 * nkh : nkh;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -112,10 +119,16 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
       if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort, wait_limit)) break;
+      int xa = kb * KE, xb = kb * KE;
+      if constexpr (SUB) {  // passes hi.hi, lo.hi, hi.lo; the lo half starts at column K
+        const int seg = kb / nkh, off = (kb - seg * nkh) * KE;
+        xa = (seg == 1 ? (int)K : 0) + off;
+        xb = (seg == 2 ? (int)K : 0) + off;
+      }
       mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
-      tma_load_2d(sA + s * A_BYTES, &tmap, kb * KE, i0, &full[s]);
-      tma_load_2d(sB + s * B_BYTES, &tmap, kb * KE, j0, &full[s]);
-      tma_load_2d(sB + s * B_BYTES + A_BYTES, &tmap, kb * KE, j0 + BM, &full[s]);
+      tma_load_2d(sA + s * A_BYTES, &tmap, xa, i0, &full[s]);
+      tma_load_2d(sB + s * B_BYTES, &tmap, xb, j0, &full[s]);
+      tma_load_2d(sB + s * B_BYTES + A_BYTES, &tmap, xb, j0 + BM, &full[s]);
       issued = kb + 1;
     }
     // drain: every issued stage's loads must have landed before the CTA may exit
@@ -159,7 +172,26 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
             "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
+      if constexpr (SUB) {
+        // T -= acc; a chunk wholly on or below the diagonal as 16-byte read-modify-writes
+        // (the host passes T 16-byte aligned with an even ldt)
+        if (row < M) {
+          double* tr = T + (size_t)row * ldt + j0 + c0;
+          if (j0 + c0 + 15 <= row) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              double2 v = reinterpret_cast<double2*>(tr)[q];
+              v.x -= (double)__uint_as_float(r[2 * q]);
+              v.y -= (double)__uint_as_float(r[2 * q + 1]);
+              reinterpret_cast<double2*>(tr)[q] = v;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+              if (j0 + c0 + q <= row) tr[q] -= (double)__uint_as_float(r[q]);
+          }
+        }
+      } else if (row < M) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const int col = j0 + c0 + q;
@@ -313,9 +345,9 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(tc::k_gram_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(tc::k_gram_tc<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
-    cudaFuncSetAttribute(tc::k_gram_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(tc::k_gram_tc<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
   }
   const int per = std::max(nsm, 1);
@@ -323,12 +355,75 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
   for (int t0 = 0; t0 < tiles; t0 += per) {
     const int nt = std::min(per, tiles - t0);
     if (prec == 1)
-      tc::k_gram_tc<0><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+      tc::k_gram_tc<0, false><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
     else
-      tc::k_gram_tc<1><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+      tc::k_gram_tc<1, false><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
     NQS_CHECK_LAUNCH("k_gram_tc");
   }
   if (g_prof_stop) cudaEventRecord(g_prof_stop, st);
+  return NQS_OK;
+}
+
+namespace tc {
+// Z[r] = [hi | lo] of the float64 row A[r][0..K): hi = v rounded to TF32 (cvt.rna), lo = the
+// float32 of the remainder v - hi. One CTA per row, one thread per column.
+__global__ void k_split_tf32(const double* __restrict__ A, int64_t lda, int K,
+                             float* __restrict__ Z) {
+  const int r = blockIdx.x;
+  for (int c = threadIdx.x; c < K; c += blockDim.x) {
+    const double v = A[(size_t)r * lda + c];
+    uint32_t hb;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"((float)v));
+    const float hi = __uint_as_float(hb);
+    Z[(size_t)r * 2 * K + c] = hi;
+    Z[(size_t)r * 2 * K + K + c] = (float)(v - (double)hi);
+  }
+}
+}  // namespace tc
+
+size_t syrk_split_tf32_scratch_floats(int M, int K) { return (size_t)M * 2 * K; }
+
+// C (lower, float64, M x M, ldc) -= A A^T for A (M x K float64, lda) through the split-TF32
+// tensor-core Gram; Z: syrk_split_tf32_scratch_floats(M, K) floats, 16-byte aligned.
+int syrk_split_tf32(const double* A, int64_t lda, int M, int K, double* C, int64_t ldc, float* Z,
+                    int* err, cudaStream_t st) {
+  if (K % 32 || (reinterpret_cast<uintptr_t>(Z) & 15) || (reinterpret_cast<uintptr_t>(C) & 15) ||
+      (ldc & 1)) {
+    set_error("syrk_split_tf32: K %% 32, scratch or C alignment");
+    return NQS_ERR_INVALID_ARG;
+  }
+  tc::EncodeTiledFn enc = tc::encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return NQS_ERR_CUDA;
+  }
+  tc::k_split_tf32<<<M, 256, 0, st>>>(A, lda, K, Z);
+  NQS_CHECK_LAUNCH("k_split_tf32");
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)(2 * K), (cuuint64_t)M};
+  const cuuint64_t strides[1] = {(cuuint64_t)(2 * K * sizeof(float))};
+  const cuuint32_t box[2] = {32, (cuuint32_t)tc::BM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, Z, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return NQS_ERR_CUDA;
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(tc::k_gram_tc<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::SMEM_BYTES);
+    attr = true;
+  }
+  const int nrt = (M + tc::BM - 1) / tc::BM;
+  int tiles = 0;
+  for (int i = 0; i < nrt; ++i) tiles += i / 2 + 1;
+  // K = 256: the tiles are bound by their read-modify-write of C, so one launch of all of them
+  tc::k_gram_tc<1, true><<<tiles, 128, tc::SMEM_BYTES, st>>>(map, M, K, C, ldc, err,
+                                                              wait_limit_or(tc::WAIT_LIMIT), 0);
+  NQS_CHECK_LAUNCH("k_gram_tc<sub>");
   return NQS_OK;
 }
 

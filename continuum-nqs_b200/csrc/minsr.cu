@@ -624,6 +624,8 @@ __global__ void __launch_bounds__(256) k_panel_update(const double* __restrict__
   }
 }
 
+bool g_chol_tc = true;  // split-TF32 tensor-core trailing updates of a preconditioner factor
+
 // Right-looking blocked Cholesky A = L L^T (lower triangle, in place), two-level: 64-column
 // panels inside 256-column outer blocks. A panel updates only the columns of its own outer block
 // (k_panel_update); the trailing matrix beyond an outer block is updated once, by all of its
@@ -704,10 +706,19 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
       const int nb = (oe - cs - CB + CB - 1) / CB;
       if (nb > 0) pupd(k0, CB, cs + CB, nb);
     } else if (cs + CB < n) {
-      // (c) the deferred trailing update beyond the next panel, by the whole outer block
-      const int m0 = cs + CB;
-      NQS_TRY(dsyrk_lower(A + (size_t)m0 * lda + ob, lda, n - m0, oe - ob, -1.0, 1.0,
-                          A + (size_t)m0 * lda + m0, lda, nullptr, 0, nsm, st));
+      // (c) the deferred trailing update beyond the next panel, by the whole outer block; for
+      //     a preconditioner (pivot floor given) on the tensor cores with split-TF32 operands,
+      //     staged past the diagonal factor's share of the scratch
+      const int m0 = cs + CB, M = n - m0;
+      double* C = A + (size_t)m0 * lda + m0;
+      if (floor_p && g_chol_tc && oe - ob == NB && (lda & 1) == 0 &&
+          (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
+          part_elems >= (size_t)CB * CB + (syrk_split_tf32_scratch_floats(M, NB) + 1) / 2)
+        NQS_TRY(syrk_split_tf32(A + (size_t)m0 * lda + ob, lda, M, NB, C, lda,
+                                reinterpret_cast<float*>(part + CB * CB), bad + 1, st));
+      else
+        NQS_TRY(dsyrk_lower(A + (size_t)m0 * lda + ob, lda, M, oe - ob, -1.0, 1.0, C, lda,
+                            nullptr, 0, nsm, st));
     }
     cudaStreamWaitEvent(st, ev_join[dev], 0);
   }
@@ -1899,6 +1910,11 @@ int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int W, int64
   return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, max_iters, tol, out_dtheta,
                               theta_io, lr, info_dev, 5, damping_out, wsp, wsb,
                               (cudaStream_t)stream);
+}
+
+int nqs_set_cholesky_tc(int enable) {
+  nqs::g_chol_tc = enable != 0;
+  return NQS_OK;
 }
 
 int nqs_set_cholesky_dag(int enable) {

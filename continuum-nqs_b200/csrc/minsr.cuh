@@ -23,5 +23,12 @@ extern bool g_chol_dag;  // nqs_set_cholesky_dag
 
 int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, double* T, int64_t ldt,
                    int* err, cudaStream_t st);
+// C (lower, float64) -= A A^T (A: M x K float64, K a multiple of 32) on the tensor cores with
+// TF32 hi/lo operand splitting (three products, ~2^-22 relative error); Z: scratch of
+// syrk_split_tf32_scratch_floats(M, K) floats, 16-byte aligned; C 16-byte aligned, ldc even.
+size_t syrk_split_tf32_scratch_floats(int M, int K);
+int syrk_split_tf32(const double* A, int64_t lda, int M, int K, double* C, int64_t ldc, float* Z,
+                    int* err, cudaStream_t st);
+extern bool g_chol_tc;  // nqs_set_cholesky_tc
 
 }  // namespace nqs

@@ -191,7 +191,8 @@ int net_forward(const HostModel& hm, const NetW<T>& w, const HeadParams& hp, Job
         g.seg[2] = GemmSeg<T>{bw.wv, bw.bv, d, d, 2 * d, 0};
         NQS_TRY(launch_gemm<T>(g, st));
       }
-      NQS_TRY(launch_attention<T>(cb.n_jobs, N, C, cb.n_tan, cb.has_lap, d, mc.H, Big, Att, st));
+      NQS_TRY(launch_attention<T>(cb.n_jobs, N, C, cb.n_tan, cb.has_lap, d, mc.H, Big, Att, st,
+                                  tcn));
       if (tcn) {
         NQS_TRY(rowgemm_tc((const float*)Att, d, rows, d, w.tc.wo[b], d, d, (const float*)bw.bo,
                            C, (const float*)X, d, (float*)X, d, w.tc.err, st, 0,

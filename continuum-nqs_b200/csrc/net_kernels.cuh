@@ -1433,12 +1433,12 @@ inline int launch_attention_mma(int n_jobs, int N, int C, int n_tan, int has_lap
 
 template <typename T>
 inline int launch_attention(int n_jobs, int N, int C, int n_tan, int has_lap, int d, int H,
-                            const T* QKV, T* OUT, cudaStream_t st) {
+                            const T* QKV, T* OUT, cudaStream_t st, bool tc = false) {
   const int hd = d / H;
   const bool aligned = ((uintptr_t)QKV % 16 == 0) && ((uintptr_t)OUT % 16 == 0) &&
                        ((size_t)d * sizeof(T)) % 16 == 0;
   if constexpr (sizeof(T) == 4) {
-    if (g_attn_mma && C > 1 && hd == kAttMmaHd && N <= 64 && aligned &&
+    if (tc && g_attn_mma && C > 1 && hd == kAttMmaHd && N <= 64 && aligned &&
         C == 1 + n_tan + has_lap) {
       const float* qf = (const float*)QKV;
       float* of = (float*)OUT;

@@ -120,6 +120,13 @@ int nqs_set_wait_limit(unsigned polls);
  * updates before the next step's factor, so the critical path waits behind them (27.3 ms
  * against 22.9 ms at n = 8192 on a B200). */
 int nqs_set_cholesky_dag(int enable);
+/* Implementation selection (no reference counterpart; process-wide, default on): the K = 256
+ * trailing updates of the preconditioner Cholesky in the mixed-precision MinSR solves
+ * (gram_prec 1 / 2) run on the tensor cores, each float64 operand split into a TF32 part and a
+ * float32 remainder (three TF32 products, float32 accumulation over 256 terms: ~1e-6 relative to
+ * the float64 update, against the 1e-4 mean(T_ii) shift the preconditioner already carries).
+ * Off: float64 CUDA-core updates. The float64 solve (gram_prec 0) always uses the latter. */
+int nqs_set_cholesky_tc(int enable);
 /* Self-test of the flag waits (no reference counterpart; used by the failure-detection test):
  * solves L x = v in place (L: float64 [n][n] lower triangular, device; n <= 64 x 255) with the
  * wavefront triangular solve whose 64-row block `dead_block` never publishes its result (-1: all
@@ -163,7 +170,8 @@ int nqs_set_attention_cta_small(int enable);
 int nqs_set_jacobian_tc(int enable);
 /* Implementation selection (no reference counterpart; process-wide, default on): with it on, the
  * attention of the float32 multi-channel batches (forward-Laplacian local energies, spin-flip
- * gradients; head width 16, up to 64 tokens) runs on the tensor cores: every product of every
+ * gradients; head width 16, up to 64 tokens) of the tensor-core network precisions (mixed,
+ * mixed_bf16; not mixed_simt) runs on the tensor cores: every product of every
  * channel as mma.sync m16n8k8 TF32 chains, the probabilities and the Laplacian accumulators held
  * in accumulator fragments. Value-only passes (sampling, the Jacobian's forward) keep the float32
  * CUDA-core kernels. On a B200 it takes the local energies of configuration 2 from 48.3 to
