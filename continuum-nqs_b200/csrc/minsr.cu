@@ -499,19 +499,18 @@ __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int6
     }
     __syncthreads();
   }
-  // L[i][k] = a_ik / sqrt(d_k) (i > k), L[k][k] = sqrt(d_k)
-  for (int idx = tid; idx < b * b; idx += blockDim.x) {
-    const int i = idx / b, k = idx - i * b;
-    if (k <= i) {
-      const double d = dval[k];
-      const bool pos = d > 0.0;
-      const double sd = pos ? sqrt(d) : NAN;
-      L[i][k] = (i == k) ? sd : L[i][k] / sd;
-    }
-  }
+  // L[i][k] = a_ik / sqrt(d_k) (i > k), L[k][k] = sqrt(d_k): one square root and one
+  // reciprocal per column, then products
   if (tid < b) {
     const double d = dval[tid];
-    rdiag[tid] = d > 0.0 ? 1.0 / sqrt(d) : NAN;
+    const double sd = d > 0.0 ? sqrt(d) : NAN;
+    rdiag[tid] = 1.0 / sd;
+    dval[tid] = sd;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < b * b; idx += blockDim.x) {
+    const int i = idx / b, k = idx - i * b;
+    if (k <= i) L[i][k] = (i == k) ? dval[k] : L[i][k] * rdiag[k];
   }
   __syncthreads();
   if (blockIdx.x == 0)
@@ -921,9 +920,11 @@ __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L,
 // through a cooperative launch), without grid barriers:
 //   forward    CTA s:  x_s = D_s (v_s - sum_{t<s} L_st x_t)        (t ascending)
 //   transposed CTA s:  x_s = D_s^T (v_s - sum_{t>s} L_ts^T x_t)    (t descending)
-// CTA s applies each x_t as soon as CTA t has published it (flag[t], release / acquire at GPU
-// scope), with its operand panel L_st already in registers, so the chain costs one flag hop and
-// two 64 x 64 mat-vecs per block. Every wait is bounded: a CTA that gives up records the timeout
+// CTA s walks its dependencies in groups of four blocks: the group's operand panels L_st are
+// loaded into registers first, then one wait on the flag of the group's last block (a block
+// publishes only after all of its own dependencies, so that flag covers the group; release /
+// acquire at GPU scope) and the four x_t are applied in order. The walk thus takes a quarter of
+// the flag round trips, and the chain costs one flag hop and two 64 x 64 mat-vecs per block. Every wait is bounded: a CTA that gives up records the timeout
 // in flag[kTrsvErrSlot], publishes NaN for its block (its dependants then finish at once) and
 // returns. v is overwritten with x. Sums run in a fixed order (deterministic).
 constexpr int kTrsvErrSlot = 255;  // flags[0..254]: blocks; flags[255]: timeout record
@@ -955,7 +956,8 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
   // slot only after every thread has passed iteration it+1's barrier, i.e. has read slot it
   __shared__ int give_up_buf[2];
   bool give_up = false;
-  // forward: output row r = tid / 4, columns q*16 .. q*16+15 (q = tid % 4) of each 64-block;
+  // forward: output row r = tid / 4, columns q, q+4, .., q+60 (q = tid % 4) of each 64-block
+  // (a warp's load covers eight rows' 32-byte segments);
   // transposed: output m = tid % 64 (a column of L), rows q*16 .. q*16+15 (q = tid / 64)
   const int r = transposed ? (tid & 63) : (tid >> 2);
   const int q = transposed ? (tid >> 6) : (tid & 3);
@@ -964,24 +966,30 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
     const double* D = dinv + (size_t)s * CB * CB;
 #pragma unroll
     for (int c = 0; c < 16; ++c)
-      dreg[c] = transposed ? D[(q * 16 + c) * CB + r] : D[r * CB + q * 16 + c];
+      dreg[c] = transposed ? D[(q * 16 + c) * CB + r] : D[r * CB + q + 4 * c];
   }
   double acc = 0.0;
   const int nt = transposed ? nblk - 1 - s : s;  // blocks this row depends on
   // this block's right-hand side: written by no other CTA, read before the wait chain
   const double vs = (tid < bs) ? v[k0 + tid] : 0.0;
   __syncthreads();
-  for (int it = 0; it < nt; ++it) {
-    const int t = transposed ? nblk - 1 - it : it;
-    const int kt = t * CB, bt = min(CB, n - kt);
-    double lreg[16];
+  constexpr int G = 4;
+  for (int it0 = 0, gi = 0; it0 < nt; it0 += G, ++gi) {
+    const int g = min(G, nt - it0);
+    double lreg[G][16];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const int jj = q * 16 + c;
-      lreg[c] = 0.0;
-      if (!transposed && r < bs && jj < bt) lreg[c] = L[(size_t)(k0 + r) * ldl + kt + jj];
-      if (transposed && r < bs && jj < bt) lreg[c] = L[(size_t)(kt + jj) * ldl + k0 + r];
+    for (int u = 0; u < G; ++u) {
+      const int t = transposed ? nblk - 1 - (it0 + u) : it0 + u;
+      const int kt = t * CB, bt = u < g ? min(CB, n - kt) : 0;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        const int jj = transposed ? q * 16 + c : q + 4 * c;
+        lreg[u][c] = 0.0;
+        if (!transposed && r < bs && jj < bt) lreg[u][c] = L[(size_t)(k0 + r) * ldl + kt + jj];
+        if (transposed && r < bs && jj < bt) lreg[u][c] = L[(size_t)(kt + jj) * ldl + k0 + r];
+      }
     }
+    const int t = transposed ? nblk - 1 - (it0 + g - 1) : it0 + g - 1;  // the group's last
     if (tid == 0) {
       int gu = 0;
       uint32_t w = 0;
@@ -992,16 +1000,23 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
         }
         if (w > 64) __nanosleep(64);
       }
-      give_up_buf[it & 1] = gu;
+      give_up_buf[gi & 1] = gu;
     }
     __syncthreads();
-    give_up = give_up_buf[it & 1] != 0;
+    give_up = give_up_buf[gi & 1] != 0;
     if (give_up) break;
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const int jj = q * 16 + c;
-      const double xj = jj < bt ? __ldcg(v + kt + jj) : 0.0;
-      acc = fma(lreg[c], xj, acc);
+    for (int u = 0; u < G; ++u) {
+      if (u < g) {
+        const int tu = transposed ? nblk - 1 - (it0 + u) : it0 + u;
+        const int kt = tu * CB, bt = min(CB, n - kt);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int jj = transposed ? q * 16 + c : q + 4 * c;
+          const double xj = jj < bt ? __ldcg(v + kt + jj) : 0.0;
+          acc = fma(lreg[u][c], xj, acc);
+        }
+      }
     }
   }
   if (give_up) {
@@ -1033,7 +1048,7 @@ __global__ void __launch_bounds__(256) k_trsv_flags(const double* __restrict__ L
   // x_s = D rhs (forward) or D^T rhs (transposed)
   double xs = 0.0;
 #pragma unroll
-  for (int c = 0; c < 16; ++c) xs = fma(dreg[c], rhs[q * 16 + c], xs);
+  for (int c = 0; c < 16; ++c) xs = fma(dreg[c], rhs[transposed ? q * 16 + c : q + 4 * c], xs);
   if (!transposed) {
     xs += __shfl_xor_sync(0xffffffffu, xs, 1);
     xs += __shfl_xor_sync(0xffffffffu, xs, 2);
