@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int6
   __shared__ double L[CB][CB + 1];
   __shared__ double rdiag[CB];
   const int b = min(CB, n - k0);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
   if (blockIdx.x == 0 && prev_k0 >= 0) {  // previous step's diagonal factor into A
     const int bp = min(CB, n - prev_k0);
     for (int idx = tid; idx < bp * bp; idx += blockDim.x) {
@@ -436,7 +436,6 @@ __global__ void __launch_bounds__(256) k_potrf_trsm(double* __restrict__ A, int6
   // rows in registers (lane l: rows j0 + l and j0 + l + 32), unscaled columns a_ik -= a_ic a_kc / d_c
   // and pivots d_c (raised to the floor when below it); then every thread applies the sub-panel's
   // rank-jw update to the trailing block, four threads per row.
-  const int lane = tid & 31;
   for (int j0 = 0; j0 < b; j0 += 8) {
     const int jw = min(8, b - j0);
     if (tid < 32) {
@@ -627,37 +626,47 @@ bool g_chol_tc = true;  // split-TF32 tensor-core trailing updates of a precondi
 
 // Right-looking blocked Cholesky A = L L^T (lower triangle, in place), two-level: 64-column
 // panels inside 256-column outer blocks. A panel updates only the columns of its own outer block
-// (k_panel_update); the trailing matrix beyond an outer block is updated once, by all of its
-// panels together (dsyrk with K = 256), so the trailing matrix is read and written once per
-// outer block instead of once per panel. One step of look-ahead: after a panel, the next 64
-// columns are updated first (at an outer-block end, by the whole outer block) and the next
-// diagonal factor + panel solve run on a side stream while the rest of the step's updates run on
-// the caller's stream (they touch disjoint columns).
-// part: scratch of at least 64 x 64 doubles for the diagonal factor.
+// (k_panel_update); the matrix beyond an outer block is updated once, by all of its panels
+// together (K = 256), so it is read and written once per outer block instead of once per panel.
+// Three streams:
+//   critical (highest priority): per panel, the update of the next 64 columns (at an
+//     outer-block end by the whole outer block) and the next diagonal factor + panel solve;
+//   bulk (the caller's stream): the rest of the outer block's columns by the panel, and at an
+//     outer-block end the next outer block's remaining columns by the finished one;
+//   far: at an outer-block end, the update of everything beyond the next outer block (the
+//     large SYRK), which the next outer block's four panels do not touch, so it runs under them
+//     and is waited for only at the next outer-block end.
+// Each stream writes columns no other stream reads or writes meanwhile; events order the rest.
+// part: scratch of at least 64 x 64 doubles for the diagonal factor (and, for the tensor-core
+// updates, the split operands after it).
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
   if (!part || part_elems < (size_t)CB * CB) {
     set_error("cholesky_lower: scratch of %zu doubles < %d", part_elems, CB * CB);
     return NQS_ERR_WORKSPACE;
   }
-  // side stream and two fork / join events per device, created once
-  static cudaStream_t side[64] = {};
-  static cudaEvent_t ev_fork[64] = {}, ev_join[64] = {};
+  // streams and events per device, created once
+  enum { EV_FORK, EV_BULK, EV_CRIT, EV_FAR, EV_JOIN, EV_JOIN_FAR, N_EV };
+  static cudaStream_t crit_s[64] = {}, far_s[64] = {};
+  static cudaEvent_t evs[64][N_EV] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return NQS_ERR_UNSUPPORTED;
-  if (!side[dev]) {
-    // highest priority: the look-ahead CTAs are scheduled as soon as trailing-update CTAs retire
+  if (!crit_s[dev]) {
+    // highest priority: the critical CTAs are scheduled as soon as update CTAs retire
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    if (cudaStreamCreateWithPriority(&side[dev], cudaStreamNonBlocking, hi) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev_fork[dev], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev_join[dev], cudaEventDisableTiming) != cudaSuccess) {
-      set_error("cholesky_lower: side stream / events");
+    bool ok = cudaStreamCreateWithPriority(&crit_s[dev], cudaStreamNonBlocking, hi) == cudaSuccess &&
+              cudaStreamCreateWithPriority(&far_s[dev], cudaStreamNonBlocking, lo) == cudaSuccess;
+    for (int e = 0; e < N_EV && ok; ++e)
+      ok = cudaEventCreateWithFlags(&evs[dev][e], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      set_error("cholesky_lower: streams / events");
       return NQS_ERR_CUDA;
     }
   }
-  cudaStream_t s2 = side[dev];
+  cudaStream_t sc = crit_s[dev], sf = far_s[dev];
+  cudaEvent_t* ev = evs[dev];
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_panel_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -675,52 +684,73 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
   };
   constexpr int NB = 4 * CB;  // outer block
   // columns [c0, c0 + 64 ncb) updated by the panel of columns [p0, p0 + kw)
-  auto pupd = [&](int p0, int kw, int c0, int ncb) {
+  auto pupd = [&](int p0, int kw, int c0, int ncb, cudaStream_t s) {
     const int rest = n - c0;
     k_panel_update<<<dim3((rest + CB - 1) / CB, ncb), 256, sizeof(double) * 2 * CB * (CB + 1),
-                     st>>>(A + (size_t)c0 * lda + p0, lda, rest, A + (size_t)c0 * lda + c0, lda,
-                           kw);
+                     s>>>(A + (size_t)c0 * lda + p0, lda, rest, A + (size_t)c0 * lda + c0, lda,
+                          kw);
     NQS_CHECK_LAUNCH("k_panel_update");
+    return NQS_OK;
   };
-  NQS_TRY(potrf(0, -1, st));
+  // rows / columns [m0, n) -= panel [ob, ob + 256) of the same rows: on the tensor cores with
+  // split-TF32 operands for a preconditioner (pivot floor given), staged past the diagonal
+  // factor's share of the scratch; float64 CUDA cores otherwise
+  auto far_update = [&](int ob, int m0, cudaStream_t s) -> int {
+    const int M = n - m0;
+    double* C = A + (size_t)m0 * lda + m0;
+    if (floor_p && g_chol_tc && (lda & 1) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
+        part_elems >= (size_t)CB * CB + (syrk_split_tf32_scratch_floats(M, NB) + 1) / 2)
+      return syrk_split_tf32(A + (size_t)m0 * lda + ob, lda, M, NB, C, lda,
+                             reinterpret_cast<float*>(part + CB * CB), bad + 1, s);
+    return dsyrk_lower(A + (size_t)m0 * lda + ob, lda, M, NB, -1.0, 1.0, C, lda, nullptr, 0,
+                       nsm, s);
+  };
+  cudaEventRecord(ev[EV_FORK], st);
+  cudaStreamWaitEvent(sc, ev[EV_FORK], 0);
+  cudaStreamWaitEvent(sf, ev[EV_FORK], 0);
+  NQS_TRY(potrf(0, -1, sc));
+  cudaEventRecord(ev[EV_BULK], st);
+  bool far_pending = false;
   int last = 0;
   for (int k0 = 0; k0 + CB < n; k0 += CB) {
     const int ob = (k0 / NB) * NB, oe = std::min(n, ob + NB);  // this panel's outer block
     const int cs = k0 + CB;  // the next panel's first column
     const bool boundary = cs == oe;
-    // (a) the next 64 columns: by this panel, or at an outer-block end by the whole outer block
-    //     (whose updates of later columns were deferred)
-    if (boundary)
-      pupd(ob, oe - ob, cs, 1);
-    else
-      pupd(k0, CB, cs, 1);
-    // next diagonal factor + panel solve on the side stream
-    cudaEventRecord(ev_fork[dev], st);
-    cudaStreamWaitEvent(s2, ev_fork[dev], 0);
-    NQS_TRY(potrf(cs, k0, s2));
-    cudaEventRecord(ev_join[dev], s2);
-    last = cs;
-    if (!boundary) {
-      // (b) the rest of this outer block's columns, by this panel
-      const int nb = (oe - cs - CB + CB - 1) / CB;
-      if (nb > 0) pupd(k0, CB, cs + CB, nb);
-    } else if (cs + CB < n) {
-      // (c) the deferred trailing update beyond the next panel, by the whole outer block; for
-      //     a preconditioner (pivot floor given) on the tensor cores with split-TF32 operands,
-      //     staged past the diagonal factor's share of the scratch
-      const int m0 = cs + CB, M = n - m0;
-      double* C = A + (size_t)m0 * lda + m0;
-      if (floor_p && g_chol_tc && oe - ob == NB && (lda & 1) == 0 &&
-          (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
-          part_elems >= (size_t)CB * CB + (syrk_split_tf32_scratch_floats(M, NB) + 1) / 2)
-        NQS_TRY(syrk_split_tf32(A + (size_t)m0 * lda + ob, lda, M, NB, C, lda,
-                                reinterpret_cast<float*>(part + CB * CB), bad + 1, st));
-      else
-        NQS_TRY(dsyrk_lower(A + (size_t)m0 * lda + ob, lda, M, oe - ob, -1.0, 1.0, C, lda,
-                            nullptr, 0, nsm, st));
+    if (boundary) {
+      // the next outer block lies in the previous far update's region
+      if (far_pending) {
+        cudaStreamWaitEvent(sc, ev[EV_FAR], 0);
+        cudaStreamWaitEvent(st, ev[EV_FAR], 0);
+      }
+      NQS_TRY(pupd(ob, oe - ob, cs, 1, sc));  // the next 64 columns by the whole outer block
+    } else {
+      cudaStreamWaitEvent(sc, ev[EV_BULK], 0);  // earlier panels' updates of these columns
+      NQS_TRY(pupd(k0, CB, cs, 1, sc));         // the next 64 columns by this panel
     }
-    cudaStreamWaitEvent(st, ev_join[dev], 0);
+    cudaEventRecord(ev[EV_CRIT], sc);  // this panel's columns final, the next panel's updated
+    NQS_TRY(potrf(cs, k0, sc));
+    last = cs;
+    cudaStreamWaitEvent(st, ev[EV_CRIT], 0);
+    if (!boundary) {
+      const int nb = (oe - cs - CB + CB - 1) / CB;  // the rest of this outer block's columns
+      if (nb > 0) NQS_TRY(pupd(k0, CB, cs + CB, nb, st));
+    } else if (cs + CB < n) {
+      const int oe2 = std::min(n, cs + NB);
+      const int nb = (oe2 - cs - CB + CB - 1) / CB;  // the rest of the next outer block
+      if (nb > 0) NQS_TRY(pupd(ob, oe - ob, cs + CB, nb, st));
+      if (oe2 < n) {
+        cudaStreamWaitEvent(sf, ev[EV_CRIT], 0);
+        NQS_TRY(far_update(ob, oe2, sf));
+        cudaEventRecord(ev[EV_FAR], sf);
+        far_pending = true;
+      }
+    }
+    cudaEventRecord(ev[EV_BULK], st);
   }
+  cudaEventRecord(ev[EV_JOIN], sc);
+  cudaStreamWaitEvent(st, ev[EV_JOIN], 0);
+  cudaEventRecord(ev[EV_JOIN_FAR], sf);
+  cudaStreamWaitEvent(st, ev[EV_JOIN_FAR], 0);
   k_store_diag<<<1, 256, 0, st>>>(A, lda, last, n, part);
   NQS_CHECK_LAUNCH("k_store_diag");
   return NQS_OK;
@@ -1560,7 +1590,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_alpha(int n, const double* 
                                                            const double* __restrict__ qn,
                                                            double* __restrict__ y,
                                                            double* __restrict__ r,
-                                                           const double* __restrict__ pcg,
+                                                           double* __restrict__ pcg,
                                                            int* __restrict__ it_info) {
   if (it_info[0]) return;
   __shared__ double red[33];
@@ -1576,6 +1606,25 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_alpha(int n, const double* 
     y[i] = fma(alpha, p[i], y[i]);
     r[i] = fma(alpha, qn[i], r[i]);
   }
+  if (threadIdx.x == 0) pcg[2] = alpha;
+}
+
+// g += alpha (O - mu)^T p alongside y += alpha p, so that g = (O - mu)^T y at every step without
+// a pass over O at the end (skipped exactly when k_pcg_alpha left y unchanged)
+__global__ void k_pcg_push(int64_t K, const double* __restrict__ u, const double* __restrict__ pcg,
+                           double* __restrict__ g, const int* __restrict__ it_info) {
+  if (it_info[0]) return;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < K) g[k] = fma(pcg[2], u[k], g[k]);
+}
+
+// the direction from g = (O - mu)^T y: out = g and / or theta -= lr g
+__global__ void k_pcg_finish(int64_t K, const double* __restrict__ g, double* __restrict__ out,
+                             double* __restrict__ theta, double lr) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  if (out) out[k] = g[k];
+  if (theta) theta[k] -= lr * g[k];
 }
 
 // z <- r (the triangular solves then overwrite z with M^-1 r)
@@ -1610,16 +1659,17 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_beta(int n, const double* _
 template <typename TO>
 static int solve_pcg(const double* L, int M, int Mh, int64_t K, const TO* O, const double* mu,
                      double lam, const double* b, double* y, double* r, double* z, double* p,
-                     double* q, double* pcg, int* it_info, double* tmpK, double* xb, int max_it,
-                     double tol, double* part, size_t part_elems, cudaStream_t st) {
+                     double* q, double* pcg, int* it_info, double* tmpK, double* g, double* xb,
+                     int max_it, double tol, double* part, size_t part_elems, cudaStream_t st) {
   double* dinv = xb + 2 * CB;
+  const unsigned kb = (unsigned)((K + 255) / 256);
   NQS_TRY(trtri_diag(L, M, M, dinv, st));
   // y0 = M^-1 b, r0 = b - A y0, z0 = M^-1 r0
   cudaMemcpyAsync(y, b, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
   NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 0, st));
   NQS_TRY(trsv_grid(L, M, M, dinv, y, xb, 1, st));
-  NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, tmpK, nullptr, nullptr, 0.0, part, part_elems, st));
-  NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, b, lam, nullptr, y, r, st));
+  NQS_TRY(gemv_t<TO>(O, M, Mh, K, mu, y, g, nullptr, nullptr, 0.0, part, part_elems, st));
+  NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, g, b, lam, nullptr, y, r, st));
   cudaMemcpyAsync(z, r, sizeof(double) * M, cudaMemcpyDeviceToDevice, st);
   NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 0, st));
   NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 1, st));
@@ -1632,6 +1682,8 @@ static int solve_pcg(const double* L, int M, int Mh, int64_t K, const TO* O, con
     NQS_TRY(gemv_n_resid<TO>(O, M, Mh, K, mu, tmpK, nullptr, lam, nullptr, p, q, st, it_info));
     k_pcg_alpha<<<1, kPcgThreads, 0, st>>>(M, p, q, y, r, pcg, it_info);
     NQS_CHECK_LAUNCH("k_pcg_alpha");
+    k_pcg_push<<<kb, 256, 0, st>>>(K, tmpK, pcg, g, it_info);
+    NQS_CHECK_LAUNCH("k_pcg_push");
     k_pcg_copy<<<(M + 255) / 256, 256, 0, st>>>(M, r, z, it_info);
     NQS_CHECK_LAUNCH("k_pcg_copy");
     NQS_TRY(trsv_grid(L, M, M, dinv, z, xb, 0, st, it_info));
@@ -1889,19 +1941,27 @@ static int minsr_direction_impl(void* O, int o_dtype, const double* eps, int W, 
       NQS_TRY(solve_refined<float>(T, n, W, P, (const float*)Oop, mu_op, lam, nullptr, et, y, r,
                                    tmpK, tmpK_lo, xb, max_it, part, part_elems, st));
   } else {
+    // the conjugate gradients keep tmpK_lo = (O - mu)^T y, so the direction needs no further
+    // pass over O
     if (op_dtype == 0)
       NQS_TRY(solve_pcg<double>(T, n, W, P, (const double*)Oop, mu_op, lam, et, y, r, z, pp, q,
-                                pcg, bad + 4, tmpK, xb, max_it, tol, part, part_elems, st));
+                                pcg, bad + 4, tmpK, tmpK_lo, xb, max_it, tol, part, part_elems,
+                                st));
     else
       NQS_TRY(solve_pcg<float>(T, n, W, P, (const float*)Oop, mu_op, lam, et, y, r, z, pp, q, pcg,
-                               bad + 4, tmpK, xb, max_it, tol, part, part_elems, st));
+                               bad + 4, tmpK, tmpK_lo, xb, max_it, tol, part, part_elems, st));
+    k_pcg_finish<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(P, tmpK_lo, out_dtheta, theta_io,
+                                                             lr);
+    NQS_CHECK_LAUNCH("k_pcg_finish");
   }
-  if (op_dtype == 0)
-    NQS_TRY(gemv_t<double>((const double*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io,
-                           lr, part, part_elems, st));
-  else
-    NQS_TRY(gemv_t<float>((const float*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io, lr,
-                          part, part_elems, st));
+  if (gram_prec == 0) {
+    if (op_dtype == 0)
+      NQS_TRY(gemv_t<double>((const double*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr,
+                             theta_io, lr, part, part_elems, st));
+    else
+      NQS_TRY(gemv_t<float>((const float*)Oop, n, W, P, mu_op, y, out_dtheta, nullptr, theta_io,
+                            lr, part, part_elems, st));
+  }
   if (info_dev) {
     k_pack_info<<<1, 32, 0, st>>>(bad, info_dev, n_info);
     NQS_CHECK_LAUNCH("k_pack_info");
