@@ -626,47 +626,37 @@ bool g_chol_tc = true;  // split-TF32 tensor-core trailing updates of a precondi
 
 // Right-looking blocked Cholesky A = L L^T (lower triangle, in place), two-level: 64-column
 // panels inside 256-column outer blocks. A panel updates only the columns of its own outer block
-// (k_panel_update); the matrix beyond an outer block is updated once, by all of its panels
-// together (K = 256), so it is read and written once per outer block instead of once per panel.
-// Three streams:
-//   critical (highest priority): per panel, the update of the next 64 columns (at an
-//     outer-block end by the whole outer block) and the next diagonal factor + panel solve;
-//   bulk (the caller's stream): the rest of the outer block's columns by the panel, and at an
-//     outer-block end the next outer block's remaining columns by the finished one;
-//   far: at an outer-block end, the update of everything beyond the next outer block (the
-//     large SYRK), which the next outer block's four panels do not touch, so it runs under them
-//     and is waited for only at the next outer-block end.
-// Each stream writes columns no other stream reads or writes meanwhile; events order the rest.
-// part: scratch of at least 64 x 64 doubles for the diagonal factor (and, for the tensor-core
-// updates, the split operands after it).
+// (k_panel_update); the trailing matrix beyond an outer block is updated once, by all of its
+// panels together (dsyrk with K = 256), so the trailing matrix is read and written once per
+// outer block instead of once per panel. One step of look-ahead: after a panel, the next 64
+// columns are updated first (at an outer-block end, by the whole outer block) and the next
+// diagonal factor + panel solve run on a side stream while the rest of the step's updates run on
+// the caller's stream (they touch disjoint columns).
+// part: scratch of at least 64 x 64 doubles for the diagonal factor.
 int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t part_elems,
                    int nsm, cudaStream_t st, const double* floor_p = nullptr) {
   if (!part || part_elems < (size_t)CB * CB) {
     set_error("cholesky_lower: scratch of %zu doubles < %d", part_elems, CB * CB);
     return NQS_ERR_WORKSPACE;
   }
-  // streams and events per device, created once
-  enum { EV_FORK, EV_BULK, EV_CRIT, EV_FAR, EV_JOIN, EV_JOIN_FAR, N_EV };
-  static cudaStream_t crit_s[64] = {}, far_s[64] = {};
-  static cudaEvent_t evs[64][N_EV] = {};
+  // side stream and two fork / join events per device, created once
+  static cudaStream_t side[64] = {};
+  static cudaEvent_t ev_fork[64] = {}, ev_join[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return NQS_ERR_UNSUPPORTED;
-  if (!crit_s[dev]) {
-    // highest priority: the critical CTAs are scheduled as soon as update CTAs retire
+  if (!side[dev]) {
+    // highest priority: the look-ahead CTAs are scheduled as soon as trailing-update CTAs retire
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    bool ok = cudaStreamCreateWithPriority(&crit_s[dev], cudaStreamNonBlocking, hi) == cudaSuccess &&
-              cudaStreamCreateWithPriority(&far_s[dev], cudaStreamNonBlocking, lo) == cudaSuccess;
-    for (int e = 0; e < N_EV && ok; ++e)
-      ok = cudaEventCreateWithFlags(&evs[dev][e], cudaEventDisableTiming) == cudaSuccess;
-    if (!ok) {
-      set_error("cholesky_lower: streams / events");
+    if (cudaStreamCreateWithPriority(&side[dev], cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork[dev], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join[dev], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("cholesky_lower: side stream / events");
       return NQS_ERR_CUDA;
     }
   }
-  cudaStream_t sc = crit_s[dev], sf = far_s[dev];
-  cudaEvent_t* ev = evs[dev];
+  cudaStream_t s2 = side[dev];
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_panel_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -684,73 +674,53 @@ int cholesky_lower(double* A, int64_t lda, int n, int* bad, double* part, size_t
   };
   constexpr int NB = 4 * CB;  // outer block
   // columns [c0, c0 + 64 ncb) updated by the panel of columns [p0, p0 + kw)
-  auto pupd = [&](int p0, int kw, int c0, int ncb, cudaStream_t s) {
+  auto pupd = [&](int p0, int kw, int c0, int ncb) {
     const int rest = n - c0;
     k_panel_update<<<dim3((rest + CB - 1) / CB, ncb), 256, sizeof(double) * 2 * CB * (CB + 1),
-                     s>>>(A + (size_t)c0 * lda + p0, lda, rest, A + (size_t)c0 * lda + c0, lda,
-                          kw);
+                     st>>>(A + (size_t)c0 * lda + p0, lda, rest, A + (size_t)c0 * lda + c0, lda,
+                           kw);
     NQS_CHECK_LAUNCH("k_panel_update");
     return NQS_OK;
   };
-  // rows / columns [m0, n) -= panel [ob, ob + 256) of the same rows: on the tensor cores with
-  // split-TF32 operands for a preconditioner (pivot floor given), staged past the diagonal
-  // factor's share of the scratch; float64 CUDA cores otherwise
-  auto far_update = [&](int ob, int m0, cudaStream_t s) -> int {
-    const int M = n - m0;
-    double* C = A + (size_t)m0 * lda + m0;
-    if (floor_p && g_chol_tc && (lda & 1) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
-        part_elems >= (size_t)CB * CB + (syrk_split_tf32_scratch_floats(M, NB) + 1) / 2)
-      return syrk_split_tf32(A + (size_t)m0 * lda + ob, lda, M, NB, C, lda,
-                             reinterpret_cast<float*>(part + CB * CB), bad + 1, s);
-    return dsyrk_lower(A + (size_t)m0 * lda + ob, lda, M, NB, -1.0, 1.0, C, lda, nullptr, 0,
-                       nsm, s);
-  };
-  cudaEventRecord(ev[EV_FORK], st);
-  cudaStreamWaitEvent(sc, ev[EV_FORK], 0);
-  cudaStreamWaitEvent(sf, ev[EV_FORK], 0);
-  NQS_TRY(potrf(0, -1, sc));
-  cudaEventRecord(ev[EV_BULK], st);
-  bool far_pending = false;
+  NQS_TRY(potrf(0, -1, st));
   int last = 0;
   for (int k0 = 0; k0 + CB < n; k0 += CB) {
     const int ob = (k0 / NB) * NB, oe = std::min(n, ob + NB);  // this panel's outer block
     const int cs = k0 + CB;  // the next panel's first column
     const bool boundary = cs == oe;
-    if (boundary) {
-      // the next outer block lies in the previous far update's region
-      if (far_pending) {
-        cudaStreamWaitEvent(sc, ev[EV_FAR], 0);
-        cudaStreamWaitEvent(st, ev[EV_FAR], 0);
-      }
-      NQS_TRY(pupd(ob, oe - ob, cs, 1, sc));  // the next 64 columns by the whole outer block
-    } else {
-      cudaStreamWaitEvent(sc, ev[EV_BULK], 0);  // earlier panels' updates of these columns
-      NQS_TRY(pupd(k0, CB, cs, 1, sc));         // the next 64 columns by this panel
-    }
-    cudaEventRecord(ev[EV_CRIT], sc);  // this panel's columns final, the next panel's updated
-    NQS_TRY(potrf(cs, k0, sc));
+    // (a) the next 64 columns: by this panel, or at an outer-block end by the whole outer block
+    //     (whose updates of later columns were deferred)
+    if (boundary)
+      NQS_TRY(pupd(ob, oe - ob, cs, 1));
+    else
+      NQS_TRY(pupd(k0, CB, cs, 1));
+    // next diagonal factor + panel solve on the side stream
+    cudaEventRecord(ev_fork[dev], st);
+    cudaStreamWaitEvent(s2, ev_fork[dev], 0);
+    NQS_TRY(potrf(cs, k0, s2));
+    cudaEventRecord(ev_join[dev], s2);
     last = cs;
-    cudaStreamWaitEvent(st, ev[EV_CRIT], 0);
     if (!boundary) {
-      const int nb = (oe - cs - CB + CB - 1) / CB;  // the rest of this outer block's columns
-      if (nb > 0) NQS_TRY(pupd(k0, CB, cs + CB, nb, st));
+      // (b) the rest of this outer block's columns, by this panel
+      const int nb = (oe - cs - CB + CB - 1) / CB;
+      if (nb > 0) NQS_TRY(pupd(k0, CB, cs + CB, nb));
     } else if (cs + CB < n) {
-      const int oe2 = std::min(n, cs + NB);
-      const int nb = (oe2 - cs - CB + CB - 1) / CB;  // the rest of the next outer block
-      if (nb > 0) NQS_TRY(pupd(ob, oe - ob, cs + CB, nb, st));
-      if (oe2 < n) {
-        cudaStreamWaitEvent(sf, ev[EV_CRIT], 0);
-        NQS_TRY(far_update(ob, oe2, sf));
-        cudaEventRecord(ev[EV_FAR], sf);
-        far_pending = true;
-      }
+      // (c) the deferred trailing update beyond the next panel, by the whole outer block; for
+      //     a preconditioner (pivot floor given) on the tensor cores with split-TF32 operands,
+      //     staged past the diagonal factor's share of the scratch
+      const int m0 = cs + CB, M = n - m0;
+      double* C = A + (size_t)m0 * lda + m0;
+      if (floor_p && g_chol_tc && oe - ob == NB && (lda & 1) == 0 &&
+          (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
+          part_elems >= (size_t)CB * CB + (syrk_split_tf32_scratch_floats(M, NB) + 1) / 2)
+        NQS_TRY(syrk_split_tf32(A + (size_t)m0 * lda + ob, lda, M, NB, C, lda,
+                                reinterpret_cast<float*>(part + CB * CB), bad + 1, st));
+      else
+        NQS_TRY(dsyrk_lower(A + (size_t)m0 * lda + ob, lda, M, oe - ob, -1.0, 1.0, C, lda,
+                            nullptr, 0, nsm, st));
     }
-    cudaEventRecord(ev[EV_BULK], st);
+    cudaStreamWaitEvent(st, ev_join[dev], 0);
   }
-  cudaEventRecord(ev[EV_JOIN], sc);
-  cudaStreamWaitEvent(st, ev[EV_JOIN], 0);
-  cudaEventRecord(ev[EV_JOIN_FAR], sf);
-  cudaStreamWaitEvent(st, ev[EV_JOIN_FAR], 0);
   k_store_diag<<<1, 256, 0, st>>>(A, lda, last, n, part);
   NQS_CHECK_LAUNCH("k_store_diag");
   return NQS_OK;
