@@ -210,6 +210,164 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const __grid_constant__ CUte
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Wide tiles: one CTA computes a 256 x 256 tile of T as two M = 128 accumulators (TMEM columns
+// 0-255 and 256-511) against the same 256-row B panel, so every operand byte brought into shared
+// memory feeds twice the MMA work of a 128 x 256 tile (L2 -> SM traffic per flop down by a
+// third); 3-stage ring of 64 KB stages.
+constexpr int WBM = 256, WSTAGES = 3;
+constexpr int WA_BYTES = WBM * ROW_BYTES;  // 32 KB
+constexpr int WSTAGE_BYTES = WA_BYTES + B_BYTES;
+constexpr int WSMEM_BYTES = WSTAGES * WSTAGE_BYTES + 1024 + 256;
+constexpr uint32_t WTMEM_COLS = 512;
+
+// lower-triangular 256 x 256 tiles (row tile ti needs column tiles 0 .. ti), bands of GRAM_BAND
+// row tiles, inside a band column tile by column tile
+__device__ __forceinline__ void tile_coords_sq(int t, int nrt, int* ti, int* tj) {
+  *ti = 0;
+  *tj = 0;
+  for (int g0 = 0; g0 < nrt; g0 += GRAM_BAND) {
+    const int g1 = min(nrt, g0 + GRAM_BAND);
+    int cnt = 0;
+    for (int i = g0; i < g1; ++i) cnt += i + 1;
+    if (t >= cnt) {
+      t -= cnt;
+      continue;
+    }
+    for (int j = 0; j < g1; ++j) {
+      const int lo = max(g0, j), c = g1 - lo;
+      if (t < c) {
+        *ti = lo + t;
+        *tj = j;
+        return;
+      }
+      t -= c;
+    }
+    return;
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128, 1) k_gram_tc_wide(const __grid_constant__ CUtensorMap tmap,
+                                                         int M, int64_t K, double* __restrict__ T,
+                                                         int64_t ldt, int* __restrict__ err,
+                                                         uint32_t wait_limit, int t0) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + WSTAGES * WSTAGE_BYTES);
+  uint64_t* empty = full + WSTAGES;
+  uint64_t* done = empty + WSTAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int ti, tj;
+  tile_coords_sq(t0 + (int)blockIdx.x, (M + WBM - 1) / WBM, &ti, &tj);
+  const int i0 = ti * WBM, j0 = tj * BN;
+  constexpr int KE = (KIND == 0) ? 64 : 32;
+  const int nk = (int)((K + KE - 1) / KE);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < WSTAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(WTMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer: A rows i0 .. i0 + 255, B rows j0 .. j0 + 255 ----------------
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % WSTAGES;
+      if (kb >= WSTAGES && !mbar_wait(&empty[s], ((kb / WSTAGES) - 1) & 1, abort, wait_limit))
+        break;
+      uint8_t* st = smem + s * WSTAGE_BYTES;
+      mbar_expect_tx(&full[s], WSTAGE_BYTES);
+      tma_load_2d(st, &tmap, kb * KE, i0, &full[s]);
+      tma_load_2d(st + A_BYTES, &tmap, kb * KE, i0 + BM, &full[s]);
+      tma_load_2d(st + WA_BYTES, &tmap, kb * KE, j0, &full[s]);
+      tma_load_2d(st + WA_BYTES + A_BYTES, &tmap, kb * KE, j0 + BM, &full[s]);
+      issued = kb + 1;
+    }
+    for (int kb = (issued > WSTAGES ? issued - WSTAGES : 0); kb < issued; ++kb)
+      mbar_wait(&full[kb % WSTAGES], (kb / WSTAGES) & 1, abort, wait_limit);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer: two accumulators share each B operand ----------------
+    constexpr uint32_t id = idesc<KIND>();
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % WSTAGES;
+      if (!mbar_wait(&full[s], (kb / WSTAGES) & 1, abort, wait_limit)) break;
+      fence_after();
+      const uint8_t* a = smem + s * WSTAGE_BYTES;
+      const uint8_t* b = a + WA_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const uint32_t acc = (kb | kk) != 0 ? 1u : 0u;
+        const uint64_t db = make_desc(b + kk * 32);
+        mma<KIND>(tmem, make_desc(a + kk * 32), db, id, acc);
+        mma<KIND>(tmem + 256, make_desc(a + A_BYTES + kk * 32), db, id, acc);
+      }
+      mma_commit(&empty[s]);
+    }
+    mma_commit(done);
+  }
+  // ---------------- epilogue (all 4 warps, both halves) ----------------
+  __syncwarp();
+  const bool ok = mbar_wait(done, 0, abort, wait_limit);
+  fence_after();
+  const bool go = __all_sync(0xffffffffu, ok && !*abort);
+  if (go) {
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const int rbase = i0 + h * BM + warp * 32;
+      const int row = rbase + lane;
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        if (j0 + c0 > rbase + 31) break;  // warp-uniform: nothing on or below the diagonal
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * 256 + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+            "%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+              "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < M) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int col = j0 + c0 + q;
+            if (col <= row) T[(size_t)row * ldt + col] = (double)__uint_as_float(r[q]);
+          }
+        }
+      }
+    }
+  }
+  if (*abort && threadIdx.x == 0) atomicExch(err, 1);
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(WTMEM_COLS));
+  }
+}
+
 // centre and convert: D[r][p] = O[r][p] - mu[half][p] (p < P), zero padding up to ldd
 template <typename TO, typename TD>
 __global__ void k_center_cvt(const TO* __restrict__ O, int W, int64_t P, int64_t ldd,
@@ -306,6 +464,8 @@ static int center_cvt(const void* O, int o_dtype, int W, int M, int64_t P, int64
   return NQS_OK;
 }
 
+bool g_gram_wide = true;  // nqs_set_gram_wide
+
 // Encode the tensor map and launch the Gram on an operand already in D (rows M, ld ldd).
 int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, double* T, int64_t ldt,
                    int* err, cudaStream_t st) {
@@ -333,10 +493,12 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
     return NQS_ERR_CUDA;
   }
-  const int nrt = (M + tc::BM - 1) / tc::BM;
+  const bool wide = g_gram_wide && M > tc::WBM;
+  const int nrt = (M + (wide ? tc::WBM : tc::BM) - 1) / (wide ? tc::WBM : tc::BM);
   int tiles = 0;
-  for (int i = 0; i < nrt; ++i) tiles += i / 2 + 1;
+  for (int i = 0; i < nrt; ++i) tiles += wide ? i + 1 : i / 2 + 1;
   // every column tile must start inside the matrix: col tile tj <= floor(ti/2) => j0 <= i0
+  // (wide: tj <= ti)
   if (g_prof_start) cudaEventRecord(g_prof_start, st);
   // one launch per round of one tile per SM: the CTAs of a round start together and stream K
   // in step, so the operand rows they share are read from DRAM about once per round
@@ -349,12 +511,20 @@ int gram_tc_launch(const void* D, int prec, int M, int64_t K, int64_t ldd, doubl
                          tc::SMEM_BYTES);
     cudaFuncSetAttribute(tc::k_gram_tc<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          tc::SMEM_BYTES);
+    cudaFuncSetAttribute(tc::k_gram_tc_wide<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::WSMEM_BYTES);
+    cudaFuncSetAttribute(tc::k_gram_tc_wide<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::WSMEM_BYTES);
   }
   const int per = std::max(nsm, 1);
   const uint32_t wl = wait_limit_or(tc::WAIT_LIMIT);
   for (int t0 = 0; t0 < tiles; t0 += per) {
     const int nt = std::min(per, tiles - t0);
-    if (prec == 1)
+    if (wide && prec == 1)
+      tc::k_gram_tc_wide<0><<<nt, 128, tc::WSMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+    else if (wide)
+      tc::k_gram_tc_wide<1><<<nt, 128, tc::WSMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
+    else if (prec == 1)
       tc::k_gram_tc<0, false><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
     else
       tc::k_gram_tc<1, false><<<nt, 128, tc::SMEM_BYTES, st>>>(map, M, K, T, ldt, err, wl, t0);
@@ -448,6 +618,11 @@ int gram_tc(const void* O, int o_dtype, const double* mu, int W, int64_t P, int 
 }
 
 }  // namespace nqs
+
+extern "C" int nqs_set_gram_wide(int enable) {
+  nqs::g_gram_wide = enable != 0;
+  return NQS_OK;
+}
 
 extern "C" int nqs_gram(const void* A, int a_dtype, int M, int64_t K, int64_t lda, double* T,
                         int64_t ldt, int* err_dev, void* stream) {

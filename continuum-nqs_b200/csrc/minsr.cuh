@@ -30,5 +30,6 @@ size_t syrk_split_tf32_scratch_floats(int M, int K);
 int syrk_split_tf32(const double* A, int64_t lda, int M, int K, double* C, int64_t ldc, float* Z,
                     int* err, cudaStream_t st);
 extern bool g_chol_tc;  // nqs_set_cholesky_tc
+extern bool g_gram_wide;  // nqs_set_gram_wide
 
 }  // namespace nqs

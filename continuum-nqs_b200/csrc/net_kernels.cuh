@@ -82,7 +82,9 @@ __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
   __syncwarp();
   for (int n = lane; n < d; n += 32) {
     double v = 0, dx = 0, dy = 0, lp = 0;
-    if (derivs) {
+    // a token's derivative channels are non-zero only when it is a tangent electron (one token
+    // of a spin-flip job): the other tokens need the value sum alone (warp-uniform branches)
+    if (derivs && is_tan && jb.has_lap) {
       for (int k = 0; k < F; ++k) {
         const double w = (double)Wemb[(size_t)k * d + n];
         v = fma(sf[wib][0][k], w, v);
@@ -90,6 +92,15 @@ __global__ void __launch_bounds__(256) k_embed(JobBatch jb, ModelConst mc,
         dy = fma(sf[wib][2][k], w, dy);
         lp = fma(sf[wib][3][k], w, lp);
       }
+    } else if (derivs && is_tan) {
+      for (int k = 0; k < F; ++k) {
+        const double w = (double)Wemb[(size_t)k * d + n];
+        v = fma(sf[wib][0][k], w, v);
+        dx = fma(sf[wib][1][k], w, dx);
+        dy = fma(sf[wib][2][k], w, dy);
+      }
+    } else if (derivs) {
+      for (int k = 0; k < F; ++k) v = fma(sf[wib][0][k], (double)Wemb[(size_t)k * d + n], v);
     } else {
       for (int k = 0; k < F; ++k) v = fma(sf[wib][0][k], (double)Wemb[(size_t)k * d + n], v);
     }

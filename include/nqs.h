@@ -127,6 +127,11 @@ int nqs_set_cholesky_dag(int enable);
  * the float64 update, against the 1e-4 mean(T_ii) shift the preconditioner already carries).
  * Off: float64 CUDA-core updates. The float64 solve (gram_prec 0) always uses the latter. */
 int nqs_set_cholesky_tc(int enable);
+/* Implementation selection (no reference counterpart; process-wide, default on): the tensor-core
+ * Gram (nqs_gram and the mixed-precision MinSR solves) computes 256 x 256 tiles per CTA, two
+ * M = 128 accumulators in tensor memory against one shared B panel; off, 128 x 256 tiles. Same
+ * float32 accumulation order per entry, so the same results. */
+int nqs_set_gram_wide(int enable);
 /* Self-test of the flag waits (no reference counterpart; used by the failure-detection test):
  * solves L x = v in place (L: float64 [n][n] lower triangular, device; n <= 64 x 255) with the
  * wavefront triangular solve whose 64-row block `dead_block` never publishes its result (-1: all

@@ -15,11 +15,18 @@ def _tf32(x):
 
 @pytest.mark.parametrize("M,K", [(128, 64), (300, 1000), (520, 3001), (1030, 777)])
 @pytest.mark.parametrize("kind", ["bf16", "tf32"])
-def test_gram_tc_matches_fp64_of_rounded_operands(M, K, kind):
+@pytest.mark.parametrize("wide", [1, 0])
+def test_gram_tc_matches_fp64_of_rounded_operands(M, K, kind, wide):
+    """wide: 256 x 256 tiles (two accumulators per CTA, the default above 256 rows); 0: 128 x 256."""
+    from nqs import _lib
     from nqs.minsr import gram_lower
     g = torch.Generator().manual_seed(M * 7 + K)
     A = torch.randn(M, K, generator=g, dtype=torch.float32)
-    T = gram_lower(A.cuda(), kind).cpu()
+    _lib.lib().nqs_set_gram_wide(wide)
+    try:
+        T = gram_lower(A.cuda(), kind).cpu()
+    finally:
+        _lib.lib().nqs_set_gram_wide(1)
     Ar = A.to(torch.bfloat16).double() if kind == "bf16" else _tf32(A).double()
     ref = torch.tril(Ar @ Ar.T)
     scale = (Ar.abs() @ Ar.abs().T).max()
