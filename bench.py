@@ -393,7 +393,8 @@ def run_ours(a, rank, world):
     # timed inside a long step: against the sustained (power-capped) BF16 figure, burst beside it
     g_peak = peaks.get("bf16_tflops_sustained", 1400.0)
     g_burst = peaks.get("bf16_tflops", 1590.0)
-    roof_gram = {"kernel": "k_gram_tc<bf16> (tcgen05 SYRK of the 2W x P Jacobian)",
+    roof_gram = {"kernel": "k_gram_tc_wide<bf16> (tcgen05 SYRK of the 2W x P Jacobian, 256 x 256 "
+                           "tiles, two TMEM accumulators per CTA)",
                  "bound": "tensor", "achieved": g_ach, "peak": g_peak, "unit": "TFLOP/s",
                  "frac": g_ach / g_peak, "peak_source": f"{src} (sustained bf16)",
                  "frac_of_burst": g_ach / g_burst, "gram_ms": g_ms, "algorithmic_flops": gflop}
