@@ -1753,6 +1753,9 @@ __global__ void __launch_bounds__(1024) k_clip(const cplx* __restrict__ e, int W
 // relative reduction of the preconditioned residual sqrt(r.z / r0.z0) at which the conjugate
 // gradients stop by default
 constexpr double kPcgDefaultTol = 1e-2;
+// shift of the preconditioner factor, relative to mean(T_ii) (nqs_set_preconditioner_shift)
+constexpr double kPrecondShiftDefault = 1e-4;
+static double g_precond_shift = kPrecondShiftDefault;
 
 // caller-facing status from the internal slots: [0] non-positive pivot, [1] Gram timeout,
 // [2] floored pivots, [3] PCG iterations, [4] PCG stop reason (0 iteration limit, 1 converged,
@@ -1891,7 +1894,8 @@ static int minsr_direction_impl(void* O, int o_dtype, const double* eps, int W, 
   } else {
     double* fl = ws.take<double>(2);
     if (!fl) return NQS_ERR_WORKSPACE;
-    k_add_diag_noise<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam, 1e-4, rsum + 2 * n + 4,
+    k_add_diag_noise<<<(n + 255) / 256, 256, 0, st>>>(T, n, n, lam, g_precond_shift,
+                                                       rsum + 2 * n + 4,
                                                        fl + 1);
     NQS_CHECK_LAUNCH("k_add_diag_noise");
     k_pivot_floor<<<1, 1024, 0, st>>>(T, n, n, gram_prec == 1 ? 0x1p-16 : 0x1p-20, fl);
@@ -1955,6 +1959,12 @@ int nqs_minsr_direction_ex(void* O, int o_dtype, const double* eps, int W, int64
   return minsr_direction_impl(O, o_dtype, eps, W, P, lam, gram_prec, max_iters, tol, out_dtheta,
                               theta_io, lr, info_dev, 5, damping_out, wsp, wsb,
                               (cudaStream_t)stream);
+}
+
+int nqs_set_preconditioner_shift(double rel) {
+  if (!(rel >= 0.0)) return NQS_ERR_INVALID_ARG;
+  nqs::g_precond_shift = rel > 0.0 ? rel : nqs::kPrecondShiftDefault;
+  return NQS_OK;
 }
 
 int nqs_set_cholesky_tc(int enable) {

@@ -210,6 +210,7 @@ _SIGS.update({
     "nqs_set_cholesky_dag": ([c_int], c_int),
     "nqs_set_cholesky_tc": ([c_int], c_int),
     "nqs_set_gram_wide": ([c_int], c_int),
+    "nqs_set_preconditioner_shift": ([c_double], c_int),
     "nqs_set_rowgemm_stages": ([c_int], c_int),
     "nqs_mcmc_sweeps_devctr": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                 c_int, c_double, c_uint64, c_void_p, c_void_p, c_void_p, c_int,

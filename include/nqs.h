@@ -132,6 +132,11 @@ int nqs_set_cholesky_tc(int enable);
  * M = 128 accumulators in tensor memory against one shared B panel; off, 128 x 256 tiles. Same
  * float32 accumulation order per entry, so the same results. */
 int nqs_set_gram_wide(int enable);
+/* Shift of the preconditioner factor in the mixed-precision MinSR solves (gram_prec 1 / 2), relative
+ * to mean(T_ii) of the tensor-core Gram (no reference counterpart; process-wide): the factor is
+ * that of T_tc + (lam + rel mean(T_ii)) I, covering the Gram's float32-accumulation indefiniteness;
+ * the conjugate gradients still solve at lam. Default 1e-4; rel = 0 restores it. */
+int nqs_set_preconditioner_shift(double rel);
 /* Self-test of the flag waits (no reference counterpart; used by the failure-detection test):
  * solves L x = v in place (L: float64 [n][n] lower triangular, device; n <= 64 x 255) with the
  * wavefront triangular solve whose 64-row block `dead_block` never publishes its result (-1: all
