@@ -924,8 +924,9 @@ __global__ void __launch_bounds__(256) k_trsv_grid(const double* __restrict__ L,
 // loaded into registers first, then one wait on the flag of the group's last block (a block
 // publishes only after all of its own dependencies, so that flag covers the group; release /
 // acquire at GPU scope) and the four x_t are applied in order. The walk thus takes a quarter of
-// the flag round trips, and the chain costs one flag hop and two 64 x 64 mat-vecs per block. Every wait is bounded: a CTA that gives up records the timeout
-// in flag[kTrsvErrSlot], publishes NaN for its block (its dependants then finish at once) and
+// the flag round trips, and the chain costs one flag hop and two 64 x 64 mat-vecs per block.
+// Every wait is bounded: a CTA that gives up records the timeout in flag[kTrsvErrSlot],
+// publishes NaN for its block (its dependants then finish at once) and
 // returns. v is overwritten with x. Sums run in a fixed order (deterministic).
 constexpr int kTrsvErrSlot = 255;  // flags[0..254]: blocks; flags[255]: timeout record
 constexpr uint32_t kTrsvWaitLimit = 1u << 21;
